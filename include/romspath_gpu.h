@@ -1,0 +1,189 @@
+/*
+ * romspath_gpu.h -- C ABI of the B200 ROMSPath particle step.
+ *
+ * Drop-in for the body of update_particles (ROMSPath.f90:608-1008) and the
+ * frame hand-off of updateHydro (hydrodynamic_module.f90:112-760).  The
+ * Fortran driver, its namelists (ROMSPath.h:59-345) and its NetCDF reader
+ * stay as they are; the driver binds these entry points with ISO_C_BINDING
+ * (see the interface module in INTEGRATION.md).
+ *
+ * Conventions
+ *  - Every array argument is a host pointer in the reference's own layout:
+ *    Fortran column-major, 1-based index semantics.  h(xi_rho,eta_rho),
+ *    U(xi_u,eta_u,N), V(xi_v,eta_v,N), W/AKs(xi_rho,eta_rho,N+1),
+ *    zeta(xi_rho,eta_rho) with xi_u = xi_rho-1, eta_u = eta_rho,
+ *    xi_v = xi_rho, eta_v = eta_rho-1.  Arrays are borrowed for the call.
+ *  - Slots are the reference's ring positions tind = 1..3 (t_b/t_c/t_f).
+ *  - Grid ids are 1..Ngrid, as par(:,pGID).
+ *  - Every call returns RP_OK (0) or a negative RP_ERR_* code; the message
+ *    of the last error is available from rp_last_error().  No call exits or
+ *    aborts the process.
+ *  - One host thread drives a context.  rp_step() and rp_upload_frame*()
+ *    are asynchronous (stream-ordered); rp_get_particles() and
+ *    rp_synchronize() wait for the device.
+ */
+#ifndef ROMSPATH_GPU_H
+#define ROMSPATH_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RP_MAXNGRID 5          /* MAXNgrid, ROMSPath.h:9 */
+
+#define RP_OK 0
+#define RP_ERR_ARG (-1)        /* bad argument, dimension, slot or grid id   */
+#define RP_ERR_CUDA (-2)       /* CUDA runtime error (message has details)   */
+#define RP_ERR_STATE (-3)      /* call made in the wrong order               */
+#define RP_ERR_NOMEM (-4)      /* device or pinned allocation failed         */
+#define RP_ERR_UNSUPPORTED (-5)/* option outside the implemented path        */
+#define RP_ERR_NOEXT (-6)      /* no CUDA device / kernels not loadable      */
+
+/* per-particle flag bits returned by rp_get_particles (deviations where the
+ * reference is undefined) */
+#define RP_FLAG_OOB 0x01u      /* a gather index left its array (clamped)      */
+#define RP_FLAG_NODE 0x02u     /* inverse-distance weight at an exact node      */
+#define RP_FLAG_WBOT 0x04u     /* w-level bracket below level 1                 */
+#define RP_FLAG_WTOP 0x08u     /* w-level bracket above level N+1               */
+#define RP_FLAG_SPLINE 0x10u   /* smoothing-spline secant loop hit its cap      */
+
+/* storage precision of the hydrodynamic fields on the device */
+#define RP_FIELD_F64 0
+#define RP_FIELD_F32 1
+
+/* Run parameters: the namelist values the hot path reads (ROMSPath.h:77-80
+ * timeparam, 140-148 turbparam, 152-154 advectparam, 161-180 behavparam,
+ * 304-319 other) plus device options. */
+typedef struct rp_params {
+    int32_t numpar;                      /* particle capacity (numparticles)  */
+    int32_t idt;                         /* internal step (s)                 */
+    int32_t dt;                          /* external step (s)                 */
+    int32_t scheme;                      /* 1 = RK4, else no advection        */
+    int32_t nsb;                         /* 0 neutral, 1 surface, 2 bottom    */
+    int32_t vturb_on;                    /* VTurbOn                           */
+    int32_t hturb_on;                    /* HTurbOn                           */
+    int32_t open_ocean_boundary;         /* OpenOceanBoundary                 */
+    int32_t behavior;                    /* Behavior; only 0 (passive)        */
+    int32_t stokes;                      /* add ustokes/vstokes on upload     */
+    int32_t field_dtype;                 /* RP_FIELD_F64 / RP_FIELD_F32       */
+    int32_t spline_max_iter;             /* cap of smooth()'s secant loop (0: 100) */
+    double vertdist;
+    double serr, smth, sub, deltat, aksback;
+    double constant_hturb[RP_MAXNGRID];  /* ConstantHTurb(ng), m^2/s          */
+    uint64_t seed;                       /* Philox key of the turbulence noise */
+    int32_t device;                      /* CUDA device ordinal               */
+    int32_t reserved[7];
+} rp_params;
+
+/* One grid (GRIDS(ng), grid_module.f90:14-35).  Pointers are borrowed for
+ * the duration of rp_create(). */
+typedef struct rp_grid {
+    int32_t xi_rho, eta_rho;             /* rho-point dimensions              */
+    int32_t n_rho;                       /* s_rho (N); s_w = N+1              */
+    int32_t vtransform;                  /* 1, 2 or 3                         */
+    double hc;
+    const double *h, *pm, *pn;           /* (xi_rho, eta_rho)                 */
+    const int32_t *mask_rho;             /* (xi_rho, eta_rho)                 */
+    const int32_t *mask_u;               /* (xi_u, eta_u)                     */
+    const int32_t *mask_v;               /* (xi_v, eta_v)                     */
+    const double *s_rho, *cs_r;          /* (N)                               */
+    const double *s_w, *cs_w;            /* (N+1)                             */
+    const double *scl, *off;             /* scl(Ngrid,2), off(Ngrid,2), Fortran order;
+                                            NULL for a single grid           */
+} rp_grid;
+
+typedef struct rp_ctx rp_ctx;
+
+/* Create a context on params->device: uploads the static grids and sizes
+ * the frame ring and particle state.  Replaces the device-side part of
+ * ini_ROMSPath (ROMSPath.f90:182-461; GRIDS from InitGrid,
+ * grid_module.f90:41-499). */
+int rp_create(const rp_params *params, int32_t ngrid, const rp_grid *grids, rp_ctx **out);
+
+/* Hand one frame of grid `ng` (1..Ngrid) to ring slot `slot` (1..3): the
+ * output of updateHydro(FIRST, tstep, tind) (hydrodynamic_module.f90:112-760)
+ * for tind = slot.  zeta(xi_rho,eta_rho), u(xi_u,eta_u,N), v(xi_v,eta_v,N),
+ * w and aks (xi_rho,eta_rho,N+1); su/sv are ustokes/vstokes (may be NULL;
+ * added to u/v in FP64 when params->stokes, hydrodynamic_module.f90:606-660).
+ * The copy runs asynchronously into a spare device slot; the arrays may be
+ * reused as soon as the call returns. */
+int rp_upload_frame(rp_ctx *ctx, int32_t ng, int32_t slot, const double *zeta, const double *u,
+                    const double *v, const double *w, const double *aks, const double *su,
+                    const double *sv);
+/* Same for single-precision source arrays. */
+int rp_upload_frame_f32(rp_ctx *ctx, int32_t ng, int32_t slot, const float *zeta, const float *u,
+                        const float *v, const float *w, const float *aks, const float *su,
+                        const float *sv);
+
+/* Set the particle state: the par(:,pX/pY/pZ/pDOB/pAge/pStatus/pGID)
+ * columns and isIn(:) of ROMSPath.f90:104-129 for particles 1..n. */
+int rp_set_particles(rp_ctx *ctx, int64_t n, const double *x, const double *y, const double *z,
+                     const double *dob, const double *age, const double *status, const double *gid,
+                     const int32_t *isin);
+
+/* Initial ownership: the grid loop of ini_ROMSPath (ROMSPath.f90:367-432)
+ * with bounds() and zbounds() on the device.  ipos/jpos are (n, Ngrid)
+ * Fortran order (particle positions in each grid's index space, the output
+ * of LL2ij); z and dob are par(:,pZ) and par(:,pDOB). */
+int rp_locate_particles(rp_ctx *ctx, int64_t n, const double *ipos, const double *jpos,
+                        const double *z, const double *dob, int32_t t_b);
+
+/* One internal step over all particles: update_particles
+ * (ROMSPath.f90:608-1008) with ex(3), ix(3), ets and the ring slots
+ * t_b/t_c/t_f from run_External_Timestep / run_Internal_Timestep
+ * (ROMSPath.f90:465-546). */
+int rp_step(rp_ctx *ctx, const double ex[3], const double ix[3], int32_t ets, int32_t t_b,
+            int32_t t_c, int32_t t_f);
+
+/* Read back par(:,pX/pY/pZ/pAge/pStatus/pGID), isIn, par(:,pWD/pZeta/pBath)
+ * and the per-particle flag bits for particles 1..n.  Any pointer may be
+ * NULL.  Waits for queued work. */
+int rp_get_particles(rp_ctx *ctx, int64_t n, double *x, double *y, double *z, double *age,
+                     double *status, double *gid, int32_t *isin, double *wd, double *zeta,
+                     double *bath, uint32_t *flags);
+
+/* Index of the next internal step in the Philox counter (default 0; each
+ * rp_step increments it). */
+int rp_set_step_index(rp_ctx *ctx, uint64_t step_index);
+
+/* Test hook: replace the Philox normals by caller-supplied N(0,1) values,
+ * laid out [step][particle][draw] with draw = 0,1 for HTurb (devX, devY)
+ * and 2..1+idt/deltat for the VTurb sub-steps; `nsteps` steps are held.
+ * NULL removes the hook. */
+int rp_set_noise_hook(rp_ctx *ctx, const double *noise, int64_t nsteps);
+
+/* Wait for all queued work of the context. */
+int rp_synchronize(rp_ctx *ctx);
+
+/* Copy the last error message (NUL-terminated, truncated to len). */
+int rp_last_error(rp_ctx *ctx, char *buf, int32_t len);
+
+/* Release the context and its device memory. */
+int rp_destroy(rp_ctx *ctx);
+
+/* Device-resident state, for callers that keep particles in HBM between
+ * calls (pointers stay valid until rp_destroy). */
+typedef struct rp_device_state {
+    int64_t n;
+    double *x, *y, *z, *age, *dob, *status, *wd, *zeta, *bath;
+    int32_t *gid;
+    int8_t *isin;
+    uint32_t *pid, *flags;
+    void *stream;                        /* cudaStream_t of the compute stream */
+} rp_device_state;
+int rp_device_state_get(rp_ctx *ctx, rp_device_state *out);
+
+/* Timing of the last rp_step launch sequence on the compute stream, in ms
+ * (CUDA events), and the number of kernels it launched. */
+int rp_last_step_stats(rp_ctx *ctx, float *ms, int32_t *kernels);
+
+/* Library version string. */
+const char *rp_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

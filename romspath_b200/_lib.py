@@ -1,0 +1,107 @@
+"""ctypes declarations of the C ABI in ``include/romspath_gpu.h``.
+
+Loading fails loudly: there is no CPU fallback for the particle step.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from . import build as _build
+
+MAXNGRID = 5
+RP_OK = 0
+ERRORS = {-1: "RP_ERR_ARG", -2: "RP_ERR_CUDA", -3: "RP_ERR_STATE", -4: "RP_ERR_NOMEM",
+          -5: "RP_ERR_UNSUPPORTED", -6: "RP_ERR_NOEXT"}
+FIELD_F64, FIELD_F32 = 0, 1
+FLAG_OOB, FLAG_NODE, FLAG_WBOT, FLAG_WTOP, FLAG_SPLINE = 1, 2, 4, 8, 16
+
+EXPORTS = [
+    "rp_create", "rp_upload_frame", "rp_upload_frame_f32", "rp_set_particles", "rp_locate_particles",
+    "rp_step", "rp_get_particles", "rp_set_step_index", "rp_set_noise_hook", "rp_synchronize",
+    "rp_last_error", "rp_destroy", "rp_device_state_get", "rp_last_step_stats", "rp_version",
+]
+
+PD = C.POINTER(C.c_double)
+PF = C.POINTER(C.c_float)
+PI32 = C.POINTER(C.c_int32)
+PU32 = C.POINTER(C.c_uint32)
+
+
+class RpParams(C.Structure):
+    _fields_ = [
+        ("numpar", C.c_int32), ("idt", C.c_int32), ("dt", C.c_int32), ("scheme", C.c_int32),
+        ("nsb", C.c_int32), ("vturb_on", C.c_int32), ("hturb_on", C.c_int32),
+        ("open_ocean_boundary", C.c_int32), ("behavior", C.c_int32), ("stokes", C.c_int32),
+        ("field_dtype", C.c_int32), ("spline_max_iter", C.c_int32),
+        ("vertdist", C.c_double), ("serr", C.c_double), ("smth", C.c_double), ("sub", C.c_double),
+        ("deltat", C.c_double), ("aksback", C.c_double),
+        ("constant_hturb", C.c_double * MAXNGRID),
+        ("seed", C.c_uint64), ("device", C.c_int32), ("reserved", C.c_int32 * 7),
+    ]
+
+
+class RpGrid(C.Structure):
+    _fields_ = [
+        ("xi_rho", C.c_int32), ("eta_rho", C.c_int32), ("n_rho", C.c_int32), ("vtransform", C.c_int32),
+        ("hc", C.c_double),
+        ("h", PD), ("pm", PD), ("pn", PD),
+        ("mask_rho", PI32), ("mask_u", PI32), ("mask_v", PI32),
+        ("s_rho", PD), ("cs_r", PD), ("s_w", PD), ("cs_w", PD),
+        ("scl", PD), ("off", PD),
+    ]
+
+
+class RpDeviceState(C.Structure):
+    _fields_ = [
+        ("n", C.c_int64),
+        ("x", C.c_void_p), ("y", C.c_void_p), ("z", C.c_void_p), ("age", C.c_void_p), ("dob", C.c_void_p),
+        ("status", C.c_void_p), ("wd", C.c_void_p), ("zeta", C.c_void_p), ("bath", C.c_void_p),
+        ("gid", C.c_void_p), ("isin", C.c_void_p), ("pid", C.c_void_p), ("flags", C.c_void_p),
+        ("stream", C.c_void_p),
+    ]
+
+
+_lib = None
+
+
+def lib_path() -> str:
+    return _build.LIB
+
+
+def load(build_if_missing: bool = True):
+    """Load the sm_100a library (building it with nvcc if absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = _build.LIB
+    if not os.path.exists(path):
+        if not build_if_missing:
+            raise RuntimeError(f"romspath_b200: CUDA library missing at {path}")
+        _build.build()
+    L = C.CDLL(path)
+    _declare(L)
+    _lib = L
+    return L
+
+
+def _declare(L):
+    P = C.c_void_p
+    L.rp_create.argtypes = [C.POINTER(RpParams), C.c_int32, C.POINTER(RpGrid), C.POINTER(P)]
+    L.rp_upload_frame.argtypes = [P, C.c_int32, C.c_int32] + [PD] * 7
+    L.rp_upload_frame_f32.argtypes = [P, C.c_int32, C.c_int32] + [PF] * 7
+    L.rp_set_particles.argtypes = [P, C.c_int64] + [PD] * 7 + [PI32]
+    L.rp_locate_particles.argtypes = [P, C.c_int64, PD, PD, PD, PD, C.c_int32]
+    L.rp_step.argtypes = [P, PD, PD, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
+    L.rp_get_particles.argtypes = [P, C.c_int64] + [PD] * 6 + [PI32, PD, PD, PD, PU32]
+    L.rp_set_step_index.argtypes = [P, C.c_uint64]
+    L.rp_set_noise_hook.argtypes = [P, PD, C.c_int64]
+    L.rp_synchronize.argtypes = [P]
+    L.rp_last_error.argtypes = [P, C.c_char_p, C.c_int32]
+    L.rp_destroy.argtypes = [P]
+    L.rp_device_state_get.argtypes = [P, C.POINTER(RpDeviceState)]
+    L.rp_last_step_stats.argtypes = [P, C.POINTER(C.c_float), C.POINTER(C.c_int32)]
+    L.rp_version.restype = C.c_char_p
+    for name in EXPORTS:
+        if name != "rp_version":
+            getattr(L, name).restype = C.c_int

@@ -1,0 +1,610 @@
+// rp_api.cu -- the C ABI (include/romspath_gpu.h): context, HBM layout,
+// frame ring, particle state and step launches.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "romspath_gpu.h"
+#include "rp_internal.h"
+
+namespace {
+
+constexpr int64_t kChunkElems = 4 << 20;     // staging chunk (elements)
+constexpr int kMaxNp = 256;                  // largest spline point count
+
+struct GridBuf {
+    int nx = 0, ny = 0, N = 0, vtransform = 2;
+    double hc = 0.0;
+    double *h = nullptr, *pm = nullptr, *pn = nullptr;
+    double *sr = nullptr, *csr = nullptr, *sw = nullptr, *csw = nullptr;
+    uint8_t *mrho = nullptr, *mu = nullptr, *mv = nullptr;
+    void *zeta = nullptr, *u = nullptr, *v = nullptr, *w = nullptr, *aks = nullptr;
+    double scl[RP_MAXNGRID][2] = {}, off[RP_MAXNGRID][2] = {};
+    int map[3] = {-1, -1, -1};                 // logical slot 1..3 -> physical 0..3
+    bool slot_loaded[RP_SLOTS] = {false, false, false, false};
+    bool free_recorded[RP_SLOTS] = {false, false, false, false};
+    cudaEvent_t slot_free[RP_SLOTS] = {};      // last reader of the physical slot done
+    cudaEvent_t slot_ready[RP_SLOTS] = {};     // upload into the physical slot done
+};
+
+}  // namespace
+
+struct rp_ctx {
+    rp_params prm{};
+    int ngrid = 0;
+    int device = 0;
+    int num_sms = 148;
+    int elem = 8;                              // bytes per stored field value
+    int npmax = 0;
+    GridBuf g[RP_MAXNGRID];
+    // particle state
+    int64_t cap = 0, n = 0;
+    double *x = nullptr, *y = nullptr, *z = nullptr, *age = nullptr, *dob = nullptr, *status = nullptr;
+    double *wd = nullptr, *zeta = nullptr, *bath = nullptr;
+    int32_t* gid = nullptr;
+    int8_t* isin = nullptr;
+    uint32_t *pid = nullptr, *flags = nullptr;
+    double* tmp_gid = nullptr;                 // host-facing conversions
+    int32_t* tmp_isin = nullptr;
+    // staging
+    void* pin[2] = {nullptr, nullptr};         // pinned, 2 x (2 arrays x chunk x 8 B)
+    void* dstage[2] = {nullptr, nullptr};      // device, same shape
+    cudaEvent_t pin_done[2] = {};
+    bool pin_used[2] = {false, false};
+    int pin_next = 0;
+    cudaStream_t s_comp = nullptr, s_copy = nullptr;
+    // noise hook
+    double* hook = nullptr;
+    int64_t hook_steps = 0, hook_pos = 0;
+    int ndraw = 0;
+    uint64_t step_index = 0;
+    // timing
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool timed = false;
+    int last_kernels = 0;
+    std::string err;
+};
+
+namespace {
+
+int fail(rp_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+#define CK(call)                                                                                        \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess) return fail(ctx, RP_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <typename P>
+cudaError_t dalloc(P** p, size_t bytes) {
+    return cudaMalloc((void**)p, bytes ? bytes : 1);
+}
+
+// host -> device through the pinned staging halves, on stream s
+int h2d(rp_ctx* ctx, void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    const size_t chunk = (size_t)kChunkElems * 8 * 2;
+    size_t done = 0;
+    while (done < bytes) {
+        const size_t nb = std::min(chunk, bytes - done);
+        const int h = ctx->pin_next;
+        ctx->pin_next ^= 1;
+        if (ctx->pin_used[h]) CK(cudaEventSynchronize(ctx->pin_done[h]));
+        std::memcpy(ctx->pin[h], (const char*)src + done, nb);
+        CK(cudaMemcpyAsync((char*)dst + done, ctx->pin[h], nb, cudaMemcpyHostToDevice, s));
+        CK(cudaEventRecord(ctx->pin_done[h], s));
+        ctx->pin_used[h] = true;
+        done += nb;
+    }
+    return RP_OK;
+}
+
+// device -> host through the pinned staging halves (synchronous)
+int d2h(rp_ctx* ctx, void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    const size_t chunk = (size_t)kChunkElems * 8 * 2;
+    size_t done = 0;
+    while (done < bytes) {
+        const size_t nb = std::min(chunk, bytes - done);
+        const int h = ctx->pin_next;
+        ctx->pin_next ^= 1;
+        if (ctx->pin_used[h]) CK(cudaEventSynchronize(ctx->pin_done[h]));
+        CK(cudaMemcpyAsync(ctx->pin[h], (const char*)src + done, nb, cudaMemcpyDeviceToHost, s));
+        CK(cudaEventRecord(ctx->pin_done[h], s));
+        CK(cudaEventSynchronize(ctx->pin_done[h]));
+        ctx->pin_used[h] = false;
+        std::memcpy((char*)dst + done, ctx->pin[h], nb);
+        done += nb;
+    }
+    return RP_OK;
+}
+
+RpParticlesDev particles_dev(const rp_ctx* c) {
+    RpParticlesDev P;
+    P.n = c->n;
+    P.x = c->x; P.y = c->y; P.z = c->z; P.age = c->age; P.dob = c->dob; P.status = c->status;
+    P.wd = c->wd; P.zeta = c->zeta; P.bath = c->bath;
+    P.gid = c->gid; P.isin = c->isin; P.pid = c->pid; P.flags = c->flags;
+    return P;
+}
+
+void fill_grids(const rp_ctx* c, RpStepArgs& A, int tb, int tc, int tf) {
+    for (int k = 0; k < c->ngrid; k++) {
+        const GridBuf& G = c->g[k];
+        RpGridDev& d = A.g[k];
+        d.nx = G.nx; d.ny = G.ny; d.N = G.N; d.vtransform = G.vtransform; d.hc = G.hc;
+        d.h = G.h; d.pm = G.pm; d.pn = G.pn;
+        d.mrho = G.mrho; d.mu = G.mu; d.mv = G.mv;
+        d.sr = G.sr; d.csr = G.csr; d.sw = G.sw; d.csw = G.csw;
+        d.zeta = G.zeta; d.u = G.u; d.v = G.v; d.w = G.w; d.aks = G.aks;
+        for (int i = 0; i < RP_MAXNGRID; i++)
+            for (int q = 0; q < 2; q++) { d.scl[i][q] = G.scl[i][q]; d.off[i][q] = G.off[i][q]; }
+        d.sb = (tb >= 1 && tb <= 3) ? G.map[tb - 1] : 0;
+        d.sc = (tc >= 1 && tc <= 3) ? G.map[tc - 1] : 0;
+        d.sf = (tf >= 1 && tf <= 3) ? G.map[tf - 1] : 0;
+    }
+}
+
+void fill_params(const rp_ctx* c, RpStepArgs& A) {
+    const rp_params& p = c->prm;
+    A.ngrid = c->ngrid;
+    A.idt = p.idt; A.scheme = p.scheme; A.nsb = p.nsb;
+    A.vturb_on = p.vturb_on; A.hturb_on = p.hturb_on; A.oob = p.open_ocean_boundary;
+    A.loop = p.idt / (int)p.deltat;
+    A.spline_max_iter = p.spline_max_iter > 0 ? p.spline_max_iter : 100;
+    A.vertdist = p.vertdist; A.serr = p.serr; A.smth = p.smth; A.sub = p.sub;
+    A.deltat = p.deltat; A.aksback = p.aksback;
+    for (int i = 0; i < RP_MAXNGRID; i++) A.khturb[i] = p.constant_hturb[i];
+    A.seed = p.seed;
+    A.ndraw = c->ndraw;
+    A.p = particles_dev(c);
+}
+
+// polintd node terms (interpolation_module.f90:72-109) for nodes xa, point x
+RpPolint polint_consts(const double xa[3], double x) {
+    RpPolint P;
+    int ns = 0;
+    double dif = std::fabs(x - xa[0]);
+    for (int i = 0; i < 3; i++) {
+        const double dift = std::fabs(x - xa[i]);
+        if (dift < dif) { ns = i; dif = dift; }
+    }
+    P.ns = ns;
+    P.d1 = xa[1] - x;
+    P.e12 = xa[1] - xa[2];
+    P.e01 = xa[0] - xa[1];
+    P.e02 = xa[0] - xa[2];
+    P.dns = xa[ns] - x;
+    P.b = (ns == 2) ? (xa[2] - x) : (xa[0] - x);
+    return P;
+}
+
+void free_ctx(rp_ctx* c) {
+    if (!c) return;
+    for (int k = 0; k < RP_MAXNGRID; k++) {
+        GridBuf& G = c->g[k];
+        void* ptrs[] = {G.h, G.pm, G.pn, G.sr, G.csr, G.sw, G.csw, G.mrho, G.mu, G.mv,
+                        G.zeta, G.u, G.v, G.w, G.aks};
+        for (void* p : ptrs) if (p) cudaFree(p);
+        for (int s = 0; s < RP_SLOTS; s++) {
+            if (G.slot_free[s]) cudaEventDestroy(G.slot_free[s]);
+            if (G.slot_ready[s]) cudaEventDestroy(G.slot_ready[s]);
+        }
+    }
+    void* ptrs[] = {c->x, c->y, c->z, c->age, c->dob, c->status, c->wd, c->zeta, c->bath,
+                    c->gid, c->isin, c->pid, c->flags, c->tmp_gid, c->tmp_isin, c->hook,
+                    c->dstage[0], c->dstage[1]};
+    for (void* p : ptrs) if (p) cudaFree(p);
+    for (int h = 0; h < 2; h++) {
+        if (c->pin[h]) cudaFreeHost(c->pin[h]);
+        if (c->pin_done[h]) cudaEventDestroy(c->pin_done[h]);
+    }
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->s_comp) cudaStreamDestroy(c->s_comp);
+    if (c->s_copy) cudaStreamDestroy(c->s_copy);
+    delete c;
+}
+
+template <typename S>
+int upload_field(rp_ctx* ctx, const S* src, const S* add, void* dst, int ni, int nj, int nk, int phys) {
+    const int64_t total = (int64_t)ni * nj * nk;
+    const int dst_f32 = (ctx->elem == 4);
+    const int src_f32 = (sizeof(S) == 4);
+    for (int64_t e0 = 0; e0 < total; e0 += kChunkElems) {
+        const int64_t cnt = std::min<int64_t>(kChunkElems, total - e0);
+        const size_t nb = (size_t)cnt * sizeof(S);
+        const int h = ctx->pin_next;
+        ctx->pin_next ^= 1;
+        if (ctx->pin_used[h]) CK(cudaEventSynchronize(ctx->pin_done[h]));
+        char* pin = (char*)ctx->pin[h];
+        char* dst_stage = (char*)ctx->dstage[h];
+        std::memcpy(pin, src + e0, nb);
+        if (add) std::memcpy(pin + (size_t)kChunkElems * 8, add + e0, nb);
+        CK(cudaMemcpyAsync(dst_stage, pin, nb, cudaMemcpyHostToDevice, ctx->s_copy));
+        if (add)
+            CK(cudaMemcpyAsync(dst_stage + (size_t)kChunkElems * 8, pin + (size_t)kChunkElems * 8, nb,
+                               cudaMemcpyHostToDevice, ctx->s_copy));
+        CK(rp::launch_convert(src_f32, dst_f32, dst_stage, add ? dst_stage + (size_t)kChunkElems * 8 : nullptr,
+                              dst, ni, nj, nk, phys, e0, cnt, ctx->s_copy));
+        CK(cudaEventRecord(ctx->pin_done[h], ctx->s_copy));
+        ctx->pin_used[h] = true;
+    }
+    return RP_OK;
+}
+
+template <typename S>
+int upload_frame(rp_ctx* ctx, int32_t ng, int32_t slot, const S* zeta, const S* u, const S* v, const S* w,
+                 const S* aks, const S* su, const S* sv) {
+    if (!ctx) return RP_ERR_ARG;
+    if (ng < 1 || ng > ctx->ngrid) return fail(ctx, RP_ERR_ARG, "rp_upload_frame: grid id out of range");
+    if (slot < 1 || slot > 3) return fail(ctx, RP_ERR_ARG, "rp_upload_frame: slot must be 1..3");
+    if (!zeta || !u || !v || !w || !aks) return fail(ctx, RP_ERR_ARG, "rp_upload_frame: null field");
+    const bool stokes = ctx->prm.stokes != 0;
+    if (stokes && (!su || !sv)) return fail(ctx, RP_ERR_ARG, "rp_upload_frame: stokes on but su/sv null");
+    GridBuf& G = ctx->g[ng - 1];
+    CK(cudaSetDevice(ctx->device));
+    // a physical slot not mapped to any logical slot
+    int phys = -1;
+    for (int p = 0; p < RP_SLOTS && phys < 0; p++) {
+        bool used = false;
+        for (int l = 0; l < 3; l++) used = used || (G.map[l] == p);
+        if (!used) phys = p;
+    }
+    if (G.free_recorded[phys]) CK(cudaStreamWaitEvent(ctx->s_copy, G.slot_free[phys], 0));
+    const int nx = G.nx, ny = G.ny, N = G.N;
+    int rc;
+    if ((rc = upload_field<S>(ctx, zeta, nullptr, G.zeta, nx, ny, 1, phys)) != RP_OK) return rc;
+    if ((rc = upload_field<S>(ctx, u, stokes ? su : nullptr, G.u, nx - 1, ny, N, phys)) != RP_OK) return rc;
+    if ((rc = upload_field<S>(ctx, v, stokes ? sv : nullptr, G.v, nx, ny - 1, N, phys)) != RP_OK) return rc;
+    if ((rc = upload_field<S>(ctx, w, nullptr, G.w, nx, ny, N + 1, phys)) != RP_OK) return rc;
+    if ((rc = upload_field<S>(ctx, aks, nullptr, G.aks, nx, ny, N + 1, phys)) != RP_OK) return rc;
+    CK(cudaEventRecord(G.slot_ready[phys], ctx->s_copy));
+    G.slot_loaded[phys] = true;
+    const int old = G.map[slot - 1];
+    G.map[slot - 1] = phys;
+    if (old >= 0) {
+        // readers of the old physical slot are all queued on the compute stream
+        CK(cudaEventRecord(G.slot_free[old], ctx->s_comp));
+        G.free_recorded[old] = true;
+        G.slot_loaded[old] = false;
+    }
+    return RP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* rp_version(void) { return "romspath_b200 0.1 (sm_100a)"; }
+
+int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_ctx** out) {
+    if (!params || !grids || !out) return RP_ERR_ARG;
+    *out = nullptr;
+    const rp_params& p = *params;
+    if (ngrid < 1 || ngrid > RP_MAXNGRID || p.numpar < 0 || p.idt <= 0 || p.dt <= 0) return RP_ERR_ARG;
+    if (p.behavior != 0) return RP_ERR_UNSUPPORTED;
+    if (p.nsb < 0 || p.nsb > 2) return RP_ERR_ARG;
+    if (!(p.deltat >= 1.0) || !(p.sub > 0.0)) return RP_ERR_ARG;
+    if (p.field_dtype != RP_FIELD_F64 && p.field_dtype != RP_FIELD_F32) return RP_ERR_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= p.device || p.device < 0) return RP_ERR_NOEXT;
+    rp_ctx* ctx = new rp_ctx();
+    ctx->prm = p;
+    ctx->ngrid = ngrid;
+    ctx->device = p.device;
+    ctx->elem = (p.field_dtype == RP_FIELD_F32) ? 4 : 8;
+    ctx->ndraw = 2 + p.idt / (int)p.deltat;
+    int rc = RP_OK;
+    auto bail = [&](int code, const std::string& m) {
+        std::fprintf(stderr, "rp_create: %s\n", m.c_str());
+        free_ctx(ctx);
+        return code;
+    };
+    if (cudaSetDevice(p.device) != cudaSuccess) return bail(RP_ERR_CUDA, "cudaSetDevice failed");
+    cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, p.device);
+    for (int k = 0; k < ngrid; k++) {
+        const rp_grid& R = grids[k];
+        GridBuf& G = ctx->g[k];
+        if (R.xi_rho < 4 || R.eta_rho < 4 || R.n_rho < 1 || R.n_rho > 510) return bail(RP_ERR_ARG, "bad grid dims");
+        if (R.vtransform < 1 || R.vtransform > 3) return bail(RP_ERR_ARG, "bad Vtransform");
+        if (!R.h || !R.pm || !R.pn || !R.mask_rho || !R.mask_u || !R.mask_v || !R.s_rho || !R.cs_r || !R.s_w || !R.cs_w)
+            return bail(RP_ERR_ARG, "null grid array");
+        if (ngrid > 1 && (!R.scl || !R.off)) return bail(RP_ERR_ARG, "nested grids need scl/off");
+        G.nx = R.xi_rho; G.ny = R.eta_rho; G.N = R.n_rho; G.vtransform = R.vtransform; G.hc = R.hc;
+        const int sw = G.N + 1;
+        const int np = (int)((double)sw * p.sub);
+        if (np < 4 || np > kMaxNp || np < sw) return bail(RP_ERR_UNSUPPORTED, "spline point count int(s_w*sub) must be in [max(4,s_w), 256]");
+        ctx->npmax = std::max(ctx->npmax, np);
+        const size_t n2 = (size_t)G.nx * G.ny;
+        const size_t nu = (size_t)(G.nx - 1) * G.ny, nv = (size_t)G.nx * (G.ny - 1);
+        std::vector<uint8_t> m8(std::max(n2, std::max(nu, nv)));
+        auto mask8 = [&](const int32_t* m, size_t cnt) -> bool {
+            for (size_t i = 0; i < cnt; i++) {
+                if (m[i] != 0 && m[i] != 1) return false;
+                m8[i] = (uint8_t)m[i];
+            }
+            return true;
+        };
+        if (dalloc(&G.h, n2 * 8) || dalloc(&G.pm, n2 * 8) || dalloc(&G.pn, n2 * 8) ||
+            dalloc(&G.sr, G.N * 8) || dalloc(&G.csr, G.N * 8) || dalloc(&G.sw, sw * 8) || dalloc(&G.csw, sw * 8) ||
+            dalloc(&G.mrho, n2) || dalloc(&G.mu, nu) || dalloc(&G.mv, nv))
+            return bail(RP_ERR_NOMEM, "grid allocation");
+        cudaMemcpy(G.h, R.h, n2 * 8, cudaMemcpyHostToDevice);
+        cudaMemcpy(G.pm, R.pm, n2 * 8, cudaMemcpyHostToDevice);
+        cudaMemcpy(G.pn, R.pn, n2 * 8, cudaMemcpyHostToDevice);
+        cudaMemcpy(G.sr, R.s_rho, G.N * 8, cudaMemcpyHostToDevice);
+        cudaMemcpy(G.csr, R.cs_r, G.N * 8, cudaMemcpyHostToDevice);
+        cudaMemcpy(G.sw, R.s_w, sw * 8, cudaMemcpyHostToDevice);
+        cudaMemcpy(G.csw, R.cs_w, sw * 8, cudaMemcpyHostToDevice);
+        if (!mask8(R.mask_rho, n2)) return bail(RP_ERR_ARG, "mask_rho values must be 0 or 1");
+        cudaMemcpy(G.mrho, m8.data(), n2, cudaMemcpyHostToDevice);
+        if (!mask8(R.mask_u, nu)) return bail(RP_ERR_ARG, "mask_u values must be 0 or 1");
+        cudaMemcpy(G.mu, m8.data(), nu, cudaMemcpyHostToDevice);
+        if (!mask8(R.mask_v, nv)) return bail(RP_ERR_ARG, "mask_v values must be 0 or 1");
+        if (cudaMemcpy(G.mv, m8.data(), nv, cudaMemcpyHostToDevice) != cudaSuccess)
+            return bail(RP_ERR_CUDA, "grid upload");
+        for (int i = 0; i < ngrid; i++) {
+            if (ngrid == 1 && !R.scl) {
+                G.scl[i][0] = G.scl[i][1] = 1.0;
+                G.off[i][0] = G.off[i][1] = 0.0;
+            } else {
+                G.scl[i][0] = R.scl[i]; G.scl[i][1] = R.scl[ngrid + i];
+                G.off[i][0] = R.off[i]; G.off[i][1] = R.off[ngrid + i];
+            }
+        }
+        const size_t e = (size_t)ctx->elem * RP_SLOTS;
+        if (dalloc(&G.zeta, n2 * e) || dalloc(&G.u, nu * G.N * e) || dalloc(&G.v, nv * G.N * e) ||
+            dalloc(&G.w, n2 * sw * e) || dalloc(&G.aks, n2 * sw * e))
+            return bail(RP_ERR_NOMEM, "frame ring allocation");
+        cudaMemset(G.zeta, 0, n2 * e);
+        cudaMemset(G.u, 0, nu * G.N * e);
+        cudaMemset(G.v, 0, nv * G.N * e);
+        cudaMemset(G.w, 0, n2 * sw * e);
+        cudaMemset(G.aks, 0, n2 * sw * e);
+        for (int s = 0; s < RP_SLOTS; s++) {
+            if (cudaEventCreateWithFlags(&G.slot_free[s], cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&G.slot_ready[s], cudaEventDisableTiming) != cudaSuccess)
+                return bail(RP_ERR_CUDA, "event creation");
+        }
+    }
+    const size_t cap = (size_t)std::max(p.numpar, 1);
+    ctx->cap = (int64_t)cap;
+    if (dalloc(&ctx->x, cap * 8) || dalloc(&ctx->y, cap * 8) || dalloc(&ctx->z, cap * 8) ||
+        dalloc(&ctx->age, cap * 8) || dalloc(&ctx->dob, cap * 8) || dalloc(&ctx->status, cap * 8) ||
+        dalloc(&ctx->wd, cap * 8) || dalloc(&ctx->zeta, cap * 8) || dalloc(&ctx->bath, cap * 8) ||
+        dalloc(&ctx->gid, cap * 4) || dalloc(&ctx->isin, cap) || dalloc(&ctx->pid, cap * 4) ||
+        dalloc(&ctx->flags, cap * 4) || dalloc(&ctx->tmp_gid, cap * 8) || dalloc(&ctx->tmp_isin, cap * 4))
+        return bail(RP_ERR_NOMEM, "particle state allocation");
+    const size_t half = (size_t)kChunkElems * 8 * 2;
+    for (int h = 0; h < 2; h++) {
+        if (cudaHostAlloc(&ctx->pin[h], half, cudaHostAllocDefault) != cudaSuccess)
+            return bail(RP_ERR_NOMEM, "pinned staging");
+        if (dalloc(&ctx->dstage[h], half)) return bail(RP_ERR_NOMEM, "device staging");
+        if (cudaEventCreateWithFlags(&ctx->pin_done[h], cudaEventDisableTiming) != cudaSuccess)
+            return bail(RP_ERR_CUDA, "event creation");
+    }
+    if (cudaStreamCreateWithFlags(&ctx->s_comp, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->s_copy, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess)
+        return bail(RP_ERR_CUDA, "stream/event creation");
+    if (cudaDeviceSynchronize() != cudaSuccess) return bail(RP_ERR_CUDA, "initial upload");
+    (void)rc;
+    *out = ctx;
+    return RP_OK;
+}
+
+int rp_destroy(rp_ctx* ctx) {
+    if (!ctx) return RP_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    if (ctx->s_comp) cudaStreamSynchronize(ctx->s_comp);
+    if (ctx->s_copy) cudaStreamSynchronize(ctx->s_copy);
+    free_ctx(ctx);
+    return RP_OK;
+}
+
+int rp_last_error(rp_ctx* ctx, char* buf, int32_t len) {
+    if (!ctx || !buf || len <= 0) return RP_ERR_ARG;
+    std::snprintf(buf, (size_t)len, "%s", ctx->err.c_str());
+    return RP_OK;
+}
+
+int rp_upload_frame(rp_ctx* ctx, int32_t ng, int32_t slot, const double* zeta, const double* u, const double* v,
+                    const double* w, const double* aks, const double* su, const double* sv) {
+    return upload_frame<double>(ctx, ng, slot, zeta, u, v, w, aks, su, sv);
+}
+
+int rp_upload_frame_f32(rp_ctx* ctx, int32_t ng, int32_t slot, const float* zeta, const float* u, const float* v,
+                        const float* w, const float* aks, const float* su, const float* sv) {
+    return upload_frame<float>(ctx, ng, slot, zeta, u, v, w, aks, su, sv);
+}
+
+int rp_set_particles(rp_ctx* ctx, int64_t n, const double* x, const double* y, const double* z,
+                     const double* dob, const double* age, const double* status, const double* gid,
+                     const int32_t* isin) {
+    if (!ctx) return RP_ERR_ARG;
+    if (n < 0 || n > ctx->cap) return fail(ctx, RP_ERR_ARG, "rp_set_particles: n exceeds numpar");
+    if (!x || !y || !z || !dob || !age || !status || !gid || !isin)
+        return fail(ctx, RP_ERR_ARG, "rp_set_particles: null column");
+    for (int64_t i = 0; i < n; i++) {
+        const int gi = (int)gid[i];
+        if (gi < 1 || gi > ctx->ngrid) return fail(ctx, RP_ERR_ARG, "rp_set_particles: grid id out of range");
+    }
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->s_comp;
+    int rc;
+    const size_t b8 = (size_t)n * 8;
+    if ((rc = h2d(ctx, ctx->x, x, b8, s)) || (rc = h2d(ctx, ctx->y, y, b8, s)) || (rc = h2d(ctx, ctx->z, z, b8, s)) ||
+        (rc = h2d(ctx, ctx->dob, dob, b8, s)) || (rc = h2d(ctx, ctx->age, age, b8, s)) ||
+        (rc = h2d(ctx, ctx->status, status, b8, s)) || (rc = h2d(ctx, ctx->tmp_gid, gid, b8, s)) ||
+        (rc = h2d(ctx, ctx->tmp_isin, isin, (size_t)n * 4, s)))
+        return rc;
+    ctx->n = n;
+    RpParticlesDev P = particles_dev(ctx);
+    CK(rp::launch_state_from_host(P, ctx->tmp_gid, ctx->tmp_isin, s));
+    CK(cudaMemsetAsync(ctx->wd, 0, b8, s));
+    CK(cudaMemsetAsync(ctx->zeta, 0, b8, s));
+    CK(cudaMemsetAsync(ctx->bath, 0, b8, s));
+    CK(cudaStreamSynchronize(s));
+    return RP_OK;
+}
+
+int rp_locate_particles(rp_ctx* ctx, int64_t n, const double* ipos, const double* jpos, const double* z,
+                        const double* dob, int32_t t_b) {
+    if (!ctx) return RP_ERR_ARG;
+    if (n < 0 || n > ctx->cap) return fail(ctx, RP_ERR_ARG, "rp_locate_particles: n exceeds numpar");
+    if (!ipos || !jpos || !z || !dob) return fail(ctx, RP_ERR_ARG, "rp_locate_particles: null array");
+    if (t_b < 1 || t_b > 3) return fail(ctx, RP_ERR_ARG, "rp_locate_particles: slot must be 1..3");
+    for (int k = 0; k < ctx->ngrid; k++)
+        if (ctx->g[k].map[t_b - 1] < 0) return fail(ctx, RP_ERR_STATE, "rp_locate_particles: frame slot not loaded");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->s_comp;
+    const size_t nb = (size_t)n * 8, nbg = nb * ctx->ngrid;
+    double *dip = nullptr, *djp = nullptr, *dz = nullptr, *ddob = nullptr;
+    CK(cudaMalloc(&dip, std::max<size_t>(nbg, 8)));
+    CK(cudaMalloc(&djp, std::max<size_t>(nbg, 8)));
+    CK(cudaMalloc(&dz, std::max<size_t>(nb, 8)));
+    CK(cudaMalloc(&ddob, std::max<size_t>(nb, 8)));
+    int rc = RP_OK;
+    if (!(rc = h2d(ctx, dip, ipos, nbg, s)) && !(rc = h2d(ctx, djp, jpos, nbg, s)) && !(rc = h2d(ctx, dz, z, nb, s)) &&
+        !(rc = h2d(ctx, ddob, dob, nb, s))) {
+        ctx->n = n;
+        RpStepArgs A{};
+        fill_params(ctx, A);
+        fill_grids(ctx, A, t_b, t_b, t_b);
+        for (int k = 0; k < ctx->ngrid; k++) {
+            const int ph = ctx->g[k].map[t_b - 1];
+            cudaStreamWaitEvent(s, ctx->g[k].slot_ready[ph], 0);
+        }
+        cudaError_t e = rp::launch_locate(A, ctx->prm.field_dtype, dip, djp, dz, ddob, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = fail(ctx, RP_ERR_CUDA, std::string("locate: ") + cudaGetErrorString(e));
+    }
+    cudaFree(dip); cudaFree(djp); cudaFree(dz); cudaFree(ddob);
+    return rc;
+}
+
+int rp_step(rp_ctx* ctx, const double ex[3], const double ix[3], int32_t ets, int32_t t_b, int32_t t_c,
+            int32_t t_f) {
+    if (!ctx || !ex || !ix) return RP_ERR_ARG;
+    if (t_b < 1 || t_b > 3 || t_c < 1 || t_c > 3 || t_f < 1 || t_f > 3)
+        return fail(ctx, RP_ERR_ARG, "rp_step: slots must be 1..3");
+    for (int k = 0; k < ctx->ngrid; k++) {
+        const GridBuf& G = ctx->g[k];
+        if (G.map[t_b - 1] < 0 || G.map[t_c - 1] < 0 || G.map[t_f - 1] < 0)
+            return fail(ctx, RP_ERR_STATE, "rp_step: a frame slot was never loaded");
+    }
+    if (ctx->hook && ctx->hook_pos >= ctx->hook_steps)
+        return fail(ctx, RP_ERR_STATE, "rp_step: noise hook exhausted");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->s_comp;
+    RpStepArgs A{};
+    fill_params(ctx, A);
+    fill_grids(ctx, A, t_b, t_c, t_f);
+    for (int q = 0; q < 3; q++) { A.ex[q] = ex[q]; A.ix[q] = ix[q]; }
+    A.pi = polint_consts(ex, ix[1]);
+    A.ets = ets;
+    A.step_index = ctx->step_index;
+    A.hook = ctx->hook ? ctx->hook + ctx->hook_pos * ctx->n * ctx->ndraw : nullptr;
+    for (int k = 0; k < ctx->ngrid; k++) {
+        const GridBuf& G = ctx->g[k];
+        const int used[3] = {G.map[t_b - 1], G.map[t_c - 1], G.map[t_f - 1]};
+        for (int q = 0; q < 3; q++) CK(cudaStreamWaitEvent(s, G.slot_ready[used[q]], 0));
+    }
+    int nl = 0;
+    CK(cudaEventRecord(ctx->ev0, s));
+    if (ctx->n > 0) CK(rp::launch_step(A, ctx->prm.field_dtype, ctx->npmax, s, ctx->num_sms, &nl));
+    CK(cudaEventRecord(ctx->ev1, s));
+    ctx->timed = true;
+    ctx->last_kernels = nl;
+    ctx->step_index++;
+    if (ctx->hook) ctx->hook_pos++;
+    return RP_OK;
+}
+
+int rp_get_particles(rp_ctx* ctx, int64_t n, double* x, double* y, double* z, double* age, double* status,
+                     double* gid, int32_t* isin, double* wd, double* zeta, double* bath, uint32_t* flags) {
+    if (!ctx) return RP_ERR_ARG;
+    if (n < 0 || n > ctx->n) return fail(ctx, RP_ERR_ARG, "rp_get_particles: n exceeds particle count");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->s_comp;
+    int rc;
+    const size_t b8 = (size_t)n * 8;
+    if (gid || isin) {
+        RpParticlesDev P = particles_dev(ctx);
+        P.n = n;
+        CK(rp::launch_state_to_host(P, ctx->tmp_gid, ctx->tmp_isin, s));
+    }
+    if ((x && (rc = d2h(ctx, x, ctx->x, b8, s))) || (y && (rc = d2h(ctx, y, ctx->y, b8, s))) ||
+        (z && (rc = d2h(ctx, z, ctx->z, b8, s))) || (age && (rc = d2h(ctx, age, ctx->age, b8, s))) ||
+        (status && (rc = d2h(ctx, status, ctx->status, b8, s))) || (gid && (rc = d2h(ctx, gid, ctx->tmp_gid, b8, s))) ||
+        (isin && (rc = d2h(ctx, isin, ctx->tmp_isin, (size_t)n * 4, s))) || (wd && (rc = d2h(ctx, wd, ctx->wd, b8, s))) ||
+        (zeta && (rc = d2h(ctx, zeta, ctx->zeta, b8, s))) || (bath && (rc = d2h(ctx, bath, ctx->bath, b8, s))) ||
+        (flags && (rc = d2h(ctx, flags, ctx->flags, (size_t)n * 4, s))))
+        return rc;
+    return RP_OK;
+}
+
+int rp_set_step_index(rp_ctx* ctx, uint64_t step_index) {
+    if (!ctx) return RP_ERR_ARG;
+    ctx->step_index = step_index;
+    return RP_OK;
+}
+
+int rp_set_noise_hook(rp_ctx* ctx, const double* noise, int64_t nsteps) {
+    if (!ctx) return RP_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    if (ctx->hook) {
+        CK(cudaStreamSynchronize(ctx->s_comp));
+        cudaFree(ctx->hook);
+        ctx->hook = nullptr;
+    }
+    ctx->hook_steps = 0;
+    ctx->hook_pos = 0;
+    if (!noise) return RP_OK;
+    if (nsteps <= 0 || ctx->n <= 0) return fail(ctx, RP_ERR_ARG, "rp_set_noise_hook: set particles first, nsteps > 0");
+    const size_t bytes = (size_t)nsteps * ctx->n * ctx->ndraw * 8;
+    CK(cudaMalloc(&ctx->hook, bytes));
+    int rc = h2d(ctx, ctx->hook, noise, bytes, ctx->s_comp);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(ctx->s_comp));
+    ctx->hook_steps = nsteps;
+    return RP_OK;
+}
+
+int rp_synchronize(rp_ctx* ctx) {
+    if (!ctx) return RP_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->s_copy));
+    CK(cudaStreamSynchronize(ctx->s_comp));
+    return RP_OK;
+}
+
+int rp_device_state_get(rp_ctx* ctx, rp_device_state* out) {
+    if (!ctx || !out) return RP_ERR_ARG;
+    out->n = ctx->n;
+    out->x = ctx->x; out->y = ctx->y; out->z = ctx->z; out->age = ctx->age; out->dob = ctx->dob;
+    out->status = ctx->status; out->wd = ctx->wd; out->zeta = ctx->zeta; out->bath = ctx->bath;
+    out->gid = ctx->gid; out->isin = ctx->isin; out->pid = ctx->pid; out->flags = ctx->flags;
+    out->stream = (void*)ctx->s_comp;
+    return RP_OK;
+}
+
+int rp_last_step_stats(rp_ctx* ctx, float* ms, int32_t* kernels) {
+    if (!ctx) return RP_ERR_ARG;
+    if (!ctx->timed) return fail(ctx, RP_ERR_STATE, "no step launched yet");
+    CK(cudaEventSynchronize(ctx->ev1));
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, ctx->ev0, ctx->ev1));
+    if (ms) *ms = t;
+    if (kernels) *kernels = ctx->last_kernels;
+    return RP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,25 @@
+// rp_internal.h -- launch entry points shared between the kernel unit
+// (compiled without FMA contraction) and the host-side C ABI unit.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "rp_device.cuh"
+
+namespace rp {
+
+constexpr int kStepBlock = 128;
+
+cudaError_t launch_step(const RpStepArgs& A, int field_dtype, int npmax, cudaStream_t s, int num_sms,
+                        int* nlaunch);
+cudaError_t launch_locate(const RpStepArgs& A, int field_dtype, const double* ipos, const double* jpos,
+                          const double* z, const double* dob, cudaStream_t s);
+cudaError_t launch_convert(int src_f32, int dst_f32, const void* src, const void* add, void* dst, int ni, int nj,
+                           int nk, int slot, int64_t e0, int64_t count, cudaStream_t s);
+cudaError_t launch_state_from_host(const RpParticlesDev& P, const double* gid_d, const int32_t* isin_i,
+                                   cudaStream_t s);
+cudaError_t launch_state_to_host(const RpParticlesDev& P, double* gid_d, int32_t* isin_i, cudaStream_t s);
+
+}  // namespace rp

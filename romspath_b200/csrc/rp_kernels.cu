@@ -1,0 +1,192 @@
+// rp_kernels.cu -- sm_100a kernels of the ROMSPath particle step.
+// Compiled with -fmad=false: every FP64 expression rounds exactly as the
+// reference's left-to-right evaluation (no FMA contraction).
+#include <cuda_runtime.h>
+
+#include "rp_internal.h"
+#include "rp_step.cuh"
+
+namespace rp {
+
+// ------------------------------------------------------------ the step
+
+template <typename T, int NPMAX>
+__global__ void __launch_bounds__(kStepBlock) k_step_fused(const __grid_constant__ RpStepArgs A) {
+    SplineWork<NPMAX> w;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < A.p.n; n += stride)
+        rp_update_one<T, NPMAX>(A, n, w);
+}
+
+template <typename T, int NPMAX>
+static cudaError_t launch_step_t(const RpStepArgs& A, cudaStream_t s, int num_sms, int* nlaunch) {
+    int occ = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_step_fused<T, NPMAX>, kStepBlock, 0);
+    if (e != cudaSuccess) return e;
+    if (occ < 1) occ = 1;
+    int64_t need = (A.p.n + kStepBlock - 1) / kStepBlock;
+    int64_t blocks = (int64_t)num_sms * occ;
+    if (need < blocks) blocks = need;
+    if (blocks < 1) blocks = 1;
+    k_step_fused<T, NPMAX><<<(unsigned)blocks, kStepBlock, 0, s>>>(A);
+    *nlaunch += 1;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_step(const RpStepArgs& A, int field_dtype, int npmax, cudaStream_t s, int num_sms,
+                        int* nlaunch) {
+    if (field_dtype == 1) {
+        if (npmax <= 64) return launch_step_t<float, 64>(A, s, num_sms, nlaunch);
+        if (npmax <= 128) return launch_step_t<float, 128>(A, s, num_sms, nlaunch);
+        return launch_step_t<float, 256>(A, s, num_sms, nlaunch);
+    }
+    if (npmax <= 64) return launch_step_t<double, 64>(A, s, num_sms, nlaunch);
+    if (npmax <= 128) return launch_step_t<double, 128>(A, s, num_sms, nlaunch);
+    return launch_step_t<double, 256>(A, s, num_sms, nlaunch);
+}
+
+// -------------------------------------------- initial ownership (init)
+
+// The grid loop of ini_ROMSPath (ROMSPath.f90:319-432): defaults, then for
+// ng = 1..Ngrid the first grid whose bounds() says in-grid takes the
+// particle, and zbounds() (boundary_module.f90:145-179) fixes z.
+template <typename T>
+__global__ void k_locate(const __grid_constant__ RpStepArgs A, const double* ipos, const double* jpos,
+                         const double* z, const double* dob) {
+    const RpParticlesDev& P = A.p;
+    const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= P.n) return;
+    P.status[n] = 9.0;
+    P.age[n] = 0.0;
+    P.gid[n] = A.ngrid;
+    P.isin[n] = 0;
+    P.wd[n] = 9999.0;
+    P.bath[n] = 9999.0;
+    P.zeta[n] = 9999.0;
+    P.x[n] = 1.0;
+    P.y[n] = 1.0;
+    P.z[n] = z[n];
+    P.dob[n] = dob[n];
+    P.pid[n] = (uint32_t)n;
+    uint32_t fl = 0;
+    for (int ng = 1; ng <= A.ngrid; ng++) {
+        const RpGridDev& g = A.g[ng - 1];
+        const double I = ipos[(int64_t)(ng - 1) * P.n + n], J = jpos[(int64_t)(ng - 1) * P.n + n];
+        bool ingrid, obound;
+        rp_bounds(g, I, J, ingrid, obound);
+        if (!P.isin[n] && ingrid) {
+            P.x[n] = I;
+            P.y[n] = J;
+            P.gid[n] = ng;
+            P.status[n] = 0.0;
+            P.isin[n] = 1;
+            bool inz = false;
+            double Z = P.z[n];
+            if (rp_ifloor(I) > 0) {
+                RhoCell rc;
+                rp_rho_cell(g, I, J, rc, fl);
+                const double tdepth = -1.0 * rp_bil(g.h, rc);
+                const double tzeta = rp_zeta_at<T>(g, rc, g.sb);
+                if ((Z < tzeta) && (Z > tdepth)) inz = true;
+                if (Z >= tzeta) {
+                    Z = tzeta - 0.01;
+                    inz = true;
+                }
+            }
+            P.z[n] = Z;
+            if (!inz) P.status[n] = 9.0;
+        }
+    }
+    P.flags[n] = fl;
+}
+
+cudaError_t launch_locate(const RpStepArgs& A, int field_dtype, const double* ipos, const double* jpos,
+                          const double* z, const double* dob, cudaStream_t s) {
+    const int block = 256;
+    const unsigned blocks = (unsigned)((A.p.n + block - 1) / block);
+    if (blocks == 0) return cudaSuccess;
+    if (field_dtype == 1) k_locate<float><<<blocks, block, 0, s>>>(A, ipos, jpos, z, dob);
+    else k_locate<double><<<blocks, block, 0, s>>>(A, ipos, jpos, z, dob);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------ frame upload
+
+// Fortran-layout source field (i fastest, then j, then k) -> device layout
+// [j][i][k][slot4].  With `add` non-null the two are summed in FP64 first
+// (u += ustokes, hydrodynamic_module.f90:606-660), then rounded to T.
+template <typename S, typename T>
+__global__ void k_convert(const S* __restrict__ src, const S* __restrict__ add, T* __restrict__ dst, int ni,
+                          int nj, int nk, int slot, int64_t e0, int64_t count) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const int64_t e = e0 + t;
+    const int64_t plane = (int64_t)ni * nj;
+    const int k = (int)(e / plane);
+    const int64_t r = e - (int64_t)k * plane;
+    const int j = (int)(r / ni);
+    const int i = (int)(r - (int64_t)j * ni);
+    double v = (double)src[t];
+    if (add) v = v + (double)add[t];
+    dst[(((int64_t)j * ni + i) * nk + k) * RP_SLOTS + slot] = (T)v;
+}
+
+cudaError_t launch_convert(int src_f32, int dst_f32, const void* src, const void* add, void* dst, int ni, int nj,
+                           int nk, int slot, int64_t e0, int64_t count, cudaStream_t s) {
+    const int block = 256;
+    const unsigned blocks = (unsigned)((count + block - 1) / block);
+    if (blocks == 0) return cudaSuccess;
+    if (src_f32) {
+        if (dst_f32)
+            k_convert<float, float><<<blocks, block, 0, s>>>((const float*)src, (const float*)add, (float*)dst, ni,
+                                                             nj, nk, slot, e0, count);
+        else
+            k_convert<float, double><<<blocks, block, 0, s>>>((const float*)src, (const float*)add, (double*)dst,
+                                                              ni, nj, nk, slot, e0, count);
+    } else {
+        if (dst_f32)
+            k_convert<double, float><<<blocks, block, 0, s>>>((const double*)src, (const double*)add, (float*)dst,
+                                                              ni, nj, nk, slot, e0, count);
+        else
+            k_convert<double, double><<<blocks, block, 0, s>>>((const double*)src, (const double*)add,
+                                                               (double*)dst, ni, nj, nk, slot, e0, count);
+    }
+    return cudaGetLastError();
+}
+
+// ----------------------------------------------------- state helpers
+
+__global__ void k_state_from_host(RpParticlesDev P, const double* gid_d, const int32_t* isin_i) {
+    const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= P.n) return;
+    P.gid[n] = (int32_t)gid_d[n];          // int(par(n,pGID))
+    P.isin[n] = isin_i[n] ? 1 : 0;
+    P.pid[n] = (uint32_t)n;
+    P.flags[n] = 0u;
+}
+
+cudaError_t launch_state_from_host(const RpParticlesDev& P, const double* gid_d, const int32_t* isin_i,
+                                   cudaStream_t s) {
+    const int block = 256;
+    const unsigned blocks = (unsigned)((P.n + block - 1) / block);
+    if (blocks == 0) return cudaSuccess;
+    k_state_from_host<<<blocks, block, 0, s>>>(P, gid_d, isin_i);
+    return cudaGetLastError();
+}
+
+__global__ void k_state_to_host(RpParticlesDev P, double* gid_d, int32_t* isin_i) {
+    const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= P.n) return;
+    gid_d[n] = (double)P.gid[n];
+    isin_i[n] = (int32_t)P.isin[n];
+}
+
+cudaError_t launch_state_to_host(const RpParticlesDev& P, double* gid_d, int32_t* isin_i, cudaStream_t s) {
+    const int block = 256;
+    const unsigned blocks = (unsigned)((P.n + block - 1) / block);
+    if (blocks == 0) return cudaSuccess;
+    k_state_to_host<<<blocks, block, 0, s>>>(P, gid_d, isin_i);
+    return cudaGetLastError();
+}
+
+}  // namespace rp

@@ -1,0 +1,512 @@
+// rp_step.cuh -- the per-particle step of update_particles
+// (ROMSPath.f90:662-905) on the device: RK4 advection, HTurb, VTurb with
+// the PPPACK smoothing spline, nest hand-off, vertical update and status.
+#pragma once
+
+#include "rp_device.cuh"
+
+// --------------------------------------------------------------- noise
+
+// Normal deviate `d` of particle `pid` at this step: the noise hook when
+// set, else Philox4x32-10 at counter (pid, step, d/2) with Box-Muller's
+// cosine branch (pdf_module.f90:26-40) on the uniforms (r+0.5)/2^32.
+__device__ __forceinline__ double rp_normal(const RpStepArgs& A, uint32_t pid, uint32_t d) {
+    if (A.hook) return A.hook[(int64_t)pid * A.ndraw + d];
+    uint32_t c[4] = {pid, (uint32_t)A.step_index, (uint32_t)(A.step_index >> 32), d >> 1};
+    rp_philox(c, (uint32_t)A.seed, (uint32_t)(A.seed >> 32));
+    const uint32_t a = (d & 1u) ? c[2] : c[0];
+    const uint32_t b = (d & 1u) ? c[3] : c[1];
+    const double u1 = ((double)a + 0.5) / 4294967296.0;
+    const double u2 = ((double)b + 0.5) / 4294967296.0;
+    return sqrt(-2.0 * rp_log_pos(u1)) * rp_cos2pi(u2);
+}
+
+// ------------------------------------------------------- find_currents
+
+struct StageState {
+    RhoCell rc;
+    double tdepth, zb, zc, zf, zeta;
+};
+
+// find_currents (advection_module.f90:129-350); Z is INOUT.
+template <typename T>
+__device__ __forceinline__ void rp_find_currents(const RpStepArgs& A, const RpGridDev& g, double X, double Y,
+                                                 double& Z, double& Uad, double& Vad, double& Wad,
+                                                 StageState& S, uint32_t& fl) {
+    rp_rho_cell(g, X, Y, S.rc, fl);
+    S.tdepth = -1.0 * rp_bil(g.h, S.rc);
+    S.zb = rp_zeta_at<T>(g, S.rc, g.sb);
+    S.zc = rp_zeta_at<T>(g, S.rc, g.sc);
+    S.zf = rp_zeta_at<T>(g, S.rc, g.sf);
+    if (Z < S.tdepth) Z = S.tdepth + RP_F_0P001;
+    S.zeta = rp_polintd(A.pi, S.zb, S.zc, S.zf);
+    if (Z > S.zeta) Z = S.zeta - RP_F_0P001;
+
+    LevelPick Lr, Lw;
+    rp_walk_rho(g, S.zeta, S.tdepth, Z, Lr);
+    rp_walk_w(g, S.zeta, S.tdepth, Z, Lw, fl);
+    const int N = g.N;
+    {
+        UVCell cu;
+        rp_u_cell(g, X, Y, cu, fl);
+        const double Ub = rp_col_uv<T>(g.u, cu, N, Lr, g.sb);
+        const double Uc = rp_col_uv<T>(g.u, cu, N, Lr, g.sc);
+        if (A.ets == 1) {
+            Uad = rp_polintd(A.pi, Ub, Ub, Uc);
+        } else {
+            const double Uf = rp_col_uv<T>(g.u, cu, N, Lr, g.sf);
+            Uad = rp_polintd(A.pi, Ub, Uc, Uf);
+        }
+    }
+    {
+        UVCell cv;
+        rp_v_cell(g, X, Y, cv, fl);
+        const double Vb = rp_col_uv<T>(g.v, cv, N, Lr, g.sb);
+        const double Vc = rp_col_uv<T>(g.v, cv, N, Lr, g.sc);
+        if (A.ets == 1) {
+            Vad = rp_polintd(A.pi, Vb, Vb, Vc);
+        } else {
+            const double Vf = rp_col_uv<T>(g.v, cv, N, Lr, g.sf);
+            Vad = rp_polintd(A.pi, Vb, Vc, Vf);
+        }
+    }
+    {
+        const double* cw = S.rc.wet4 ? S.rc.cb : S.rc.ci;
+        const double Wb = rp_col_rho<T>(g.w, S.rc, cw, N + 1, Lw, g.sb);
+        const double Wc = rp_col_rho<T>(g.w, S.rc, cw, N + 1, Lw, g.sc);
+        if (A.ets == 1) {
+            Wad = rp_polintd(A.pi, Wb, Wb, Wc);
+        } else {
+            const double Wf = rp_col_rho<T>(g.w, S.rc, cw, N + 1, Lw, g.sf);
+            Wad = rp_polintd(A.pi, Wb, Wc, Wf);
+        }
+    }
+}
+
+// ----------------------------------------------------------- spline
+
+// Workspace of one particle's smoothing-spline fit (1-based views).
+template <int NPMAX>
+struct SplineWork {
+    double fitz[NPMAX + 1];   // breaks fitz(1..np)
+    double y[NPMAX + 1];      // fitKH(1..np)
+    double r[NPMAX + 1];      // serr / (fitz(i+1) - fitz(i))
+    double qty[NPMAX + 1];    // Q'y
+    double d[NPMAX + 1];      // pivots of the factorisation
+    double r1[NPMAX + 1];     // v(i,2) after factorisation
+    double r2[NPMAX + 1];     // v(i,3) after factorisation
+    double u[NPMAX + 1];      // solution u(1..np)
+};
+
+// chol1d (pppack.f90:1428-1566) for p, with the setupq bands rebuilt on the
+// fly from r(i) (the data weights dy are all serr, so
+// v(i,1) = r(i-1), v(i,2) = -r(i) - r(i-1), v(i,3) = r(i)).  Factorisation
+// and forward substitution run in one sweep, back substitution in the
+// reverse sweep; returns sum_i (qu(i)^2 dy(i)^2) in the reference's order
+// and optionally utru (smooth, pppack.f90:5219-5223).
+template <int NPMAX>
+__device__ __forceinline__ double rp_chol1d(SplineWork<NPMAX>& w, int np, double p, double dy2,
+                                            double* utru_out) {
+    const double six1mp = 6.0 * (1.0 - p);
+    const double twop = 2.0 * p;
+    // setupq bands for index i (2 <= i <= np-1)
+    auto v2s = [&](int i) -> double { return -w.r[i] - w.r[i - 1]; };
+    auto v4 = [&](int i) -> double { return w.fitz[i + 1] - w.fitz[i]; };
+    auto V1b = [&](int i) -> double {
+        const double a = w.r[i - 1], b = v2s(i), c = w.r[i];
+        const double v5 = a * a + b * b + c * c;
+        return six1mp * v5 + twop * (v4(i - 1) + v4(i));
+    };
+    auto V2b = [&](int i) -> double {
+        const double v6 = (i <= np - 2) ? (v2s(i) * w.r[i] + w.r[i] * v2s(i + 1)) : 0.0;
+        return six1mp * v6 + p * v4(i);
+    };
+    auto V3b = [&](int i) -> double {
+        const double v7 = (i <= np - 3) ? (w.r[i] * w.r[i + 1]) : 0.0;
+        return six1mp * v7;
+    };
+
+    // factorisation (i = 2..np-2) fused with forward substitution
+    double a1 = V1b(2), a2 = V2b(2), b1 = V1b(3);
+    double uprev = 0.0, ucur = w.qty[2], r2prev = 0.0;
+    w.u[1] = 0.0;
+    w.u[2] = ucur;
+    for (int i = 2; i <= np - 2; i++) {
+        const double V3i = V3b(i);
+        const double ratio1 = a2 / a1;
+        b1 = b1 - ratio1 * a2;
+        const double c2 = V2b(i + 1) - ratio1 * V3i;
+        const double ratio2 = V3i / a1;
+        const double c1 = (i + 2 <= np - 1) ? (V1b(i + 2) - ratio2 * V3i) : 0.0;
+        w.d[i] = a1;
+        w.r1[i] = ratio1;
+        w.r2[i] = ratio2;
+        const double unext = w.qty[i + 1] - ratio1 * ucur - r2prev * uprev;
+        w.u[i + 1] = unext;
+        uprev = ucur;
+        ucur = unext;
+        r2prev = ratio2;
+        a1 = b1;
+        a2 = c2;
+        b1 = c1;
+    }
+    w.d[np - 1] = a1;
+    // back substitution
+    w.u[np] = 0.0;
+    double up2 = 0.0;                         // u(i+2)
+    double up1 = w.u[np - 1] / w.d[np - 1];   // u(i+1)
+    w.u[np - 1] = up1;
+    for (int i = np - 2; i >= 2; i--) {
+        const double ui = w.u[i] / w.d[i] - up1 * w.r1[i] - up2 * w.r2[i];
+        w.u[i] = ui;
+        up2 = up1;
+        up1 = ui;
+    }
+    // qu(i) = Q u and the weighted sum of squares, i = 1..np in order
+    double prev = 0.0, sum = 0.0, utru = 0.0;
+    double ulast = w.u[1];
+    for (int i = 2; i <= np; i++) {
+        const double ui = w.u[i];
+        const double raw = (ui - ulast) / v4(i - 1);
+        const double fin = raw - prev;
+        sum = sum + (fin * fin) * dy2;
+        if (utru_out) utru = utru + v4(i - 1) * (ulast * (ulast + ui) + ui * ui);
+        prev = raw;
+        ulast = ui;
+    }
+    const double finn = -prev;
+    sum = sum + (finn * finn) * dy2;
+    if (utru_out) *utru_out = utru;
+    return sum;
+}
+
+// smooth (pppack.f90:5108-5317) on fitz/y already in w; dy(i) = serr for
+// all i.  Returns p; w.u holds the final u (a(:,3)/(6p) of the reference).
+template <int NPMAX>
+__device__ __forceinline__ double rp_smooth(SplineWork<NPMAX>& w, int np, double serr, double s, int max_iter,
+                                            uint32_t& fl) {
+    const double dy2 = serr * serr;
+    // setupq (pppack.f90:4726-4825): r(i) and Q'y
+    for (int i = 1; i <= np - 1; i++) w.r[i] = serr / (w.fitz[i + 1] - w.fitz[i]);
+    {
+        double prev = (w.y[2] - w.y[1]) / (w.fitz[2] - w.fitz[1]);
+        for (int i = 2; i <= np - 1; i++) {
+            const double diff = (w.y[i + 1] - w.y[i]) / (w.fitz[i + 1] - w.fitz[i]);
+            w.qty[i] = diff - prev;
+            prev = diff;
+        }
+    }
+    double p, q, sfq;
+    if (s <= 0.0) {
+        p = 1.0;
+        rp_chol1d<NPMAX>(w, np, p, dy2, nullptr);
+    } else {
+        p = 0.0;
+        double utru = 0.0;
+        sfq = 36.0 * rp_chol1d<NPMAX>(w, np, p, dy2, &utru);
+        if (s < sfq) {
+            const double ooss = 1.0 / sqrt(s);
+            double oosf = 1.0 / sqrt(sfq);
+            q = -(oosf - ooss) * sfq / (6.0 * utru * oosf);
+            double prevq = 0.0, prevsf = oosf;
+            int it = 0;
+            for (;;) {
+                const double sum = rp_chol1d<NPMAX>(w, np, q / (1.0 + q), dy2, nullptr);
+                sfq = 36.0 * sum / ((1.0 + q) * (1.0 + q));
+                it++;
+                if (fabs(sfq - s) <= 0.01 * s) break;
+                if (it >= max_iter) { fl |= RP_FL_SPLINE; break; }
+                oosf = 1.0 / sqrt(sfq);
+                const double change = (q - prevq) / (oosf - prevsf) * (oosf - ooss);
+                prevq = q;
+                q = q - change;
+                prevsf = oosf;
+            }
+            p = q / (1.0 + q);
+        }
+    }
+    return p;
+}
+
+// ppvalu (pppack.f90:4246-4362) of the smoothing spline at x, with the
+// coefficients of the one piece it needs formed from u and y exactly as
+// smooth's epilogue forms a(:,1..4) (pppack.f90:5303-5316).
+template <int NPMAX>
+__device__ __forceinline__ double rp_ppvalu(const SplineWork<NPMAX>& w, int np, double p, double serr,
+                                            double x, int jderiv) {
+    // interv (pppack.f90:3363-3576) for strictly increasing breaks
+    int i;
+    if (!(x >= w.fitz[1])) {
+        i = 1;
+    } else {
+        int lo = 1, hi = np;   // fitz(lo) <= x; answer in [lo, hi-1]
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (w.fitz[mid] <= x) lo = mid; else hi = mid;
+        }
+        i = lo;
+    }
+    const double dy2 = serr * serr;
+    const double K1 = 6.0 * (1.0 - p) * dy2;
+    auto v4 = [&](int k) -> double { return w.fitz[k + 1] - w.fitz[k]; };
+    auto raw = [&](int k) -> double { return (w.u[k] - w.u[k - 1]) / v4(k - 1); };  // k >= 2
+    auto fin = [&](int k) -> double {
+        if (k == 1) return raw(2) - 0.0;
+        if (k == np) return -raw(np);
+        return raw(k + 1) - raw(k);
+    };
+    const double a1i = w.y[i] - K1 * fin(i);
+    const double a1n = w.y[i + 1] - K1 * fin(i + 1);
+    const double a3i = w.u[i] * 6.0 * p;
+    const double a3n = w.u[i + 1] * 6.0 * p;
+    const double h4 = v4(i);
+    const double a4i = (a3n - a3i) / h4;
+    const double a2i = (a1n - a1i) / h4 - (a3i + a4i / 3.0 * h4) / 2.0 * h4;
+    const double coef[4] = {a1i, a2i, a3i, a4i};
+    const int k = 4;
+    double fmmjdr = (double)(k - jderiv);
+    double value = 0.0;
+    const double h = x - w.fitz[i];
+    int m = k;
+    for (;;) {
+        value = (value / fmmjdr) * h + coef[m - 1];
+        m = m - 1;
+        fmmjdr = fmmjdr - 1.0;
+        if (fmmjdr <= 0.0) break;
+    }
+    return value;
+}
+
+// ----------------------------------------------------------------- VTurb
+
+// VTurb (ver_turb_module.f90:31-329).  The 2-D quantities at (Xpar, Ypar)
+// are those of RK stage 1 (identical operations and operands).
+template <typename T, int NPMAX>
+__device__ double rp_vturb(const RpStepArgs& A, const RpGridDev& g, const StageState& S, double Zpar,
+                           uint32_t pid, uint32_t& fl, SplineWork<NPMAX>& w) {
+    const int sw = g.N + 1;
+    const int np = (int)((double)sw * A.sub);
+    const double tdepth = S.tdepth, zeta = S.zeta;
+    const double h = -1.0 * tdepth;
+    // column z(k), KH(k) (ver_turb_module.f90:100-124); stored in y/qty
+    // scratch slots past np to keep one workspace
+    double* zc = w.r;      // z(1..sw)   (r is rebuilt by setupq later)
+    double* kh = w.qty;    // KH(1..sw)  (qty is rebuilt by setupq later)
+    const double* cw = S.rc.wet4 ? S.rc.cb : S.rc.ci;
+    const int64_t o[4] = {S.rc.o00, S.rc.o10, S.rc.o11, S.rc.o01};
+    for (int k = 1; k <= sw; k++) {
+        const double s = __ldg(g.sw + k - 1), cs = __ldg(g.csw + k - 1);
+        double zb, zcv, zf;
+        if (g.vtransform == 2) {
+            const double Sk = (g.hc * s + h * cs) / (g.hc + h);
+            zb = S.zb + (S.zb + h) * Sk;
+            zcv = S.zc + (S.zc + h) * Sk;
+            zf = S.zf + (S.zf + h) * Sk;
+        } else {
+            zb = rp_zlevel(g.vtransform, g.hc, s, cs, S.zb, h);
+            zcv = rp_zlevel(g.vtransform, g.hc, s, cs, S.zc, h);
+            zf = rp_zlevel(g.vtransform, g.hc, s, cs, S.zf, h);
+        }
+        zc[k] = rp_polintd(A.pi, zb, zcv, zf);
+        double ab[4], ac[4], af[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int64_t base = (o[q] * sw + (k - 1)) * RP_SLOTS;
+            ab[q] = rp_ld<T>(g.aks, base + g.sb);
+            ac[q] = rp_ld<T>(g.aks, base + g.sc);
+            af[q] = rp_ld<T>(g.aks, base + g.sf);
+        }
+        const double Kb = cw[0] * ab[0] + cw[1] * ab[1] + cw[2] * ab[2] + cw[3] * ab[3];
+        const double Kc = cw[0] * ac[0] + cw[1] * ac[1] + cw[2] * ac[2] + cw[3] * ac[3];
+        const double Kf = cw[0] * af[0] + cw[1] * af[1] + cw[2] * af[2] + cw[3] * af[3];
+        kh[k] = rp_polintd(A.pi, Kb, Kc, Kf);
+    }
+    // resample to np points (ver_turb_module.f90:126-136), linint per point
+    const double dz = (zc[sw] - zc[1]) / (double)(np - 1);
+    w.fitz[1] = zc[1];
+    w.fitz[np] = zc[sw];
+    w.y[1] = kh[1];
+    w.y[np] = kh[sw];
+    for (int i = 2; i <= np - 1; i++) {
+        const double x = w.fitz[i - 1] + dz;
+        w.fitz[i] = x;
+        int jlo = 1, jhi = sw;
+        for (;;) {
+            const int k = (jhi + jlo) / 2;
+            if (zc[k] > x) jhi = k; else jlo = k;
+            if (jhi - jlo == 1) break;
+        }
+        const double m = (kh[jlo] - kh[jhi]) / (zc[jlo] - zc[jhi]);
+        const double b = kh[jlo] - m * zc[jlo];
+        w.y[i] = m * x + b;
+    }
+    const double p = rp_smooth<NPMAX>(w, np, A.serr, A.smth, A.spline_max_iter, fl);
+
+    // random displacement sub-steps (ver_turb_module.f90:231-293)
+    const double deltat = A.deltat;
+    double ParZc = Zpar;
+    for (int i = 1; i <= A.loop; i++) {
+        double Kprimec = 0.0;
+        if (ParZc <= tdepth || ParZc >= zeta) Kprimec = 0.0;
+        else Kprimec = rp_ppvalu<NPMAX>(w, np, p, A.serr, ParZc, 1);
+        const double KprimeZc = Kprimec * deltat;
+        const double Z3rdc = ParZc + 0.5 * KprimeZc;
+        double KH3rdc;
+        if (Z3rdc < tdepth || Z3rdc > zeta) {
+            KH3rdc = A.aksback;
+        } else {
+            KH3rdc = rp_ppvalu<NPMAX>(w, np, p, A.serr, Z3rdc, 0);
+            if (KH3rdc < A.aksback) KH3rdc = A.aksback;
+        }
+        const double DEV = rp_normal(A, pid, (uint32_t)(1 + i));
+        const double r = 1.0;
+        const double dTz = KprimeZc + DEV * sqrt(2.0 / r * KH3rdc * deltat);
+        ParZc = ParZc + dTz;
+        if (ParZc <= tdepth) ParZc = tdepth + fabs(ParZc - tdepth);
+        if (ParZc >= zeta) ParZc = zeta - fabs(ParZc - zeta);
+    }
+    return ParZc - Zpar;
+}
+
+// ------------------------------------------------------------ one particle
+
+template <typename T, int NPMAX>
+__device__ void rp_update_one(const RpStepArgs& A, int64_t n, SplineWork<NPMAX>& w) {
+    const RpParticlesDev& P = A.p;
+    if (A.ix[2] <= P.dob[n]) return;                       // ROMSPath.f90:672
+    if (P.status[n] == 9.0) return;                        // 676
+    if (A.oob && !P.isin[n]) return;                       // 688
+    P.age[n] = P.age[n] + (double)(float)A.idt;            // 693
+
+    uint32_t fl = 0;
+    int gid = P.gid[n];
+    const RpGridDev& g = A.g[gid - 1];
+    const uint32_t pid = P.pid[n];
+    const double Xpar = P.x[n], Ypar = P.y[n], z0 = P.z[n];
+    double Zpar = z0;
+
+    double pm, pn;                                         // 727-728
+    {
+        const int I = rp_ifloor(Xpar), J = rp_ifloor(Ypar);
+        const double X = Xpar - (double)I, Y = Ypar - (double)J;
+        const int i0 = rp_clamp(I, 1, g.nx, fl), i1 = rp_clamp(I + 1, 1, g.nx, fl);
+        const int j0 = rp_clamp(J, 1, g.ny, fl), j1 = rp_clamp(J + 1, 1, g.ny, fl);
+        const int64_t o00 = (int64_t)(j0 - 1) * g.nx + (i0 - 1), o10 = (int64_t)(j0 - 1) * g.nx + (i1 - 1);
+        const int64_t o11 = (int64_t)(j1 - 1) * g.nx + (i1 - 1), o01 = (int64_t)(j1 - 1) * g.nx + (i0 - 1);
+        const double c0 = (1 - X) * (1 - Y), c1 = X * (1 - Y), c2 = X * Y, c3 = (1 - X) * Y;
+        pm = c0 * __ldg(g.pm + o00) + c1 * __ldg(g.pm + o10) + c2 * __ldg(g.pm + o11) + c3 * __ldg(g.pm + o01);
+        pn = c0 * __ldg(g.pn + o00) + c1 * __ldg(g.pn + o10) + c2 * __ldg(g.pn + o11) + c3 * __ldg(g.pn + o01);
+    }
+
+    double AdvectX = 0.0, AdvectY = 0.0, AdvectZ = 0.0;
+    StageState S1;
+    bool have_s1 = false;
+    if (A.scheme == 1) {                                   // RKAdvect, advection_module.f90:20-125
+        const double didt = (double)A.idt;
+        double Uad, Vad, Wad;
+        StageState St;
+        rp_find_currents<T>(A, g, Xpar, Ypar, Zpar, Uad, Vad, Wad, S1, fl);
+        have_s1 = true;
+        const double kn1_u = Uad * pm, kn1_v = Vad * pn, kn1_w = Wad;
+        double x1 = Xpar + Uad * pm * didt / 2.0;
+        double y1 = Ypar + Vad * pn * didt / 2.0;
+        double z1 = Zpar + Wad * didt / 2.0;
+        rp_find_currents<T>(A, g, x1, y1, z1, Uad, Vad, Wad, St, fl);
+        const double kn2_u = Uad * pm, kn2_v = Vad * pn, kn2_w = Wad;
+        double x2 = Xpar + Uad * pm * didt / 2.0;
+        double y2 = Ypar + Vad * pn * didt / 2.0;
+        double z2 = Zpar + Wad * didt / 2.0;
+        rp_find_currents<T>(A, g, x2, y2, z2, Uad, Vad, Wad, St, fl);
+        const double kn3_u = Uad * pm, kn3_v = Vad * pn, kn3_w = Wad;
+        double x3 = Xpar + Uad * pm * didt / 2.0;
+        double y3 = Ypar + Vad * pn * didt / 2.0;
+        double z3 = Zpar + Wad * didt / 2.0;
+        rp_find_currents<T>(A, g, x3, y3, z3, Uad, Vad, Wad, St, fl);
+        const double kn4_u = Uad * pm, kn4_v = Vad * pn, kn4_w = Wad;
+        const double P_U = (kn1_u + 2.0 * kn2_u + 2.0 * kn3_u + kn4_u) / 6.0;
+        const double P_V = (kn1_v + 2.0 * kn2_v + 2.0 * kn3_v + kn4_v) / 6.0;
+        const double P_W = (kn1_w + 2.0 * kn2_w + 2.0 * kn3_w + kn4_w) / 6.0;
+        AdvectX = didt * P_U;
+        AdvectY = didt * P_V;
+        AdvectZ = didt * P_W;
+    }
+
+    double TurbHx = 0.0, TurbHy = 0.0;
+    if (A.hturb_on) {                                      // HTurb, hor_turb_module.f90:30-51
+        const double r = 1.0;
+        const double KM = A.khturb[gid - 1];
+        const double devX = rp_normal(A, pid, 0u);
+        const double devY = rp_normal(A, pid, 1u);
+        TurbHx = devX * sqrt(2.0 / r * KM * (double)A.idt);
+        TurbHy = devY * sqrt(2.0 / r * KM * (double)A.idt);
+    }
+    TurbHx = TurbHx * pm;
+    TurbHy = TurbHy * pn;
+
+    double TurbV = 0.0;
+    if (A.vturb_on) {                                      // VTurb, 783
+        if (!have_s1) {
+            rp_rho_cell(g, Xpar, Ypar, S1.rc, fl);
+            S1.tdepth = -1.0 * rp_bil(g.h, S1.rc);
+            S1.zb = rp_zeta_at<T>(g, S1.rc, g.sb);
+            S1.zc = rp_zeta_at<T>(g, S1.rc, g.sc);
+            S1.zf = rp_zeta_at<T>(g, S1.rc, g.sf);
+            S1.zeta = rp_polintd(A.pi, S1.zb, S1.zc, S1.zf);
+        }
+        TurbV = rp_vturb<T, NPMAX>(A, g, S1, Zpar, pid, fl, w);
+    }
+    const double ZBehav = 0.0;                             // behave(): passive
+
+    // new position and nest hand-off (821-836)
+    const double newXpos = P.x[n] + AdvectX + TurbHx;
+    const double newYpos = P.y[n] + AdvectY + TurbHy;
+    double tempX = newXpos, tempY = newYpos;
+    bool ingrid = false, obound = false;
+    for (int i = 1; i <= A.ngrid; i++) {
+        tempX = g.scl[i - 1][0] * newXpos + g.off[i - 1][0];
+        tempY = g.scl[i - 1][1] * newYpos + g.off[i - 1][1];
+        rp_bounds(A.g[i - 1], tempX, tempY, ingrid, obound);
+        if (ingrid) { gid = i; break; }
+    }
+    const RpGridDev& gn = A.g[gid - 1];
+    RhoCell rn;
+    rp_rho_cell(gn, tempX, tempY, rn, fl);
+    const double tdepth = -1.0 * rp_bil(gn.h, rn);         // 837
+    const double e0 = 1.0 * rp_zeta_at<T>(gn, rn, gn.sb);
+    const double e1 = 1.0 * rp_zeta_at<T>(gn, rn, gn.sc);
+    const double e2 = 1.0 * rp_zeta_at<T>(gn, rn, gn.sf);
+    const double P_zeta = rp_polintd(A.pi, e0, e1, e2);    // 843
+    P.wd[n] = (-1.0 * tdepth) + P_zeta;
+    P.zeta[n] = P_zeta;
+    P.bath[n] = -1.0 * tdepth;
+    bool hbot = false, htop = false;
+    double newZpos;
+    if (A.nsb == 0) {                                      // 852-872
+        newZpos = z0 + AdvectZ + TurbV + ZBehav;
+        if (newZpos < tdepth) { newZpos = tdepth + fabs(newZpos - tdepth); hbot = true; }
+        if (newZpos > P_zeta) { newZpos = P_zeta - fabs(newZpos - P_zeta); htop = true; }
+    } else if (A.nsb == 1) {
+        newZpos = P_zeta - A.vertdist;
+    } else {
+        newZpos = tdepth + A.vertdist;
+    }
+    if (ingrid) {                                          // 874-892
+        P.isin[n] = 1;
+        P.x[n] = tempX;
+        P.y[n] = tempY;
+        P.z[n] = newZpos;
+        double st = 1.0;
+        if (htop) st = RP_F_1P1;
+        if (hbot) st = RP_F_1P2;
+        P.status[n] = st;
+        P.gid[n] = gid;
+    } else if (obound) {
+        P.isin[n] = 0;
+        P.gid[n] = A.ngrid;
+        P.status[n] = -8.0;
+    } else {
+        P.isin[n] = 1;
+        P.status[n] = -9.0;
+    }
+    if (fl) P.flags[n] |= fl;
+}

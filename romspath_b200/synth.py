@@ -1,0 +1,335 @@
+"""Synthetic ROMS-shaped grids, hydrodynamic frames and particle releases.
+
+The reference reads its grid (grid_module.f90:41-499) and its hourly frames
+(hydrodynamic_module.f90:112-760, ``updateHydro``) from ROMS NetCDF output.
+No ocean-model output exists on this machine, so the workloads are analytic
+fields with the shapes, sizes and value ranges of the published benchmark
+configurations:
+
+* s-coordinates: ROMS ``Vtransform=2`` / ``Vstretching=4`` stretching
+  (published ROMS formulas; the reference reads ``Cs_r``/``Cs_w`` from the
+  file, grid_module.f90:350-373, and never computes them itself);
+* bathymetry ``h = 20 + 180 (1 - exp(-x / 30 km))``;
+* velocity: a time-dependent double gyre plus a progressive M2 tide, peak
+  speed ~0.3 m/s; ``w`` from continuity of the divergent (tidal) part;
+* ``zeta``: M2 wave of 0.5 m amplitude;
+* ``AKs``: parabolic in depth, peak 1e-2 m^2/s, tidally modulated;
+* optional Stokes drift ``0.05 m/s * exp(z / 5 m)``.
+
+Every array is returned in Fortran (column-major) order with the reference's
+shapes: ``h(xi_rho, eta_rho)``, ``u(xi_u, eta_u, N)``, ``v(xi_v, eta_v, N)``,
+``w/AKs(xi_rho, eta_rho, N+1)``, ``zeta(xi_rho, eta_rho)``.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import Dict, List, Optional
+
+import numpy as np
+
+M2_PERIOD = 44712.0  # s
+
+
+@dataclasses.dataclass
+class GridSpec:
+    xi_rho: int
+    eta_rho: int
+    N: int
+    vtransform: int = 2
+    theta_s: float = 5.0
+    theta_b: float = 0.4
+    hc: float = 10.0
+    dx: float = 1000.0
+    dy: float = 1000.0
+    land: str = "corner"          # "corner" | "islands" | "none"
+    land_frac: float = 0.08
+    land_seed: int = 0
+    stokes: bool = False
+    eddy: float = 0.0             # extra submesoscale eddy amplitude (m/s)
+    field_dtype: str = "f64"      # storage precision of frames: f64 | f32
+    x0: float = 0.0               # physical offset of rho point (1,1) (m)
+    y0: float = 0.0
+    gyre_lx: Optional[float] = None   # gyre domain size; default: this grid
+    gyre_ly: Optional[float] = None
+
+    @property
+    def xi_u(self) -> int:
+        return self.xi_rho - 1
+
+    @property
+    def eta_v(self) -> int:
+        return self.eta_rho - 1
+
+
+def s_coordinate(N: int, theta_s: float, theta_b: float):
+    """ROMS Vstretching=4 s-coordinate and stretching curves.
+
+    Returns ``(s_rho[N], Cs_r[N], s_w[N+1], Cs_w[N+1])`` ordered bottom to
+    top, the order the reference's ``getSlevel``/``getWlevel`` index them
+    (grid_module.f90:513-598).
+    """
+    def stretch(s):
+        if theta_s > 0:
+            c = (1.0 - np.cosh(theta_s * s)) / (np.cosh(theta_s) - 1.0)
+        else:
+            c = -s * s
+        if theta_b > 0:
+            c = (np.exp(theta_b * c) - 1.0) / (1.0 - np.exp(-theta_b))
+        return c
+
+    k_w = np.arange(N + 1, dtype=np.float64)
+    s_w = (k_w - N) / N
+    k_r = np.arange(1, N + 1, dtype=np.float64)
+    s_rho = (k_r - N - 0.5) / N
+    cs_w = stretch(s_w)
+    cs_r = stretch(s_rho)
+    s_w[0], cs_w[0] = -1.0, -1.0
+    s_w[-1], cs_w[-1] = 0.0, 0.0
+    return s_rho, cs_r, s_w, cs_w
+
+
+def _land_mask(spec: GridSpec) -> np.ndarray:
+    nx, ny = spec.xi_rho, spec.eta_rho
+    mask = np.ones((nx, ny), dtype=np.int32, order="F")
+    if spec.land == "corner":
+        mask[:10, :10] = 0
+    elif spec.land == "islands":
+        rng = np.random.default_rng(spec.land_seed)
+        ii, jj = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+        target = spec.land_frac * nx * ny
+        while (mask == 0).sum() < target:
+            ci = rng.uniform(4, nx - 5)
+            cj = rng.uniform(4, ny - 5)
+            r = rng.uniform(1.5, 6.0)
+            mask[(ii - ci) ** 2 + (jj - cj) ** 2 <= r * r] = 0
+    return np.asfortranarray(mask)
+
+
+def make_grid(spec: GridSpec) -> Dict[str, np.ndarray]:
+    """Static grid arrays (the GRIDS(ng) fields the hot path reads)."""
+    nx, ny, N = spec.xi_rho, spec.eta_rho, spec.N
+    x = spec.x0 + np.arange(nx, dtype=np.float64) * spec.dx
+    y = spec.y0 + np.arange(ny, dtype=np.float64) * spec.dy
+    X, _ = np.meshgrid(x, y, indexing="ij")
+    h = 20.0 + 180.0 * (1.0 - np.exp(-X / 30000.0))
+    mask = _land_mask(spec)
+    mask_u = np.asfortranarray((mask[:-1, :] * mask[1:, :]).astype(np.int32))
+    mask_v = np.asfortranarray((mask[:, :-1] * mask[:, 1:]).astype(np.int32))
+    s_rho, cs_r, s_w, cs_w = s_coordinate(N, spec.theta_s, spec.theta_b)
+    return {
+        "h": np.asfortranarray(h),
+        "pm": np.asfortranarray(np.full((nx, ny), 1.0 / spec.dx)),
+        "pn": np.asfortranarray(np.full((nx, ny), 1.0 / spec.dy)),
+        "mask_rho": mask,
+        "mask_u": mask_u,
+        "mask_v": mask_v,
+        "s_rho": s_rho, "cs_r": cs_r, "s_w": s_w, "cs_w": cs_w,
+    }
+
+
+def _zlevels(zeta, h, S):
+    # Vtransform=2: z = zeta + (zeta + h) * S  (grid_module.f90:540)
+    return zeta[..., None] + (zeta + h)[..., None] * S
+
+
+def _stretch_S(h, s, cs, hc):
+    return (hc * s[None, None, :] + h[..., None] * cs[None, None, :]) / (hc + h)[..., None]
+
+
+def _gyre_uv(xp, yp, t, spec: GridSpec):
+    """Double-gyre velocity (m/s) at physical points, time-dependent."""
+    Lx = spec.gyre_lx if spec.gyre_lx else (spec.xi_rho - 1) * spec.dx
+    Ly = spec.gyre_ly if spec.gyre_ly else (spec.eta_rho - 1) * spec.dy
+    xs = 2.0 * xp / Lx
+    ys = yp / Ly
+    eps, om = 0.1, 2.0 * math.pi / (10.0 * 86400.0)
+    a = eps * math.sin(om * t)
+    b = 1.0 - 2.0 * a
+    f = a * xs * xs + b * xs
+    fx = 2.0 * a * xs + b
+    psi0 = 0.3 * Ly / math.pi
+    u = -psi0 * np.sin(math.pi * f) * math.pi * np.cos(math.pi * ys) / Ly
+    v = psi0 * math.pi * np.cos(math.pi * f) * np.sin(math.pi * ys) * fx * (2.0 / Lx)
+    if spec.eddy > 0.0:
+        # submesoscale eddy field (divergence free): psi_e = A L sin(kx) sin(ky)
+        k = 2.0 * math.pi / 20000.0
+        u = u - spec.eddy * np.sin(k * xp) * np.cos(k * yp)
+        v = v + spec.eddy * np.cos(k * xp) * np.sin(k * yp)
+    return u, v
+
+
+def make_frame(spec: GridSpec, grid: Dict[str, np.ndarray], t: float) -> Dict[str, np.ndarray]:
+    """One hydrodynamic frame at model time ``t`` (s), HYDRODATA layout."""
+    nx, ny, N = spec.xi_rho, spec.eta_rho, spec.N
+    h = grid["h"]
+    mask = grid["mask_rho"]
+    x = spec.x0 + np.arange(nx, dtype=np.float64) * spec.dx
+    y = spec.y0 + np.arange(ny, dtype=np.float64) * spec.dy
+    Lx = (spec.xi_rho - 1) * spec.dx
+    om = 2.0 * math.pi / M2_PERIOD
+    kx = 2.0 * math.pi / max(Lx, 1.0)
+    phase_r = om * t - kx * (x[:, None] - spec.x0) + 0.0 * y[None, :]
+    zeta = 0.5 * np.cos(phase_r) * mask
+    S_r = _stretch_S(h, grid["s_rho"], grid["cs_r"], spec.hc)
+    S_w = _stretch_S(h, grid["s_w"], grid["cs_w"], spec.hc)
+    z_r = _zlevels(zeta, h, S_r)
+    z_w = _zlevels(zeta, h, S_w)
+
+    # u points: between rho i and i+1
+    hu = 0.5 * (h[:-1, :] + h[1:, :])
+    zu = 0.5 * (z_r[:-1, :, :] + z_r[1:, :, :])
+    xu = x[:-1] + 0.5 * spec.dx
+    Xu, Yu = np.meshgrid(xu, y, indexing="ij")
+    ug, _ = _gyre_uv(Xu, Yu, t, spec)
+    ut = 0.1 * np.cos(om * t - kx * (Xu - spec.x0))
+    u = (ug[..., None] * np.exp(zu / 100.0)) + ut[..., None]
+    u = u * grid["mask_u"][..., None]
+
+    yv = y[:-1] + 0.5 * spec.dy
+    Xv, Yv = np.meshgrid(x, yv, indexing="ij")
+    _, vg = _gyre_uv(Xv, Yv, t, spec)
+    zv = 0.5 * (z_r[:, :-1, :] + z_r[:, 1:, :])
+    v = vg[..., None] * np.exp(zv / 100.0)
+    v = v * grid["mask_v"][..., None]
+
+    # w from continuity of the depth-uniform tidal current: w = -(z+h) du_t/dx
+    dudx = 0.1 * kx * np.sin(om * t - kx * (x[:, None] - spec.x0)) * np.ones((1, ny))
+    w = -(z_w + h[..., None]) * dudx[..., None]
+    w = w * mask[..., None]
+
+    # AKs: parabolic in depth, peak 1e-2 m^2/s, tidally modulated
+    xi = (z_w + h[..., None]) / (zeta + h)[..., None]
+    kmax = 1e-2 * (0.75 + 0.25 * math.cos(2.0 * om * t))
+    aks = kmax * 4.0 * xi * (1.0 - xi)
+    aks = np.clip(aks, 0.0, None) * mask[..., None]
+
+    out = {"zeta": zeta, "u": u, "v": v, "w": w, "aks": aks}
+    if spec.stokes:
+        su = 0.05 * np.exp(zu / 5.0) * math.cos(math.radians(30.0)) * grid["mask_u"][..., None]
+        sv = 0.05 * np.exp(zv / 5.0) * math.sin(math.radians(30.0)) * grid["mask_v"][..., None]
+        out["su"] = su
+        out["sv"] = sv
+    dt = np.float32 if spec.field_dtype == "f32" else np.float64
+    return {k: np.asfortranarray(a.astype(dt)) for k, a in out.items()}
+
+
+def frame_as_f64(frame: Dict[str, np.ndarray]) -> Dict[str, np.ndarray]:
+    """The frame as the reference holds it (DOUBLE PRECISION), values exact."""
+    return {k: np.asfortranarray(a.astype(np.float64)) for k, a in frame.items()}
+
+
+def frame_with_stokes(frame: Dict[str, np.ndarray]) -> Dict[str, np.ndarray]:
+    """u += ustokes, v += vstokes in FP64, as updateHydro does under -DSTOKES
+    (hydrodynamic_module.f90:606-660)."""
+    f = frame_as_f64(frame)
+    if "su" in f:
+        f["u"] = np.asfortranarray(f["u"] + f["su"])
+        f["v"] = np.asfortranarray(f["v"] + f["sv"])
+    return f
+
+
+def stored_frame(frame: Dict[str, np.ndarray], field_dtype: str, stokes: bool) -> Dict[str, np.ndarray]:
+    """The values the device ring holds for ``frame`` (as FP64 arrays): the
+    Stokes sum is formed in FP64 (as updateHydro does) and then rounded to
+    the storage precision."""
+    f = frame_as_f64(frame)
+    if stokes and "su" in f:
+        f["u"] = f["u"] + f["su"]
+        f["v"] = f["v"] + f["sv"]
+    out = {}
+    for k in ("zeta", "u", "v", "w", "aks"):
+        a = f[k]
+        if field_dtype == "f32":
+            a = a.astype(np.float32).astype(np.float64)
+        out[k] = np.asfortranarray(a)
+    return out
+
+
+@dataclasses.dataclass
+class Release:
+    """Initial particle positions in each grid's fractional index space."""
+    ipos: np.ndarray   # (ngrid, n)
+    jpos: np.ndarray   # (ngrid, n)
+    z: np.ndarray      # (n,) initial depth (m, negative down)
+    dob: np.ndarray    # (n,) release time (s)
+
+
+def uniform_release(spec: GridSpec, grid, frame1, n: int, seed: int = 0,
+                    dob: float = 0.0) -> Release:
+    """n particles uniform in (X, Y, s) over the wet interior of one grid.
+
+    Positions are fractional rho indices in [2, xi_rho-1) x [2, eta_rho-1),
+    the range the reference's bounds() accepts (boundary_module.f90:71);
+    points whose four surrounding rho points are not all wet are redrawn.
+    z = zeta + (zeta + h) s with h, zeta bilinear at the point.
+    """
+    rng = np.random.default_rng(seed)
+    nx, ny = spec.xi_rho, spec.eta_rho
+    mask = grid["mask_rho"]
+    X = np.empty(n)
+    Y = np.empty(n)
+    filled = 0
+    while filled < n:
+        m = (n - filled) * 2 + 16
+        xs = rng.uniform(2.0, nx - 1.0, m)
+        ys = rng.uniform(2.0, ny - 1.0, m)
+        I = np.floor(xs).astype(np.int64) - 1
+        J = np.floor(ys).astype(np.int64) - 1
+        ok = (I >= 1) & (J >= 1) & (I + 1 < nx - 1) & (J + 1 < ny - 1)
+        I = np.clip(I, 0, nx - 2)
+        J = np.clip(J, 0, ny - 2)
+        wet = (mask[I, J] + mask[I + 1, J] + mask[I, J + 1] + mask[I + 1, J + 1]) == 4
+        sel = np.nonzero(ok & wet)[0][: n - filled]
+        X[filled:filled + len(sel)] = xs[sel]
+        Y[filled:filled + len(sel)] = ys[sel]
+        filled += len(sel)
+    s = rng.uniform(-0.98, -0.02, n)
+    I = np.floor(X).astype(np.int64)
+    J = np.floor(Y).astype(np.int64)
+    fx = X - I
+    fy = Y - J
+    I -= 1
+    J -= 1
+
+    def bil(a):
+        return ((1 - fx) * (1 - fy) * a[I, J] + fx * (1 - fy) * a[I + 1, J]
+                + fx * fy * a[I + 1, J + 1] + (1 - fx) * fy * a[I, J + 1])
+
+    h = bil(grid["h"])
+    zeta = bil(frame1["zeta"].astype(np.float64))
+    z = zeta + (zeta + h) * s
+    return Release(ipos=X[None, :].copy(), jpos=Y[None, :].copy(), z=z,
+                   dob=np.full(n, dob, dtype=np.float64))
+
+
+# ------------------------------------------------------------------ configs
+
+def config_spec(name: str) -> List[GridSpec]:
+    """Grid specs of the named workload (one entry per grid, finest first)."""
+    if name in ("cfg1", "cfg3", "cfg5"):
+        return [GridSpec(130, 98, 20, land="corner", field_dtype="f64")]
+    if name == "cfg2":
+        return [GridSpec(512, 384, 30, land="islands", land_frac=0.08, land_seed=2,
+                         stokes=True, field_dtype="f32")]
+    if name == "tiny":
+        return [GridSpec(24, 20, 6, land="corner", field_dtype="f64")]
+    raise KeyError(name)
+
+
+def config_params(name: str) -> dict:
+    """Namelist values (ROMSPath.data groups turbparam / timeparam /
+    advectparam) of the named workload."""
+    base = dict(idt=300, dt=3600, scheme=1, nsb=0, vturb_on=1, hturb_on=0,
+                open_ocean_boundary=0, vertdist=0.25, serr=1e-4, smth=0.6,
+                sub=4.0, deltat=30.0, aksback=1e-8, constant_hturb=[0.0] * 5)
+    if name == "cfg2":
+        base.update(hturb_on=1, constant_hturb=[1.0] * 5)
+    if name == "tiny":
+        base.update(hturb_on=1, constant_hturb=[1.0] * 5)
+    return base
+
+
+CONFIG_PARTICLES = {"cfg1": 10_000, "cfg2": 1_048_576, "cfg3": 4_194_304,
+                    "cfg5": 262_144, "tiny": 64}
+CONFIG_DAYS = {"cfg1": 2.0, "cfg2": 10.0, "cfg3": 10.0, "cfg5": 3.0, "tiny": 0.25}

@@ -1,0 +1,209 @@
+"""Host mirror of the reference's particle-step interface.
+
+``Tracker`` is the Python face of the C ABI: it owns one device context
+(grids, frame ring, particle state) and exposes the calls the kept Fortran
+driver makes -- ``updateHydro`` hand-off (``upload_frame``), the initial
+ownership loop (``locate``), ``update_particles`` (``step``) and the state
+read-back used by ``dataOutput`` (``get_particles``).  ``run`` replays the
+driver's external/internal time loop (ROMSPath.f90:151-178, 465-546).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Callable, Dict, List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from . import schedule as _sched
+
+
+class RomsPathError(RuntimeError):
+    pass
+
+
+def _pd(a):
+    return a.ctypes.data_as(_lib.PD) if a is not None else None
+
+
+def _pf(a):
+    return a.ctypes.data_as(_lib.PF) if a is not None else None
+
+
+class Tracker:
+    def __init__(self, specs, grids: Sequence[Dict[str, np.ndarray]], params: dict, numpar: int,
+                 field_dtype: str = "f64", stokes: bool = False, seed: int = 0, device: int = 0,
+                 scl: Optional[np.ndarray] = None, off: Optional[np.ndarray] = None,
+                 spline_max_iter: int = 100):
+        L = _lib.load()
+        self.L = L
+        self.ng = len(grids)
+        self.field_dtype = field_dtype
+        self._keep: List[np.ndarray] = []
+        P = _lib.RpParams()
+        P.numpar = int(numpar)
+        P.idt = int(params["idt"])
+        P.dt = int(params["dt"])
+        P.scheme = int(params["scheme"])
+        P.nsb = int(params["nsb"])
+        P.vturb_on = int(params["vturb_on"])
+        P.hturb_on = int(params["hturb_on"])
+        P.open_ocean_boundary = int(params["open_ocean_boundary"])
+        P.behavior = 0
+        P.stokes = int(bool(stokes))
+        P.field_dtype = _lib.FIELD_F32 if field_dtype == "f32" else _lib.FIELD_F64
+        P.spline_max_iter = int(spline_max_iter)
+        for k in ("vertdist", "serr", "smth", "sub", "deltat", "aksback"):
+            setattr(P, k, float(params[k]))
+        for i, v in enumerate(list(params["constant_hturb"])[:_lib.MAXNGRID]):
+            P.constant_hturb[i] = float(v)
+        P.seed = int(seed)
+        P.device = int(device)
+        G = (_lib.RpGrid * self.ng)()
+        for k, (sp, gr) in enumerate(zip(specs, grids)):
+            g = G[k]
+            g.xi_rho, g.eta_rho, g.n_rho = sp.xi_rho, sp.eta_rho, sp.N
+            g.vtransform, g.hc = sp.vtransform, sp.hc
+            for name in ("h", "pm", "pn", "s_rho", "cs_r", "s_w", "cs_w"):
+                a = np.asfortranarray(gr[name], dtype=np.float64)
+                self._keep.append(a)
+                setattr(g, name, _pd(a))
+            for name in ("mask_rho", "mask_u", "mask_v"):
+                a = np.asfortranarray(gr[name], dtype=np.int32)
+                self._keep.append(a)
+                setattr(g, name, a.ctypes.data_as(_lib.PI32))
+            if scl is not None:
+                s = np.asfortranarray(np.asarray(scl[k], dtype=np.float64).reshape(self.ng, 2))
+                o = np.asfortranarray(np.asarray(off[k], dtype=np.float64).reshape(self.ng, 2))
+                self._keep += [s, o]
+                g.scl, g.off = _pd(s), _pd(o)
+        self.params = P
+        self.ndraw = 2 + P.idt // int(P.deltat)
+        h = C.c_void_p()
+        rc = L.rp_create(C.byref(P), self.ng, G, C.byref(h))
+        if rc != 0:
+            raise RomsPathError(f"rp_create failed: {_lib.ERRORS.get(rc, rc)}")
+        self.h = h
+        self.n = 0
+
+    # ------------------------------------------------------------ basics
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            buf = C.create_string_buffer(512)
+            self.L.rp_last_error(self.h, buf, 512)
+            raise RomsPathError(f"{what}: {_lib.ERRORS.get(rc, rc)}: {buf.value.decode()}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.rp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------ frames
+    def upload_frame(self, ng: int, slot: int, frame: Dict[str, np.ndarray]):
+        """updateHydro(FIRST, tstep, tind=slot) output of grid ng."""
+        f32 = frame["u"].dtype == np.float32
+        conv = (lambda a: np.asfortranarray(a, dtype=np.float32)) if f32 else \
+            (lambda a: np.asfortranarray(a, dtype=np.float64))
+        arrs = [conv(frame[k]) for k in ("zeta", "u", "v", "w", "aks")]
+        su = conv(frame["su"]) if "su" in frame else None
+        sv = conv(frame["sv"]) if "sv" in frame else None
+        if not self.params.stokes:
+            su = sv = None
+        fn = self.L.rp_upload_frame_f32 if f32 else self.L.rp_upload_frame
+        p = _pf if f32 else _pd
+        rc = fn(self.h, ng, slot, *[p(a) for a in arrs], p(su), p(sv))
+        self._check(rc, "rp_upload_frame")
+
+    # --------------------------------------------------------- particles
+    def set_particles(self, x, y, z, dob, age, status, gid, isin):
+        cols = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z, dob, age, status, gid)]
+        isin = np.ascontiguousarray(isin, dtype=np.int32)
+        rc = self.L.rp_set_particles(self.h, len(cols[0]), *[_pd(a) for a in cols], isin.ctypes.data_as(_lib.PI32))
+        self._check(rc, "rp_set_particles")
+        self.n = len(cols[0])
+
+    def locate(self, release, t_b: int = 1):
+        """ini_ROMSPath ownership loop (ROMSPath.f90:367-432) on the device."""
+        n = release.z.shape[0]
+        ip = np.ascontiguousarray(release.ipos, dtype=np.float64)
+        jp = np.ascontiguousarray(release.jpos, dtype=np.float64)
+        z = np.ascontiguousarray(release.z, dtype=np.float64)
+        dob = np.ascontiguousarray(release.dob, dtype=np.float64)
+        rc = self.L.rp_locate_particles(self.h, n, _pd(ip), _pd(jp), _pd(z), _pd(dob), t_b)
+        self._check(rc, "rp_locate_particles")
+        self.n = n
+
+    def get_particles(self, n: Optional[int] = None) -> Dict[str, np.ndarray]:
+        n = self.n if n is None else n
+        out = {k: np.empty(n) for k in ("x", "y", "z", "age", "status", "gid", "wd", "zeta", "bath")}
+        isin = np.empty(n, dtype=np.int32)
+        flags = np.empty(n, dtype=np.uint32)
+        rc = self.L.rp_get_particles(self.h, n, _pd(out["x"]), _pd(out["y"]), _pd(out["z"]), _pd(out["age"]),
+                                     _pd(out["status"]), _pd(out["gid"]), isin.ctypes.data_as(_lib.PI32),
+                                     _pd(out["wd"]), _pd(out["zeta"]), _pd(out["bath"]),
+                                     flags.ctypes.data_as(_lib.PU32))
+        self._check(rc, "rp_get_particles")
+        out["isin"] = isin
+        out["flags"] = flags
+        return out
+
+    # --------------------------------------------------------------- step
+    def step(self, ex, ix, ets: int, tb: int, tc: int, tf: int):
+        exa = (C.c_double * 3)(*ex)
+        ixa = (C.c_double * 3)(*ix)
+        rc = self.L.rp_step(self.h, exa, ixa, ets, tb, tc, tf)
+        self._check(rc, "rp_step")
+
+    def set_step_index(self, k: int):
+        self._check(self.L.rp_set_step_index(self.h, int(k)), "rp_set_step_index")
+
+    def set_noise_hook(self, noise: Optional[np.ndarray]):
+        """noise[step, particle, draw] of N(0,1) values, or None."""
+        if noise is None:
+            self._check(self.L.rp_set_noise_hook(self.h, None, 0), "rp_set_noise_hook")
+            return
+        a = np.ascontiguousarray(noise, dtype=np.float64)
+        self._check(self.L.rp_set_noise_hook(self.h, _pd(a), a.shape[0]), "rp_set_noise_hook")
+
+    def synchronize(self):
+        self._check(self.L.rp_synchronize(self.h), "rp_synchronize")
+
+    def last_step_stats(self):
+        ms = C.c_float()
+        k = C.c_int32()
+        self._check(self.L.rp_last_step_stats(self.h, C.byref(ms), C.byref(k)), "rp_last_step_stats")
+        return ms.value, k.value
+
+    def device_state(self) -> _lib.RpDeviceState:
+        st = _lib.RpDeviceState()
+        self._check(self.L.rp_device_state_get(self.h, C.byref(st)), "rp_device_state_get")
+        return st
+
+    # ------------------------------------------------------------ driver
+    def run(self, days: float, frame_for: Callable[[int, int], Dict[str, np.ndarray]],
+            on_step: Optional[Callable] = None, max_steps: Optional[int] = None, load_initial: bool = True):
+        """Replay run_ROMSPath's time loop: frames from frame_for(ng, k)."""
+        P = self.params
+        if load_initial:
+            for (k, slot) in _sched.initial_loads():
+                for ng in range(1, self.ng + 1):
+                    self.upload_frame(ng, slot, frame_for(ng, k))
+        done = 0
+        for ext in _sched.external_steps(days, P.dt, P.idt):
+            for (k, slot) in ext.loads:
+                for ng in range(1, self.ng + 1):
+                    self.upload_frame(ng, slot, frame_for(ng, k))
+            for it in ext.internal:
+                self.step(it.ex, it.ix, it.ets, it.tb, it.tc, it.tf)
+                if on_step:
+                    on_step(it)
+                done += 1
+                if max_steps is not None and done >= max_steps:
+                    return done
+        return done
