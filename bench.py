@@ -1,0 +1,388 @@
+#!/usr/bin/env python
+"""Benchmark: particle-steps/s of the B200 ROMSPath particle step.
+
+Workload (the plain-method-at-scale configuration): one ROMS grid of
+512 x 384 rho points x 30 s-levels (Vtransform 2 / Vstretching 4), 8 %
+seeded island land mask, analytic double gyre + M2 tide fields stored in
+FP32 with a 0.05 m/s surface Stokes drift (e-folding 5 m) added on upload,
+horizontal diffusivity Kh = 1 m^2/s, the vertical random displacement model
+on a 30 s sub-step, 1,048,576 particles released uniformly in (x, y, s),
+idt = 300 s, hourly frames.  Arithmetic is FP64 (bit-identical to the CPU
+oracle).  Inputs are synthetic (no ocean-model output on this machine).
+
+One benchmark step = one hydrodynamic frame interval = 12 internal steps
+(update_particles calls) over all particles.
+
+  value   device-resident: frames already in the ring, particles in HBM;
+          CUDA events on the library's compute stream.
+  e2e     through the C ABI with page-locked host buffers: every step
+          uploads one frame (FP32 + Stokes) and reads the particle state
+          back (the dataOutput columns), host clock between device syncs.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+For N > 1 (torchrun), each rank advances its own 1,048,576 particles
+(replicas of the fields, no collective on the data path: weak scaling);
+the reported time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from romspath_b200 import schedule, synth  # noqa: E402
+
+B_ALG = {"cfg2": 3192, "cfg1": 5288}   # algorithmic bytes per particle-step
+WORKLOAD_DESC = ("cfg2: 512x384x30 ROMS grid, 8% islands, FP32-stored u/v/w/AKs/zeta + Stokes, "
+                 "Kh=1 m^2/s, VTurb dt_turb=30 s, RK4 idt=300 s")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cfg2")
+    ap.add_argument("--particles", type=int, default=None)
+    ap.add_argument("--cpu-sample", type=int, default=32768, help="particles in the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback (6.65 TB/s)"
+
+
+def profile_traffic(workload):
+    """DRAM bytes per launch of the step kernel from the committed ncu
+    summary (scaled to the full launch), or None."""
+    p = os.path.join(ROOT, "profiles", f"step_{workload}_traffic.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p)).get("dram_bytes_per_launch")
+        except Exception:
+            return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        loaded = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": float(np.median(loaded)), "sm_max_mhz": float(max(smax)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def pinned_like(a: np.ndarray):
+    """A Fortran-ordered copy of ``a`` in page-locked host memory."""
+    import torch
+    t = torch.empty(a.size, dtype={np.float32: torch.float32, np.float64: torch.float64}[a.dtype.type],
+                    pin_memory=True)
+    buf = t.numpy()
+    buf[:] = np.asfortranarray(a).ravel(order="F")
+    out = buf.reshape(a.shape, order="F")
+    return out, t
+
+
+def pinned_empty(n, dtype):
+    import torch
+    tdt = {np.float64: torch.float64, np.int32: torch.int32, np.uint32: torch.int32}[dtype]
+    t = torch.empty(n, dtype=tdt, pin_memory=True)
+    return t.numpy().view(dtype), t
+
+
+# ------------------------------------------------------------------ CPU arm
+
+def cpu_timing(workload, npart, steps, warmup, threads):
+    """The CPU restatement of the reference step (oracle) on the host cores:
+    `steps` frame intervals of 12 internal steps over `npart` particles."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle import oracle as O
+    spec = synth.config_spec(workload)[0]
+    grid = synth.make_grid(spec)
+    params = synth.config_params(workload)
+    frames = {k: synth.stored_frame(synth.make_frame(spec, grid, (k - 1) * 3600.0), spec.field_dtype, spec.stokes)
+              for k in (1, 2, 3)}
+    m = O.OracleModel([spec], [grid], params)
+    for slot, k in ((1, 1), (2, 2), (3, 3)):
+        m.set_frame(1, slot, frames[k])
+    rel = synth.uniform_release(spec, grid, synth.make_frame(spec, grid, 0.0), npart, seed=0)
+    m.init_particles(rel)
+    ext = list(schedule.external_steps(2.0, 3600, 300))[2]      # ets = 3 pattern
+    t_total, n_steps = 0.0, 0
+    for s in range(warmup + steps):
+        t0 = time.perf_counter()
+        for it in ext.internal:
+            m.step(it.ex, it.ix, it.ets, 1, 2, 3, noise="philox", seed=7, step_index=s * 12 + it.its,
+                   nthreads=threads)
+        dt = time.perf_counter() - t0
+        if s >= warmup:
+            t_total += dt
+            n_steps += 1
+    return npart * 12 * n_steps / t_total, t_total / max(n_steps, 1)
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    npart = min(args.cpu_sample, 16384)
+    val, per = cpu_timing(args.workload, npart, args.steps, args.warmup, threads)
+    line = {
+        "impl": "reference", "metric": "particle-steps/s", "value": val, "unit": "particle-steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": WORKLOAD_DESC,
+                                        "step": "one frame interval = 12 internal steps",
+                                        "sample_particles": npart},
+        "cpu_baseline": {"value": val, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+                         "sample": f"{args.workload} grid, {npart} particles x 12 internal steps per step, "
+                                   f"Philox noise, {threads} OpenMP threads (oracle restatement; the "
+                                   f"Fortran reference cannot be built here)"},
+        "e2e": {"value": val, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU arm
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    from romspath_b200 import Tracker
+
+    wl = args.workload
+    spec = synth.config_spec(wl)[0]
+    grid = synth.make_grid(spec)
+    params = synth.config_params(wl)
+    npart = args.particles or synth.CONFIG_PARTICLES[wl]
+    nframes = 4
+    frames = [synth.make_frame(spec, grid, k * 3600.0) for k in range(nframes)]
+    rel = synth.uniform_release(spec, grid, frames[0], npart, seed=rank)
+
+    T = Tracker([spec], [grid], params, numpar=npart, field_dtype=spec.field_dtype, stokes=spec.stokes,
+                seed=7 + rank, device=local)
+    for k, slot in enumerate((1, 2, 3)):
+        T.upload_frame(1, slot, frames[k])
+    T.locate(rel, t_b=1)
+    T.synchronize()
+    st = T.device_state()
+    stream = torch.cuda.ExternalStream(st.stream, device=torch.device("cuda", local))
+
+    exts = list(schedule.external_steps(30.0, int(params["dt"]), int(params["idt"])))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---------------- value: device-resident, K frame intervals of 12 steps
+    def resident_steps(e0, n_ext, record):
+        evs = []
+        for e in exts[e0:e0 + n_ext]:
+            for it in e.internal:
+                if record:
+                    a = torch.cuda.Event(enable_timing=True)
+                    b = torch.cuda.Event(enable_timing=True)
+                    a.record(stream)
+                T.step(it.ex, it.ix, it.ets, 1, 2, 3)
+                if record:
+                    b.record(stream)
+                    evs.append((a, b))
+        return evs
+
+    resident_steps(2, args.warmup, False)
+    T.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    launches0 = T.kernel_launches()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    evs = resident_steps(2 + args.warmup, args.steps, True)
+    t_end.record(stream)
+    T.synchronize()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    launches = T.kernel_launches() - launches0
+    region_ms = max_over_ranks(t_start.elapsed_time(t_end))
+    kern_ms = [a.elapsed_time(b) for a, b in evs]
+    avg_kernel_ms = max_over_ranks(float(np.mean(kern_ms)))
+    ms_per_step = region_ms / args.steps
+    total_ps = npart * 12 * args.steps * world
+    value = total_ps / (region_ms / 1e3)
+
+    # ---------------- e2e: frames up, particles back, pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        keep = []
+        pframes = []
+        for f in frames:
+            d = {}
+            for k, a in f.items():
+                arr, t = pinned_like(a)
+                keep.append(t)
+                d[k] = arr
+            pframes.append(d)
+        out = {}
+        for k in ("x", "y", "z", "age", "status", "gid", "wd", "zeta", "bath"):
+            out[k], t = pinned_empty(npart, np.float64)
+            keep.append(t)
+        out["isin"], t = pinned_empty(npart, np.int32)
+        keep.append(t)
+        out["flags"], t = pinned_empty(npart, np.uint32)
+        keep.append(t)
+        h2d = sum(pframes[0][k].nbytes for k in ("zeta", "u", "v", "w", "aks", "su", "sv") if k in pframes[0])
+        d2h = sum(v.nbytes for v in out.values())
+
+        def e2e_step(e, fi):
+            for (kf, slot) in e.loads:
+                T.upload_frame(1, slot, pframes[fi % nframes])
+            for it in e.internal:
+                T.step(it.ex, it.ix, it.ets, it.tb, it.tc, it.tf)
+            T.get_particles(npart, out=out)
+
+        base = 2 + args.warmup + args.steps
+        for i in range(args.warmup):
+            e2e_step(exts[base + i], i)
+        T.synchronize()
+        barrier()
+        l0 = T.kernel_launches()
+        t0 = time.perf_counter()
+        for i in range(args.steps):
+            e2e_step(exts[base + args.warmup + i], i + 1)
+        T.synchronize()
+        t1 = time.perf_counter()
+        e2e_s = max_over_ranks(t1 - t0)
+        e2e = {"value": npart * 12 * args.steps * world / e2e_s, "unit": "particle-steps/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "ms_per_step": e2e_s * 1e3 / args.steps, "gpu_launches": T.kernel_launches() - l0,
+               "timing": "host clock between device synchronizations; frames and particle columns in "
+                         "page-locked host memory"}
+
+    # ---------------- roofline of the step kernel (algorithmic bytes)
+    peak, peak_src = measured_peaks()
+    balg = B_ALG.get(wl, 3192)
+    achieved = balg * npart / (avg_kernel_ms / 1e3) / 1e9
+    traffic = profile_traffic(wl)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
+                "kernel": "k_step_fused (one launch per internal step)",
+                "avg_launch_ms": avg_kernel_ms,
+                "algorithmic_bytes": f"{balg} B/particle-step x {npart} particles per launch"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        cval, _ = cpu_timing(wl, args.cpu_sample, 1, 0, threads)
+        cpu = {"value": cval, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+               "sample": f"{wl} grid, {args.cpu_sample} particles x 12 internal steps, Philox noise, "
+                         f"{threads} OpenMP threads (FP64 C restatement of the reference; the Fortran "
+                         f"reference cannot be built here)"}
+
+    T.close()
+    if rank == 0:
+        line = {
+            "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (analytic ROMS-shaped fields, seeded release)",
+            "config": {"workload": WORKLOAD_DESC, "particles_per_gpu": npart,
+                       "step": "one hydro frame interval = 12 internal steps (idt=300 s)",
+                       "form": "plain FP64 arithmetic, FP32-stored fields (bit-identical to the oracle)",
+                       "l2": "inputs larger than L2 (frame ring ~390 MB, particle state ~80 MB)",
+                       "parallelism": f"replicas x{world}: particles split per rank, no data-path collective"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+            "gpu_launches": int(launches),
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

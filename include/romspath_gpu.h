@@ -180,6 +180,9 @@ int rp_device_state_get(rp_ctx *ctx, rp_device_state *out);
  * (CUDA events), and the number of kernels it launched. */
 int rp_last_step_stats(rp_ctx *ctx, float *ms, int32_t *kernels);
 
+/* Total number of kernels this context has launched since creation. */
+int rp_kernel_launches(rp_ctx *ctx, int64_t *count);
+
 /* Library version string. */
 const char *rp_version(void);
 

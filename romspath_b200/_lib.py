@@ -19,7 +19,8 @@ FLAG_OOB, FLAG_NODE, FLAG_WBOT, FLAG_WTOP, FLAG_SPLINE = 1, 2, 4, 8, 16
 EXPORTS = [
     "rp_create", "rp_upload_frame", "rp_upload_frame_f32", "rp_set_particles", "rp_locate_particles",
     "rp_step", "rp_get_particles", "rp_set_step_index", "rp_set_noise_hook", "rp_synchronize",
-    "rp_last_error", "rp_destroy", "rp_device_state_get", "rp_last_step_stats", "rp_version",
+    "rp_last_error", "rp_destroy", "rp_device_state_get", "rp_last_step_stats", "rp_kernel_launches",
+    "rp_version",
 ]
 
 PD = C.POINTER(C.c_double)
@@ -101,6 +102,7 @@ def _declare(L):
     L.rp_destroy.argtypes = [P]
     L.rp_device_state_get.argtypes = [P, C.POINTER(RpDeviceState)]
     L.rp_last_step_stats.argtypes = [P, C.POINTER(C.c_float), C.POINTER(C.c_int32)]
+    L.rp_kernel_launches.argtypes = [P, C.POINTER(C.c_int64)]
     L.rp_version.restype = C.c_char_p
     for name in EXPORTS:
         if name != "rp_version":

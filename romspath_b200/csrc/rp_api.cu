@@ -67,6 +67,7 @@ struct rp_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool timed = false;
     int last_kernels = 0;
+    int64_t launches = 0;
     std::string err;
 };
 
@@ -88,8 +89,22 @@ cudaError_t dalloc(P** p, size_t bytes) {
     return cudaMalloc((void**)p, bytes ? bytes : 1);
 }
 
-// host -> device through the pinned staging halves, on stream s
+bool is_pinned(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// host -> device through the pinned staging halves, on stream s (direct
+// when the caller's buffer is already page-locked)
 int h2d(rp_ctx* ctx, void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    if (bytes && is_pinned(src)) {
+        CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+        return RP_OK;
+    }
     const size_t chunk = (size_t)kChunkElems * 8 * 2;
     size_t done = 0;
     while (done < bytes) {
@@ -106,8 +121,14 @@ int h2d(rp_ctx* ctx, void* dst, const void* src, size_t bytes, cudaStream_t s) {
     return RP_OK;
 }
 
-// device -> host through the pinned staging halves (synchronous)
+// device -> host through the pinned staging halves (synchronous; direct
+// when the caller's buffer is already page-locked)
 int d2h(rp_ctx* ctx, void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    if (bytes && is_pinned(dst)) {
+        CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        return RP_OK;
+    }
     const size_t chunk = (size_t)kChunkElems * 8 * 2;
     size_t done = 0;
     while (done < bytes) {
@@ -233,6 +254,7 @@ int upload_field(rp_ctx* ctx, const S* src, const S* add, void* dst, int ni, int
                                cudaMemcpyHostToDevice, ctx->s_copy));
         CK(rp::launch_convert(src_f32, dst_f32, dst_stage, add ? dst_stage + (size_t)kChunkElems * 8 : nullptr,
                               dst, ni, nj, nk, phys, e0, cnt, ctx->s_copy));
+        ctx->launches++;
         CK(cudaEventRecord(ctx->pin_done[h], ctx->s_copy));
         ctx->pin_used[h] = true;
     }
@@ -448,6 +470,7 @@ int rp_set_particles(rp_ctx* ctx, int64_t n, const double* x, const double* y, c
     ctx->n = n;
     RpParticlesDev P = particles_dev(ctx);
     CK(rp::launch_state_from_host(P, ctx->tmp_gid, ctx->tmp_isin, s));
+    ctx->launches++;
     CK(cudaMemsetAsync(ctx->wd, 0, b8, s));
     CK(cudaMemsetAsync(ctx->zeta, 0, b8, s));
     CK(cudaMemsetAsync(ctx->bath, 0, b8, s));
@@ -483,6 +506,7 @@ int rp_locate_particles(rp_ctx* ctx, int64_t n, const double* ipos, const double
             cudaStreamWaitEvent(s, ctx->g[k].slot_ready[ph], 0);
         }
         cudaError_t e = rp::launch_locate(A, ctx->prm.field_dtype, dip, djp, dz, ddob, s);
+        ctx->launches++;
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) rc = fail(ctx, RP_ERR_CUDA, std::string("locate: ") + cudaGetErrorString(e));
     }
@@ -523,6 +547,7 @@ int rp_step(rp_ctx* ctx, const double ex[3], const double ix[3], int32_t ets, in
     CK(cudaEventRecord(ctx->ev1, s));
     ctx->timed = true;
     ctx->last_kernels = nl;
+    ctx->launches += nl;
     ctx->step_index++;
     if (ctx->hook) ctx->hook_pos++;
     return RP_OK;
@@ -540,6 +565,7 @@ int rp_get_particles(rp_ctx* ctx, int64_t n, double* x, double* y, double* z, do
         RpParticlesDev P = particles_dev(ctx);
         P.n = n;
         CK(rp::launch_state_to_host(P, ctx->tmp_gid, ctx->tmp_isin, s));
+        ctx->launches++;
     }
     if ((x && (rc = d2h(ctx, x, ctx->x, b8, s))) || (y && (rc = d2h(ctx, y, ctx->y, b8, s))) ||
         (z && (rc = d2h(ctx, z, ctx->z, b8, s))) || (age && (rc = d2h(ctx, age, ctx->age, b8, s))) ||
@@ -593,6 +619,12 @@ int rp_device_state_get(rp_ctx* ctx, rp_device_state* out) {
     out->status = ctx->status; out->wd = ctx->wd; out->zeta = ctx->zeta; out->bath = ctx->bath;
     out->gid = ctx->gid; out->isin = ctx->isin; out->pid = ctx->pid; out->flags = ctx->flags;
     out->stream = (void*)ctx->s_comp;
+    return RP_OK;
+}
+
+int rp_kernel_launches(rp_ctx* ctx, int64_t* count) {
+    if (!ctx || !count) return RP_ERR_ARG;
+    *count = ctx->launches;
     return RP_OK;
 }
 

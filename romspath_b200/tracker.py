@@ -139,18 +139,22 @@ class Tracker:
         self._check(rc, "rp_locate_particles")
         self.n = n
 
-    def get_particles(self, n: Optional[int] = None) -> Dict[str, np.ndarray]:
+    def get_particles(self, n: Optional[int] = None, out: Optional[Dict[str, np.ndarray]] = None
+                      ) -> Dict[str, np.ndarray]:
+        """par columns, isIn, pWD/pZeta/pBath and flags; ``out`` may hold
+        preallocated (e.g. page-locked) arrays to fill."""
         n = self.n if n is None else n
-        out = {k: np.empty(n) for k in ("x", "y", "z", "age", "status", "gid", "wd", "zeta", "bath")}
-        isin = np.empty(n, dtype=np.int32)
-        flags = np.empty(n, dtype=np.uint32)
+        if out is None:
+            out = {k: np.empty(n) for k in ("x", "y", "z", "age", "status", "gid", "wd", "zeta", "bath")}
+            out["isin"] = np.empty(n, dtype=np.int32)
+            out["flags"] = np.empty(n, dtype=np.uint32)
+        isin = out["isin"]
+        flags = out["flags"]
         rc = self.L.rp_get_particles(self.h, n, _pd(out["x"]), _pd(out["y"]), _pd(out["z"]), _pd(out["age"]),
                                      _pd(out["status"]), _pd(out["gid"]), isin.ctypes.data_as(_lib.PI32),
                                      _pd(out["wd"]), _pd(out["zeta"]), _pd(out["bath"]),
                                      flags.ctypes.data_as(_lib.PU32))
         self._check(rc, "rp_get_particles")
-        out["isin"] = isin
-        out["flags"] = flags
         return out
 
     # --------------------------------------------------------------- step
@@ -179,6 +183,11 @@ class Tracker:
         k = C.c_int32()
         self._check(self.L.rp_last_step_stats(self.h, C.byref(ms), C.byref(k)), "rp_last_step_stats")
         return ms.value, k.value
+
+    def kernel_launches(self) -> int:
+        c = C.c_int64()
+        self._check(self.L.rp_kernel_launches(self.h, C.byref(c)), "rp_kernel_launches")
+        return c.value
 
     def device_state(self) -> _lib.RpDeviceState:
         st = _lib.RpDeviceState()

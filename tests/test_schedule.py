@@ -1,0 +1,39 @@
+"""The kept Fortran driver's frame-slot schedule (ROMSPath.f90:307-309,
+465-546), including the frame-3-loaded-twice quirk."""
+from romspath_b200 import schedule
+
+
+def frames_held(n_ext):
+    slots = {}
+    for f, s in schedule.initial_loads():
+        slots[s] = f
+    held = []
+    for ext in schedule.external_steps(n_ext / 24.0, 3600, 300):
+        for f, s in ext.loads:
+            slots[s] = f
+        held.append((slots[ext.tb], slots[ext.tc], slots[ext.tf]))
+    return held
+
+
+def test_frames_held_per_external_step():
+    held = frames_held(7)
+    assert held[:5] == [(1, 2, 3), (1, 2, 3), (2, 3, 3), (3, 3, 4), (3, 4, 5)]
+    assert held[5] == (4, 5, 6)
+    assert held[6] == (5, 6, 7)
+
+
+def test_times():
+    ext = list(schedule.external_steps(1.0, 3600, 300))
+    assert len(ext) == 24
+    assert all(len(e.internal) == 12 for e in ext)
+    e1 = ext[0]
+    assert e1.ex == (-3600.0, 0.0, 3600.0)
+    assert e1.internal[0].ix == (-300.0, 0.0, 300.0)
+    assert e1.internal[-1].ix == (3000.0, 3300.0, 3600.0)
+    idx = [it.step_index for e in ext for it in e.internal]
+    assert idx == list(range(288))
+
+
+def test_days_uses_single_precision_product():
+    # seconds = int(days*86400.0) in REAL arithmetic
+    assert len(list(schedule.external_steps(10.0, 3600, 300))) == 240
