@@ -70,15 +70,17 @@ def measured_peaks():
     return 6650.0, "fallback (6.65 TB/s)"
 
 
-def profile_traffic(workload):
-    """DRAM bytes per launch of the step kernel from the committed ncu
-    summary (scaled to the full launch), or None."""
+def profile_traffic(workload, kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary of
+    the same workload, or None when the summary covers another kernel."""
     p = os.path.join(ROOT, "profiles", f"step_{workload}_traffic.json")
     if os.path.exists(p):
         try:
-            return json.load(open(p)).get("dram_bytes_per_launch")
+            d = json.load(open(p))
         except Exception:
             return None
+        if d.get("kernel") == kernel:
+            return d.get("dram_bytes_per_launch")
     return None
 
 
@@ -347,7 +349,7 @@ def main():
     peak, peak_src = measured_peaks()
     balg = B_ALG.get(wl, 3192)
     achieved = balg * npart / (avg_kernel_ms / 1e3) / 1e9
-    traffic = profile_traffic(wl)
+    traffic = profile_traffic(wl, "k_step_fused")
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                 "kernel": "k_step_fused (one launch per internal step)",
