@@ -75,7 +75,8 @@ typedef struct rp_params {
     double constant_hturb[RP_MAXNGRID];  /* ConstantHTurb(ng), m^2/s          */
     uint64_t seed;                       /* Philox key of the turbulence noise */
     int32_t device;                      /* CUDA device ordinal               */
-    int32_t reserved[7];
+    int32_t reserved[7];                 /* [0]: kernel form, 0 fused (default),
+                                            1 split; others must be 0        */
 } rp_params;
 
 /* One grid (GRIDS(ng), grid_module.f90:14-35).  Pointers are borrowed for

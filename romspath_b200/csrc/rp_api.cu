@@ -15,7 +15,7 @@
 namespace {
 
 constexpr int64_t kChunkElems = 4 << 20;     // staging chunk (elements)
-constexpr int kMaxNp = 256;                  // largest spline point count
+using rp::kMaxNp;
 
 struct GridBuf {
     int nx = 0, ny = 0, N = 0, vtransform = 2;
@@ -49,6 +49,7 @@ struct rp_ctx {
     int32_t* gid = nullptr;
     int8_t* isin = nullptr;
     uint32_t *pid = nullptr, *flags = nullptr;
+    double* turbv = nullptr;                   // scratch: VTurb displacement per particle
     double* tmp_gid = nullptr;                 // host-facing conversions
     int32_t* tmp_isin = nullptr;
     // staging
@@ -203,6 +204,9 @@ RpPolint polint_consts(const double xa[3], double x) {
     P.e02 = xa[0] - xa[2];
     P.dns = xa[ns] - x;
     P.b = (ns == 2) ? (xa[2] - x) : (xa[0] - x);
+    P.re12 = 1.0 / P.e12;
+    P.re01 = 1.0 / P.e01;
+    P.re02 = 1.0 / P.e02;
     return P;
 }
 
@@ -219,7 +223,7 @@ void free_ctx(rp_ctx* c) {
         }
     }
     void* ptrs[] = {c->x, c->y, c->z, c->age, c->dob, c->status, c->wd, c->zeta, c->bath,
-                    c->gid, c->isin, c->pid, c->flags, c->tmp_gid, c->tmp_isin, c->hook,
+                    c->gid, c->isin, c->pid, c->flags, c->tmp_gid, c->tmp_isin, c->hook, c->turbv,
                     c->dstage[0], c->dstage[1]};
     for (void* p : ptrs) if (p) cudaFree(p);
     for (int h = 0; h < 2; h++) {
@@ -323,7 +327,6 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
     ctx->device = p.device;
     ctx->elem = (p.field_dtype == RP_FIELD_F32) ? 4 : 8;
     ctx->ndraw = 2 + p.idt / (int)p.deltat;
-    int rc = RP_OK;
     auto bail = [&](int code, const std::string& m) {
         std::fprintf(stderr, "rp_create: %s\n", m.c_str());
         free_ctx(ctx);
@@ -342,7 +345,7 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
         G.nx = R.xi_rho; G.ny = R.eta_rho; G.N = R.n_rho; G.vtransform = R.vtransform; G.hc = R.hc;
         const int sw = G.N + 1;
         const int np = (int)((double)sw * p.sub);
-        if (np < 4 || np > kMaxNp || np < sw) return bail(RP_ERR_UNSUPPORTED, "spline point count int(s_w*sub) must be in [max(4,s_w), 256]");
+        if (np < 4 || np > kMaxNp || np < sw) return bail(RP_ERR_UNSUPPORTED, "spline point count int(s_w*sub) must be in [max(4,s_w), 144]");
         ctx->npmax = std::max(ctx->npmax, np);
         const size_t n2 = (size_t)G.nx * G.ny;
         const size_t nu = (size_t)(G.nx - 1) * G.ny, nv = (size_t)G.nx * (G.ny - 1);
@@ -402,7 +405,8 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
         dalloc(&ctx->age, cap * 8) || dalloc(&ctx->dob, cap * 8) || dalloc(&ctx->status, cap * 8) ||
         dalloc(&ctx->wd, cap * 8) || dalloc(&ctx->zeta, cap * 8) || dalloc(&ctx->bath, cap * 8) ||
         dalloc(&ctx->gid, cap * 4) || dalloc(&ctx->isin, cap) || dalloc(&ctx->pid, cap * 4) ||
-        dalloc(&ctx->flags, cap * 4) || dalloc(&ctx->tmp_gid, cap * 8) || dalloc(&ctx->tmp_isin, cap * 4))
+        dalloc(&ctx->flags, cap * 4) || dalloc(&ctx->tmp_gid, cap * 8) || dalloc(&ctx->tmp_isin, cap * 4) ||
+        dalloc(&ctx->turbv, cap * 8))
         return bail(RP_ERR_NOMEM, "particle state allocation");
     const size_t half = (size_t)kChunkElems * 8 * 2;
     for (int h = 0; h < 2; h++) {
@@ -417,7 +421,6 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
         cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess)
         return bail(RP_ERR_CUDA, "stream/event creation");
     if (cudaDeviceSynchronize() != cudaSuccess) return bail(RP_ERR_CUDA, "initial upload");
-    (void)rc;
     *out = ctx;
     return RP_OK;
 }
@@ -543,7 +546,9 @@ int rp_step(rp_ctx* ctx, const double ex[3], const double ix[3], int32_t ets, in
     }
     int nl = 0;
     CK(cudaEventRecord(ctx->ev0, s));
-    if (ctx->n > 0) CK(rp::launch_step(A, ctx->prm.field_dtype, ctx->npmax, s, ctx->num_sms, &nl));
+    if (ctx->n > 0)
+        CK(rp::launch_step(A, ctx->prm.field_dtype, ctx->npmax, ctx->turbv, ctx->prm.reserved[0] == 1 ? 0 : 1, s,
+                           ctx->num_sms, &nl));
     CK(cudaEventRecord(ctx->ev1, s));
     ctx->timed = true;
     ctx->last_kernels = nl;

@@ -88,6 +88,7 @@ struct RpPolint {
     double e02;   // xa(1)-xa(3)
     double dns;   // xa(ns)-x
     double b;     // xa(3)-x (ns==3) or xa(1)-x
+    double re12, re01, re02;  // RN(1/e12), RN(1/e01), RN(1/e02)
     int ns;       // 0-based nearest node
 };
 
@@ -128,12 +129,41 @@ __device__ __forceinline__ double rp_ld(const void* base, int64_t idx) {
     return (double)__ldg(reinterpret_cast<const T*>(base) + idx);
 }
 
+// ------------------------------------------------------ exact division
+//
+// a / b rounded to nearest, given y = RN(1/b) (CUDA's __drcp_rn): two
+// residual corrections q <- q + (a - b q) y with the residual formed exactly
+// by an FMA.  By Markstein's theorem (P. Markstein, "Computation of
+// elementary functions on the IBM RISC System/6000 processor", IBM J. Res.
+// Dev. 34(1), 1990), if y = RN(1/b) and q is within one ulp of a/b, then
+// RN(q + (a - bq) y) = RN(a/b); the first correction brings RN(a y) within
+// one ulp.  Operands outside [1e-150, 1e150] in magnitude (where a residual
+// could underflow), zero, Inf or NaN take the IEEE division instead, so the
+// result is always the correctly rounded quotient -- the value `a / b`
+// gives -- while divisions sharing a denominator share one reciprocal.
+__device__ __forceinline__ bool rp_div_safe(double b) {
+    const double ab = fabs(b);
+    return ab > 1e-150 && ab < 1e150;
+}
+
+__device__ __forceinline__ double rp_rcp(double b) { return __drcp_rn(b); }
+
+__device__ __forceinline__ double rp_div_by(double a, double b, double y) {
+    const double aa = fabs(a);
+    if (!(aa > 1e-150 && aa < 1e150) || !rp_div_safe(b)) return a / b;
+    const double q0 = a * y;
+    const double r0 = fma(-b, q0, a);
+    const double q1 = fma(r0, y, q0);
+    const double r1 = fma(-b, q1, a);
+    return fma(r1, y, q1);
+}
+
 __device__ __forceinline__ double rp_polintd(const RpPolint& P, double y0, double y1, double y2) {
-    const double q12 = (y2 - y1) / P.e12;
-    const double q01 = (y1 - y0) / P.e01;
+    const double q12 = rp_div_by(y2 - y1, P.e12, P.re12);
+    const double q01 = rp_div_by(y1 - y0, P.e01, P.re01);
     double c = P.d1 * q12;
     c = c - P.d1 * q01;
-    c = c / P.e02;
+    c = rp_div_by(c, P.e02, P.re02);
     const double a = (P.ns == 2) ? q12 : q01;
     const double yns = (P.ns == 0) ? y0 : ((P.ns == 1) ? y1 : y2);
     return yns + P.dns * a + P.b * c;
@@ -158,7 +188,8 @@ __device__ __forceinline__ void rp_getcoeff(double X, double Y, const double m[4
             }
             W[k] = 0.0;
         } else {
-            W[k] = m[k] / dist[k];
+            // masks are 0 or 1: m/dist is RN(1/dist) or +0
+            W[k] = (m[k] != 0.0) ? rp_rcp(dist[k]) : m[k] / dist[k];
         }
     }
     const double WT = W[0] + W[1] + W[2] + W[3];
@@ -166,8 +197,9 @@ __device__ __forceinline__ void rp_getcoeff(double X, double Y, const double m[4
 #pragma unroll
         for (int k = 0; k < 4; k++) cff[k] = 0.0;
     } else {
+        const double yWT = rp_rcp(WT);
 #pragma unroll
-        for (int k = 0; k < 4; k++) cff[k] = W[k] / WT;
+        for (int k = 0; k < 4; k++) cff[k] = rp_div_by(W[k], WT, yWT);
     }
 }
 
@@ -333,6 +365,35 @@ __device__ __forceinline__ double rp_zlevel(int vtransform, double hc, double s,
     return zeta * (1.0 + s) + hc * s + (h - hc) * cs;
 }
 
+// getSlevel/getWlevel with the per-point divisor's reciprocal shared
+// across levels (same quotients as the reference's divisions).
+struct ZCtx {
+    int vt;
+    double hc, h, den, yden, yh;
+};
+
+__device__ __forceinline__ ZCtx rp_zctx(int vtransform, double hc, double h) {
+    ZCtx c;
+    c.vt = vtransform;
+    c.hc = hc;
+    c.h = h;
+    c.den = hc + h;
+    c.yden = rp_rcp(c.den);
+    c.yh = rp_rcp(h);
+    return c;
+}
+
+__device__ __forceinline__ double rp_zlevel_c(const ZCtx& c, double s, double cs, double zeta) {
+    if (c.vt == 2) {
+        const double S = rp_div_by(c.hc * s + c.h * cs, c.den, c.yden);
+        return zeta + (zeta + c.h) * S;
+    } else if (c.vt == 1) {
+        const double S = c.hc * s + (c.h - c.hc) * cs;
+        return S + zeta * (1.0 + rp_div_by(S, c.h, c.yh));
+    }
+    return zeta * (1.0 + s) + c.hc * s + (c.h - c.hc) * cs;
+}
+
 struct LevelPick {
     int ibot, itop;                // 1-based levels
     double z1, z2;                 // zcff(1), zcff(2)
@@ -342,11 +403,12 @@ struct LevelPick {
 __device__ __forceinline__ void rp_walk_rho(const RpGridDev& g, double zeta, double depth, double zpar,
                                             LevelPick& L) {
     const double h = -1.0 * depth;
+    const ZCtx zc = rp_zctx(g.vtransform, g.hc, h);
     const int nz = g.N;
     double zl1 = depth, zl2 = 0.0;
     int i;
     for (i = 1; i <= nz; i++) {
-        zl2 = rp_zlevel(g.vtransform, g.hc, __ldg(g.sr + i - 1), __ldg(g.csr + i - 1), zeta, h);
+        zl2 = rp_zlevel_c(zc, __ldg(g.sr + i - 1), __ldg(g.csr + i - 1), zeta);
         if (zl2 > zpar) break;
         zl1 = zl2;
     }
@@ -365,11 +427,12 @@ __device__ __forceinline__ void rp_walk_rho(const RpGridDev& g, double zeta, dou
 __device__ __forceinline__ void rp_walk_w(const RpGridDev& g, double zeta, double depth, double zpar,
                                           LevelPick& L, uint32_t& fl) {
     const double h = -1.0 * depth;
+    const ZCtx zc = rp_zctx(g.vtransform, g.hc, h);
     const int nz = g.N + 1;
     double zl1 = 0.0, zl2 = 0.0;
     int i;
     for (i = 1; i <= nz; i++) {
-        zl2 = rp_zlevel(g.vtransform, g.hc, __ldg(g.sw + i - 1), __ldg(g.csw + i - 1), zeta, h);
+        zl2 = rp_zlevel_c(zc, __ldg(g.sw + i - 1), __ldg(g.csw + i - 1), zeta);
         if (zl2 > zpar) break;
         zl1 = zl2;
     }
@@ -571,3 +634,4 @@ __device__ __forceinline__ double rp_cos2pi(double u) {
     }
     return sign * r;
 }
+

@@ -12,8 +12,12 @@ namespace rp {
 
 constexpr int kStepBlock = 128;
 
-cudaError_t launch_step(const RpStepArgs& A, int field_dtype, int npmax, cudaStream_t s, int num_sms,
-                        int* nlaunch);
+constexpr int kMaxNp = 144;   // largest spline point count int(s_w*sub)
+
+// variant 1: fused single kernel with a local-memory spline workspace;
+// variant 0: split (k_vturb + k_advect, `turbv` is n doubles of scratch)
+cudaError_t launch_step(const RpStepArgs& A, int field_dtype, int npmax, double* turbv, int variant,
+                        cudaStream_t s, int num_sms, int* nlaunch);
 cudaError_t launch_locate(const RpStepArgs& A, int field_dtype, const double* ipos, const double* jpos,
                           const double* z, const double* dob, cudaStream_t s);
 cudaError_t launch_convert(int src_f32, int dst_f32, const void* src, const void* add, void* dst, int ni, int nj,

@@ -9,40 +9,96 @@
 namespace rp {
 
 // ------------------------------------------------------------ the step
+//
+// Split form (default): k_vturb (one warp per block; the smoothing-spline
+// workspace of its 32 particles lane-interleaved in shared memory) writes
+// each particle's VTurb displacement to scratch; k_advect (RK4, HTurb,
+// hand-off, vertical update, status) then runs at full occupancy.
+// Fused form: one kernel per particle with the workspace in local memory.
 
-template <typename T, int NPMAX>
-__global__ void __launch_bounds__(kStepBlock) k_step_fused(const __grid_constant__ RpStepArgs A) {
-    SplineWork<NPMAX> w;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < A.p.n; n += stride)
-        rp_update_one<T, NPMAX>(A, n, w);
+template <int NPMAX>
+constexpr size_t vturb_smem_bytes() {
+    return (size_t)kSplineArrays * (NPMAX + 1) * 32 * sizeof(double);
 }
 
 template <typename T, int NPMAX>
-static cudaError_t launch_step_t(const RpStepArgs& A, cudaStream_t s, int num_sms, int* nlaunch) {
+__global__ void __launch_bounds__(32, 1) k_vturb(const __grid_constant__ RpStepArgs A, double* __restrict__ turbv) {
+    extern __shared__ double sm[];
+    const SplineView<NPMAX, 32> w{sm + threadIdx.x};
+    const int64_t stride = (int64_t)gridDim.x * 32;
+    for (int64_t n = (int64_t)blockIdx.x * 32 + threadIdx.x; n < A.p.n; n += stride)
+        rp_vturb_one<T>(A, n, w, turbv);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kStepBlock) k_advect(const __grid_constant__ RpStepArgs A,
+                                                      const double* __restrict__ turbv) {
+    const SplineView<1, 1> none{nullptr};
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < A.p.n; n += stride)
+        rp_update_one<T>(A, n, none, turbv);
+}
+
+template <typename T, int NPMAX>
+__global__ void __launch_bounds__(kStepBlock) k_step_fused(const __grid_constant__ RpStepArgs A) {
+    double buf[kSplineArrays * (NPMAX + 1)];
+    const SplineView<NPMAX, 1> w{buf};
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < A.p.n; n += stride)
+        rp_update_one<T>(A, n, w, nullptr);
+}
+
+template <class K>
+static int64_t grid_for(K kernel, int block, size_t smem, int64_t n, int num_sms, cudaError_t* err) {
     int occ = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_step_fused<T, NPMAX>, kStepBlock, 0);
-    if (e != cudaSuccess) return e;
+    *err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, block, smem);
     if (occ < 1) occ = 1;
-    int64_t need = (A.p.n + kStepBlock - 1) / kStepBlock;
+    int64_t need = (n + block - 1) / block;
     int64_t blocks = (int64_t)num_sms * occ;
     if (need < blocks) blocks = need;
-    if (blocks < 1) blocks = 1;
-    k_step_fused<T, NPMAX><<<(unsigned)blocks, kStepBlock, 0, s>>>(A);
+    return blocks < 1 ? 1 : blocks;
+}
+
+template <typename T, int NPMAX>
+static cudaError_t launch_step_t(const RpStepArgs& A, double* turbv, int variant, cudaStream_t s, int num_sms,
+                                 int* nlaunch) {
+    cudaError_t e = cudaSuccess;
+    if (NPMAX > 128) variant = 1;     // the split form's workspace would exceed shared memory
+    if (variant == 1) {
+        const int64_t blocks = grid_for(k_step_fused<T, NPMAX>, kStepBlock, 0, A.p.n, num_sms, &e);
+        if (e != cudaSuccess) return e;
+        k_step_fused<T, NPMAX><<<(unsigned)blocks, kStepBlock, 0, s>>>(A);
+        *nlaunch += 1;
+        return cudaGetLastError();
+    }
+    if (A.vturb_on) {
+        constexpr int NPS = NPMAX > 128 ? 128 : NPMAX;
+        constexpr size_t smem = vturb_smem_bytes<NPS>();
+        e = cudaFuncSetAttribute(k_vturb<T, NPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        const int64_t blocks = grid_for(k_vturb<T, NPS>, 32, smem, A.p.n, num_sms, &e);
+        if (e != cudaSuccess) return e;
+        k_vturb<T, NPS><<<(unsigned)blocks, 32, smem, s>>>(A, turbv);
+        *nlaunch += 1;
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    const int64_t blocks = grid_for(k_advect<T>, kStepBlock, 0, A.p.n, num_sms, &e);
+    if (e != cudaSuccess) return e;
+    k_advect<T><<<(unsigned)blocks, kStepBlock, 0, s>>>(A, A.vturb_on ? turbv : nullptr);
     *nlaunch += 1;
     return cudaGetLastError();
 }
 
-cudaError_t launch_step(const RpStepArgs& A, int field_dtype, int npmax, cudaStream_t s, int num_sms,
-                        int* nlaunch) {
+cudaError_t launch_step(const RpStepArgs& A, int field_dtype, int npmax, double* turbv, int variant,
+                        cudaStream_t s, int num_sms, int* nlaunch) {
     if (field_dtype == 1) {
-        if (npmax <= 64) return launch_step_t<float, 64>(A, s, num_sms, nlaunch);
-        if (npmax <= 128) return launch_step_t<float, 128>(A, s, num_sms, nlaunch);
-        return launch_step_t<float, 256>(A, s, num_sms, nlaunch);
+        if (npmax <= 88) return launch_step_t<float, 88>(A, turbv, variant, s, num_sms, nlaunch);
+        if (npmax <= 128) return launch_step_t<float, 128>(A, turbv, variant, s, num_sms, nlaunch);
+        return launch_step_t<float, 144>(A, turbv, variant, s, num_sms, nlaunch);
     }
-    if (npmax <= 64) return launch_step_t<double, 64>(A, s, num_sms, nlaunch);
-    if (npmax <= 128) return launch_step_t<double, 128>(A, s, num_sms, nlaunch);
-    return launch_step_t<double, 256>(A, s, num_sms, nlaunch);
+    if (npmax <= 88) return launch_step_t<double, 88>(A, turbv, variant, s, num_sms, nlaunch);
+    if (npmax <= 128) return launch_step_t<double, 128>(A, turbv, variant, s, num_sms, nlaunch);
+    return launch_step_t<double, 144>(A, turbv, variant, s, num_sms, nlaunch);
 }
 
 // -------------------------------------------- initial ownership (init)

@@ -85,92 +85,112 @@ __device__ __forceinline__ void rp_find_currents(const RpStepArgs& A, const RpGr
 
 // ----------------------------------------------------------- spline
 
-// Workspace of one particle's smoothing-spline fit (1-based views).
-template <int NPMAX>
-struct SplineWork {
-    double fitz[NPMAX + 1];   // breaks fitz(1..np)
-    double y[NPMAX + 1];      // fitKH(1..np)
-    double r[NPMAX + 1];      // serr / (fitz(i+1) - fitz(i))
-    double qty[NPMAX + 1];    // Q'y
-    double d[NPMAX + 1];      // pivots of the factorisation
-    double r1[NPMAX + 1];     // v(i,2) after factorisation
-    double r2[NPMAX + 1];     // v(i,3) after factorisation
-    double u[NPMAX + 1];      // solution u(1..np)
+// Workspace of one particle's smoothing-spline fit: six arrays of
+// (NPMAX+1) doubles with 1-based element i of array a at
+// base[(a*(NPMAX+1) + i) * S].  S = 1 for a private array, S = 32 for a
+// warp's lane-interleaved shared-memory block (bank-conflict free).
+constexpr int kSplineArrays = 6;
+
+template <int NPMAX, int S>
+struct SplineView {
+    double* base;
+    __device__ __forceinline__ double& at(int a, int i) const { return base[(a * (NPMAX + 1) + i) * S]; }
+    __device__ __forceinline__ double& fitz(int i) const { return at(0, i); }  // breaks fitz(1..np)
+    __device__ __forceinline__ double& y(int i) const { return at(1, i); }     // fitKH(1..np)
+    __device__ __forceinline__ double& qty(int i) const { return at(2, i); }   // Q'y
+    __device__ __forceinline__ double& r1(int i) const { return at(3, i); }    // v(i,2) after factorisation
+    __device__ __forceinline__ double& r2(int i) const { return at(4, i); }    // v(i,3) after factorisation
+    __device__ __forceinline__ double& u(int i) const { return at(5, i); }     // u(i)/v(i,1), then u(i)
 };
 
-// chol1d (pppack.f90:1428-1566) for p, with the setupq bands rebuilt on the
-// fly from r(i) (the data weights dy are all serr, so
-// v(i,1) = r(i-1), v(i,2) = -r(i) - r(i-1), v(i,3) = r(i)).  Factorisation
-// and forward substitution run in one sweep, back substitution in the
-// reverse sweep; returns sum_i (qu(i)^2 dy(i)^2) in the reference's order
-// and optionally utru (smooth, pppack.f90:5219-5223).
-template <int NPMAX>
-__device__ __forceinline__ double rp_chol1d(SplineWork<NPMAX>& w, int np, double p, double dy2,
+// chol1d (pppack.f90:1428-1566) for p.  The setupq bands are rebuilt on the
+// fly: with all data weights dy(i) = serr, v(i,1) = r(i-1),
+// v(i,2) = -r(i) - r(i-1), v(i,3) = r(i) where r(k) = serr / v(k,4) and
+// v(k,4) = fitz(k+1) - fitz(k), each formed by the same operation as in
+// setupq.  Factorisation and forward substitution run in one ascending
+// sweep that stores v(i,2), v(i,3) and u(i)/v(i,1); back substitution runs
+// descending; then Q u and sum_i qu(i)^2 dy(i)^2 are formed ascending (the
+// reference's summation order), with utru (pppack.f90:5219-5223) on request.
+template <class W>
+__device__ __forceinline__ double rp_chol1d(const W& w, int np, double p, double serr, double dy2,
                                             double* utru_out) {
     const double six1mp = 6.0 * (1.0 - p);
     const double twop = 2.0 * p;
-    // setupq bands for index i (2 <= i <= np-1)
-    auto v2s = [&](int i) -> double { return -w.r[i] - w.r[i - 1]; };
-    auto v4 = [&](int i) -> double { return w.fitz[i + 1] - w.fitz[i]; };
-    auto V1b = [&](int i) -> double {
-        const double a = w.r[i - 1], b = v2s(i), c = w.r[i];
-        const double v5 = a * a + b * b + c * c;
-        return six1mp * v5 + twop * (v4(i - 1) + v4(i));
-    };
-    auto V2b = [&](int i) -> double {
-        const double v6 = (i <= np - 2) ? (v2s(i) * w.r[i] + w.r[i] * v2s(i + 1)) : 0.0;
-        return six1mp * v6 + p * v4(i);
-    };
-    auto V3b = [&](int i) -> double {
-        const double v7 = (i <= np - 3) ? (w.r[i] * w.r[i + 1]) : 0.0;
-        return six1mp * v7;
-    };
-
-    // factorisation (i = 2..np-2) fused with forward substitution
-    double a1 = V1b(2), a2 = V2b(2), b1 = V1b(3);
-    double uprev = 0.0, ucur = w.qty[2], r2prev = 0.0;
-    w.u[1] = 0.0;
-    w.u[2] = ucur;
+    double v4a = w.fitz(2) - w.fitz(1);          // v4(1)
+    double v4b = w.fitz(3) - w.fitz(2);          // v4(2)
+    double v4c = w.fitz(4) - w.fitz(3);          // v4(3)
+    const double r1_ = serr / v4a;               // r(1)
+    double ri = serr / v4b;                      // r(i),   i = 2
+    double rn = serr / v4c;                      // r(i+1)
+    double v4n = v4c;                            // v4(i+1)
+    double a1, a2, b1;
+    {
+        const double v2s2 = -ri - r1_;
+        const double v2s3 = -rn - ri;
+        const double v5_2 = r1_ * r1_ + v2s2 * v2s2 + ri * ri;
+        a1 = six1mp * v5_2 + twop * (v4a + v4b);                         // V1(2)
+        const double v6_2 = (2 <= np - 2) ? (v2s2 * ri + ri * v2s3) : 0.0;
+        a2 = six1mp * v6_2 + p * v4b;                                     // V2(2)
+        const double v5_3 = ri * ri + v2s3 * v2s3 + rn * rn;
+        b1 = six1mp * v5_3 + twop * (v4b + v4c);                         // V1(3)
+    }
+    double uprev = 0.0, ucur = w.qty(2), r2prev = 0.0;
+    w.u(1) = 0.0;
     for (int i = 2; i <= np - 2; i++) {
-        const double V3i = V3b(i);
+        // r(i+2), v4(i+2) (defined while i+2 <= np-1)
+        double rnn = 0.0, v4nn = 0.0;
+        if (i + 2 <= np - 1) {
+            v4nn = w.fitz(i + 3) - w.fitz(i + 2);
+            rnn = serr / v4nn;
+        }
+        const double V3i = six1mp * ((i <= np - 3) ? (ri * rn) : 0.0);
         const double ratio1 = a2 / a1;
         b1 = b1 - ratio1 * a2;
-        const double c2 = V2b(i + 1) - ratio1 * V3i;
+        const double v2sn = -rn - ri;             // v(i+1,2) of setupq
+        const double v2snn = -rnn - rn;           // v(i+2,2)
+        const double v6n = (i + 1 <= np - 2) ? (v2sn * rn + rn * v2snn) : 0.0;
+        const double c2 = (six1mp * v6n + p * v4n) - ratio1 * V3i;
         const double ratio2 = V3i / a1;
-        const double c1 = (i + 2 <= np - 1) ? (V1b(i + 2) - ratio2 * V3i) : 0.0;
-        w.d[i] = a1;
-        w.r1[i] = ratio1;
-        w.r2[i] = ratio2;
-        const double unext = w.qty[i + 1] - ratio1 * ucur - r2prev * uprev;
-        w.u[i + 1] = unext;
+        double c1 = 0.0;
+        if (i + 2 <= np - 1) {
+            const double v5nn = rn * rn + v2snn * v2snn + rnn * rnn;
+            c1 = (six1mp * v5nn + twop * (v4n + v4nn)) - ratio2 * V3i;
+        }
+        w.r1(i) = ratio1;
+        w.r2(i) = ratio2;
+        w.u(i) = ucur / a1;                       // u(i)/v(i,1)
+        const double unext = w.qty(i + 1) - ratio1 * ucur - r2prev * uprev;
         uprev = ucur;
         ucur = unext;
         r2prev = ratio2;
         a1 = b1;
         a2 = c2;
         b1 = c1;
+        ri = rn;
+        rn = rnn;
+        v4n = v4nn;
     }
-    w.d[np - 1] = a1;
     // back substitution
-    w.u[np] = 0.0;
-    double up2 = 0.0;                         // u(i+2)
-    double up1 = w.u[np - 1] / w.d[np - 1];   // u(i+1)
-    w.u[np - 1] = up1;
+    const double unm1 = ucur / a1;                // u(np-1)/v(np-1,1)
+    w.u(np - 1) = unm1;
+    w.u(np) = 0.0;
+    double up2 = 0.0, up1 = unm1;
     for (int i = np - 2; i >= 2; i--) {
-        const double ui = w.u[i] / w.d[i] - up1 * w.r1[i] - up2 * w.r2[i];
-        w.u[i] = ui;
+        const double ui = w.u(i) - up1 * w.r1(i) - up2 * w.r2(i);
+        w.u(i) = ui;
         up2 = up1;
         up1 = ui;
     }
-    // qu(i) = Q u and the weighted sum of squares, i = 1..np in order
+    // qu = Q u and the weighted sum of squares, i = 1..np in order
     double prev = 0.0, sum = 0.0, utru = 0.0;
-    double ulast = w.u[1];
+    double ulast = 0.0;                           // u(1)
     for (int i = 2; i <= np; i++) {
-        const double ui = w.u[i];
-        const double raw = (ui - ulast) / v4(i - 1);
+        const double ui = w.u(i);
+        const double v4i = w.fitz(i) - w.fitz(i - 1);
+        const double raw = (ui - ulast) / v4i;
         const double fin = raw - prev;
         sum = sum + (fin * fin) * dy2;
-        if (utru_out) utru = utru + v4(i - 1) * (ulast * (ulast + ui) + ui * ui);
+        if (utru_out) utru = utru + v4i * (ulast * (ulast + ui) + ui * ui);
         prev = raw;
         ulast = ui;
     }
@@ -181,29 +201,28 @@ __device__ __forceinline__ double rp_chol1d(SplineWork<NPMAX>& w, int np, double
 }
 
 // smooth (pppack.f90:5108-5317) on fitz/y already in w; dy(i) = serr for
-// all i.  Returns p; w.u holds the final u (a(:,3)/(6p) of the reference).
-template <int NPMAX>
-__device__ __forceinline__ double rp_smooth(SplineWork<NPMAX>& w, int np, double serr, double s, int max_iter,
+// all i.  Returns p; w.u holds the final u.
+template <class W>
+__device__ __forceinline__ double rp_smooth(const W& w, int np, double serr, double s, int max_iter,
                                             uint32_t& fl) {
     const double dy2 = serr * serr;
-    // setupq (pppack.f90:4726-4825): r(i) and Q'y
-    for (int i = 1; i <= np - 1; i++) w.r[i] = serr / (w.fitz[i + 1] - w.fitz[i]);
+    // setupq's Q'y (pppack.f90:4816-4822)
     {
-        double prev = (w.y[2] - w.y[1]) / (w.fitz[2] - w.fitz[1]);
+        double prev = (w.y(2) - w.y(1)) / (w.fitz(2) - w.fitz(1));
         for (int i = 2; i <= np - 1; i++) {
-            const double diff = (w.y[i + 1] - w.y[i]) / (w.fitz[i + 1] - w.fitz[i]);
-            w.qty[i] = diff - prev;
+            const double diff = (w.y(i + 1) - w.y(i)) / (w.fitz(i + 1) - w.fitz(i));
+            w.qty(i) = diff - prev;
             prev = diff;
         }
     }
     double p, q, sfq;
     if (s <= 0.0) {
         p = 1.0;
-        rp_chol1d<NPMAX>(w, np, p, dy2, nullptr);
+        rp_chol1d(w, np, p, serr, dy2, nullptr);
     } else {
         p = 0.0;
         double utru = 0.0;
-        sfq = 36.0 * rp_chol1d<NPMAX>(w, np, p, dy2, &utru);
+        sfq = 36.0 * rp_chol1d(w, np, p, serr, dy2, &utru);
         if (s < sfq) {
             const double ooss = 1.0 / sqrt(s);
             double oosf = 1.0 / sqrt(sfq);
@@ -211,7 +230,7 @@ __device__ __forceinline__ double rp_smooth(SplineWork<NPMAX>& w, int np, double
             double prevq = 0.0, prevsf = oosf;
             int it = 0;
             for (;;) {
-                const double sum = rp_chol1d<NPMAX>(w, np, q / (1.0 + q), dy2, nullptr);
+                const double sum = rp_chol1d(w, np, q / (1.0 + q), serr, dy2, nullptr);
                 sfq = 36.0 * sum / ((1.0 + q) * (1.0 + q));
                 it++;
                 if (fabs(sfq - s) <= 0.01 * s) break;
@@ -231,48 +250,48 @@ __device__ __forceinline__ double rp_smooth(SplineWork<NPMAX>& w, int np, double
 // ppvalu (pppack.f90:4246-4362) of the smoothing spline at x, with the
 // coefficients of the one piece it needs formed from u and y exactly as
 // smooth's epilogue forms a(:,1..4) (pppack.f90:5303-5316).
-template <int NPMAX>
-__device__ __forceinline__ double rp_ppvalu(const SplineWork<NPMAX>& w, int np, double p, double serr,
-                                            double x, int jderiv) {
+template <class W>
+__device__ __forceinline__ double rp_ppvalu(const W& w, int np, double p, double serr, double x, int jderiv) {
     // interv (pppack.f90:3363-3576) for strictly increasing breaks
     int i;
-    if (!(x >= w.fitz[1])) {
+    if (!(x >= w.fitz(1))) {
         i = 1;
     } else {
         int lo = 1, hi = np;   // fitz(lo) <= x; answer in [lo, hi-1]
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
-            if (w.fitz[mid] <= x) lo = mid; else hi = mid;
+            if (w.fitz(mid) <= x) lo = mid; else hi = mid;
         }
         i = lo;
     }
     const double dy2 = serr * serr;
     const double K1 = 6.0 * (1.0 - p) * dy2;
-    auto v4 = [&](int k) -> double { return w.fitz[k + 1] - w.fitz[k]; };
-    auto raw = [&](int k) -> double { return (w.u[k] - w.u[k - 1]) / v4(k - 1); };  // k >= 2
+    auto v4 = [&](int k) -> double { return w.fitz(k + 1) - w.fitz(k); };
+    auto raw = [&](int k) -> double { return (w.u(k) - w.u(k - 1)) / v4(k - 1); };  // k >= 2
     auto fin = [&](int k) -> double {
         if (k == 1) return raw(2) - 0.0;
         if (k == np) return -raw(np);
         return raw(k + 1) - raw(k);
     };
-    const double a1i = w.y[i] - K1 * fin(i);
-    const double a1n = w.y[i + 1] - K1 * fin(i + 1);
-    const double a3i = w.u[i] * 6.0 * p;
-    const double a3n = w.u[i + 1] * 6.0 * p;
+    const double a1i = w.y(i) - K1 * fin(i);
+    const double a1n = w.y(i + 1) - K1 * fin(i + 1);
+    const double a3i = w.u(i) * 6.0 * p;
+    const double a3n = w.u(i + 1) * 6.0 * p;
     const double h4 = v4(i);
     const double a4i = (a3n - a3i) / h4;
     const double a2i = (a1n - a1i) / h4 - (a3i + a4i / 3.0 * h4) / 2.0 * h4;
-    const double coef[4] = {a1i, a2i, a3i, a4i};
-    const int k = 4;
-    double fmmjdr = (double)(k - jderiv);
+    // Horner loop of ppvalu with k = 4: value = (value/fmmjdr)*h + coef(m)
+    const double h = x - w.fitz(i);
     double value = 0.0;
-    const double h = x - w.fitz[i];
-    int m = k;
-    for (;;) {
-        value = (value / fmmjdr) * h + coef[m - 1];
-        m = m - 1;
-        fmmjdr = fmmjdr - 1.0;
-        if (fmmjdr <= 0.0) break;
+    if (jderiv == 0) {
+        value = (value / 4.0) * h + a4i;
+        value = (value / 3.0) * h + a3i;
+        value = (value / 2.0) * h + a2i;
+        value = (value / 1.0) * h + a1i;
+    } else {
+        value = (value / 3.0) * h + a4i;
+        value = (value / 2.0) * h + a3i;
+        value = (value / 1.0) * h + a2i;
     }
     return value;
 }
@@ -281,33 +300,34 @@ __device__ __forceinline__ double rp_ppvalu(const SplineWork<NPMAX>& w, int np, 
 
 // VTurb (ver_turb_module.f90:31-329).  The 2-D quantities at (Xpar, Ypar)
 // are those of RK stage 1 (identical operations and operands).
-template <typename T, int NPMAX>
+template <typename T, class W>
 __device__ double rp_vturb(const RpStepArgs& A, const RpGridDev& g, const StageState& S, double Zpar,
-                           uint32_t pid, uint32_t& fl, SplineWork<NPMAX>& w) {
+                           uint32_t pid, uint32_t& fl, const W& w) {
     const int sw = g.N + 1;
     const int np = (int)((double)sw * A.sub);
     const double tdepth = S.tdepth, zeta = S.zeta;
     const double h = -1.0 * tdepth;
-    // column z(k), KH(k) (ver_turb_module.f90:100-124); stored in y/qty
-    // scratch slots past np to keep one workspace
-    double* zc = w.r;      // z(1..sw)   (r is rebuilt by setupq later)
-    double* kh = w.qty;    // KH(1..sw)  (qty is rebuilt by setupq later)
+    const ZCtx zx = rp_zctx(g.vtransform, g.hc, h);
+    // column z(k), KH(k) (ver_turb_module.f90:100-124), held in the r1/r2
+    // arrays until the fit overwrites them
+    auto zc = [&](int k) -> double& { return w.r1(k); };
+    auto kh = [&](int k) -> double& { return w.r2(k); };
     const double* cw = S.rc.wet4 ? S.rc.cb : S.rc.ci;
     const int64_t o[4] = {S.rc.o00, S.rc.o10, S.rc.o11, S.rc.o01};
     for (int k = 1; k <= sw; k++) {
         const double s = __ldg(g.sw + k - 1), cs = __ldg(g.csw + k - 1);
         double zb, zcv, zf;
         if (g.vtransform == 2) {
-            const double Sk = (g.hc * s + h * cs) / (g.hc + h);
+            const double Sk = rp_div_by(g.hc * s + h * cs, zx.den, zx.yden);
             zb = S.zb + (S.zb + h) * Sk;
             zcv = S.zc + (S.zc + h) * Sk;
             zf = S.zf + (S.zf + h) * Sk;
         } else {
-            zb = rp_zlevel(g.vtransform, g.hc, s, cs, S.zb, h);
-            zcv = rp_zlevel(g.vtransform, g.hc, s, cs, S.zc, h);
-            zf = rp_zlevel(g.vtransform, g.hc, s, cs, S.zf, h);
+            zb = rp_zlevel_c(zx, s, cs, S.zb);
+            zcv = rp_zlevel_c(zx, s, cs, S.zc);
+            zf = rp_zlevel_c(zx, s, cs, S.zf);
         }
-        zc[k] = rp_polintd(A.pi, zb, zcv, zf);
+        zc(k) = rp_polintd(A.pi, zb, zcv, zf);
         double ab[4], ac[4], af[4];
 #pragma unroll
         for (int q = 0; q < 4; q++) {
@@ -319,28 +339,29 @@ __device__ double rp_vturb(const RpStepArgs& A, const RpGridDev& g, const StageS
         const double Kb = cw[0] * ab[0] + cw[1] * ab[1] + cw[2] * ab[2] + cw[3] * ab[3];
         const double Kc = cw[0] * ac[0] + cw[1] * ac[1] + cw[2] * ac[2] + cw[3] * ac[3];
         const double Kf = cw[0] * af[0] + cw[1] * af[1] + cw[2] * af[2] + cw[3] * af[3];
-        kh[k] = rp_polintd(A.pi, Kb, Kc, Kf);
+        kh(k) = rp_polintd(A.pi, Kb, Kc, Kf);
     }
     // resample to np points (ver_turb_module.f90:126-136), linint per point
-    const double dz = (zc[sw] - zc[1]) / (double)(np - 1);
-    w.fitz[1] = zc[1];
-    w.fitz[np] = zc[sw];
-    w.y[1] = kh[1];
-    w.y[np] = kh[sw];
+    const double dz = (zc(sw) - zc(1)) / (double)(np - 1);
+    w.fitz(1) = zc(1);
+    w.fitz(np) = zc(sw);
+    w.y(1) = kh(1);
+    w.y(np) = kh(sw);
+    double x = zc(1);
     for (int i = 2; i <= np - 1; i++) {
-        const double x = w.fitz[i - 1] + dz;
-        w.fitz[i] = x;
+        x = x + dz;
+        w.fitz(i) = x;
         int jlo = 1, jhi = sw;
         for (;;) {
             const int k = (jhi + jlo) / 2;
-            if (zc[k] > x) jhi = k; else jlo = k;
+            if (zc(k) > x) jhi = k; else jlo = k;
             if (jhi - jlo == 1) break;
         }
-        const double m = (kh[jlo] - kh[jhi]) / (zc[jlo] - zc[jhi]);
-        const double b = kh[jlo] - m * zc[jlo];
-        w.y[i] = m * x + b;
+        const double m = (kh(jlo) - kh(jhi)) / (zc(jlo) - zc(jhi));
+        const double b = kh(jlo) - m * zc(jlo);
+        w.y(i) = m * x + b;
     }
-    const double p = rp_smooth<NPMAX>(w, np, A.serr, A.smth, A.spline_max_iter, fl);
+    const double p = rp_smooth(w, np, A.serr, A.smth, A.spline_max_iter, fl);
 
     // random displacement sub-steps (ver_turb_module.f90:231-293)
     const double deltat = A.deltat;
@@ -348,14 +369,14 @@ __device__ double rp_vturb(const RpStepArgs& A, const RpGridDev& g, const StageS
     for (int i = 1; i <= A.loop; i++) {
         double Kprimec = 0.0;
         if (ParZc <= tdepth || ParZc >= zeta) Kprimec = 0.0;
-        else Kprimec = rp_ppvalu<NPMAX>(w, np, p, A.serr, ParZc, 1);
+        else Kprimec = rp_ppvalu(w, np, p, A.serr, ParZc, 1);
         const double KprimeZc = Kprimec * deltat;
         const double Z3rdc = ParZc + 0.5 * KprimeZc;
         double KH3rdc;
         if (Z3rdc < tdepth || Z3rdc > zeta) {
             KH3rdc = A.aksback;
         } else {
-            KH3rdc = rp_ppvalu<NPMAX>(w, np, p, A.serr, Z3rdc, 0);
+            KH3rdc = rp_ppvalu(w, np, p, A.serr, Z3rdc, 0);
             if (KH3rdc < A.aksback) KH3rdc = A.aksback;
         }
         const double DEV = rp_normal(A, pid, (uint32_t)(1 + i));
@@ -370,12 +391,48 @@ __device__ double rp_vturb(const RpStepArgs& A, const RpGridDev& g, const StageS
 
 // ------------------------------------------------------------ one particle
 
-template <typename T, int NPMAX>
-__device__ void rp_update_one(const RpStepArgs& A, int64_t n, SplineWork<NPMAX>& w) {
+// Skip tests of update_particles (ROMSPath.f90:672-690).
+__device__ __forceinline__ bool rp_active(const RpStepArgs& A, int64_t n) {
     const RpParticlesDev& P = A.p;
-    if (A.ix[2] <= P.dob[n]) return;                       // ROMSPath.f90:672
-    if (P.status[n] == 9.0) return;                        // 676
-    if (A.oob && !P.isin[n]) return;                       // 688
+    if (A.ix[2] <= P.dob[n]) return false;
+    if (P.status[n] == 9.0) return false;
+    if (A.oob && !P.isin[n]) return false;
+    return true;
+}
+
+// VTurb of one particle on its own (the first kernel of the split step):
+// the stage-1 z clamp of find_currents (advection_module.f90:171-183) is
+// applied first when RK4 runs, exactly as RKAdvect hands Zpar to VTurb.
+template <typename T, class W>
+__device__ void rp_vturb_one(const RpStepArgs& A, int64_t n, const W& w, double* turbv) {
+    const RpParticlesDev& P = A.p;
+    if (!rp_active(A, n)) return;
+    uint32_t fl = 0;
+    const int gid = P.gid[n];
+    const RpGridDev& g = A.g[gid - 1];
+    const double Xpar = P.x[n], Ypar = P.y[n];
+    double Zpar = P.z[n];
+    StageState S1;
+    rp_rho_cell(g, Xpar, Ypar, S1.rc, fl);
+    S1.tdepth = -1.0 * rp_bil(g.h, S1.rc);
+    S1.zb = rp_zeta_at<T>(g, S1.rc, g.sb);
+    S1.zc = rp_zeta_at<T>(g, S1.rc, g.sc);
+    S1.zf = rp_zeta_at<T>(g, S1.rc, g.sf);
+    S1.zeta = rp_polintd(A.pi, S1.zb, S1.zc, S1.zf);
+    if (A.scheme == 1) {
+        if (Zpar < S1.tdepth) Zpar = S1.tdepth + RP_F_0P001;
+        if (Zpar > S1.zeta) Zpar = S1.zeta - RP_F_0P001;
+    }
+    turbv[n] = rp_vturb<T>(A, g, S1, Zpar, P.pid[n], fl, w);
+    if (fl) P.flags[n] |= fl;
+}
+
+// One particle of update_particles.  With turbv_in non-null the VTurb
+// displacement comes from the split kernel instead of being computed here.
+template <typename T, class W>
+__device__ void rp_update_one(const RpStepArgs& A, int64_t n, const W& w, const double* turbv_in) {
+    const RpParticlesDev& P = A.p;
+    if (!rp_active(A, n)) return;                          // ROMSPath.f90:672-690
     P.age[n] = P.age[n] + (double)(float)A.idt;            // 693
 
     uint32_t fl = 0;
@@ -444,7 +501,9 @@ __device__ void rp_update_one(const RpStepArgs& A, int64_t n, SplineWork<NPMAX>&
     TurbHy = TurbHy * pn;
 
     double TurbV = 0.0;
-    if (A.vturb_on) {                                      // VTurb, 783
+    if (A.vturb_on && turbv_in) {                          // VTurb, 783 (split kernel)
+        TurbV = turbv_in[n];
+    } else if (A.vturb_on) {                               // VTurb, 783
         if (!have_s1) {
             rp_rho_cell(g, Xpar, Ypar, S1.rc, fl);
             S1.tdepth = -1.0 * rp_bil(g.h, S1.rc);
@@ -453,7 +512,7 @@ __device__ void rp_update_one(const RpStepArgs& A, int64_t n, SplineWork<NPMAX>&
             S1.zf = rp_zeta_at<T>(g, S1.rc, g.sf);
             S1.zeta = rp_polintd(A.pi, S1.zb, S1.zc, S1.zf);
         }
-        TurbV = rp_vturb<T, NPMAX>(A, g, S1, Zpar, pid, fl, w);
+        TurbV = rp_vturb<T>(A, g, S1, Zpar, pid, fl, w);
     }
     const double ZBehav = 0.0;                             // behave(): passive
 

@@ -34,7 +34,7 @@ class Tracker:
     def __init__(self, specs, grids: Sequence[Dict[str, np.ndarray]], params: dict, numpar: int,
                  field_dtype: str = "f64", stokes: bool = False, seed: int = 0, device: int = 0,
                  scl: Optional[np.ndarray] = None, off: Optional[np.ndarray] = None,
-                 spline_max_iter: int = 100):
+                 spline_max_iter: int = 100, variant: str = "fused"):
         L = _lib.load()
         self.L = L
         self.ng = len(grids)
@@ -59,6 +59,10 @@ class Tracker:
             P.constant_hturb[i] = float(v)
         P.seed = int(seed)
         P.device = int(device)
+        # kernel form: "fused" (one kernel, spline workspace in local
+        # memory) or "split" (VTurb kernel with the spline workspace in
+        # shared memory writing a scratch array, then the advection kernel)
+        P.reserved[0] = {"fused": 0, "split": 1}[variant]
         G = (_lib.RpGrid * self.ng)()
         for k, (sp, gr) in enumerate(zip(specs, grids)):
             g = G[k]

@@ -69,10 +69,11 @@ def _steps(case: Case, nsteps: int):
 
 
 def run_gpu(case: Case, nsteps: int, noise: str = "philox", seed: int = 7,
-            hook: Optional[np.ndarray] = None, tracker=None):
+            hook: Optional[np.ndarray] = None, tracker=None, variant: str = "split"):
     from romspath_b200 import Tracker
     T = tracker or Tracker([case.spec], [case.grid], case.params, numpar=case.release.z.shape[0],
-                           field_dtype=case.spec.field_dtype, stokes=case.spec.stokes, seed=seed)
+                           field_dtype=case.spec.field_dtype, stokes=case.spec.stokes, seed=seed,
+                           variant=variant)
     for (k, slot) in schedule.initial_loads():
         T.upload_frame(1, slot, case.frame(k))
     T.locate(case.release, t_b=1)

@@ -38,11 +38,12 @@ CASES = [
 ]
 
 
+@pytest.mark.parametrize("variant", ["split", "fused"])
 @pytest.mark.parametrize("cid,name,npart,nsteps,noise,sov,pov", CASES, ids=[c[0] for c in CASES])
-def test_step_bit_exact(cid, name, npart, nsteps, noise, sov, pov):
+def test_step_bit_exact(cid, name, npart, nsteps, noise, sov, pov, variant):
     case = harness.make_case(name, npart, seed=3, spec_over=sov, param_over=pov)
     hook = harness.noise_array(case, nsteps) if noise == "hook" else None
-    g, T = harness.run_gpu(case, nsteps, noise=noise, hook=hook)
+    g, T = harness.run_gpu(case, nsteps, noise=noise, hook=hook, variant=variant)
     T.close()
     o, _ = harness.run_oracle(case, nsteps, noise=noise, hook=hook)
     _assert_same(g, o, cid)
