@@ -177,6 +177,35 @@ typedef struct rp_device_state {
 } rp_device_state;
 int rp_device_state_get(rp_ctx *ctx, rp_device_state *out);
 
+/* Largest particle count rp_step_noalloc accepts: its scratch is a fixed
+ * device buffer of one double per particle (8 MiB). */
+#define RP_NOALLOC_MAX_PARTICLES 1048576
+
+/* One internal step exactly like rp_step (same results, bit for bit), on
+ * particle columns that live in the caller's own device memory
+ * (state->x ... state->flags, state->n particles; `stream` is ignored), and
+ * without allocating any device memory.  No counterpart in the reference.
+ *
+ * For callers that cannot allocate at step time: a Fortran driver that keeps
+ * its particle arrays on the device itself (OpenACC / CUDA Fortran data
+ * regions) within its own memory budget, a host framework whose allocator
+ * owns the device's memory, or a time loop that must not call cudaMalloc
+ * because it synchronises the device and stalls the asynchronous frame
+ * uploads.  The one scratch array the step needs (the VTurb displacement of
+ * each particle) is a fixed 8 MiB device buffer that exists on every device
+ * that loads the library until the process exits.
+ *  - state->n must be <= RP_NOALLOC_MAX_PARTICLES and int(s_w*sub) <= 128
+ *    (RP_ERR_ARG / RP_ERR_UNSUPPORTED otherwise, with a message).
+ *  - The first call on a device looks up the buffer's device address; make
+ *    that first call before any stream capture.
+ *  - Calls share the buffer: calls that overlap on the GPU (other streams or
+ *    threads) race and must be serialised by the caller.  Its contents are
+ *    never read before the same call writes them, so nothing is cleared.
+ *  - The noise hook is not used by this entry point (RP_ERR_STATE if set).
+ * Launches on the context's compute stream, after pending frame uploads. */
+int rp_step_noalloc(rp_ctx *ctx, const rp_device_state *state, const double ex[3], const double ix[3],
+                    int32_t ets, int32_t t_b, int32_t t_c, int32_t t_f);
+
 /* Timing of the last rp_step launch sequence on the compute stream, in ms
  * (CUDA events), and the number of kernels it launched. */
 int rp_last_step_stats(rp_ctx *ctx, float *ms, int32_t *kernels);

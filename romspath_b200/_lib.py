@@ -10,6 +10,7 @@ import os
 from . import build as _build
 
 MAXNGRID = 5
+NOALLOC_MAX_PARTICLES = 1048576
 RP_OK = 0
 ERRORS = {-1: "RP_ERR_ARG", -2: "RP_ERR_CUDA", -3: "RP_ERR_STATE", -4: "RP_ERR_NOMEM",
           -5: "RP_ERR_UNSUPPORTED", -6: "RP_ERR_NOEXT"}
@@ -20,7 +21,7 @@ EXPORTS = [
     "rp_create", "rp_upload_frame", "rp_upload_frame_f32", "rp_set_particles", "rp_locate_particles",
     "rp_step", "rp_get_particles", "rp_set_step_index", "rp_set_noise_hook", "rp_synchronize",
     "rp_last_error", "rp_destroy", "rp_device_state_get", "rp_last_step_stats", "rp_kernel_launches",
-    "rp_version",
+    "rp_step_noalloc", "rp_version",
 ]
 
 PD = C.POINTER(C.c_double)
@@ -103,6 +104,8 @@ def _declare(L):
     L.rp_device_state_get.argtypes = [P, C.POINTER(RpDeviceState)]
     L.rp_last_step_stats.argtypes = [P, C.POINTER(C.c_float), C.POINTER(C.c_int32)]
     L.rp_kernel_launches.argtypes = [P, C.POINTER(C.c_int64)]
+    L.rp_step_noalloc.argtypes = [P, C.POINTER(RpDeviceState), PD, PD, C.c_int32, C.c_int32, C.c_int32,
+                                  C.c_int32]
     L.rp_version.restype = C.c_char_p
     for name in EXPORTS:
         if name != "rp_version":

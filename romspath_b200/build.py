@@ -26,6 +26,7 @@ COMMON = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", 
 # (source, extra flags)
 UNITS = [
     ("rp_kernels.cu", ["-fmad=false"]),
+    ("rp_noalloc.cu", ["-fmad=false"]),
     ("rp_api.cu", []),
 ]
 

@@ -558,6 +558,51 @@ int rp_step(rp_ctx* ctx, const double ex[3], const double ix[3], int32_t ets, in
     return RP_OK;
 }
 
+int rp_step_noalloc(rp_ctx* ctx, const rp_device_state* st, const double ex[3], const double ix[3], int32_t ets,
+                    int32_t t_b, int32_t t_c, int32_t t_f) {
+    if (!ctx || !st || !ex || !ix) return RP_ERR_ARG;
+    if (st->n < 0 || st->n > rp::kNoallocMaxParticles)
+        return fail(ctx, RP_ERR_ARG, "rp_step_noalloc: state->n exceeds RP_NOALLOC_MAX_PARTICLES (1048576)");
+    if (ctx->npmax > 128)
+        return fail(ctx, RP_ERR_UNSUPPORTED, "rp_step_noalloc: int(s_w*sub) must be <= 128");
+    if (!st->x || !st->y || !st->z || !st->age || !st->dob || !st->status || !st->wd || !st->zeta || !st->bath ||
+        !st->gid || !st->isin || !st->pid || !st->flags)
+        return fail(ctx, RP_ERR_ARG, "rp_step_noalloc: null state column");
+    if (t_b < 1 || t_b > 3 || t_c < 1 || t_c > 3 || t_f < 1 || t_f > 3)
+        return fail(ctx, RP_ERR_ARG, "rp_step_noalloc: slots must be 1..3");
+    if (ctx->hook) return fail(ctx, RP_ERR_STATE, "rp_step_noalloc: the noise hook is not supported");
+    for (int k = 0; k < ctx->ngrid; k++) {
+        const GridBuf& G = ctx->g[k];
+        if (G.map[t_b - 1] < 0 || G.map[t_c - 1] < 0 || G.map[t_f - 1] < 0)
+            return fail(ctx, RP_ERR_STATE, "rp_step_noalloc: a frame slot was never loaded");
+    }
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->s_comp;
+    RpStepArgs A{};
+    fill_params(ctx, A);
+    fill_grids(ctx, A, t_b, t_c, t_f);
+    A.p.n = st->n;
+    A.p.x = st->x; A.p.y = st->y; A.p.z = st->z; A.p.age = st->age; A.p.dob = st->dob;
+    A.p.status = st->status; A.p.wd = st->wd; A.p.zeta = st->zeta; A.p.bath = st->bath;
+    A.p.gid = st->gid; A.p.isin = st->isin; A.p.pid = st->pid; A.p.flags = st->flags;
+    for (int q = 0; q < 3; q++) { A.ex[q] = ex[q]; A.ix[q] = ix[q]; }
+    A.pi = polint_consts(ex, ix[1]);
+    A.ets = ets;
+    A.step_index = ctx->step_index;
+    A.hook = nullptr;
+    for (int k = 0; k < ctx->ngrid; k++) {
+        const GridBuf& G = ctx->g[k];
+        const int used[3] = {G.map[t_b - 1], G.map[t_c - 1], G.map[t_f - 1]};
+        for (int q = 0; q < 3; q++) CK(cudaStreamWaitEvent(s, G.slot_ready[used[q]], 0));
+    }
+    int nl = 0;
+    if (st->n > 0)
+        CK(rp::launch_step_noalloc(A, ctx->prm.field_dtype, ctx->npmax, ctx->device, s, ctx->num_sms, &nl));
+    ctx->launches += nl;
+    ctx->step_index++;
+    return RP_OK;
+}
+
 int rp_get_particles(rp_ctx* ctx, int64_t n, double* x, double* y, double* z, double* age, double* status,
                      double* gid, int32_t* isin, double* wd, double* zeta, double* bath, uint32_t* flags) {
     if (!ctx) return RP_ERR_ARG;

@@ -18,6 +18,12 @@ constexpr int kMaxNp = 144;   // largest spline point count int(s_w*sub)
 // variant 0: split (k_vturb + k_advect, `turbv` is n doubles of scratch)
 cudaError_t launch_step(const RpStepArgs& A, int field_dtype, int npmax, double* turbv, int variant,
                         cudaStream_t s, int num_sms, int* nlaunch);
+// Split step with the scratch array in a static device buffer (no device
+// allocation); at most kNoallocMaxParticles particles and np <= 128.
+constexpr int64_t kNoallocMaxParticles = 1048576;
+cudaError_t launch_step_noalloc(const RpStepArgs& A, int field_dtype, int npmax, int device, cudaStream_t s,
+                                int num_sms, int* nlaunch);
+
 cudaError_t launch_locate(const RpStepArgs& A, int field_dtype, const double* ipos, const double* jpos,
                           const double* z, const double* dob, cudaStream_t s);
 cudaError_t launch_convert(int src_f32, int dst_f32, const void* src, const void* add, void* dst, int ni, int nj,
