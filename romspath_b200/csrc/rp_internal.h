@@ -11,6 +11,10 @@
 namespace rp {
 
 constexpr int kStepBlock = 128;
+#ifndef RP_VTURB_MIN_BLOCKS
+#define RP_VTURB_MIN_BLOCKS 8
+#endif
+constexpr int kVturbMinBlocks = RP_VTURB_MIN_BLOCKS;   // resident 128-thread blocks per SM
 
 constexpr int kMaxNp = 144;   // largest spline point count int(s_w*sub)
 

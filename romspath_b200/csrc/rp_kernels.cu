@@ -10,23 +10,21 @@ namespace rp {
 
 // ------------------------------------------------------------ the step
 //
-// Split form (default): k_vturb (one warp per block; the smoothing-spline
-// workspace of its 32 particles lane-interleaved in shared memory) writes
-// each particle's VTurb displacement to scratch; k_advect (RK4, HTurb,
-// hand-off, vertical update, status) then runs at full occupancy.
-// Fused form: one kernel per particle with the workspace in local memory.
+// Split form: k_vturb_local (VTurb of each particle, spline workspace in
+// local memory, many resident warps) writes each particle's displacement to
+// scratch; k_advect (RK4, HTurb, hand-off, vertical update, status) then
+// runs at its own register count.  Fused form: one kernel per particle.
 
-template <int NPMAX>
-constexpr size_t vturb_smem_bytes() {
-    return (size_t)kSplineArrays * (NPMAX + 1) * 32 * sizeof(double);
-}
-
+// VTurb alone with the spline workspace in local memory, at high occupancy
+// (the latency of the FP64 dependency chains and of the workspace loads is
+// hidden by many resident warps).
 template <typename T, int NPMAX>
-__global__ void __launch_bounds__(32, 1) k_vturb(const __grid_constant__ RpStepArgs A, double* __restrict__ turbv) {
-    extern __shared__ double sm[];
-    const SplineView<NPMAX, 32> w{sm + threadIdx.x};
-    const int64_t stride = (int64_t)gridDim.x * 32;
-    for (int64_t n = (int64_t)blockIdx.x * 32 + threadIdx.x; n < A.p.n; n += stride)
+__global__ void __launch_bounds__(kStepBlock, kVturbMinBlocks) k_vturb_local(const __grid_constant__ RpStepArgs A,
+                                                                            double* __restrict__ turbv) {
+    double buf[kSplineArrays * (NPMAX + 1)];
+    const SplineView<NPMAX, 1> w{buf};
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < A.p.n; n += stride)
         rp_vturb_one<T>(A, n, w, turbv);
 }
 
@@ -40,7 +38,7 @@ __global__ void __launch_bounds__(kStepBlock) k_advect(const __grid_constant__ R
 }
 
 template <typename T, int NPMAX>
-__global__ void __launch_bounds__(kStepBlock) k_step_fused(const __grid_constant__ RpStepArgs A) {
+__global__ void __launch_bounds__(kStepBlock, kVturbMinBlocks) k_step_fused(const __grid_constant__ RpStepArgs A) {
     double buf[kSplineArrays * (NPMAX + 1)];
     const SplineView<NPMAX, 1> w{buf};
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -63,7 +61,6 @@ template <typename T, int NPMAX>
 static cudaError_t launch_step_t(const RpStepArgs& A, double* turbv, int variant, cudaStream_t s, int num_sms,
                                  int* nlaunch) {
     cudaError_t e = cudaSuccess;
-    if (NPMAX > 128) variant = 1;     // the split form's workspace would exceed shared memory
     if (variant == 1) {
         const int64_t blocks = grid_for(k_step_fused<T, NPMAX>, kStepBlock, 0, A.p.n, num_sms, &e);
         if (e != cudaSuccess) return e;
@@ -72,13 +69,9 @@ static cudaError_t launch_step_t(const RpStepArgs& A, double* turbv, int variant
         return cudaGetLastError();
     }
     if (A.vturb_on) {
-        constexpr int NPS = NPMAX > 128 ? 128 : NPMAX;
-        constexpr size_t smem = vturb_smem_bytes<NPS>();
-        e = cudaFuncSetAttribute(k_vturb<T, NPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        const int64_t blocks = grid_for(k_vturb_local<T, NPMAX>, kStepBlock, 0, A.p.n, num_sms, &e);
         if (e != cudaSuccess) return e;
-        const int64_t blocks = grid_for(k_vturb<T, NPS>, 32, smem, A.p.n, num_sms, &e);
-        if (e != cudaSuccess) return e;
-        k_vturb<T, NPS><<<(unsigned)blocks, 32, smem, s>>>(A, turbv);
+        k_vturb_local<T, NPMAX><<<(unsigned)blocks, kStepBlock, 0, s>>>(A, turbv);
         *nlaunch += 1;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }

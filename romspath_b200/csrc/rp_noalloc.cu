@@ -9,7 +9,10 @@
 // no cudaMalloc, cudaFree or allocating library routine.
 //
 // Compiled with -fmad=false, like rp_kernels.cu: the results are bit-
-// identical to rp_step.
+// identical to rp_step.  The VTurb kernel here keeps the spline workspace of
+// its warp's 32 particles in shared memory (no local-memory frame), because
+// a kernel with a large local-memory frame can make the driver enlarge its
+// local-memory reservation at launch -- an allocation.
 #include <cuda_runtime.h>
 
 #include <algorithm>

@@ -136,13 +136,18 @@ __device__ __forceinline__ double rp_chol1d(const W& w, int np, double p, double
     }
     double uprev = 0.0, ucur = w.qty(2), r2prev = 0.0;
     w.u(1) = 0.0;
+    // The sweeps are written without branches on the element index (values
+    // past the ends are formed from clamped in-range loads and discarded by
+    // the selects), so that unrolled iterations issue their independent
+    // workspace loads together.
+#pragma unroll 4
     for (int i = 2; i <= np - 2; i++) {
-        // r(i+2), v4(i+2) (defined while i+2 <= np-1)
-        double rnn = 0.0, v4nn = 0.0;
-        if (i + 2 <= np - 1) {
-            v4nn = w.fitz(i + 3) - w.fitz(i + 2);
-            rnn = serr / v4nn;
-        }
+        // r(i+2), v4(i+2) (used while i+2 <= np-1)
+        const bool has2 = (i + 2 <= np - 1);
+        const int i3 = has2 ? i + 3 : np;
+        const double v4nn = w.fitz(i3) - w.fitz(i3 - 1);
+        const double rnn = serr / v4nn;
+        const double qn = w.qty(i + 1);
         const double V3i = six1mp * ((i <= np - 3) ? (ri * rn) : 0.0);
         const double ratio1 = a2 / a1;
         b1 = b1 - ratio1 * a2;
@@ -151,15 +156,12 @@ __device__ __forceinline__ double rp_chol1d(const W& w, int np, double p, double
         const double v6n = (i + 1 <= np - 2) ? (v2sn * rn + rn * v2snn) : 0.0;
         const double c2 = (six1mp * v6n + p * v4n) - ratio1 * V3i;
         const double ratio2 = V3i / a1;
-        double c1 = 0.0;
-        if (i + 2 <= np - 1) {
-            const double v5nn = rn * rn + v2snn * v2snn + rnn * rnn;
-            c1 = (six1mp * v5nn + twop * (v4n + v4nn)) - ratio2 * V3i;
-        }
+        const double v5nn = rn * rn + v2snn * v2snn + rnn * rnn;
+        const double c1 = has2 ? ((six1mp * v5nn + twop * (v4n + v4nn)) - ratio2 * V3i) : 0.0;
         w.r1(i) = ratio1;
         w.r2(i) = ratio2;
         w.u(i) = ucur / a1;                       // u(i)/v(i,1)
-        const double unext = w.qty(i + 1) - ratio1 * ucur - r2prev * uprev;
+        const double unext = qn - ratio1 * ucur - r2prev * uprev;
         uprev = ucur;
         ucur = unext;
         r2prev = ratio2;
@@ -175,8 +177,10 @@ __device__ __forceinline__ double rp_chol1d(const W& w, int np, double p, double
     w.u(np - 1) = unm1;
     w.u(np) = 0.0;
     double up2 = 0.0, up1 = unm1;
+#pragma unroll 4
     for (int i = np - 2; i >= 2; i--) {
-        const double ui = w.u(i) - up1 * w.r1(i) - up2 * w.r2(i);
+        const double qi = w.u(i), s1 = w.r1(i), s2 = w.r2(i);
+        const double ui = qi - up1 * s1 - up2 * s2;
         w.u(i) = ui;
         up2 = up1;
         up1 = ui;
@@ -184,15 +188,19 @@ __device__ __forceinline__ double rp_chol1d(const W& w, int np, double p, double
     // qu = Q u and the weighted sum of squares, i = 1..np in order
     double prev = 0.0, sum = 0.0, utru = 0.0;
     double ulast = 0.0;                           // u(1)
+    double flast = w.fitz(1);
+#pragma unroll 4
     for (int i = 2; i <= np; i++) {
         const double ui = w.u(i);
-        const double v4i = w.fitz(i) - w.fitz(i - 1);
+        const double fi = w.fitz(i);
+        const double v4i = fi - flast;
         const double raw = (ui - ulast) / v4i;
         const double fin = raw - prev;
         sum = sum + (fin * fin) * dy2;
         if (utru_out) utru = utru + v4i * (ulast * (ulast + ui) + ui * ui);
         prev = raw;
         ulast = ui;
+        flast = fi;
     }
     const double finn = -prev;
     sum = sum + (finn * finn) * dy2;
