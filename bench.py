@@ -238,7 +238,8 @@ def main():
     rel = synth.uniform_release(spec, grid, frames[0], npart, seed=rank)
 
     T = Tracker([spec], [grid], params, numpar=npart, field_dtype=spec.field_dtype, stokes=spec.stokes,
-                seed=7 + rank, device=local)
+                seed=7, device=local)
+    T.set_id_base(rank * npart)         # global particle ids: rank r holds [r*npart, (r+1)*npart)
     for k, slot in enumerate((1, 2, 3)):
         T.upload_frame(1, slot, frames[k])
     T.locate(rel, t_b=1)

@@ -146,6 +146,13 @@ int rp_get_particles(rp_ctx *ctx, int64_t n, double *x, double *y, double *z, do
                      double *status, double *gid, int32_t *isin, double *wd, double *zeta,
                      double *bath, uint32_t *flags);
 
+/* First particle id of this context (default 0).  Particle k of the next
+ * rp_set_particles / rp_locate_particles call gets id base + k; the id keys
+ * its Philox noise, so a run split over several contexts (one per GPU) with
+ * disjoint id ranges draws the same noise as one context holding all
+ * particles.  The noise hook is indexed by id - base. */
+int rp_set_id_base(rp_ctx *ctx, uint32_t base);
+
 /* Index of the next internal step in the Philox counter (default 0; each
  * rp_step increments it). */
 int rp_set_step_index(rp_ctx *ctx, uint64_t step_index);

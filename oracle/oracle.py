@@ -305,11 +305,12 @@ class OracleModel:
         P.pid = s["pid"].ctypes.data_as(C.POINTER(C.c_uint32))
         self.P = P
 
-    def init_particles(self, release, tb: int = 1):
+    def init_particles(self, release, tb: int = 1, pid=None):
         """ini_ROMSPath ownership + zbounds (ROMSPath.f90:367-432)."""
         n = release.z.shape[0]
         self.set_particles(np.ones(n), np.ones(n), release.z, release.dob, np.zeros(n),
-                           np.full(n, 9.0), np.full(n, self.ng, dtype=np.int32), np.zeros(n, dtype=np.int8))
+                           np.full(n, 9.0), np.full(n, self.ng, dtype=np.int32), np.zeros(n, dtype=np.int8),
+                           pid=pid)
         ip = np.ascontiguousarray(release.ipos, dtype=np.float64)
         jp = np.ascontiguousarray(release.jpos, dtype=np.float64)
         lib().orc_init_particles(C.byref(self.params), self.g, C.byref(self.P), _pd(ip), _pd(jp), tb)

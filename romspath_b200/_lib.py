@@ -19,7 +19,7 @@ FLAG_OOB, FLAG_NODE, FLAG_WBOT, FLAG_WTOP, FLAG_SPLINE = 1, 2, 4, 8, 16
 
 EXPORTS = [
     "rp_create", "rp_upload_frame", "rp_upload_frame_f32", "rp_set_particles", "rp_locate_particles",
-    "rp_step", "rp_get_particles", "rp_set_step_index", "rp_set_noise_hook", "rp_synchronize",
+    "rp_step", "rp_get_particles", "rp_set_id_base", "rp_set_step_index", "rp_set_noise_hook", "rp_synchronize",
     "rp_last_error", "rp_destroy", "rp_device_state_get", "rp_last_step_stats", "rp_kernel_launches",
     "rp_step_noalloc", "rp_version",
 ]
@@ -97,6 +97,7 @@ def _declare(L):
     L.rp_step.argtypes = [P, PD, PD, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
     L.rp_get_particles.argtypes = [P, C.c_int64] + [PD] * 6 + [PI32, PD, PD, PD, PU32]
     L.rp_set_step_index.argtypes = [P, C.c_uint64]
+    L.rp_set_id_base.argtypes = [P, C.c_uint32]
     L.rp_set_noise_hook.argtypes = [P, PD, C.c_int64]
     L.rp_synchronize.argtypes = [P]
     L.rp_last_error.argtypes = [P, C.c_char_p, C.c_int32]

@@ -64,6 +64,7 @@ struct rp_ctx {
     int64_t hook_steps = 0, hook_pos = 0;
     int ndraw = 0;
     uint64_t step_index = 0;
+    uint32_t pid_base = 0;
     // timing
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool timed = false;
@@ -185,6 +186,7 @@ void fill_params(const rp_ctx* c, RpStepArgs& A) {
     for (int i = 0; i < RP_MAXNGRID; i++) A.khturb[i] = p.constant_hturb[i];
     A.seed = p.seed;
     A.ndraw = c->ndraw;
+    A.pid_base = c->pid_base;
     A.p = particles_dev(c);
 }
 
@@ -472,7 +474,7 @@ int rp_set_particles(rp_ctx* ctx, int64_t n, const double* x, const double* y, c
         return rc;
     ctx->n = n;
     RpParticlesDev P = particles_dev(ctx);
-    CK(rp::launch_state_from_host(P, ctx->tmp_gid, ctx->tmp_isin, s));
+    CK(rp::launch_state_from_host(P, ctx->tmp_gid, ctx->tmp_isin, ctx->pid_base, s));
     ctx->launches++;
     CK(cudaMemsetAsync(ctx->wd, 0, b8, s));
     CK(cudaMemsetAsync(ctx->zeta, 0, b8, s));
@@ -624,6 +626,12 @@ int rp_get_particles(rp_ctx* ctx, int64_t n, double* x, double* y, double* z, do
         (zeta && (rc = d2h(ctx, zeta, ctx->zeta, b8, s))) || (bath && (rc = d2h(ctx, bath, ctx->bath, b8, s))) ||
         (flags && (rc = d2h(ctx, flags, ctx->flags, (size_t)n * 4, s))))
         return rc;
+    return RP_OK;
+}
+
+int rp_set_id_base(rp_ctx* ctx, uint32_t base) {
+    if (!ctx) return RP_ERR_ARG;
+    ctx->pid_base = base;
     return RP_OK;
 }
 

@@ -105,6 +105,7 @@ struct RpStepArgs {
     uint64_t seed, step_index;
     const double* hook;            // noise hook for this step, or nullptr
     int ndraw;
+    uint32_t pid_base;             // hook row of particle id p is p - pid_base
     RpGridDev g[RP_MAXNGRID_D];
     RpParticlesDev p;
 };

@@ -33,7 +33,7 @@ cudaError_t launch_locate(const RpStepArgs& A, int field_dtype, const double* ip
 cudaError_t launch_convert(int src_f32, int dst_f32, const void* src, const void* add, void* dst, int ni, int nj,
                            int nk, int slot, int64_t e0, int64_t count, cudaStream_t s);
 cudaError_t launch_state_from_host(const RpParticlesDev& P, const double* gid_d, const int32_t* isin_i,
-                                   cudaStream_t s);
+                                   uint32_t base, cudaStream_t s);
 cudaError_t launch_state_to_host(const RpParticlesDev& P, double* gid_d, int32_t* isin_i, cudaStream_t s);
 
 }  // namespace rp

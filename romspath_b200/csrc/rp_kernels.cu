@@ -116,7 +116,7 @@ __global__ void k_locate(const __grid_constant__ RpStepArgs A, const double* ipo
     P.y[n] = 1.0;
     P.z[n] = z[n];
     P.dob[n] = dob[n];
-    P.pid[n] = (uint32_t)n;
+    P.pid[n] = A.pid_base + (uint32_t)n;
     uint32_t fl = 0;
     for (int ng = 1; ng <= A.ngrid; ng++) {
         const RpGridDev& g = A.g[ng - 1];
@@ -205,21 +205,21 @@ cudaError_t launch_convert(int src_f32, int dst_f32, const void* src, const void
 
 // ----------------------------------------------------- state helpers
 
-__global__ void k_state_from_host(RpParticlesDev P, const double* gid_d, const int32_t* isin_i) {
+__global__ void k_state_from_host(RpParticlesDev P, const double* gid_d, const int32_t* isin_i, uint32_t base) {
     const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= P.n) return;
     P.gid[n] = (int32_t)gid_d[n];          // int(par(n,pGID))
     P.isin[n] = isin_i[n] ? 1 : 0;
-    P.pid[n] = (uint32_t)n;
+    P.pid[n] = base + (uint32_t)n;
     P.flags[n] = 0u;
 }
 
 cudaError_t launch_state_from_host(const RpParticlesDev& P, const double* gid_d, const int32_t* isin_i,
-                                   cudaStream_t s) {
+                                   uint32_t base, cudaStream_t s) {
     const int block = 256;
     const unsigned blocks = (unsigned)((P.n + block - 1) / block);
     if (blocks == 0) return cudaSuccess;
-    k_state_from_host<<<blocks, block, 0, s>>>(P, gid_d, isin_i);
+    k_state_from_host<<<blocks, block, 0, s>>>(P, gid_d, isin_i, base);
     return cudaGetLastError();
 }
 

@@ -11,7 +11,7 @@
 // set, else Philox4x32-10 at counter (pid, step, d/2) with Box-Muller's
 // cosine branch (pdf_module.f90:26-40) on the uniforms (r+0.5)/2^32.
 __device__ __forceinline__ double rp_normal(const RpStepArgs& A, uint32_t pid, uint32_t d) {
-    if (A.hook) return A.hook[(int64_t)pid * A.ndraw + d];
+    if (A.hook) return A.hook[(int64_t)(pid - A.pid_base) * A.ndraw + d];
     uint32_t c[4] = {pid, (uint32_t)A.step_index, (uint32_t)(A.step_index >> 32), d >> 1};
     rp_philox(c, (uint32_t)A.seed, (uint32_t)(A.seed >> 32));
     const uint32_t a = (d & 1u) ? c[2] : c[0];

@@ -166,10 +166,10 @@ def make_frame(spec: GridSpec, grid: Dict[str, np.ndarray], t: float) -> Dict[st
     mask = grid["mask_rho"]
     x = spec.x0 + np.arange(nx, dtype=np.float64) * spec.dx
     y = spec.y0 + np.arange(ny, dtype=np.float64) * spec.dy
-    Lx = (spec.xi_rho - 1) * spec.dx
+    Lx = spec.gyre_lx if spec.gyre_lx else (spec.xi_rho - 1) * spec.dx
     om = 2.0 * math.pi / M2_PERIOD
     kx = 2.0 * math.pi / max(Lx, 1.0)
-    phase_r = om * t - kx * (x[:, None] - spec.x0) + 0.0 * y[None, :]
+    phase_r = om * t - kx * x[:, None] + 0.0 * y[None, :]
     zeta = 0.5 * np.cos(phase_r) * mask
     S_r = _stretch_S(h, grid["s_rho"], grid["cs_r"], spec.hc)
     S_w = _stretch_S(h, grid["s_w"], grid["cs_w"], spec.hc)
@@ -182,7 +182,7 @@ def make_frame(spec: GridSpec, grid: Dict[str, np.ndarray], t: float) -> Dict[st
     xu = x[:-1] + 0.5 * spec.dx
     Xu, Yu = np.meshgrid(xu, y, indexing="ij")
     ug, _ = _gyre_uv(Xu, Yu, t, spec)
-    ut = 0.1 * np.cos(om * t - kx * (Xu - spec.x0))
+    ut = 0.1 * np.cos(om * t - kx * Xu)
     u = (ug[..., None] * np.exp(zu / 100.0)) + ut[..., None]
     u = u * grid["mask_u"][..., None]
 
@@ -194,7 +194,7 @@ def make_frame(spec: GridSpec, grid: Dict[str, np.ndarray], t: float) -> Dict[st
     v = v * grid["mask_v"][..., None]
 
     # w from continuity of the depth-uniform tidal current: w = -(z+h) du_t/dx
-    dudx = 0.1 * kx * np.sin(om * t - kx * (x[:, None] - spec.x0)) * np.ones((1, ny))
+    dudx = 0.1 * kx * np.sin(om * t - kx * x[:, None]) * np.ones((1, ny))
     w = -(z_w + h[..., None]) * dudx[..., None]
     w = w * mask[..., None]
 
@@ -303,6 +303,76 @@ def uniform_release(spec: GridSpec, grid, frame1, n: int, seed: int = 0,
                    dob=np.full(n, dob, dtype=np.float64))
 
 
+# ------------------------------------------------------------------ nesting
+
+def nest_maps(specs: List[GridSpec]):
+    """Affine index maps between every pair of grids (GRIDS(ng)%scl/off,
+    grid_module.f90:441-481): X_b = scl(b)*X_a + off(b) with
+    X_g = 1 + (x - x0_g)/dx_g.  Returns scl, off of shape (ngrid, ngrid, 2):
+    [a][b] maps grid a's indices to grid b's.  The reference derives them
+    from the first exactly coincident lon/lat point of a chain of grids;
+    these are the same affine maps for any pair, siblings included."""
+    ng = len(specs)
+    scl = np.zeros((ng, ng, 2))
+    off = np.zeros((ng, ng, 2))
+    for a, A in enumerate(specs):
+        for b, B in enumerate(specs):
+            for c, (x0a, da, x0b, db) in enumerate(((A.x0, A.dx, B.x0, B.dx), (A.y0, A.dy, B.y0, B.dy))):
+                scl[a, b, c] = da / db
+                off[a, b, c] = 1.0 + (x0a - x0b - da) / db
+    return scl, off
+
+
+def index_of(spec: GridSpec, x: np.ndarray, y: np.ndarray):
+    """Fractional rho indices of physical points in a grid."""
+    return 1.0 + (x - spec.x0) / spec.dx, 1.0 + (y - spec.y0) / spec.dy
+
+
+def nested_release(specs: List[GridSpec], grids, frames1, n: int, seed: int = 0,
+                   child_frac: float = 0.5, dob: float = 0.0) -> Release:
+    """n particles: a fraction uniform over each child's interior, the rest
+    over the parent's; ipos/jpos hold each particle's indices in every grid
+    (the LL2ij output of ini_ROMSPath for every grid)."""
+    rng = np.random.default_rng(seed)
+    parent = specs[-1]
+    pg = grids[-1]
+    n_child = int(n * child_frac)
+    xs, ys = [], []
+    kids = specs[:-1]
+    per = [n_child // max(len(kids), 1)] * len(kids)
+    for k, sp in enumerate(kids):
+        m = per[k]
+        xs.append(sp.x0 + rng.uniform(2.0, sp.xi_rho - 2.0, m) * sp.dx)
+        ys.append(sp.y0 + rng.uniform(2.0, sp.eta_rho - 2.0, m) * sp.dy)
+    m = n - sum(per)
+    cnt = 0
+    px, py = [], []
+    while cnt < m:
+        X = rng.uniform(2.0, parent.xi_rho - 1.0, 2 * m + 8)
+        Y = rng.uniform(2.0, parent.eta_rho - 1.0, 2 * m + 8)
+        I = np.floor(X).astype(int) - 1
+        J = np.floor(Y).astype(int) - 1
+        I = np.clip(I, 0, parent.xi_rho - 2)
+        J = np.clip(J, 0, parent.eta_rho - 2)
+        mk = pg["mask_rho"]
+        wet = (mk[I, J] + mk[I + 1, J] + mk[I, J + 1] + mk[I + 1, J + 1]) == 4
+        sel = np.nonzero(wet)[0][: m - cnt]
+        px.append(parent.x0 + (X[sel] - 1.0) * parent.dx)
+        py.append(parent.y0 + (Y[sel] - 1.0) * parent.dy)
+        cnt += len(sel)
+    x = np.concatenate(xs + px)
+    y = np.concatenate(ys + py)
+    ipos = np.empty((len(specs), n))
+    jpos = np.empty((len(specs), n))
+    for g, sp in enumerate(specs):
+        ipos[g], jpos[g] = index_of(sp, x, y)
+    # depth from the parent's bathymetry (same analytic h everywhere)
+    s = rng.uniform(-0.95, -0.05, n)
+    h = 20.0 + 180.0 * (1.0 - np.exp(-x / 30000.0))
+    z = h * s
+    return Release(ipos=ipos, jpos=jpos, z=z, dob=np.full(n, dob))
+
+
 # ------------------------------------------------------------------ configs
 
 def config_spec(name: str) -> List[GridSpec]:
@@ -314,6 +384,25 @@ def config_spec(name: str) -> List[GridSpec]:
                          stokes=True, field_dtype="f32")]
     if name == "tiny":
         return [GridSpec(24, 20, 6, land="corner", field_dtype="f64")]
+    if name == "nest_tiny":
+        # child (3x) inside a 40x32 parent, finest grid first
+        P = GridSpec(40, 32, 6, land="corner", field_dtype="f64")
+        lx, ly = (P.xi_rho - 1) * P.dx, (P.eta_rho - 1) * P.dy
+        child = GridSpec(31, 25, 6, land="none", field_dtype="f64", dx=1000.0 / 3, dy=1000.0 / 3,
+                         x0=14000.0, y0=9000.0, eddy=0.1, gyre_lx=lx, gyre_ly=ly)
+        P.gyre_lx, P.gyre_ly = lx, ly
+        return [child, P]
+    if name == "cfg4":
+        # parent 400x300x30; child A 240x180x30 (3x); child B 300x250x30 (5x)
+        P = GridSpec(400, 300, 30, land="islands", land_frac=0.08, land_seed=4, field_dtype="f32",
+                     stokes=True)
+        lx, ly = (P.xi_rho - 1) * P.dx, (P.eta_rho - 1) * P.dy
+        A = GridSpec(240, 180, 30, land="none", field_dtype="f32", stokes=True, dx=1000.0 / 3, dy=1000.0 / 3,
+                     x0=60000.0, y0=60000.0, eddy=0.1, gyre_lx=lx, gyre_ly=ly)
+        B = GridSpec(300, 250, 30, land="none", field_dtype="f32", stokes=True, dx=200.0, dy=200.0,
+                     x0=250000.0, y0=150000.0, eddy=0.1, gyre_lx=lx, gyre_ly=ly)
+        P.gyre_lx, P.gyre_ly = lx, ly
+        return [B, A, P]
     raise KeyError(name)
 
 
@@ -325,7 +414,9 @@ def config_params(name: str) -> dict:
                 sub=4.0, deltat=30.0, aksback=1e-8, constant_hturb=[0.0] * 5)
     if name == "cfg2":
         base.update(hturb_on=1, constant_hturb=[1.0] * 5)
-    if name == "tiny":
+    if name in ("tiny", "nest_tiny"):
+        base.update(hturb_on=1, constant_hturb=[1.0] * 5)
+    if name == "cfg4":
         base.update(hturb_on=1, constant_hturb=[1.0] * 5)
     return base
 

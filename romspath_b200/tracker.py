@@ -168,6 +168,10 @@ class Tracker:
         rc = self.L.rp_step(self.h, exa, ixa, ets, tb, tc, tf)
         self._check(rc, "rp_step")
 
+    def set_id_base(self, base: int):
+        """Particle k of the next locate/set_particles gets id base + k."""
+        self._check(self.L.rp_set_id_base(self.h, int(base)), "rp_set_id_base")
+
     def set_step_index(self, k: int):
         self._check(self.L.rp_set_step_index(self.h, int(k)), "rp_set_step_index")
 

@@ -30,25 +30,27 @@ CASES = {
     "tiny_hook": ("tiny", 80, 24, "hook", None, None),
     "tiny_philox": ("tiny", 80, 24, "philox", None, None),
     "tiny_f32_stokes": ("tiny", 80, 24, "philox", {"field_dtype": "f32", "stokes": True}, None),
+    "nest_philox": ("nest_tiny", 120, 36, "philox", None, None),
 }
 
 
 def case_from_fixture(d):
     """Rebuild a harness.Case from a fixture's stored arrays."""
-    import dataclasses
     from romspath_b200 import synth
-    spec = synth.GridSpec(**{k: (v.item() if hasattr(v, "item") else v)
-                             for k, v in d["spec"].item().items()})
-    grid = {k[5:]: d[k] for k in d.files if k.startswith("grid_")}
+    specs = [synth.GridSpec(**{k: (v.item() if hasattr(v, "item") else v) for k, v in sp.items()})
+             for sp in d["specs"]]
+    ng = len(specs)
+    grids = [{k[len(f"grid{g}_"):]: d[k] for k in d.files if k.startswith(f"grid{g}_")} for g in range(1, ng + 1)]
     params = d["params"].item()
     release = synth.Release(ipos=d["rel_ipos"], jpos=d["rel_jpos"], z=d["rel_z"], dob=d["rel_dob"])
     frames = {}
     for k in d.files:
-        if k.startswith("frame"):
-            num, field = k[5:].split("_", 1)
-            frames.setdefault(int(num), {})[field] = d[k]
-    c = harness.Case("fixture", spec, grid, params, release, frames)
-    _ = dataclasses
+        if k.startswith("frame_"):
+            _, g, num, field = k.split("_", 3)
+            frames.setdefault((int(g), int(num)), {})[field] = d[k]
+    c = harness.Case("fixture", specs, grids, params, release, frames)
+    if ng > 1:
+        c.scl, c.off = d["scl"], d["off"]
     return c
 
 
@@ -59,17 +61,20 @@ def make(name):
     o, _ = harness.run_oracle(case, nsteps, noise=noise, hook=hook, seed=5, nthreads=1)
     nframes = 2 + (nsteps + 11) // 12 + 1
     out = {
-        "spec": np.array(vars(case.spec), dtype=object),
+        "specs": np.array([vars(sp) for sp in case.specs], dtype=object),
         "params": np.array(case.params, dtype=object),
         "rel_ipos": case.release.ipos, "rel_jpos": case.release.jpos,
         "rel_z": case.release.z, "rel_dob": case.release.dob,
         "nsteps": np.array(nsteps), "noise": np.array(noise), "seed": np.array(5),
     }
-    for k, v in case.grid.items():
-        out["grid_" + k] = v
-    for k in range(1, nframes + 1):
-        for f, v in case.frame(k).items():
-            out[f"frame{k}_{f}"] = v
+    for g in range(1, case.ngrid + 1):
+        for k, v in case.grids[g - 1].items():
+            out[f"grid{g}_" + k] = v
+        for k in range(1, nframes + 1):
+            for f, v in case.frame(k, g).items():
+                out[f"frame_{g}_{k}_{f}"] = v
+    if case.ngrid > 1:
+        out["scl"], out["off"] = case.scl, case.off
     if hook is not None:
         out["hook"] = hook
     for f in harness.FIELDS:

@@ -1,16 +1,17 @@
 """Run the CUDA path and the CPU oracle side by side on the same inputs.
 
 Used by the GPU parity tests and by ``__graft_entry__.smoke``.  Both sides
-get identical grids, identical stored frame values (FP64 sums of Stokes
-drift rounded to the device storage precision), identical initial releases
-and identical noise (noise hook arrays, or Philox with the same key and
-step counter), and follow the same frame-slot schedule of the Fortran
-driver (``romspath_b200.schedule``).
+get identical grids (and, for nested grids, identical index maps),
+identical stored frame values (FP64 sums of Stokes drift rounded to the
+device storage precision), identical initial releases and identical noise
+(noise hook arrays, or Philox with the same key and step counter), and
+follow the same frame-slot schedule of the Fortran driver
+(``romspath_b200.schedule``).
 """
 from __future__ import annotations
 
 import dataclasses
-from typing import Dict, Optional
+from typing import Dict, List, Optional
 
 import numpy as np
 
@@ -22,33 +23,53 @@ FIELDS = ("x", "y", "z", "age", "status", "gid", "isin", "wd", "zeta", "bath", "
 @dataclasses.dataclass
 class Case:
     name: str
-    spec: synth.GridSpec
-    grid: Dict[str, np.ndarray]
+    specs: List[synth.GridSpec]
+    grids: List[Dict[str, np.ndarray]]
     params: dict
     release: synth.Release
-    frames: Dict[int, Dict[str, np.ndarray]]
+    frames: Dict
+    scl: Optional[np.ndarray] = None
+    off: Optional[np.ndarray] = None
 
-    def frame(self, k: int) -> Dict[str, np.ndarray]:
-        if k not in self.frames:
-            self.frames[k] = synth.make_frame(self.spec, self.grid, (k - 1) * float(self.params["dt"]))
-        return self.frames[k]
+    @property
+    def spec(self) -> synth.GridSpec:
+        return self.specs[0]
 
-    def stored(self, k: int) -> Dict[str, np.ndarray]:
-        return synth.stored_frame(self.frame(k), self.spec.field_dtype, self.spec.stokes)
+    @property
+    def grid(self) -> Dict[str, np.ndarray]:
+        return self.grids[0]
+
+    @property
+    def ngrid(self) -> int:
+        return len(self.specs)
+
+    def frame(self, k: int, ng: int = 1) -> Dict[str, np.ndarray]:
+        key = (ng, k)
+        if key not in self.frames:
+            self.frames[key] = synth.make_frame(self.specs[ng - 1], self.grids[ng - 1],
+                                                (k - 1) * float(self.params["dt"]))
+        return self.frames[key]
+
+    def stored(self, k: int, ng: int = 1) -> Dict[str, np.ndarray]:
+        sp = self.specs[ng - 1]
+        return synth.stored_frame(self.frame(k, ng), sp.field_dtype, sp.stokes)
 
 
 def make_case(name: str, npart: int, seed: int = 0, spec_over: Optional[dict] = None,
               param_over: Optional[dict] = None) -> Case:
-    spec = synth.config_spec(name)[0]
+    specs = synth.config_spec(name)
     if spec_over:
-        spec = dataclasses.replace(spec, **spec_over)
-    grid = synth.make_grid(spec)
+        specs = [dataclasses.replace(sp, **spec_over) for sp in specs]
+    grids = [synth.make_grid(sp) for sp in specs]
     params = dict(synth.config_params(name))
     if param_over:
         params.update(param_over)
-    frames: Dict[int, Dict[str, np.ndarray]] = {}
-    c = Case(name, spec, grid, params, None, frames)  # type: ignore[arg-type]
-    c.release = synth.uniform_release(spec, grid, c.frame(1), npart, seed=seed)
+    c = Case(name, specs, grids, params, None, {})  # type: ignore[arg-type]
+    if len(specs) > 1:
+        c.scl, c.off = synth.nest_maps(specs)
+        c.release = synth.nested_release(specs, grids, c.frame(1, len(specs)), npart, seed=seed)
+    else:
+        c.release = synth.uniform_release(specs[0], grids[0], c.frame(1), npart, seed=seed)
     return c
 
 
@@ -69,20 +90,22 @@ def _steps(case: Case, nsteps: int):
 
 
 def run_gpu(case: Case, nsteps: int, noise: str = "philox", seed: int = 7,
-            hook: Optional[np.ndarray] = None, tracker=None, variant: str = "split"):
+            hook: Optional[np.ndarray] = None, tracker=None, variant: str = "fused"):
     from romspath_b200 import Tracker
-    T = tracker or Tracker([case.spec], [case.grid], case.params, numpar=case.release.z.shape[0],
+    T = tracker or Tracker(case.specs, case.grids, case.params, numpar=case.release.z.shape[0],
                            field_dtype=case.spec.field_dtype, stokes=case.spec.stokes, seed=seed,
-                           variant=variant)
+                           scl=case.scl, off=case.off, variant=variant)
     for (k, slot) in schedule.initial_loads():
-        T.upload_frame(1, slot, case.frame(k))
+        for ng in range(1, case.ngrid + 1):
+            T.upload_frame(ng, slot, case.frame(k, ng))
     T.locate(case.release, t_b=1)
     if noise == "hook":
         T.set_noise_hook(hook)
     done = 0
     for ext, internal in _steps(case, nsteps):
         for (k, slot) in ext.loads:
-            T.upload_frame(1, slot, case.frame(k))
+            for ng in range(1, case.ngrid + 1):
+                T.upload_frame(ng, slot, case.frame(k, ng))
         for it in internal:
             if done >= nsteps:
                 break
@@ -95,14 +118,16 @@ def run_gpu(case: Case, nsteps: int, noise: str = "philox", seed: int = 7,
 def run_oracle(case: Case, nsteps: int, noise: str = "philox", seed: int = 7,
                hook: Optional[np.ndarray] = None, nthreads: int = 8):
     from oracle import oracle as O
-    m = O.OracleModel([case.spec], [case.grid], case.params)
+    m = O.OracleModel(case.specs, case.grids, case.params, scl=case.scl, off=case.off)
     for (k, slot) in schedule.initial_loads():
-        m.set_frame(1, slot, case.stored(k))
+        for ng in range(1, case.ngrid + 1):
+            m.set_frame(ng, slot, case.stored(k, ng))
     m.init_particles(case.release, tb=1)
     done = 0
     for ext, internal in _steps(case, nsteps):
         for (k, slot) in ext.loads:
-            m.set_frame(1, slot, case.stored(k))
+            for ng in range(1, case.ngrid + 1):
+                m.set_frame(ng, slot, case.stored(k, ng))
         for it in internal:
             if done >= nsteps:
                 break
