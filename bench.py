@@ -353,6 +353,9 @@ def main():
     traffic = profile_traffic(wl, "k_step_fused")
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
+                "dram_gbs_from_traffic": (traffic / (avg_kernel_ms / 1e3) / 1e9) if traffic else None,
+                "note": "achieved counts the field and particle bytes the reference arithmetic consumes; "
+                        "the DRAM traffic is dominated by the smoothing-spline workspace (see profiles/)",
                 "kernel": "k_step_fused (one launch per internal step)",
                 "avg_launch_ms": avg_kernel_ms,
                 "algorithmic_bytes": f"{balg} B/particle-step x {npart} particles per launch"}
