@@ -53,6 +53,14 @@ extern "C" {
 /* storage precision of the hydrodynamic fields on the device */
 #define RP_FIELD_F64 0
 #define RP_FIELD_F32 1
+/* The mixed-precision form: u, v, w, AKs stored in FP16 with a power-of-two
+ * scale per (slot, level), zeta in FP32; positions in FP32 with Kahan-
+ * compensated accumulation; interpolation and RK4 in FP32; age, the
+ * smoothing-spline fit and the random-displacement sub-steps in FP64, with
+ * the spline's smoothing parameter warm-started from the particle's
+ * previous step.  Not bit-exact; its error against RP_FIELD_F64 on the
+ * same noise is measured by the tests. */
+#define RP_FIELD_MIXED 2
 
 /* Run parameters: the namelist values the hot path reads (ROMSPath.h:77-80
  * timeparam, 140-148 turbparam, 152-154 advectparam, 161-180 behavparam,
@@ -68,7 +76,7 @@ typedef struct rp_params {
     int32_t open_ocean_boundary;         /* OpenOceanBoundary                 */
     int32_t behavior;                    /* Behavior; only 0 (passive)        */
     int32_t stokes;                      /* add ustokes/vstokes on upload     */
-    int32_t field_dtype;                 /* RP_FIELD_F64 / RP_FIELD_F32       */
+    int32_t field_dtype;                 /* RP_FIELD_F64 / _F32 / _MIXED      */
     int32_t spline_max_iter;             /* cap of smooth()'s secant loop (0: 100) */
     double vertdist;
     double serr, smth, sub, deltat, aksback;
@@ -173,7 +181,10 @@ int rp_last_error(rp_ctx *ctx, char *buf, int32_t len);
 int rp_destroy(rp_ctx *ctx);
 
 /* Device-resident state, for callers that keep particles in HBM between
- * calls (pointers stay valid until rp_destroy). */
+ * calls (pointers stay valid until rp_destroy).  In the mixed form the
+ * positions live in compensated FP32 columns: rp_device_state_get first
+ * writes x, y, z from them (and waits), and the mixed step does not read
+ * x, y, z back. */
 typedef struct rp_device_state {
     int64_t n;
     double *x, *y, *z, *age, *dob, *status, *wd, *zeta, *bath;
@@ -209,6 +220,7 @@ int rp_device_state_get(rp_ctx *ctx, rp_device_state *out);
  *    threads) race and must be serialised by the caller.  Its contents are
  *    never read before the same call writes them, so nothing is cleared.
  *  - The noise hook is not used by this entry point (RP_ERR_STATE if set).
+ *  - FP64 and FP32 field storage only (RP_ERR_UNSUPPORTED for RP_FIELD_MIXED).
  * Launches on the context's compute stream, after pending frame uploads. */
 int rp_step_noalloc(rp_ctx *ctx, const rp_device_state *state, const double ex[3], const double ix[3],
                     int32_t ets, int32_t t_b, int32_t t_c, int32_t t_f);

@@ -27,6 +27,7 @@ COMMON = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", 
 UNITS = [
     ("rp_kernels.cu", ["-fmad=false"]),
     ("rp_noalloc.cu", ["-fmad=false"]),
+    ("rp_mixed.cu", []),          # mixed-precision form: FMA contraction allowed
     ("rp_api.cu", []),
 ]
 
@@ -56,20 +57,22 @@ def build(verbose: bool = False, ptxas_info: bool = False, force: bool = False) 
         return LIB
     nvcc = _nvcc()
     os.makedirs(OUT_DIR, exist_ok=True)
-    objs = []
-    for src, extra in UNITS:
+    objs, procs = [], []
+    for src, extra in UNITS:          # the units compile in parallel
         obj = os.path.join(OUT_DIR, src.replace(".cu", ".o"))
         cmd = [nvcc, *COMMON, *extra, "-c", os.path.join(CSRC, src), "-o", obj]
         if ptxas_info:
             cmd += ["-Xptxas", "-v"]
         if verbose:
             print(" ".join(cmd), flush=True)
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")
-        if ptxas_info or verbose:
-            sys.stdout.write(r.stderr)
+        procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
         objs.append(obj)
+    for src, pr in procs:
+        out, err = pr.communicate()
+        if pr.returncode != 0:
+            raise RuntimeError(f"nvcc failed for {src}:\n{out}\n{err}")
+        if ptxas_info or verbose:
+            sys.stdout.write(err)
     tmp = LIB + ".tmp"
     cmd = [nvcc, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)

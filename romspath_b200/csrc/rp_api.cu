@@ -24,6 +24,7 @@ struct GridBuf {
     double *sr = nullptr, *csr = nullptr, *sw = nullptr, *csw = nullptr;
     uint8_t *mrho = nullptr, *mu = nullptr, *mv = nullptr;
     void *zeta = nullptr, *u = nullptr, *v = nullptr, *w = nullptr, *aks = nullptr;
+    float *qs_u = nullptr, *qs_v = nullptr, *qs_w = nullptr, *qs_aks = nullptr;  // mixed form: [slot][k]
     double scl[RP_MAXNGRID][2] = {}, off[RP_MAXNGRID][2] = {};
     int map[3] = {-1, -1, -1};                 // logical slot 1..3 -> physical 0..3
     bool slot_loaded[RP_SLOTS] = {false, false, false, false};
@@ -39,7 +40,8 @@ struct rp_ctx {
     int ngrid = 0;
     int device = 0;
     int num_sms = 148;
-    int elem = 8;                              // bytes per stored field value
+    int elem = 8;                              // bytes per stored field value (FP64/FP32 forms)
+    bool mixed = false;                        // RP_FIELD_MIXED
     int npmax = 0;
     GridBuf g[RP_MAXNGRID];
     // particle state
@@ -50,6 +52,13 @@ struct rp_ctx {
     int8_t* isin = nullptr;
     uint32_t *pid = nullptr, *flags = nullptr;
     double* turbv = nullptr;                   // scratch: VTurb displacement per particle
+    // mixed form: compensated FP32 positions, spline warm start, and the
+    // FP32 staging field plus per-level maxima of the FP16 quantisation
+    float *x32 = nullptr, *y32 = nullptr, *z32 = nullptr, *cx = nullptr, *cy = nullptr, *cz = nullptr;
+    double* qwarm = nullptr;
+    double* gwarm = nullptr;
+    float* ftmp = nullptr;
+    uint32_t* qmax = nullptr;
     double* tmp_gid = nullptr;                 // host-facing conversions
     int32_t* tmp_isin = nullptr;
     // staging
@@ -154,6 +163,8 @@ RpParticlesDev particles_dev(const rp_ctx* c) {
     P.x = c->x; P.y = c->y; P.z = c->z; P.age = c->age; P.dob = c->dob; P.status = c->status;
     P.wd = c->wd; P.zeta = c->zeta; P.bath = c->bath;
     P.gid = c->gid; P.isin = c->isin; P.pid = c->pid; P.flags = c->flags;
+    P.x32 = c->x32; P.y32 = c->y32; P.z32 = c->z32; P.cx = c->cx; P.cy = c->cy; P.cz = c->cz;
+    P.qwarm = c->qwarm; P.gwarm = c->gwarm;
     return P;
 }
 
@@ -166,6 +177,7 @@ void fill_grids(const rp_ctx* c, RpStepArgs& A, int tb, int tc, int tf) {
         d.mrho = G.mrho; d.mu = G.mu; d.mv = G.mv;
         d.sr = G.sr; d.csr = G.csr; d.sw = G.sw; d.csw = G.csw;
         d.zeta = G.zeta; d.u = G.u; d.v = G.v; d.w = G.w; d.aks = G.aks;
+        d.qs_u = G.qs_u; d.qs_v = G.qs_v; d.qs_w = G.qs_w; d.qs_aks = G.qs_aks;
         for (int i = 0; i < RP_MAXNGRID; i++)
             for (int q = 0; q < 2; q++) { d.scl[i][q] = G.scl[i][q]; d.off[i][q] = G.off[i][q]; }
         d.sb = (tb >= 1 && tb <= 3) ? G.map[tb - 1] : 0;
@@ -217,7 +229,7 @@ void free_ctx(rp_ctx* c) {
     for (int k = 0; k < RP_MAXNGRID; k++) {
         GridBuf& G = c->g[k];
         void* ptrs[] = {G.h, G.pm, G.pn, G.sr, G.csr, G.sw, G.csw, G.mrho, G.mu, G.mv,
-                        G.zeta, G.u, G.v, G.w, G.aks};
+                        G.zeta, G.u, G.v, G.w, G.aks, G.qs_u, G.qs_v, G.qs_w, G.qs_aks};
         for (void* p : ptrs) if (p) cudaFree(p);
         for (int s = 0; s < RP_SLOTS; s++) {
             if (G.slot_free[s]) cudaEventDestroy(G.slot_free[s]);
@@ -226,7 +238,8 @@ void free_ctx(rp_ctx* c) {
     }
     void* ptrs[] = {c->x, c->y, c->z, c->age, c->dob, c->status, c->wd, c->zeta, c->bath,
                     c->gid, c->isin, c->pid, c->flags, c->tmp_gid, c->tmp_isin, c->hook, c->turbv,
-                    c->dstage[0], c->dstage[1]};
+                    c->dstage[0], c->dstage[1], c->x32, c->y32, c->z32, c->cx, c->cy, c->cz, c->qwarm, c->gwarm,
+                    c->ftmp, c->qmax};
     for (void* p : ptrs) if (p) cudaFree(p);
     for (int h = 0; h < 2; h++) {
         if (c->pin[h]) cudaFreeHost(c->pin[h]);
@@ -239,10 +252,15 @@ void free_ctx(rp_ctx* c) {
     delete c;
 }
 
+// One field of a frame into physical slot `phys`.  FP64/FP32 forms (and the
+// FP32 zeta of the mixed form, `f32` set) convert each staged chunk straight
+// into the slot; the mixed form's u, v, w, AKs (`qs` non-null) are staged
+// whole as FP32, then quantised to FP16 with per-level scales.
 template <typename S>
-int upload_field(rp_ctx* ctx, const S* src, const S* add, void* dst, int ni, int nj, int nk, int phys) {
+int upload_field(rp_ctx* ctx, const S* src, const S* add, void* dst, int ni, int nj, int nk, int phys,
+                 bool f32 = false, float* qs = nullptr) {
     const int64_t total = (int64_t)ni * nj * nk;
-    const int dst_f32 = (ctx->elem == 4);
+    const int dst_f32 = (ctx->elem == 4 || f32);
     const int src_f32 = (sizeof(S) == 4);
     for (int64_t e0 = 0; e0 < total; e0 += kChunkElems) {
         const int64_t cnt = std::min<int64_t>(kChunkElems, total - e0);
@@ -258,11 +276,19 @@ int upload_field(rp_ctx* ctx, const S* src, const S* add, void* dst, int ni, int
         if (add)
             CK(cudaMemcpyAsync(dst_stage + (size_t)kChunkElems * 8, pin + (size_t)kChunkElems * 8, nb,
                                cudaMemcpyHostToDevice, ctx->s_copy));
-        CK(rp::launch_convert(src_f32, dst_f32, dst_stage, add ? dst_stage + (size_t)kChunkElems * 8 : nullptr,
-                              dst, ni, nj, nk, phys, e0, cnt, ctx->s_copy));
+        if (qs)
+            CK(rp::launch_stage_f32(src_f32, dst_stage, add ? dst_stage + (size_t)kChunkElems * 8 : nullptr,
+                                    ctx->ftmp, e0, cnt, ctx->s_copy));
+        else
+            CK(rp::launch_convert(src_f32, dst_f32, dst_stage, add ? dst_stage + (size_t)kChunkElems * 8 : nullptr,
+                                  dst, ni, nj, nk, phys, e0, cnt, ctx->s_copy));
         ctx->launches++;
         CK(cudaEventRecord(ctx->pin_done[h], ctx->s_copy));
         ctx->pin_used[h] = true;
+    }
+    if (qs) {
+        CK(rp::launch_quantize(ctx->ftmp, ctx->qmax, qs, dst, ni, nj, nk, phys, ctx->num_sms, ctx->s_copy));
+        ctx->launches += 2;
     }
     return RP_OK;
 }
@@ -288,11 +314,14 @@ int upload_frame(rp_ctx* ctx, int32_t ng, int32_t slot, const S* zeta, const S* 
     if (G.free_recorded[phys]) CK(cudaStreamWaitEvent(ctx->s_copy, G.slot_free[phys], 0));
     const int nx = G.nx, ny = G.ny, N = G.N;
     int rc;
-    if ((rc = upload_field<S>(ctx, zeta, nullptr, G.zeta, nx, ny, 1, phys)) != RP_OK) return rc;
-    if ((rc = upload_field<S>(ctx, u, stokes ? su : nullptr, G.u, nx - 1, ny, N, phys)) != RP_OK) return rc;
-    if ((rc = upload_field<S>(ctx, v, stokes ? sv : nullptr, G.v, nx, ny - 1, N, phys)) != RP_OK) return rc;
-    if ((rc = upload_field<S>(ctx, w, nullptr, G.w, nx, ny, N + 1, phys)) != RP_OK) return rc;
-    if ((rc = upload_field<S>(ctx, aks, nullptr, G.aks, nx, ny, N + 1, phys)) != RP_OK) return rc;
+    const bool mx = ctx->mixed;
+    if ((rc = upload_field<S>(ctx, zeta, nullptr, G.zeta, nx, ny, 1, phys, mx)) != RP_OK) return rc;
+    if ((rc = upload_field<S>(ctx, u, stokes ? su : nullptr, G.u, nx - 1, ny, N, phys, mx, G.qs_u)) != RP_OK)
+        return rc;
+    if ((rc = upload_field<S>(ctx, v, stokes ? sv : nullptr, G.v, nx, ny - 1, N, phys, mx, G.qs_v)) != RP_OK)
+        return rc;
+    if ((rc = upload_field<S>(ctx, w, nullptr, G.w, nx, ny, N + 1, phys, mx, G.qs_w)) != RP_OK) return rc;
+    if ((rc = upload_field<S>(ctx, aks, nullptr, G.aks, nx, ny, N + 1, phys, mx, G.qs_aks)) != RP_OK) return rc;
     CK(cudaEventRecord(G.slot_ready[phys], ctx->s_copy));
     G.slot_loaded[phys] = true;
     const int old = G.map[slot - 1];
@@ -320,7 +349,8 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
     if (p.behavior != 0) return RP_ERR_UNSUPPORTED;
     if (p.nsb < 0 || p.nsb > 2) return RP_ERR_ARG;
     if (!(p.deltat >= 1.0) || !(p.sub > 0.0)) return RP_ERR_ARG;
-    if (p.field_dtype != RP_FIELD_F64 && p.field_dtype != RP_FIELD_F32) return RP_ERR_ARG;
+    if (p.field_dtype != RP_FIELD_F64 && p.field_dtype != RP_FIELD_F32 && p.field_dtype != RP_FIELD_MIXED)
+        return RP_ERR_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= p.device || p.device < 0) return RP_ERR_NOEXT;
     rp_ctx* ctx = new rp_ctx();
@@ -328,6 +358,7 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
     ctx->ngrid = ngrid;
     ctx->device = p.device;
     ctx->elem = (p.field_dtype == RP_FIELD_F32) ? 4 : 8;
+    ctx->mixed = (p.field_dtype == RP_FIELD_MIXED);
     ctx->ndraw = 2 + p.idt / (int)p.deltat;
     auto bail = [&](int code, const std::string& m) {
         std::fprintf(stderr, "rp_create: %s\n", m.c_str());
@@ -386,15 +417,26 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
                 G.off[i][0] = R.off[i]; G.off[i][1] = R.off[ngrid + i];
             }
         }
-        const size_t e = (size_t)ctx->elem * RP_SLOTS;
-        if (dalloc(&G.zeta, n2 * e) || dalloc(&G.u, nu * G.N * e) || dalloc(&G.v, nv * G.N * e) ||
+        // bytes per (point, level) over the ring: zeta and the 3-D fields
+        const size_t ez = (size_t)(ctx->mixed ? 4 : ctx->elem) * RP_SLOTS;
+        const size_t e = (size_t)(ctx->mixed ? 2 : ctx->elem) * RP_SLOTS;
+        if (dalloc(&G.zeta, n2 * ez) || dalloc(&G.u, nu * G.N * e) || dalloc(&G.v, nv * G.N * e) ||
             dalloc(&G.w, n2 * sw * e) || dalloc(&G.aks, n2 * sw * e))
             return bail(RP_ERR_NOMEM, "frame ring allocation");
-        cudaMemset(G.zeta, 0, n2 * e);
+        cudaMemset(G.zeta, 0, n2 * ez);
         cudaMemset(G.u, 0, nu * G.N * e);
         cudaMemset(G.v, 0, nv * G.N * e);
         cudaMemset(G.w, 0, n2 * sw * e);
         cudaMemset(G.aks, 0, n2 * sw * e);
+        if (ctx->mixed) {
+            const size_t qn = (size_t)RP_SLOTS * sw * 4;
+            if (dalloc(&G.qs_u, qn) || dalloc(&G.qs_v, qn) || dalloc(&G.qs_w, qn) || dalloc(&G.qs_aks, qn))
+                return bail(RP_ERR_NOMEM, "scale allocation");
+            cudaMemset(G.qs_u, 0, qn);
+            cudaMemset(G.qs_v, 0, qn);
+            cudaMemset(G.qs_w, 0, qn);
+            cudaMemset(G.qs_aks, 0, qn);
+        }
         for (int s = 0; s < RP_SLOTS; s++) {
             if (cudaEventCreateWithFlags(&G.slot_free[s], cudaEventDisableTiming) != cudaSuccess ||
                 cudaEventCreateWithFlags(&G.slot_ready[s], cudaEventDisableTiming) != cudaSuccess)
@@ -403,6 +445,17 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
     }
     const size_t cap = (size_t)std::max(p.numpar, 1);
     ctx->cap = (int64_t)cap;
+    if (ctx->mixed) {
+        size_t fmax = 0, lmax = 0;
+        for (int k = 0; k < ngrid; k++) {
+            fmax = std::max(fmax, (size_t)ctx->g[k].nx * ctx->g[k].ny * (ctx->g[k].N + 1));
+            lmax = std::max(lmax, (size_t)ctx->g[k].N + 1);
+        }
+        if (dalloc(&ctx->x32, cap * 4) || dalloc(&ctx->y32, cap * 4) || dalloc(&ctx->z32, cap * 4) ||
+            dalloc(&ctx->cx, cap * 4) || dalloc(&ctx->cy, cap * 4) || dalloc(&ctx->cz, cap * 4) ||
+            dalloc(&ctx->qwarm, cap * 8) || dalloc(&ctx->gwarm, cap * 8) || dalloc(&ctx->ftmp, fmax * 4) || dalloc(&ctx->qmax, lmax * 4))
+            return bail(RP_ERR_NOMEM, "mixed-form allocation");
+    }
     if (dalloc(&ctx->x, cap * 8) || dalloc(&ctx->y, cap * 8) || dalloc(&ctx->z, cap * 8) ||
         dalloc(&ctx->age, cap * 8) || dalloc(&ctx->dob, cap * 8) || dalloc(&ctx->status, cap * 8) ||
         dalloc(&ctx->wd, cap * 8) || dalloc(&ctx->zeta, cap * 8) || dalloc(&ctx->bath, cap * 8) ||
@@ -476,6 +529,10 @@ int rp_set_particles(rp_ctx* ctx, int64_t n, const double* x, const double* y, c
     RpParticlesDev P = particles_dev(ctx);
     CK(rp::launch_state_from_host(P, ctx->tmp_gid, ctx->tmp_isin, ctx->pid_base, s));
     ctx->launches++;
+    if (ctx->mixed) {
+        CK(rp::launch_mixed_convert(P, 0, s));
+        ctx->launches++;
+    }
     CK(cudaMemsetAsync(ctx->wd, 0, b8, s));
     CK(cudaMemsetAsync(ctx->zeta, 0, b8, s));
     CK(cudaMemsetAsync(ctx->bath, 0, b8, s));
@@ -510,8 +567,12 @@ int rp_locate_particles(rp_ctx* ctx, int64_t n, const double* ipos, const double
             const int ph = ctx->g[k].map[t_b - 1];
             cudaStreamWaitEvent(s, ctx->g[k].slot_ready[ph], 0);
         }
-        cudaError_t e = rp::launch_locate(A, ctx->prm.field_dtype, dip, djp, dz, ddob, s);
+        cudaError_t e = rp::launch_locate(A, ctx->mixed ? RP_FIELD_F32 : ctx->prm.field_dtype, dip, djp, dz, ddob, s);
         ctx->launches++;
+        if (e == cudaSuccess && ctx->mixed) {
+            e = rp::launch_mixed_convert(A.p, 0, s);
+            ctx->launches++;
+        }
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) rc = fail(ctx, RP_ERR_CUDA, std::string("locate: ") + cudaGetErrorString(e));
     }
@@ -548,7 +609,9 @@ int rp_step(rp_ctx* ctx, const double ex[3], const double ix[3], int32_t ets, in
     }
     int nl = 0;
     CK(cudaEventRecord(ctx->ev0, s));
-    if (ctx->n > 0)
+    if (ctx->n > 0 && ctx->mixed)
+        CK(rp::launch_step_mixed(A, ctx->npmax, s, ctx->num_sms, &nl));
+    else if (ctx->n > 0)
         CK(rp::launch_step(A, ctx->prm.field_dtype, ctx->npmax, ctx->turbv, ctx->prm.reserved[0] == 1 ? 0 : 1, s,
                            ctx->num_sms, &nl));
     CK(cudaEventRecord(ctx->ev1, s));
@@ -567,6 +630,7 @@ int rp_step_noalloc(rp_ctx* ctx, const rp_device_state* st, const double ex[3], 
         return fail(ctx, RP_ERR_ARG, "rp_step_noalloc: state->n exceeds RP_NOALLOC_MAX_PARTICLES (1048576)");
     if (ctx->npmax > 128)
         return fail(ctx, RP_ERR_UNSUPPORTED, "rp_step_noalloc: int(s_w*sub) must be <= 128");
+    if (ctx->mixed) return fail(ctx, RP_ERR_UNSUPPORTED, "rp_step_noalloc: not available in the mixed form");
     if (!st->x || !st->y || !st->z || !st->age || !st->dob || !st->status || !st->wd || !st->zeta || !st->bath ||
         !st->gid || !st->isin || !st->pid || !st->flags)
         return fail(ctx, RP_ERR_ARG, "rp_step_noalloc: null state column");
@@ -613,6 +677,12 @@ int rp_get_particles(rp_ctx* ctx, int64_t n, double* x, double* y, double* z, do
     cudaStream_t s = ctx->s_comp;
     int rc;
     const size_t b8 = (size_t)n * 8;
+    if (ctx->mixed && (x || y || z)) {
+        RpParticlesDev P = particles_dev(ctx);
+        P.n = n;
+        CK(rp::launch_mixed_convert(P, 1, s));
+        ctx->launches++;
+    }
     if (gid || isin) {
         RpParticlesDev P = particles_dev(ctx);
         P.n = n;
@@ -672,6 +742,12 @@ int rp_synchronize(rp_ctx* ctx) {
 
 int rp_device_state_get(rp_ctx* ctx, rp_device_state* out) {
     if (!ctx || !out) return RP_ERR_ARG;
+    if (ctx->mixed && ctx->n > 0) {
+        CK(cudaSetDevice(ctx->device));
+        CK(rp::launch_mixed_convert(particles_dev(ctx), 1, ctx->s_comp));
+        ctx->launches++;
+        CK(cudaStreamSynchronize(ctx->s_comp));
+    }
     out->n = ctx->n;
     out->x = ctx->x; out->y = ctx->y; out->z = ctx->z; out->age = ctx->age; out->dob = ctx->dob;
     out->status = ctx->status; out->wd = ctx->wd; out->zeta = ctx->zeta; out->bath = ctx->bath;

@@ -60,6 +60,11 @@ struct RpGridDev {
     double scl[RP_MAXNGRID_D][2];  // GRIDS(ng)%scl(i,1:2)
     double off[RP_MAXNGRID_D][2];
     int sb, sc, sf;                // physical ring slots of t_b, t_c, t_f
+    // mixed form: per-(slot, level) scales of the FP16 fields, [slot][k]
+    const float* qs_u;
+    const float* qs_v;
+    const float* qs_w;
+    const float* qs_aks;
 };
 
 struct RpParticlesDev {
@@ -77,6 +82,17 @@ struct RpParticlesDev {
     int8_t* isin;
     uint32_t* pid;
     uint32_t* flags;
+    // mixed form: FP32 positions with Kahan compensation (value = p - c)
+    // and the smoothing-spline warm start (last q, < 0 for none; slope of
+    // 1/sqrt(SF) in q there, <= 0 for none)
+    float* x32;
+    float* y32;
+    float* z32;
+    float* cx;
+    float* cy;
+    float* cz;
+    double* qwarm;
+    double* gwarm;
 };
 
 // polintd (interpolation_module.f90:72-109) at fixed nodes ex(3) and point
@@ -572,27 +588,34 @@ __device__ __forceinline__ void rp_philox(uint32_t c[4], uint32_t k0, uint32_t k
 #define RP_TWOPI_HI 6.283185307179586
 #define RP_TWOPI_LO 2.4492935982947064e-16
 
+// The products and sums are written with the round-to-nearest intrinsics,
+// which are never contracted into FMAs, so the noise is bit-identical in
+// every compilation unit whatever its contraction setting.
+#define RP_MUL(a, b) __dmul_rn((a), (b))
+#define RP_ADD(a, b) __dadd_rn((a), (b))
+#define RP_SUB(a, b) __dsub_rn((a), (b))
+
 __device__ __forceinline__ double rp_log_pos(double x) {
     unsigned long long b = (unsigned long long)__double_as_longlong(x);
     int e = (int)((b >> 52) & 0x7ffull) - 1023;
     double m = __longlong_as_double((long long)((b & 0x000fffffffffffffull) | 0x3ff0000000000000ull));
     if (m > RP_SQRT2) { m = m * 0.5; e = e + 1; }
     const double z = (m - 1.0) / (m + 1.0);
-    const double z2 = z * z;
+    const double z2 = RP_MUL(z, z);
     double p = 1.0 / 23.0;
-    p = p * z2 + 1.0 / 21.0;
-    p = p * z2 + 1.0 / 19.0;
-    p = p * z2 + 1.0 / 17.0;
-    p = p * z2 + 1.0 / 15.0;
-    p = p * z2 + 1.0 / 13.0;
-    p = p * z2 + 1.0 / 11.0;
-    p = p * z2 + 1.0 / 9.0;
-    p = p * z2 + 1.0 / 7.0;
-    p = p * z2 + 1.0 / 5.0;
-    p = p * z2 + 1.0 / 3.0;
-    p = p * z2 + 1.0;
+    p = RP_ADD(RP_MUL(p, z2), 1.0 / 21.0);
+    p = RP_ADD(RP_MUL(p, z2), 1.0 / 19.0);
+    p = RP_ADD(RP_MUL(p, z2), 1.0 / 17.0);
+    p = RP_ADD(RP_MUL(p, z2), 1.0 / 15.0);
+    p = RP_ADD(RP_MUL(p, z2), 1.0 / 13.0);
+    p = RP_ADD(RP_MUL(p, z2), 1.0 / 11.0);
+    p = RP_ADD(RP_MUL(p, z2), 1.0 / 9.0);
+    p = RP_ADD(RP_MUL(p, z2), 1.0 / 7.0);
+    p = RP_ADD(RP_MUL(p, z2), 1.0 / 5.0);
+    p = RP_ADD(RP_MUL(p, z2), 1.0 / 3.0);
+    p = RP_ADD(RP_MUL(p, z2), 1.0);
     const double de = (double)e;
-    return de * RP_LN2_HI + (de * RP_LN2_LO + 2.0 * z * p);
+    return RP_ADD(RP_MUL(de, RP_LN2_HI), RP_ADD(RP_MUL(de, RP_LN2_LO), RP_MUL(RP_MUL(2.0, z), p)));
 }
 
 // cos(2 pi u) for u in [0,1]: exact reductions (1-u, 1/2-v, 1/4-v are exact
@@ -604,34 +627,34 @@ __device__ __forceinline__ double rp_cos2pi(double u) {
     if (v > 0.25) { v = 0.5 - v; sign = -1.0; }
     double r;
     if (v <= 0.125) {
-        const double x = v * RP_TWOPI_HI + v * RP_TWOPI_LO;
-        const double x2 = x * x;
-        double p = 1.0 / 2432902008176640000.0;          // 1/20!
-        p = p * x2 - 1.0 / 6402373705728000.0;            // 1/18!
-        p = p * x2 + 1.0 / 20922789888000.0;              // 1/16!
-        p = p * x2 - 1.0 / 87178291200.0;                 // 1/14!
-        p = p * x2 + 1.0 / 479001600.0;                   // 1/12!
-        p = p * x2 - 1.0 / 3628800.0;                     // 1/10!
-        p = p * x2 + 1.0 / 40320.0;                       // 1/8!
-        p = p * x2 - 1.0 / 720.0;                         // 1/6!
-        p = p * x2 + 1.0 / 24.0;                          // 1/4!
-        p = p * x2 - 0.5;                                 // 1/2!
-        r = p * x2 + 1.0;
+        const double x = RP_ADD(RP_MUL(v, RP_TWOPI_HI), RP_MUL(v, RP_TWOPI_LO));
+        const double x2 = RP_MUL(x, x);
+        double p = 1.0 / 2432902008176640000.0;                          // 1/20!
+        p = RP_SUB(RP_MUL(p, x2), 1.0 / 6402373705728000.0);             // 1/18!
+        p = RP_ADD(RP_MUL(p, x2), 1.0 / 20922789888000.0);               // 1/16!
+        p = RP_SUB(RP_MUL(p, x2), 1.0 / 87178291200.0);                  // 1/14!
+        p = RP_ADD(RP_MUL(p, x2), 1.0 / 479001600.0);                    // 1/12!
+        p = RP_SUB(RP_MUL(p, x2), 1.0 / 3628800.0);                      // 1/10!
+        p = RP_ADD(RP_MUL(p, x2), 1.0 / 40320.0);                        // 1/8!
+        p = RP_SUB(RP_MUL(p, x2), 1.0 / 720.0);                          // 1/6!
+        p = RP_ADD(RP_MUL(p, x2), 1.0 / 24.0);                           // 1/4!
+        p = RP_SUB(RP_MUL(p, x2), 0.5);                                  // 1/2!
+        r = RP_ADD(RP_MUL(p, x2), 1.0);
     } else {
         const double w = 0.25 - v;
-        const double x = w * RP_TWOPI_HI + w * RP_TWOPI_LO;
-        const double x2 = x * x;
-        double p = 1.0 / 121645100408832000.0;            // 1/19!
-        p = p * x2 - 1.0 / 355687428096000.0;             // 1/17!
-        p = p * x2 + 1.0 / 1307674368000.0;               // 1/15!
-        p = p * x2 - 1.0 / 6227020800.0;                  // 1/13!
-        p = p * x2 + 1.0 / 39916800.0;                    // 1/11!
-        p = p * x2 - 1.0 / 362880.0;                      // 1/9!
-        p = p * x2 + 1.0 / 5040.0;                        // 1/7!
-        p = p * x2 - 1.0 / 120.0;                         // 1/5!
-        p = p * x2 + 1.0 / 6.0;                           // 1/3!  (sign below)
-        p = p * x2;
-        r = x - x * p;                                    // x (1 - x^2/3! + ...)
+        const double x = RP_ADD(RP_MUL(w, RP_TWOPI_HI), RP_MUL(w, RP_TWOPI_LO));
+        const double x2 = RP_MUL(x, x);
+        double p = 1.0 / 121645100408832000.0;                           // 1/19!
+        p = RP_SUB(RP_MUL(p, x2), 1.0 / 355687428096000.0);              // 1/17!
+        p = RP_ADD(RP_MUL(p, x2), 1.0 / 1307674368000.0);                // 1/15!
+        p = RP_SUB(RP_MUL(p, x2), 1.0 / 6227020800.0);                   // 1/13!
+        p = RP_ADD(RP_MUL(p, x2), 1.0 / 39916800.0);                     // 1/11!
+        p = RP_SUB(RP_MUL(p, x2), 1.0 / 362880.0);                       // 1/9!
+        p = RP_ADD(RP_MUL(p, x2), 1.0 / 5040.0);                         // 1/7!
+        p = RP_SUB(RP_MUL(p, x2), 1.0 / 120.0);                          // 1/5!
+        p = RP_ADD(RP_MUL(p, x2), 1.0 / 6.0);                            // 1/3!  (sign below)
+        p = RP_MUL(p, x2);
+        r = RP_SUB(x, RP_MUL(x, p));                                     // x (1 - x^2/3! + ...)
     }
     return sign * r;
 }

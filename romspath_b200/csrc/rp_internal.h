@@ -15,6 +15,10 @@ constexpr int kStepBlock = 128;
 #define RP_VTURB_MIN_BLOCKS 8
 #endif
 constexpr int kVturbMinBlocks = RP_VTURB_MIN_BLOCKS;   // resident 128-thread blocks per SM
+#ifndef RP_MIXED_MIN_BLOCKS
+#define RP_MIXED_MIN_BLOCKS 6
+#endif
+constexpr int kMixedMinBlocks = RP_MIXED_MIN_BLOCKS;   // same, mixed-precision step
 
 constexpr int kMaxNp = 144;   // largest spline point count int(s_w*sub)
 
@@ -27,6 +31,16 @@ cudaError_t launch_step(const RpStepArgs& A, int field_dtype, int npmax, double*
 constexpr int64_t kNoallocMaxParticles = 1048576;
 cudaError_t launch_step_noalloc(const RpStepArgs& A, int field_dtype, int npmax, int device, cudaStream_t s,
                                 int num_sms, int* nlaunch);
+
+// Mixed-precision form (rp_mixed.cu): the step, the FP16 quantisation of a
+// frame field staged as FP32 (Fortran order), and the conversions between
+// the FP64 columns and the compensated FP32 positions.
+cudaError_t launch_step_mixed(const RpStepArgs& A, int npmax, cudaStream_t s, int num_sms, int* nlaunch);
+cudaError_t launch_stage_f32(int src_f32, const void* src, const void* add, float* dst, int64_t e0, int64_t count,
+                             cudaStream_t s);
+cudaError_t launch_quantize(const float* f, uint32_t* maxbits, float* qs, void* dst, int ni, int nj, int nk, int slot,
+                            int num_sms, cudaStream_t s);
+cudaError_t launch_mixed_convert(const RpParticlesDev& P, int to_f64, cudaStream_t s);
 
 cudaError_t launch_locate(const RpStepArgs& A, int field_dtype, const double* ipos, const double* jpos,
                           const double* z, const double* dob, cudaStream_t s);

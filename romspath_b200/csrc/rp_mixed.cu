@@ -1,0 +1,164 @@
+// rp_mixed.cu -- kernels of the mixed-precision form: the step, the FP16
+// frame quantisation with per-level scales, and the conversions between
+// the FP64 particle columns and the compensated FP32 positions.
+// Compiled with FMA contraction (the default): this form is not bit-exact.
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include "rp_internal.h"
+#include "rp_mixed.cuh"
+
+namespace rp {
+
+template <int NPMAX>
+__global__ void __launch_bounds__(kStepBlock, kMixedMinBlocks) k_step_mixed(const __grid_constant__ RpStepArgs A) {
+    double buf[kMixedArrays * (NPMAX + 1)];
+    const MSpline<NPMAX> w{buf};
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < A.p.n; n += stride)
+        m_update_one<NPMAX>(A, n, w);
+}
+
+template <int NPMAX>
+static cudaError_t launch_mixed_t(const RpStepArgs& A, cudaStream_t s, int num_sms, int* nlaunch) {
+    int occ = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_step_mixed<NPMAX>, kStepBlock, 0);
+    if (e != cudaSuccess) return e;
+    if (occ < 1) occ = 1;
+    int64_t blocks = (int64_t)num_sms * occ;
+    const int64_t need = (A.p.n + kStepBlock - 1) / kStepBlock;
+    if (need < blocks) blocks = need;
+    if (blocks < 1) blocks = 1;
+    k_step_mixed<NPMAX><<<(unsigned)blocks, kStepBlock, 0, s>>>(A);
+    *nlaunch += 1;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_step_mixed(const RpStepArgs& A, int npmax, cudaStream_t s, int num_sms, int* nlaunch) {
+    if (npmax <= 88) return launch_mixed_t<88>(A, s, num_sms, nlaunch);
+    if (npmax <= 128) return launch_mixed_t<128>(A, s, num_sms, nlaunch);
+    return launch_mixed_t<144>(A, s, num_sms, nlaunch);
+}
+
+// ------------------------------------------------------ frame upload
+
+// one staged chunk of a Fortran-ordered field (plus the Stokes term) into
+// the FP32 field buffer, same order
+template <typename S>
+__global__ void k_stage_f32(const S* __restrict__ src, const S* __restrict__ add, float* __restrict__ dst,
+                            int64_t e0, int64_t count) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    double v = (double)src[t];
+    if (add) v = v + (double)add[t];
+    dst[e0 + t] = (float)v;
+}
+
+cudaError_t launch_stage_f32(int src_f32, const void* src, const void* add, float* dst, int64_t e0, int64_t count,
+                             cudaStream_t s) {
+    const int block = 256;
+    const unsigned blocks = (unsigned)((count + block - 1) / block);
+    if (blocks == 0) return cudaSuccess;
+    if (src_f32)
+        k_stage_f32<float><<<blocks, block, 0, s>>>((const float*)src, (const float*)add, dst, e0, count);
+    else
+        k_stage_f32<double><<<blocks, block, 0, s>>>((const double*)src, (const double*)add, dst, e0, count);
+    return cudaGetLastError();
+}
+
+// max |v| over each level k of a Fortran-ordered field (level = slowest
+// index), as the bits of a non-negative float (integer order = float order)
+__global__ void k_level_maxabs(const float* __restrict__ f, int64_t plane, uint32_t* __restrict__ maxbits) {
+    const int k = blockIdx.y;
+    const float* lev = f + (int64_t)k * plane;
+    float m = 0.f;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < plane; e += (int64_t)gridDim.x * blockDim.x)
+        m = fmaxf(m, fabsf(lev[e]));
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __shared__ float wm[32];
+    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m = (threadIdx.x < (blockDim.x >> 5)) ? wm[threadIdx.x] : 0.f;
+        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (threadIdx.x == 0) atomicMax(maxbits + k, __float_as_uint(m));
+    }
+}
+
+// the power-of-two scale of a level: |v| / scale <= 16384 (exact scaling)
+__device__ __forceinline__ float m_level_scale(uint32_t bits) {
+    const float mx = __uint_as_float(bits);
+    if (!(mx > 0.f) || !(mx < 3.0e38f)) return 1.0f;
+    int e = 0;
+    frexpf(mx, &e);                        // mx = m 2^e, m in [0.5, 1)
+    return ldexpf(1.0f, e - 14);
+}
+
+// FP32 field (Fortran order) -> FP16 device layout [j][i][k][slot4] and the
+// per-level scales qs[slot][k]
+__global__ void k_quantize(const float* __restrict__ f, const uint32_t* __restrict__ maxbits, float* __restrict__ qs,
+                           __half* __restrict__ dst, int ni, int nj, int nk, int slot) {
+    const int64_t plane = (int64_t)ni * nj;
+    const int64_t total = plane * nk;
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < nk) qs[slot * nk + e] = m_level_scale(maxbits[e]);
+    if (e >= total) return;
+    const int k = (int)(e / plane);
+    const int64_t r = e - (int64_t)k * plane;
+    const int j = (int)(r / ni);
+    const int i = (int)(r - (int64_t)j * ni);
+    const float inv = 1.0f / m_level_scale(maxbits[k]);
+    dst[(((int64_t)j * ni + i) * nk + k) * RP_SLOTS + slot] = __float2half_rn(f[e] * inv);
+}
+
+cudaError_t launch_quantize(const float* f, uint32_t* maxbits, float* qs, void* dst, int ni, int nj, int nk, int slot,
+                            int num_sms, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(maxbits, 0, sizeof(uint32_t) * nk, s);
+    if (e != cudaSuccess) return e;
+    const int64_t plane = (int64_t)ni * nj;
+    const int block = 256;
+    int64_t bx = (plane + block - 1) / block;
+    const int64_t cap = (int64_t)num_sms * 4 / (nk > 0 ? nk : 1) + 1;
+    if (bx > cap) bx = cap;
+    k_level_maxabs<<<dim3((unsigned)bx, (unsigned)nk), block, 0, s>>>(f, plane, maxbits);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    const int64_t total = plane * nk;
+    const unsigned blocks = (unsigned)((total + block - 1) / block);
+    k_quantize<<<blocks, block, 0, s>>>(f, maxbits, qs, (__half*)dst, ni, nj, nk, slot);
+    return cudaGetLastError();
+}
+
+// ----------------------------------------------- particle conversions
+
+// FP64 columns -> compensated FP32 positions (value = p - c) and no
+// smoothing-parameter warm start
+__global__ void k_mixed_from_f64(RpParticlesDev P) {
+    const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= P.n) return;
+    const double x = P.x[n], y = P.y[n], z = P.z[n];
+    const float px = (float)x, py = (float)y, pz = (float)z;
+    P.x32[n] = px; P.cx[n] = (float)((double)px - x);
+    P.y32[n] = py; P.cy[n] = (float)((double)py - y);
+    P.z32[n] = pz; P.cz[n] = (float)((double)pz - z);
+    P.qwarm[n] = -1.0;
+    P.gwarm[n] = 0.0;
+}
+
+__global__ void k_mixed_to_f64(RpParticlesDev P) {
+    const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= P.n) return;
+    P.x[n] = (double)P.x32[n] - (double)P.cx[n];
+    P.y[n] = (double)P.y32[n] - (double)P.cy[n];
+    P.z[n] = (double)P.z32[n] - (double)P.cz[n];
+}
+
+cudaError_t launch_mixed_convert(const RpParticlesDev& P, int to_f64, cudaStream_t s) {
+    const int block = 256;
+    const unsigned blocks = (unsigned)((P.n + block - 1) / block);
+    if (blocks == 0) return cudaSuccess;
+    if (to_f64) k_mixed_to_f64<<<blocks, block, 0, s>>>(P);
+    else k_mixed_from_f64<<<blocks, block, 0, s>>>(P);
+    return cudaGetLastError();
+}
+
+}  // namespace rp

@@ -51,7 +51,10 @@ class Tracker:
         P.open_ocean_boundary = int(params["open_ocean_boundary"])
         P.behavior = 0
         P.stokes = int(bool(stokes))
-        P.field_dtype = _lib.FIELD_F32 if field_dtype == "f32" else _lib.FIELD_F64
+        # "f64" / "f32": fields stored at that width, FP64 arithmetic (exact);
+        # "mixed": FP16 fields with per-level scales, FP32 positions with
+        # compensated accumulation, FP64 age and spline fit (not exact)
+        P.field_dtype = {"f64": _lib.FIELD_F64, "f32": _lib.FIELD_F32, "mixed": _lib.FIELD_MIXED}[field_dtype]
         P.spline_max_iter = int(spline_max_iter)
         for k in ("vertdist", "serr", "smth", "sub", "deltat", "aksback"):
             setattr(P, k, float(params[k]))

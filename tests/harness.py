@@ -90,10 +90,13 @@ def _steps(case: Case, nsteps: int):
 
 
 def run_gpu(case: Case, nsteps: int, noise: str = "philox", seed: int = 7,
-            hook: Optional[np.ndarray] = None, tracker=None, variant: str = "fused"):
+            hook: Optional[np.ndarray] = None, tracker=None, variant: str = "fused",
+            field_dtype: Optional[str] = None):
+    """Run the CUDA path; ``field_dtype="mixed"`` selects the mixed-precision
+    form (the frames it is given are the same)."""
     from romspath_b200 import Tracker
     T = tracker or Tracker(case.specs, case.grids, case.params, numpar=case.release.z.shape[0],
-                           field_dtype=case.spec.field_dtype, stokes=case.spec.stokes, seed=seed,
+                           field_dtype=field_dtype or case.spec.field_dtype, stokes=case.spec.stokes, seed=seed,
                            scl=case.scl, off=case.off, variant=variant)
     for (k, slot) in schedule.initial_loads():
         for ng in range(1, case.ngrid + 1):

@@ -1,0 +1,147 @@
+"""The mixed-precision form against the exact FP64 form on the GPU.
+
+The mixed form (FP16 u/v/w/AKs with per-level power-of-two scales, FP32
+zeta, FP32 positions with compensated accumulation, FP32 interpolation and
+RK4, FP64 age, spline fit and sub-steps, warm-started smoothing parameter)
+is not bit-exact.  These tests run it and the FP64 form on the same inputs
+and the same noise and bound the differences; they also run the
+well-mixed-condition test (Visser 1997) on the mixed form, since its
+random walk uses a re-implemented spline.
+
+Tolerances (stated per test): deterministic trajectories (turbulence off)
+RMS horizontal error below 2e-3 grid cells after 96 steps; with identical
+noise hooks, RMS horizontal error below 2e-3 cells and RMS vertical error
+below 1 % of the mean water depth after 24 steps; status identical for at
+least 99 % of particles; the vertical concentration profile within
+3 sqrt(count) per bin of the FP64 form's.
+"""
+import numpy as np
+import pytest
+
+import harness
+
+pytestmark = pytest.mark.gpu
+
+
+def _err(a, b):
+    dx = a["x"] - b["x"]
+    dy = a["y"] - b["y"]
+    dh = np.sqrt(dx * dx + dy * dy)
+    dz = a["z"] - b["z"]
+    return {"rms_h": float(np.sqrt(np.mean(dh * dh))), "max_h": float(dh.max()),
+            "rms_z": float(np.sqrt(np.mean(dz * dz))), "max_z": float(np.abs(dz).max()),
+            "status_same": float(np.mean(a["status"] == b["status"]))}
+
+
+def _moved(st):
+    return np.isin(st["status"], [1.0, np.float32(1.1), np.float32(1.2)])
+
+
+def test_mixed_deterministic_close_to_fp64():
+    case = harness.make_case("tiny", 400, seed=3, param_over={"vturb_on": 0, "hturb_on": 0})
+    ref, T0 = harness.run_gpu(case, 96, noise="philox")
+    mix, T1 = harness.run_gpu(case, 96, noise="philox", field_dtype="mixed")
+    e = _err(mix, ref)
+    print("deterministic mixed vs fp64:", e)
+    assert _moved(ref).sum() > 300
+    assert e["status_same"] >= 0.99
+    ok = _moved(ref) & _moved(mix)
+    d = np.hypot(mix["x"][ok] - ref["x"][ok], mix["y"][ok] - ref["y"][ok])
+    assert np.sqrt(np.mean(d * d)) < 2e-3
+    assert np.all(mix["age"] == ref["age"])            # FP64 age, same increments
+    T0.close()
+    T1.close()
+
+
+def test_mixed_hook_noise_close_to_fp64():
+    case = harness.make_case("tiny", 300, seed=5)      # RK4 + HTurb + VTurb
+    hook = harness.noise_array(case, 24, seed=17)
+    ref, T0 = harness.run_gpu(case, 24, noise="hook", hook=hook)
+    mix, T1 = harness.run_gpu(case, 24, noise="hook", hook=hook, field_dtype="mixed")
+    e = _err(mix, ref)
+    print("hook-noise mixed vs fp64:", e)
+    assert e["status_same"] >= 0.99
+    ok = _moved(ref) & _moved(mix)
+    d = np.hypot(mix["x"][ok] - ref["x"][ok], mix["y"][ok] - ref["y"][ok])
+    assert np.sqrt(np.mean(d * d)) < 2e-3
+    depth = float(np.mean(ref["bath"][ok] + ref["zeta"][ok]))
+    dz = mix["z"][ok] - ref["z"][ok]
+    assert np.sqrt(np.mean(dz * dz)) < 0.01 * depth
+    T0.close()
+    T1.close()
+
+
+def test_mixed_philox_runs_and_flags_clean():
+    case = harness.make_case("tiny", 500, seed=6)
+    mix, T = harness.run_gpu(case, 36, noise="philox", field_dtype="mixed")
+    assert np.all(np.isfinite(mix["x"])) and np.all(np.isfinite(mix["z"]))
+    ok = _moved(mix)
+    assert ok.sum() > 400
+    # inside the water column
+    assert np.all(mix["z"][ok] >= -mix["bath"][ok] - 1e-6)
+    assert np.all(mix["z"][ok] <= mix["zeta"][ok] + 1e-6)
+    assert not np.any(mix["flags"] & 0x10)            # no spline cap hit
+    T.close()
+
+
+def _column_hist(st):
+    rel = (st["z"] + st["bath"]) / (st["bath"] + st["zeta"])
+    counts, _ = np.histogram(rel, bins=20, range=(0.0, 1.0))
+    return counts
+
+
+def test_mixed_well_mixed_condition():
+    """Visser (1997): a uniform distribution stays uniform under VTurb alone,
+    chi-square on 20 bins below 43.8 (19 dof, p = 0.001), at the sample
+    size where the reference algorithm itself passes it (3000 particles)."""
+    case = harness.make_case("tiny", 3000, seed=9, spec_over={"land": "none"},
+                             param_over={"scheme": 0, "hturb_on": 0})
+    mix, T = harness.run_gpu(case, 48, noise="philox", seed=21, field_dtype="mixed")
+    counts = _column_hist(mix)
+    exp = counts.sum() / 20
+    chi2 = float(((counts - exp) ** 2 / exp).sum())
+    print("mixed WMC chi2 (3000):", chi2)
+    assert chi2 < 43.8
+    T.close()
+
+
+def test_mixed_column_profile_matches_fp64():
+    """With 20000 particles the reference algorithm's own random walk is
+    measurably non-uniform near the reflecting bottom and surface (the CPU
+    oracle gives chi-square ~90 on 20 bins, the end bins ~18 % short), so
+    the mixed form is held to the FP64 form's profile instead: same release,
+    same Philox noise, every bin within 3 sqrt(count) and total L1 below 2 %
+    of the particles."""
+    case = harness.make_case("tiny", 20000, seed=9, spec_over={"land": "none"},
+                             param_over={"scheme": 0, "hturb_on": 0})
+    ref, T0 = harness.run_gpu(case, 48, noise="philox", seed=21)
+    mix, T1 = harness.run_gpu(case, 48, noise="philox", seed=21, field_dtype="mixed")
+    hr, hm = _column_hist(ref), _column_hist(mix)
+    print("fp64 profile:", hr.tolist())
+    print("mixed profile:", hm.tolist())
+    assert np.all(np.abs(hm - hr) <= 3 * np.sqrt(np.maximum(hr, 1)))
+    assert np.abs(hm - hr).sum() < 0.02 * hr.sum()
+    T0.close()
+    T1.close()
+
+
+def test_mixed_set_get_roundtrip_and_noalloc_refused():
+    import ctypes as C
+    from romspath_b200 import Tracker, schedule
+    case = harness.make_case("tiny", 64, seed=2)
+    T = Tracker(case.specs, case.grids, case.params, numpar=64, field_dtype="mixed", seed=1)
+    for (k, slot) in schedule.initial_loads():
+        T.upload_frame(1, slot, case.frame(k))
+    T.locate(case.release, t_b=1)
+    st = T.get_particles()
+    rng = np.random.default_rng(0)
+    x = st["x"] + rng.uniform(-0.3, 0.3, 64)
+    T.set_particles(x, st["y"], st["z"], case.release.dob, st["age"], st["status"], st["gid"], st["isin"])
+    back = T.get_particles()
+    assert np.allclose(back["x"], x, rtol=0, atol=1e-12)
+    S = T.device_state()
+    assert np.isclose(np.asarray(back["x"]).sum(), x.sum())
+    exa = (C.c_double * 3)(0.0, 3600.0, 7200.0)
+    rc = T.L.rp_step_noalloc(T.h, C.byref(S), exa, exa, 2, 1, 2, 3)
+    assert rc == -5
+    T.close()
