@@ -3,12 +3,18 @@
 
 Workload (the plain-method-at-scale configuration): one ROMS grid of
 512 x 384 rho points x 30 s-levels (Vtransform 2 / Vstretching 4), 8 %
-seeded island land mask, analytic double gyre + M2 tide fields stored in
+seeded island land mask, analytic double gyre + M2 tide fields supplied in
 FP32 with a 0.05 m/s surface Stokes drift (e-folding 5 m) added on upload,
 horizontal diffusivity Kh = 1 m^2/s, the vertical random displacement model
 on a 30 s sub-step, 1,048,576 particles released uniformly in (x, y, s),
-idt = 300 s, hourly frames.  Arithmetic is FP64 (bit-identical to the CPU
-oracle).  Inputs are synthetic (no ocean-model output on this machine).
+idt = 300 s, hourly frames.  Inputs are synthetic (no ocean-model output on
+this machine).
+
+Three forms of the step are timed on it, one after the other:
+  mixed  (headline) FP16 u/v/w/AKs with per-level scales, FP32 positions
+         with Kahan compensation, FP64 age and smoothing spline;
+  f32    FP64 arithmetic on FP32-stored fields (bit-identical to the oracle);
+  f64    plain FP64 (FP64-stored fields; bit-identical to the oracle).
 
 One benchmark step = one hydrodynamic frame interval = 12 internal steps
 (update_particles calls) over all particles.
@@ -20,6 +26,7 @@ One benchmark step = one hydrodynamic frame interval = 12 internal steps
           back (the dataOutput columns), host clock between device syncs.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+  python bench.py --error-study [--workload cfg3 --days 10 --deterministic]
 
 For N > 1 (torchrun), each rank advances its own 1,048,576 particles
 (replicas of the fields, no collective on the data path: weak scaling);
@@ -43,8 +50,7 @@ sys.path.insert(0, ROOT)
 
 from romspath_b200 import schedule, synth  # noqa: E402
 
-B_ALG = {"cfg2": 3192, "cfg1": 5288}   # algorithmic bytes per particle-step
-WORKLOAD_DESC = ("cfg2: 512x384x30 ROMS grid, 8% islands, FP32-stored u/v/w/AKs/zeta + Stokes, "
+WORKLOAD_DESC = ("cfg2: 512x384x30 ROMS grid, 8% islands, FP32 u/v/w/AKs/zeta frames + Stokes, "
                  "Kh=1 m^2/s, VTurb dt_turb=30 s, RK4 idt=300 s")
 
 
@@ -59,6 +65,19 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=32768, help="particles in the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--form", default="mixed", choices=["mixed", "exact"],
+                    help="headline form: mixed precision (default) or exact FP64 arithmetic on the workload's "
+                         "field storage; the other forms are timed beside it")
+    ap.add_argument("--error-study", action="store_true",
+                    help="instead of timing: run the exact and the mixed form in lockstep on the same "
+                         "frames and noise and report the mixed form's position / profile error")
+    ap.add_argument("--days", type=float, default=10.0, help="error study length")
+    ap.add_argument("--deterministic", action="store_true", help="error study with turbulence off")
+    ap.add_argument("--mixed-kind", default="mixed", choices=["mixed", "mixed-i16"],
+                    help="16-bit field storage of the mixed form: FP16 (default) or int16 fixed point")
+    ap.add_argument("--perturb", type=float, default=0.0,
+                    help="error study of the exact form against itself with initial x, y moved by up to "
+                         "this many grid cells (the flow's own sensitivity)")
     return ap.parse_args()
 
 
@@ -72,15 +91,16 @@ def measured_peaks():
 
 def profile_traffic(workload, kernel):
     """DRAM bytes per launch of `kernel` from the committed ncu summary of
-    the same workload, or None when the summary covers another kernel."""
+    the same workload, or None when no summary covers that kernel."""
     p = os.path.join(ROOT, "profiles", f"step_{workload}_traffic.json")
     if os.path.exists(p):
         try:
             d = json.load(open(p))
         except Exception:
             return None
-        if d.get("kernel") == kernel:
-            return d.get("dram_bytes_per_launch")
+        k = d.get("kernels", {}).get(kernel)
+        if k:
+            return k.get("dram_bytes_per_launch")
     return None
 
 
@@ -207,12 +227,122 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------ error study
+
+MOVED = (1.0, float(np.float32(1.1)), float(np.float32(1.2)))
+
+
+def error_stats(ref, mix, spec):
+    """Mixed-form error against the exact form: horizontal position (grid
+    cells) and depth (m) over particles active in both, the vertical
+    concentration profile (20 bins of the water-column fraction) and the
+    horizontal one (cells of 8 x 8 rho points), as L1 distances of the
+    normalised histograms."""
+    ok = np.isin(ref["status"], MOVED) & np.isin(mix["status"], MOVED)
+    dh = np.hypot(mix["x"] - ref["x"], mix["y"] - ref["y"])[ok]
+    dz = (mix["z"] - ref["z"])[ok]
+    depth = (ref["bath"] + ref["zeta"])[ok]
+    frac = lambda st: ((st["z"] + st["bath"]) / (st["bath"] + st["zeta"]))[ok]
+    hv = [np.histogram(frac(st), bins=20, range=(0.0, 1.0))[0] for st in (ref, mix)]
+    bx, by = np.arange(0, spec.xi_rho + 8, 8), np.arange(0, spec.eta_rho + 8, 8)
+    hh = [np.histogram2d(st["x"][ok], st["y"][ok], bins=(bx, by))[0] for st in (ref, mix)]
+    n = max(int(ok.sum()), 1)
+    return {"particles_compared": int(ok.sum()), "status_agreement": float(np.mean(ref["status"] == mix["status"])),
+            "rms_position_cells": float(np.sqrt(np.mean(dh ** 2))) if dh.size else None,
+            "median_position_cells": float(np.median(dh)) if dh.size else None,
+            "p99_position_cells": float(np.percentile(dh, 99)) if dh.size else None,
+            "max_position_cells": float(dh.max()) if dh.size else None,
+            "rms_depth_m": float(np.sqrt(np.mean(dz ** 2))) if dz.size else None,
+            "rms_depth_frac_of_column": float(np.sqrt(np.mean((dz / depth) ** 2))) if dz.size else None,
+            "vertical_profile_L1": float(np.abs(hv[0] - hv[1]).sum() / n),
+            "horizontal_profile_L1": float(np.abs(hh[0] - hh[1]).sum() / n)}
+
+
+def error_study(args):
+    """The mixed form against the exact FP64 form (bit-identical to the CPU
+    restatement of the reference, by the parity tests) on one GPU: same
+    grid, frames, release and Philox noise, stepped in lockstep."""
+    from romspath_b200 import Tracker
+    wl = args.workload
+    spec = synth.config_spec(wl)[0]
+    grid = synth.make_grid(spec)
+    params = dict(synth.config_params(wl))
+    if args.deterministic:
+        params.update(vturb_on=0, hturb_on=0)
+    npart = args.particles or 65536
+    cache = {}
+
+    def frame(k):
+        if k not in cache:
+            cache[k] = synth.make_frame(spec, grid, (k - 1) * float(params["dt"]))
+            for old in [j for j in cache if j < k - 3]:
+                del cache[old]
+        return cache[k]
+
+    rel = synth.uniform_release(spec, grid, frame(1), npart, seed=0)
+    forms = {"exact": spec.field_dtype, "mixed": spec.field_dtype if args.perturb > 0 else args.mixed_kind}
+    T = {f: Tracker([spec], [grid], params, numpar=npart, field_dtype=d, stokes=spec.stokes, seed=7)
+         for f, d in forms.items()}
+    for (k, slot) in schedule.initial_loads():
+        for t in T.values():
+            t.upload_frame(1, slot, frame(k))
+    for t in T.values():
+        t.locate(rel, t_b=1)
+    if args.perturb > 0:
+        st = T["mixed"].get_particles()
+        rng = np.random.default_rng(1)
+        dx, dy = rng.uniform(-args.perturb, args.perturb, (2, npart))
+        T["mixed"].set_particles(st["x"] + dx, st["y"] + dy, st["z"], rel.dob, st["age"], st["status"], st["gid"],
+                                 st["isin"])
+    out = {"mode": "error-study", "workload": wl, "days": args.days, "particles": npart,
+           "compared_form": (f"exact, initial x/y perturbed by U(-{args.perturb}, {args.perturb}) cells"
+                             if args.perturb > 0 else args.mixed_kind),
+           "turbulence": "off" if args.deterministic else "as configured (same Philox noise in both forms)",
+           "reference_form": f"exact FP64 arithmetic on {spec.field_dtype}-stored fields", "checkpoints": []}
+    t0 = time.time()
+    day_steps = 86400 // int(params["idt"])
+    done = 0
+    for ext in schedule.external_steps(args.days, int(params["dt"]), int(params["idt"])):
+        for (k, slot) in ext.loads:
+            for t in T.values():
+                t.upload_frame(1, slot, frame(k))
+        for it in ext.internal:
+            for t in T.values():
+                t.step(it.ex, it.ix, it.ets, it.tb, it.tc, it.tf)
+            done += 1
+            if done % day_steps == 0:
+                st = {f: t.get_particles() for f, t in T.items()}
+                e = error_stats(st["exact"], st["mixed"], spec)
+                e["day"] = done / day_steps
+                out["checkpoints"].append(e)
+    out["wall_s"] = time.time() - t0
+    for t in T.values():
+        t.close()
+    print(json.dumps(out), flush=True)
+
+
 # ------------------------------------------------------------------ GPU arm
+
+FORM_DESC = {
+    "mixed": "mixed precision: FP16 u/v/w/AKs with per-level power-of-two scales, FP32 zeta, FP32 positions with "
+             "Kahan compensation, FP32 interpolation/RK4, FP64 age, smoothing-spline fit and sub-steps",
+    "mixed-i16": "mixed precision with int16 fixed-point u/v/w/AKs (scale = level max / 32767)",
+    "f32": "exact: FP64 arithmetic on FP32-stored fields (bit-identical to the CPU oracle)",
+    "f64": "plain FP64: FP64-stored fields, FP64 arithmetic (bit-identical to the CPU oracle)",
+}
+KERNEL = {"mixed": "k_step_mixed", "mixed-i16": "k_step_mixed", "f32": "k_step_fused", "f64": "k_step_fused"}
+# algorithmic bytes per particle-step of each form on the cfg2 / cfg3 grids
+B_ALG_FORM = {("cfg2", "mixed"): 1872, ("cfg2", "mixed-i16"): 1872, ("cfg2", "f32"): 3192, ("cfg2", "f64"): 6248,
+              ("cfg3", "mixed"): 1632, ("cfg3", "mixed-i16"): 1632, ("cfg3", "f64"): 5288, ("cfg1", "f64"): 5288}
+
 
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.error_study:
+        error_study(args)
         return
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -236,18 +366,9 @@ def main():
     nframes = 4
     frames = [synth.make_frame(spec, grid, k * 3600.0) for k in range(nframes)]
     rel = synth.uniform_release(spec, grid, frames[0], npart, seed=rank)
-
-    T = Tracker([spec], [grid], params, numpar=npart, field_dtype=spec.field_dtype, stokes=spec.stokes,
-                seed=7, device=local)
-    T.set_id_base(rank * npart)         # global particle ids: rank r holds [r*npart, (r+1)*npart)
-    for k, slot in enumerate((1, 2, 3)):
-        T.upload_frame(1, slot, frames[k])
-    T.locate(rel, t_b=1)
-    T.synchronize()
-    st = T.device_state()
-    stream = torch.cuda.ExternalStream(st.stream, device=torch.device("cuda", local))
-
     exts = list(schedule.external_steps(30.0, int(params["dt"]), int(params["idt"])))
+    head = args.mixed_kind if args.form == "mixed" else spec.field_dtype
+    forms = [head] + [f for f in (spec.field_dtype, "f64") if f != head]
 
     def barrier():
         if dist is not None:
@@ -260,46 +381,74 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # ---------------- value: device-resident, K frame intervals of 12 steps
-    def resident_steps(e0, n_ext, record):
-        evs = []
-        for e in exts[e0:e0 + n_ext]:
-            for it in e.internal:
-                if record:
-                    a = torch.cuda.Event(enable_timing=True)
-                    b = torch.cuda.Event(enable_timing=True)
-                    a.record(stream)
-                T.step(it.ex, it.ix, it.ets, 1, 2, 3)
-                if record:
-                    b.record(stream)
-                    evs.append((a, b))
-        return evs
+    def make_tracker(form):
+        T = Tracker([spec], [grid], params, numpar=npart, field_dtype=form, stokes=spec.stokes, seed=7,
+                    device=local)
+        T.set_id_base(rank * npart)     # global particle ids: rank r holds [r*npart, (r+1)*npart)
+        for k, slot in enumerate((1, 2, 3)):
+            T.upload_frame(1, slot, frames[k])
+        T.locate(rel, t_b=1)
+        T.synchronize()
+        return T
 
-    resident_steps(2, args.warmup, False)
-    T.synchronize()
-    barrier()
-    torch.cuda.synchronize()
-    sampler = ClockSampler(local)
-    sampler.start()
-    launches0 = T.kernel_launches()
-    t_start = torch.cuda.Event(enable_timing=True)
-    t_end = torch.cuda.Event(enable_timing=True)
-    t_start.record(stream)
-    evs = resident_steps(2 + args.warmup, args.steps, True)
-    t_end.record(stream)
-    T.synchronize()
-    torch.cuda.synchronize()
-    clocks = sampler.stop()
-    launches = T.kernel_launches() - launches0
-    region_ms = max_over_ranks(t_start.elapsed_time(t_end))
-    kern_ms = [a.elapsed_time(b) for a, b in evs]
-    avg_kernel_ms = max_over_ranks(float(np.mean(kern_ms)))
-    ms_per_step = region_ms / args.steps
-    total_ps = npart * 12 * args.steps * world
-    value = total_ps / (region_ms / 1e3)
+    def time_resident(T, clocks_on):
+        """W untimed + K timed frame intervals (12 internal steps each) on
+        device-resident frames and particles; CUDA events on the library's
+        compute stream."""
+        st = T.device_state()
+        stream = torch.cuda.ExternalStream(st.stream, device=torch.device("cuda", local))
 
-    # ---------------- e2e: frames up, particles back, pinned host buffers
+        def run(e0, n_ext, record):
+            evs = []
+            for e in exts[e0:e0 + n_ext]:
+                for it in e.internal:
+                    if record:
+                        a = torch.cuda.Event(enable_timing=True)
+                        b = torch.cuda.Event(enable_timing=True)
+                        a.record(stream)
+                    T.step(it.ex, it.ix, it.ets, 1, 2, 3)
+                    if record:
+                        b.record(stream)
+                        evs.append((a, b))
+            return evs
+
+        run(2, args.warmup, False)
+        T.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        sampler = ClockSampler(local) if clocks_on else None
+        if sampler:
+            sampler.start()
+        l0 = T.kernel_launches()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        evs = run(2 + args.warmup, args.steps, True)
+        t1.record(stream)
+        T.synchronize()
+        torch.cuda.synchronize()
+        clocks = sampler.stop() if sampler else None
+        region_ms = max_over_ranks(t0.elapsed_time(t1))
+        kern = max_over_ranks(float(np.mean([a.elapsed_time(b) for a, b in evs])))
+        return {"region_ms": region_ms, "avg_launch_ms": kern, "launches": T.kernel_launches() - l0,
+                "clocks": clocks}
+
+    results = {}
     e2e = None
+    head_T = None
+    for form in forms:
+        T = make_tracker(form)
+        r = time_resident(T, form == head)
+        r["value"] = npart * 12 * args.steps * world / (r["region_ms"] / 1e3)
+        r["ms_per_step"] = r["region_ms"] / args.steps
+        results[form] = r
+        if form == head:
+            head_T = T
+        else:
+            T.close()
+
+    # ---------------- e2e of the headline form: frames up, particles back
+    T = head_T
     if not args.no_e2e:
         keep = []
         pframes = []
@@ -343,21 +492,26 @@ def main():
         e2e = {"value": npart * 12 * args.steps * world / e2e_s, "unit": "particle-steps/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "ms_per_step": e2e_s * 1e3 / args.steps, "gpu_launches": T.kernel_launches() - l0,
-               "timing": "host clock between device synchronizations; frames and particle columns in "
-                         "page-locked host memory"}
+               "form": head,
+               "timing": "host clock between device synchronizations; every step uploads one frame "
+                         "(quantised on the device in the mixed form) and reads the particle columns "
+                         "back into page-locked host memory"}
+    T.close()
 
-    # ---------------- roofline of the step kernel (algorithmic bytes)
+    # ---------------- roofline of the headline step kernel (algorithmic bytes)
+    hr = results[head]
     peak, peak_src = measured_peaks()
-    balg = B_ALG.get(wl, 3192)
-    achieved = balg * npart / (avg_kernel_ms / 1e3) / 1e9
-    traffic = profile_traffic(wl, "k_step_fused")
+    balg = B_ALG_FORM.get((wl, head), 1872)
+    achieved = balg * npart / (hr["avg_launch_ms"] / 1e3) / 1e9
+    traffic = profile_traffic(wl, KERNEL[head])
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
-                "dram_gbs_from_traffic": (traffic / (avg_kernel_ms / 1e3) / 1e9) if traffic else None,
-                "note": "achieved counts the field and particle bytes the reference arithmetic consumes; "
-                        "the DRAM traffic is dominated by the smoothing-spline workspace (see profiles/)",
-                "kernel": "k_step_fused (one launch per internal step)",
-                "avg_launch_ms": avg_kernel_ms,
+                "dram_gbs_from_traffic": (traffic / (hr["avg_launch_ms"] / 1e3) / 1e9) if traffic else None,
+                "note": "achieved counts the field and particle bytes the reference arithmetic consumes at the "
+                        "form's storage widths; DRAM traffic is dominated by the smoothing-spline workspace in "
+                        "local memory (see profiles/)",
+                "kernel": f"{KERNEL[head]} (one launch per internal step)",
+                "avg_launch_ms": hr["avg_launch_ms"],
                 "algorithmic_bytes": f"{balg} B/particle-step x {npart} particles per launch"}
 
     cpu = None
@@ -369,20 +523,26 @@ def main():
                          f"{threads} OpenMP threads (FP64 C restatement of the reference; the Fortran "
                          f"reference cannot be built here)"}
 
-    T.close()
     if rank == 0:
+        plain = results.get("f64")
         line = {
-            "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "metric": "particle-steps/s", "value": hr["value"], "unit": "particle-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": hr["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f16/f32/f64 (mixed)" if head.startswith("mixed") else "f64",
             "data": "synthetic (analytic ROMS-shaped fields, seeded release)",
             "config": {"workload": WORKLOAD_DESC, "particles_per_gpu": npart,
                        "step": "one hydro frame interval = 12 internal steps (idt=300 s)",
-                       "form": "plain FP64 arithmetic, FP32-stored fields (bit-identical to the oracle)",
-                       "l2": "inputs larger than L2 (frame ring ~390 MB, particle state ~80 MB)",
+                       "form": FORM_DESC[head],
+                       "l2": "inputs larger than L2 (frame ring 390 MB FP32 / 195 MB FP16, particle state "
+                             "~80 MB, spline workspace in local memory ~0.5-1 GB)",
                        "parallelism": f"replicas x{world}: particles split per rank, no data-path collective"},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
-            "gpu_launches": int(launches),
+            "forms": {f: {"value": r["value"], "ms_per_step": r["ms_per_step"],
+                          "avg_launch_ms": r["avg_launch_ms"], "desc": FORM_DESC[f],
+                          "speedup_vs_plain_fp64": (r["value"] / plain["value"]) if plain else None}
+                      for f, r in results.items()},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": hr["clocks"],
+            "gpu_launches": int(hr["launches"]),
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -61,6 +61,10 @@ extern "C" {
  * previous step.  Not bit-exact; its error against RP_FIELD_F64 on the
  * same noise is measured by the tests. */
 #define RP_FIELD_MIXED 2
+/* The same form with u, v, w, AKs in int16 fixed point, scale = level
+ * max / 32767 (15 bits for the largest values of a level, where FP16 keeps
+ * 11; absolute rather than relative resolution below them). */
+#define RP_FIELD_MIXED_I16 3
 
 /* Run parameters: the namelist values the hot path reads (ROMSPath.h:77-80
  * timeparam, 140-148 turbparam, 152-154 advectparam, 161-180 behavparam,

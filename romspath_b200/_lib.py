@@ -14,7 +14,7 @@ NOALLOC_MAX_PARTICLES = 1048576
 RP_OK = 0
 ERRORS = {-1: "RP_ERR_ARG", -2: "RP_ERR_CUDA", -3: "RP_ERR_STATE", -4: "RP_ERR_NOMEM",
           -5: "RP_ERR_UNSUPPORTED", -6: "RP_ERR_NOEXT"}
-FIELD_F64, FIELD_F32, FIELD_MIXED = 0, 1, 2
+FIELD_F64, FIELD_F32, FIELD_MIXED, FIELD_MIXED_I16 = 0, 1, 2, 3
 FLAG_OOB, FLAG_NODE, FLAG_WBOT, FLAG_WTOP, FLAG_SPLINE = 1, 2, 4, 8, 16
 
 EXPORTS = [

@@ -41,7 +41,8 @@ struct rp_ctx {
     int device = 0;
     int num_sms = 148;
     int elem = 8;                              // bytes per stored field value (FP64/FP32 forms)
-    bool mixed = false;                        // RP_FIELD_MIXED
+    bool mixed = false;                        // RP_FIELD_MIXED or RP_FIELD_MIXED_I16
+    bool i16 = false;                          // RP_FIELD_MIXED_I16: int16 fixed point instead of FP16
     int npmax = 0;
     GridBuf g[RP_MAXNGRID];
     // particle state
@@ -287,7 +288,7 @@ int upload_field(rp_ctx* ctx, const S* src, const S* add, void* dst, int ni, int
         ctx->pin_used[h] = true;
     }
     if (qs) {
-        CK(rp::launch_quantize(ctx->ftmp, ctx->qmax, qs, dst, ni, nj, nk, phys, ctx->num_sms, ctx->s_copy));
+        CK(rp::launch_quantize(ctx->ftmp, ctx->qmax, qs, dst, ni, nj, nk, phys, ctx->i16, ctx->num_sms, ctx->s_copy));
         ctx->launches += 2;
     }
     return RP_OK;
@@ -349,7 +350,8 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
     if (p.behavior != 0) return RP_ERR_UNSUPPORTED;
     if (p.nsb < 0 || p.nsb > 2) return RP_ERR_ARG;
     if (!(p.deltat >= 1.0) || !(p.sub > 0.0)) return RP_ERR_ARG;
-    if (p.field_dtype != RP_FIELD_F64 && p.field_dtype != RP_FIELD_F32 && p.field_dtype != RP_FIELD_MIXED)
+    if (p.field_dtype != RP_FIELD_F64 && p.field_dtype != RP_FIELD_F32 && p.field_dtype != RP_FIELD_MIXED &&
+        p.field_dtype != RP_FIELD_MIXED_I16)
         return RP_ERR_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= p.device || p.device < 0) return RP_ERR_NOEXT;
@@ -358,7 +360,8 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
     ctx->ngrid = ngrid;
     ctx->device = p.device;
     ctx->elem = (p.field_dtype == RP_FIELD_F32) ? 4 : 8;
-    ctx->mixed = (p.field_dtype == RP_FIELD_MIXED);
+    ctx->mixed = (p.field_dtype == RP_FIELD_MIXED || p.field_dtype == RP_FIELD_MIXED_I16);
+    ctx->i16 = (p.field_dtype == RP_FIELD_MIXED_I16);
     ctx->ndraw = 2 + p.idt / (int)p.deltat;
     auto bail = [&](int code, const std::string& m) {
         std::fprintf(stderr, "rp_create: %s\n", m.c_str());
@@ -610,7 +613,7 @@ int rp_step(rp_ctx* ctx, const double ex[3], const double ix[3], int32_t ets, in
     int nl = 0;
     CK(cudaEventRecord(ctx->ev0, s));
     if (ctx->n > 0 && ctx->mixed)
-        CK(rp::launch_step_mixed(A, ctx->npmax, s, ctx->num_sms, &nl));
+        CK(rp::launch_step_mixed(A, ctx->npmax, ctx->i16, s, ctx->num_sms, &nl));
     else if (ctx->n > 0)
         CK(rp::launch_step(A, ctx->prm.field_dtype, ctx->npmax, ctx->turbv, ctx->prm.reserved[0] == 1 ? 0 : 1, s,
                            ctx->num_sms, &nl));

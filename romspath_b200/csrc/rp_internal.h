@@ -32,14 +32,15 @@ constexpr int64_t kNoallocMaxParticles = 1048576;
 cudaError_t launch_step_noalloc(const RpStepArgs& A, int field_dtype, int npmax, int device, cudaStream_t s,
                                 int num_sms, int* nlaunch);
 
-// Mixed-precision form (rp_mixed.cu): the step, the FP16 quantisation of a
+// Mixed-precision form (rp_mixed.cu): the step, the 16-bit (FP16 or int16
+// fixed point, `i16`) quantisation of a
 // frame field staged as FP32 (Fortran order), and the conversions between
 // the FP64 columns and the compensated FP32 positions.
-cudaError_t launch_step_mixed(const RpStepArgs& A, int npmax, cudaStream_t s, int num_sms, int* nlaunch);
+cudaError_t launch_step_mixed(const RpStepArgs& A, int npmax, int i16, cudaStream_t s, int num_sms, int* nlaunch);
 cudaError_t launch_stage_f32(int src_f32, const void* src, const void* add, float* dst, int64_t e0, int64_t count,
                              cudaStream_t s);
 cudaError_t launch_quantize(const float* f, uint32_t* maxbits, float* qs, void* dst, int ni, int nj, int nk, int slot,
-                            int num_sms, cudaStream_t s);
+                            int i16, int num_sms, cudaStream_t s);
 cudaError_t launch_mixed_convert(const RpParticlesDev& P, int to_f64, cudaStream_t s);
 
 cudaError_t launch_locate(const RpStepArgs& A, int field_dtype, const double* ipos, const double* jpos,

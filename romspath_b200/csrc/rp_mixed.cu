@@ -5,39 +5,47 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "rp_internal.h"
 #include "rp_mixed.cuh"
 
 namespace rp {
 
-template <int NPMAX>
+template <typename E, int NPMAX>
 __global__ void __launch_bounds__(kStepBlock, kMixedMinBlocks) k_step_mixed(const __grid_constant__ RpStepArgs A) {
     double buf[kMixedArrays * (NPMAX + 1)];
     const MSpline<NPMAX> w{buf};
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < A.p.n; n += stride)
-        m_update_one<NPMAX>(A, n, w);
+        m_update_one<E, NPMAX>(A, n, w);
 }
 
-template <int NPMAX>
+template <typename E, int NPMAX>
 static cudaError_t launch_mixed_t(const RpStepArgs& A, cudaStream_t s, int num_sms, int* nlaunch) {
     int occ = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_step_mixed<NPMAX>, kStepBlock, 0);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_step_mixed<E, NPMAX>, kStepBlock, 0);
     if (e != cudaSuccess) return e;
     if (occ < 1) occ = 1;
     int64_t blocks = (int64_t)num_sms * occ;
     const int64_t need = (A.p.n + kStepBlock - 1) / kStepBlock;
     if (need < blocks) blocks = need;
     if (blocks < 1) blocks = 1;
-    k_step_mixed<NPMAX><<<(unsigned)blocks, kStepBlock, 0, s>>>(A);
+    k_step_mixed<E, NPMAX><<<(unsigned)blocks, kStepBlock, 0, s>>>(A);
     *nlaunch += 1;
     return cudaGetLastError();
 }
 
-cudaError_t launch_step_mixed(const RpStepArgs& A, int npmax, cudaStream_t s, int num_sms, int* nlaunch) {
-    if (npmax <= 88) return launch_mixed_t<88>(A, s, num_sms, nlaunch);
-    if (npmax <= 128) return launch_mixed_t<128>(A, s, num_sms, nlaunch);
-    return launch_mixed_t<144>(A, s, num_sms, nlaunch);
+template <typename E>
+static cudaError_t launch_mixed_e(const RpStepArgs& A, int npmax, cudaStream_t s, int num_sms, int* nlaunch) {
+    if (npmax <= 88) return launch_mixed_t<E, 88>(A, s, num_sms, nlaunch);
+    if (npmax <= 128) return launch_mixed_t<E, 128>(A, s, num_sms, nlaunch);
+    return launch_mixed_t<E, 144>(A, s, num_sms, nlaunch);
+}
+
+cudaError_t launch_step_mixed(const RpStepArgs& A, int npmax, int i16, cudaStream_t s, int num_sms, int* nlaunch) {
+    return i16 ? launch_mixed_e<int16_t>(A, npmax, s, num_sms, nlaunch)
+               : launch_mixed_e<__half>(A, npmax, s, num_sms, nlaunch);
 }
 
 // ------------------------------------------------------ frame upload
@@ -85,34 +93,45 @@ __global__ void k_level_maxabs(const float* __restrict__ f, int64_t plane, uint3
     }
 }
 
-// the power-of-two scale of a level: |v| / scale <= 16384 (exact scaling)
-__device__ __forceinline__ float m_level_scale(uint32_t bits) {
+// The scale of a level.  FP16: the power of two with |v| / scale <= 16384
+// (exact scaling, keeps w and AKs out of the FP16 subnormal range).  int16:
+// level max / 32767.
+__device__ __forceinline__ float m_level_scale(uint32_t bits, bool i16) {
     const float mx = __uint_as_float(bits);
     if (!(mx > 0.f) || !(mx < 3.0e38f)) return 1.0f;
+    if (i16) return mx / 32767.0f;
     int e = 0;
     frexpf(mx, &e);                        // mx = m 2^e, m in [0.5, 1)
     return ldexpf(1.0f, e - 14);
 }
 
-// FP32 field (Fortran order) -> FP16 device layout [j][i][k][slot4] and the
-// per-level scales qs[slot][k]
+__device__ __forceinline__ void m_store16(__half* d, float v) { *d = __float2half_rn(v); }
+__device__ __forceinline__ void m_store16(int16_t* d, float v) {
+    const float r = fminf(fmaxf(rintf(v), -32767.0f), 32767.0f);
+    *d = (int16_t)r;
+}
+
+// FP32 field (Fortran order) -> 16-bit device layout [j][i][k][slot4] and
+// the per-level scales qs[slot][k]
+template <typename E>
 __global__ void k_quantize(const float* __restrict__ f, const uint32_t* __restrict__ maxbits, float* __restrict__ qs,
-                           __half* __restrict__ dst, int ni, int nj, int nk, int slot) {
+                           E* __restrict__ dst, int ni, int nj, int nk, int slot) {
+    constexpr bool i16 = sizeof(E) == 2 && !std::is_same<E, __half>::value;
     const int64_t plane = (int64_t)ni * nj;
     const int64_t total = plane * nk;
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e < nk) qs[slot * nk + e] = m_level_scale(maxbits[e]);
+    if (e < nk) qs[slot * nk + e] = m_level_scale(maxbits[e], i16);
     if (e >= total) return;
     const int k = (int)(e / plane);
     const int64_t r = e - (int64_t)k * plane;
     const int j = (int)(r / ni);
     const int i = (int)(r - (int64_t)j * ni);
-    const float inv = 1.0f / m_level_scale(maxbits[k]);
-    dst[(((int64_t)j * ni + i) * nk + k) * RP_SLOTS + slot] = __float2half_rn(f[e] * inv);
+    const float sc = m_level_scale(maxbits[k], i16);
+    m_store16(dst + (((int64_t)j * ni + i) * nk + k) * RP_SLOTS + slot, i16 ? f[e] / sc : f[e] * (1.0f / sc));
 }
 
 cudaError_t launch_quantize(const float* f, uint32_t* maxbits, float* qs, void* dst, int ni, int nj, int nk, int slot,
-                            int num_sms, cudaStream_t s) {
+                            int i16, int num_sms, cudaStream_t s) {
     cudaError_t e = cudaMemsetAsync(maxbits, 0, sizeof(uint32_t) * nk, s);
     if (e != cudaSuccess) return e;
     const int64_t plane = (int64_t)ni * nj;
@@ -124,7 +143,8 @@ cudaError_t launch_quantize(const float* f, uint32_t* maxbits, float* qs, void* 
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const int64_t total = plane * nk;
     const unsigned blocks = (unsigned)((total + block - 1) / block);
-    k_quantize<<<blocks, block, 0, s>>>(f, maxbits, qs, (__half*)dst, ni, nj, nk, slot);
+    if (i16) k_quantize<int16_t><<<blocks, block, 0, s>>>(f, maxbits, qs, (int16_t*)dst, ni, nj, nk, slot);
+    else k_quantize<__half><<<blocks, block, 0, s>>>(f, maxbits, qs, (__half*)dst, ni, nj, nk, slot);
     return cudaGetLastError();
 }
 

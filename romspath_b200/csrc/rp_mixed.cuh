@@ -9,6 +9,8 @@
 //     in FP64, with the secant search for the smoothing parameter started
 //     from the particle's value of the previous step (one chol1d pass when
 //     it still meets smooth()'s 1 % criterion).
+// The 16-bit storage is FP16 (RP_FIELD_MIXED) or int16 fixed point
+// (RP_FIELD_MIXED_I16, |v| / scale <= 32767 with scale = level max / 32767).
 // Results differ from the exact form by rounding; the error is measured
 // against the FP64 form on identical noise.
 #pragma once
@@ -204,12 +206,16 @@ __device__ __forceinline__ void m_walk(const double* s, const double* cs, int nz
     }
 }
 
+// one stored 16-bit field value (before its level scale): FP16, or int16
+// fixed point
 __device__ __forceinline__ float m_h(const __half* f, int64_t idx) { return __half2float(__ldg(f + idx)); }
+__device__ __forceinline__ float m_h(const int16_t* f, int64_t idx) { return (float)__ldg(f + idx); }
 
 // zcff1*zprof(Ibot) + zcff2*zprof(Itop) of one slot of an FP16 field
+template <typename E>
 __device__ __forceinline__ float m_col(const void* fv, const float* qs, const int64_t o[4], const float cff[4],
                                        const bool use[4], int nlev, const MPick& L, int slot) {
-    const __half* f = reinterpret_cast<const __half*>(fv);
+    const E* f = reinterpret_cast<const E*>(fv);
     float pb = 0.f, pt = 0.f;
 #pragma unroll
     for (int k = 0; k < 4; k++) {
@@ -261,7 +267,9 @@ __device__ __forceinline__ void m_stage_2d(const MPol& P, const RpGridDev& g, MS
     S.zeta = m_polintd(P, S.zb, S.zc, S.zf);
 }
 
-// with cell_ready the caller has already filled S.rc for (X, Y)
+// with cell_ready the caller has already filled S.rc for (X, Y); E is the
+// 16-bit storage type of u, v, w (and AKs)
+template <typename E>
 __device__ __forceinline__ void m_find_currents(const RpStepArgs& A, const MPol& P, const RpGridDev& g, float X,
                                                 float Y, float& Z, float& U, float& V, float& Wv, MStage& S,
                                                 bool cell_ready, uint32_t& fl) {
@@ -277,22 +285,22 @@ __device__ __forceinline__ void m_find_currents(const RpStepArgs& A, const MPol&
     MUV cu, cv;
     m_uv_cell(g, X, Y, true, cu, fl);
     m_uv_cell(g, X, Y, false, cv, fl);
-    const float Ub = m_col(g.u, g.qs_u, cu.o, cu.cff, cu.use, N, Lr, g.sb);
-    const float Uc = m_col(g.u, g.qs_u, cu.o, cu.cff, cu.use, N, Lr, g.sc);
-    const float Vb = m_col(g.v, g.qs_v, cv.o, cv.cff, cv.use, N, Lr, g.sb);
-    const float Vc = m_col(g.v, g.qs_v, cv.o, cv.cff, cv.use, N, Lr, g.sc);
+    const float Ub = m_col<E>(g.u, g.qs_u, cu.o, cu.cff, cu.use, N, Lr, g.sb);
+    const float Uc = m_col<E>(g.u, g.qs_u, cu.o, cu.cff, cu.use, N, Lr, g.sc);
+    const float Vb = m_col<E>(g.v, g.qs_v, cv.o, cv.cff, cv.use, N, Lr, g.sb);
+    const float Vc = m_col<E>(g.v, g.qs_v, cv.o, cv.cff, cv.use, N, Lr, g.sc);
     const bool all[4] = {true, true, true, true};
     const float* cw = S.rc.wet4 ? S.rc.cb : S.rc.ci;
-    const float Wb = m_col(g.w, g.qs_w, S.rc.o, cw, all, N + 1, Lw, g.sb);
-    const float Wc = m_col(g.w, g.qs_w, S.rc.o, cw, all, N + 1, Lw, g.sc);
+    const float Wb = m_col<E>(g.w, g.qs_w, S.rc.o, cw, all, N + 1, Lw, g.sb);
+    const float Wc = m_col<E>(g.w, g.qs_w, S.rc.o, cw, all, N + 1, Lw, g.sc);
     if (A.ets == 1) {
         U = m_polintd(P, Ub, Ub, Uc);
         V = m_polintd(P, Vb, Vb, Vc);
         Wv = m_polintd(P, Wb, Wb, Wc);
     } else {
-        const float Uf = m_col(g.u, g.qs_u, cu.o, cu.cff, cu.use, N, Lr, g.sf);
-        const float Vf = m_col(g.v, g.qs_v, cv.o, cv.cff, cv.use, N, Lr, g.sf);
-        const float Wf = m_col(g.w, g.qs_w, S.rc.o, cw, all, N + 1, Lw, g.sf);
+        const float Uf = m_col<E>(g.u, g.qs_u, cu.o, cu.cff, cu.use, N, Lr, g.sf);
+        const float Vf = m_col<E>(g.v, g.qs_v, cv.o, cv.cff, cv.use, N, Lr, g.sf);
+        const float Wf = m_col<E>(g.w, g.qs_w, S.rc.o, cw, all, N + 1, Lw, g.sf);
         U = m_polintd(P, Ub, Uc, Uf);
         V = m_polintd(P, Vb, Vc, Vf);
         Wv = m_polintd(P, Wb, Wc, Wf);
@@ -563,7 +571,7 @@ __device__ __forceinline__ double m_ppvalu(const MSpline<NPMAX>& w, const MFit& 
 
 // VTurb (ver_turb_module.f90:31-329): column in FP32 from FP16 AKs, fit and
 // random-displacement sub-steps in FP64
-template <int NPMAX>
+template <typename E, int NPMAX>
 __device__ float m_vturb(const RpStepArgs& A, const MPol& P, const RpGridDev& g, const MStage& S, float Zpar,
                          uint32_t pid, double& qstate, double& gstate, uint32_t& fl, const MSpline<NPMAX>& w) {
     const int sw = g.N + 1;
@@ -577,7 +585,7 @@ __device__ float m_vturb(const RpStepArgs& A, const MPol& P, const RpGridDev& g,
     const float hc = (float)g.hc;
     const float den_r = 1.f / (hc + h);
     const float* cwt = S.rc.wet4 ? S.rc.cb : S.rc.ci;
-    const __half* aks = reinterpret_cast<const __half*>(g.aks);
+    const E* aks = reinterpret_cast<const E*>(g.aks);
     const int slots[3] = {g.sb, g.sc, g.sf};
     double zprev = 0.0, kprev = 0.0;
     for (int k = 1; k <= sw; k++) {
@@ -645,7 +653,7 @@ __device__ __forceinline__ void m_kahan_add(float& p, float& c, float d) {
 
 // ----------------------------------------------------------- one particle
 
-template <int NPMAX>
+template <typename E, int NPMAX>
 __device__ void m_update_one(const RpStepArgs& A, int64_t n, const MSpline<NPMAX>& w) {
     const RpParticlesDev& Pt = A.p;
     if (!rp_active(A, n)) return;
@@ -687,7 +695,7 @@ __device__ void m_update_one(const RpStepArgs& A, int64_t n, const MSpline<NPMAX
                 ys = Ypar + ky * half_dt;
                 zs = Zpar + kz * half_dt;
             }
-            m_find_currents(A, P, g, xs, ys, zs, U, V, Wv, Sx, false, fl);
+            m_find_currents<E>(A, P, g, xs, ys, zs, U, V, Wv, Sx, false, fl);
             if (st == 0) Zpar = zs;                    // Z is INOUT in find_currents
             kx = U * pm;
             ky = V * pn;
@@ -717,7 +725,7 @@ __device__ void m_update_one(const RpStepArgs& A, int64_t n, const MSpline<NPMAX
     float TurbV = 0.f;
     if (A.vturb_on) {
         double q = Pt.qwarm[n], gs = Pt.gwarm[n];
-        TurbV = m_vturb(A, P, g, S1, Zpar, pid, q, gs, fl, w);
+        TurbV = m_vturb<E>(A, P, g, S1, Zpar, pid, q, gs, fl, w);
         Pt.qwarm[n] = q;
         Pt.gwarm[n] = gs;
     }

@@ -53,8 +53,10 @@ class Tracker:
         P.stokes = int(bool(stokes))
         # "f64" / "f32": fields stored at that width, FP64 arithmetic (exact);
         # "mixed": FP16 fields with per-level scales, FP32 positions with
-        # compensated accumulation, FP64 age and spline fit (not exact)
-        P.field_dtype = {"f64": _lib.FIELD_F64, "f32": _lib.FIELD_F32, "mixed": _lib.FIELD_MIXED}[field_dtype]
+        # compensated accumulation, FP64 age and spline fit (not exact);
+        # "mixed-i16": the same with int16 fixed-point fields
+        P.field_dtype = {"f64": _lib.FIELD_F64, "f32": _lib.FIELD_F32, "mixed": _lib.FIELD_MIXED,
+                         "mixed-i16": _lib.FIELD_MIXED_I16}[field_dtype]
         P.spline_max_iter = int(spline_max_iter)
         for k in ("vertdist", "serr", "smth", "sub", "deltat", "aksback"):
             setattr(P, k, float(params[k]))
