@@ -24,7 +24,7 @@ struct GridBuf {
     double *sr = nullptr, *csr = nullptr, *sw = nullptr, *csw = nullptr;
     uint8_t *mrho = nullptr, *mu = nullptr, *mv = nullptr;
     void *zeta = nullptr, *u = nullptr, *v = nullptr, *w = nullptr, *aks = nullptr;
-    float *qs_u = nullptr, *qs_v = nullptr, *qs_w = nullptr, *qs_aks = nullptr;  // mixed form: [slot][k]
+    float *qs_u = nullptr, *qs_v = nullptr, *qs_w = nullptr, *qs_aks = nullptr;  // mixed form: [k][slot4]
     double scl[RP_MAXNGRID][2] = {}, off[RP_MAXNGRID][2] = {};
     int map[3] = {-1, -1, -1};                 // logical slot 1..3 -> physical 0..3
     bool slot_loaded[RP_SLOTS] = {false, false, false, false};
@@ -223,6 +223,21 @@ RpPolint polint_consts(const double xa[3], double x) {
     P.re01 = 1.0 / P.e01;
     P.re02 = 1.0 / P.e02;
     return P;
+}
+
+// polintd's interpolant at x as Lagrange weights of its three values (the
+// mixed form folds them into the gathers): [0] for (b, c, f), [1] for the
+// u/v/w values, which at ets == 1 are (b, b, c) (advection_module.f90:277-287)
+void lagrange_weights(const double xa[3], double x, int ets, float lw[2][3]) {
+    const double a0 = (x - xa[1]) * (x - xa[2]) / ((xa[0] - xa[1]) * (xa[0] - xa[2]));
+    const double a1 = (x - xa[0]) * (x - xa[2]) / ((xa[1] - xa[0]) * (xa[1] - xa[2]));
+    const double a2 = (x - xa[0]) * (x - xa[1]) / ((xa[2] - xa[0]) * (xa[2] - xa[1]));
+    lw[0][0] = (float)a0; lw[0][1] = (float)a1; lw[0][2] = (float)a2;
+    if (ets == 1) {
+        lw[1][0] = (float)(a0 + a1); lw[1][1] = (float)a2; lw[1][2] = 0.f;
+    } else {
+        lw[1][0] = lw[0][0]; lw[1][1] = lw[0][1]; lw[1][2] = lw[0][2];
+    }
 }
 
 void free_ctx(rp_ctx* c) {
@@ -602,6 +617,7 @@ int rp_step(rp_ctx* ctx, const double ex[3], const double ix[3], int32_t ets, in
     fill_grids(ctx, A, t_b, t_c, t_f);
     for (int q = 0; q < 3; q++) { A.ex[q] = ex[q]; A.ix[q] = ix[q]; }
     A.pi = polint_consts(ex, ix[1]);
+    lagrange_weights(ex, ix[1], ets, A.lw);
     A.ets = ets;
     A.step_index = ctx->step_index;
     A.hook = ctx->hook ? ctx->hook + ctx->hook_pos * ctx->n * ctx->ndraw : nullptr;
@@ -613,7 +629,8 @@ int rp_step(rp_ctx* ctx, const double ex[3], const double ix[3], int32_t ets, in
     int nl = 0;
     CK(cudaEventRecord(ctx->ev0, s));
     if (ctx->n > 0 && ctx->mixed)
-        CK(rp::launch_step_mixed(A, ctx->npmax, ctx->i16, s, ctx->num_sms, &nl));
+        CK(rp::launch_step_mixed(A, ctx->npmax, ctx->i16, (float*)ctx->turbv, ctx->prm.reserved[0] == 1, s,
+                                 ctx->num_sms, &nl));
     else if (ctx->n > 0)
         CK(rp::launch_step(A, ctx->prm.field_dtype, ctx->npmax, ctx->turbv, ctx->prm.reserved[0] == 1 ? 0 : 1, s,
                            ctx->num_sms, &nl));
@@ -656,6 +673,7 @@ int rp_step_noalloc(rp_ctx* ctx, const rp_device_state* st, const double ex[3], 
     A.p.gid = st->gid; A.p.isin = st->isin; A.p.pid = st->pid; A.p.flags = st->flags;
     for (int q = 0; q < 3; q++) { A.ex[q] = ex[q]; A.ix[q] = ix[q]; }
     A.pi = polint_consts(ex, ix[1]);
+    lagrange_weights(ex, ix[1], ets, A.lw);
     A.ets = ets;
     A.step_index = ctx->step_index;
     A.hook = nullptr;

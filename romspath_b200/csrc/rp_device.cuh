@@ -60,7 +60,7 @@ struct RpGridDev {
     double scl[RP_MAXNGRID_D][2];  // GRIDS(ng)%scl(i,1:2)
     double off[RP_MAXNGRID_D][2];
     int sb, sc, sf;                // physical ring slots of t_b, t_c, t_f
-    // mixed form: per-(slot, level) scales of the FP16 fields, [slot][k]
+    // mixed form: per-(level, slot) scales of the 16-bit fields, [k][slot4]
     const float* qs_u;
     const float* qs_v;
     const float* qs_w;
@@ -111,6 +111,10 @@ struct RpPolint {
 struct RpStepArgs {
     double ex[3], ix[3];
     RpPolint pi;                   // polintd constants for x = ix(2)
+    // mixed form: polintd at ix(2) as Lagrange weights of the b, c, f slots;
+    // [0] zeta, AKs and level depths, [1] u, v, w (at ets == 1 the values
+    // are (b, b, c), advection_module.f90:277-287)
+    float lw[2][3];
     int ets;
     int ngrid;
     int idt, scheme, nsb, vturb_on, hturb_on, oob;

@@ -16,9 +16,13 @@ constexpr int kStepBlock = 128;
 #endif
 constexpr int kVturbMinBlocks = RP_VTURB_MIN_BLOCKS;   // resident 128-thread blocks per SM
 #ifndef RP_MIXED_MIN_BLOCKS
-#define RP_MIXED_MIN_BLOCKS 6
+#define RP_MIXED_MIN_BLOCKS 8
 #endif
 constexpr int kMixedMinBlocks = RP_MIXED_MIN_BLOCKS;   // same, mixed-precision step
+#ifndef RP_MIXED_VT_BLOCKS
+#define RP_MIXED_VT_BLOCKS 2
+#endif
+constexpr int kMixedVtMinBlocks = RP_MIXED_VT_BLOCKS;  // split mixed form: VTurb kernel blocks per SM
 
 constexpr int kMaxNp = 144;   // largest spline point count int(s_w*sub)
 
@@ -36,7 +40,9 @@ cudaError_t launch_step_noalloc(const RpStepArgs& A, int field_dtype, int npmax,
 // fixed point, `i16`) quantisation of a
 // frame field staged as FP32 (Fortran order), and the conversions between
 // the FP64 columns and the compensated FP32 positions.
-cudaError_t launch_step_mixed(const RpStepArgs& A, int npmax, int i16, cudaStream_t s, int num_sms, int* nlaunch);
+// split: VTurb kernel (displacements into `turbv`, n floats) then the rest
+cudaError_t launch_step_mixed(const RpStepArgs& A, int npmax, int i16, float* turbv, int split, cudaStream_t s,
+                              int num_sms, int* nlaunch);
 cudaError_t launch_stage_f32(int src_f32, const void* src, const void* add, float* dst, int64_t e0, int64_t count,
                              cudaStream_t s);
 cudaError_t launch_quantize(const float* f, uint32_t* maxbits, float* qs, void* dst, int ni, int nj, int nk, int slot,

@@ -12,40 +12,86 @@
 
 namespace rp {
 
+// Fused form: one thread per particle for the whole step.
 template <typename E, int NPMAX>
 __global__ void __launch_bounds__(kStepBlock, kMixedMinBlocks) k_step_mixed(const __grid_constant__ RpStepArgs A) {
     double buf[kMixedArrays * (NPMAX + 1)];
     const MSpline<NPMAX> w{buf};
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < A.p.n; n += stride)
-        m_update_one<E, NPMAX>(A, n, w);
+        m_update_one<E, NPMAX>(A, n, w, nullptr);
+}
+
+// Split form: VTurb alone at a resident-thread count whose spline
+// workspace stays in L2, writing each particle's displacement; then the
+// rest of the step at full occupancy.
+template <typename E, int NPMAX>
+__global__ void __launch_bounds__(kStepBlock, kMixedVtMinBlocks) k_vturb_mixed(const __grid_constant__ RpStepArgs A,
+                                                                               float* __restrict__ turbv) {
+    double buf[kMixedArrays * (NPMAX + 1)];
+    const MSpline<NPMAX> w{buf};
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < A.p.n; n += stride)
+        m_vturb_one<E, NPMAX>(A, n, w, turbv);
+}
+
+template <typename E>
+__global__ void __launch_bounds__(kStepBlock, kMixedMinBlocks) k_advect_mixed(const __grid_constant__ RpStepArgs A,
+                                                             const float* __restrict__ turbv) {
+    const MSpline<1> none{nullptr};
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < A.p.n; n += stride)
+        m_update_one<E, 1>(A, n, none, turbv);
+}
+
+template <class K>
+static cudaError_t resident_grid(K kernel, int64_t n, int num_sms, int cap_per_sm, int64_t* blocks) {
+    int occ = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kStepBlock, 0);
+    if (e != cudaSuccess) return e;
+    if (occ < 1) occ = 1;
+    if (cap_per_sm > 0 && occ > cap_per_sm) occ = cap_per_sm;
+    int64_t b = (int64_t)num_sms * occ;
+    const int64_t need = (n + kStepBlock - 1) / kStepBlock;
+    if (need < b) b = need;
+    *blocks = b < 1 ? 1 : b;
+    return cudaSuccess;
 }
 
 template <typename E, int NPMAX>
-static cudaError_t launch_mixed_t(const RpStepArgs& A, cudaStream_t s, int num_sms, int* nlaunch) {
-    int occ = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_step_mixed<E, NPMAX>, kStepBlock, 0);
-    if (e != cudaSuccess) return e;
-    if (occ < 1) occ = 1;
-    int64_t blocks = (int64_t)num_sms * occ;
-    const int64_t need = (A.p.n + kStepBlock - 1) / kStepBlock;
-    if (need < blocks) blocks = need;
-    if (blocks < 1) blocks = 1;
-    k_step_mixed<E, NPMAX><<<(unsigned)blocks, kStepBlock, 0, s>>>(A);
+static cudaError_t launch_mixed_t(const RpStepArgs& A, float* turbv, int split, cudaStream_t s, int num_sms,
+                                  int* nlaunch) {
+    int64_t blocks = 0;
+    cudaError_t e;
+    if (!split || !A.vturb_on) {
+        if ((e = resident_grid(k_step_mixed<E, NPMAX>, A.p.n, num_sms, 0, &blocks)) != cudaSuccess) return e;
+        k_step_mixed<E, NPMAX><<<(unsigned)blocks, kStepBlock, 0, s>>>(A);
+        *nlaunch += 1;
+        return cudaGetLastError();
+    }
+    if ((e = resident_grid(k_vturb_mixed<E, NPMAX>, A.p.n, num_sms, kMixedVtMinBlocks, &blocks)) != cudaSuccess)
+        return e;
+    k_vturb_mixed<E, NPMAX><<<(unsigned)blocks, kStepBlock, 0, s>>>(A, turbv);
+    *nlaunch += 1;
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = resident_grid(k_advect_mixed<E>, A.p.n, num_sms, 0, &blocks)) != cudaSuccess) return e;
+    k_advect_mixed<E><<<(unsigned)blocks, kStepBlock, 0, s>>>(A, turbv);
     *nlaunch += 1;
     return cudaGetLastError();
 }
 
 template <typename E>
-static cudaError_t launch_mixed_e(const RpStepArgs& A, int npmax, cudaStream_t s, int num_sms, int* nlaunch) {
-    if (npmax <= 88) return launch_mixed_t<E, 88>(A, s, num_sms, nlaunch);
-    if (npmax <= 128) return launch_mixed_t<E, 128>(A, s, num_sms, nlaunch);
-    return launch_mixed_t<E, 144>(A, s, num_sms, nlaunch);
+static cudaError_t launch_mixed_e(const RpStepArgs& A, int npmax, float* turbv, int split, cudaStream_t s,
+                                  int num_sms, int* nlaunch) {
+    if (npmax <= 88) return launch_mixed_t<E, 88>(A, turbv, split, s, num_sms, nlaunch);
+    if (npmax <= 128) return launch_mixed_t<E, 128>(A, turbv, split, s, num_sms, nlaunch);
+    return launch_mixed_t<E, 144>(A, turbv, split, s, num_sms, nlaunch);
 }
 
-cudaError_t launch_step_mixed(const RpStepArgs& A, int npmax, int i16, cudaStream_t s, int num_sms, int* nlaunch) {
-    return i16 ? launch_mixed_e<int16_t>(A, npmax, s, num_sms, nlaunch)
-               : launch_mixed_e<__half>(A, npmax, s, num_sms, nlaunch);
+cudaError_t launch_step_mixed(const RpStepArgs& A, int npmax, int i16, float* turbv, int split, cudaStream_t s,
+                              int num_sms, int* nlaunch) {
+    return i16 ? launch_mixed_e<int16_t>(A, npmax, turbv, split, s, num_sms, nlaunch)
+               : launch_mixed_e<__half>(A, npmax, turbv, split, s, num_sms, nlaunch);
 }
 
 // ------------------------------------------------------ frame upload
@@ -112,7 +158,7 @@ __device__ __forceinline__ void m_store16(int16_t* d, float v) {
 }
 
 // FP32 field (Fortran order) -> 16-bit device layout [j][i][k][slot4] and
-// the per-level scales qs[slot][k]
+// the per-level scales qs[k][slot4]
 template <typename E>
 __global__ void k_quantize(const float* __restrict__ f, const uint32_t* __restrict__ maxbits, float* __restrict__ qs,
                            E* __restrict__ dst, int ni, int nj, int nk, int slot) {
@@ -120,7 +166,7 @@ __global__ void k_quantize(const float* __restrict__ f, const uint32_t* __restri
     const int64_t plane = (int64_t)ni * nj;
     const int64_t total = plane * nk;
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e < nk) qs[slot * nk + e] = m_level_scale(maxbits[e], i16);
+    if (e < nk) qs[e * RP_SLOTS + slot] = m_level_scale(maxbits[e], i16);
     if (e >= total) return;
     const int k = (int)(e / plane);
     const int64_t r = e - (int64_t)k * plane;

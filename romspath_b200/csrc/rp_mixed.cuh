@@ -11,15 +11,18 @@
 //     it still meets smooth()'s 1 % criterion).
 // The 16-bit storage is FP16 (RP_FIELD_MIXED) or int16 fixed point
 // (RP_FIELD_MIXED_I16, |v| / scale <= 32767 with scale = level max / 32767).
-// Results differ from the exact form by rounding; the error is measured
-// against the FP64 form on identical noise.
+// The four ring slots of one (point, level) are one 8-byte load (16 bytes
+// for zeta), and polintd's time interpolation at ix(2) is applied as its
+// Lagrange weights on the b/c/f slots (host-computed, RpStepArgs::lw),
+// combined with the level scales before the corner sum.  polintd is linear
+// in its values, so the s-level depths are formed once from the
+// interpolated zeta.  Results differ from the exact form by rounding; the
+// error is measured against the FP64 form on identical noise.
 #pragma once
 
 #include <cuda_fp16.h>
 
 #include "rp_step.cuh"
-
-constexpr float kHalfRange = 16384.0f;   // |stored value| <= 16384 after scaling
 
 // ------------------------------------------------------------ cells (FP32)
 
@@ -91,10 +94,28 @@ __device__ __forceinline__ float m_bil(const double* a, const MRho& c) {
            c.cb[2] * (float)__ldg(a + c.o[2]) + c.cb[3] * (float)__ldg(a + c.o[3]);
 }
 
-__device__ __forceinline__ float m_zeta(const RpGridDev& g, const MRho& c, int slot) {
-    const float* z = reinterpret_cast<const float*>(g.zeta);
-    return c.ci[0] * __ldg(z + c.o[0] * RP_SLOTS + slot) + c.ci[1] * __ldg(z + c.o[1] * RP_SLOTS + slot) +
-           c.ci[2] * __ldg(z + c.o[2] * RP_SLOTS + slot) + c.ci[3] * __ldg(z + c.o[3] * RP_SLOTS + slot);
+// time weights of the b, c, f ring slots (polintd at ix(2) in Lagrange
+// form) and the physical slots they sit in
+struct MTime {
+    float wb, wc, wf;
+    int sb, sc, sf;
+};
+
+__device__ __forceinline__ float m_pick4(const float4& v, int s) {
+    return s == 0 ? v.x : (s == 1 ? v.y : (s == 2 ? v.z : v.w));
+}
+
+// time-interpolated zeta at the cell's corners, inverse-distance weights
+// (getInterp2D's zeta rule, interpolation_module.f90:478-486)
+__device__ __forceinline__ float m_zeta(const RpGridDev& g, const MRho& c, const MTime& t) {
+    const float4* z = reinterpret_cast<const float4*>(g.zeta);
+    float acc = 0.f;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const float4 v = __ldg(z + c.o[q]);
+        acc += c.ci[q] * (t.wb * m_pick4(v, t.sb) + t.wc * m_pick4(v, t.sc) + t.wf * m_pick4(v, t.sf));
+    }
+    return acc;
 }
 
 struct MUV {
@@ -179,132 +200,152 @@ __device__ __forceinline__ float m_zlev(int vt, float hc, float h, float den_r, 
     return zeta * (1.f + s) + hc * s + (h - hc) * cs;
 }
 
-// first level k in 1..nz with z_k > zpar by bisection over the monotone
-// levels, with the reference's boundary cases (rho: constant outside;
-// w: pinned as in the FP64 form)
-__device__ __forceinline__ void m_walk(const double* s, const double* cs, int nz, int vt, float hc, float zeta,
-                                       float depth, float zpar, bool wlev, MPick& L, uint32_t& fl) {
+// The level brackets of getInterp3D for rho levels (ztype 1) and w levels
+// (ztype 2) (interpolation_module.f90:529-582), with the reference's
+// boundary cases (rho: constant outside; w: pinned as in the FP64 form).
+// The first w level above zpar is found by bisection over the monotone
+// levels; rho level k lies between w levels k and k+1, so one more depth
+// decides the rho bracket.
+__device__ __forceinline__ void m_walk2(const RpGridDev& g, float zeta, float depth, float zpar, MPick& Lr,
+                                        MPick& Lw, uint32_t& fl) {
+    const int N = g.N, vt = g.vtransform;
+    const float hc = (float)g.hc;
     const float h = -depth;
     const float den_r = 1.f / (hc + h);
-    auto zl = [&](int k) -> float { return m_zlev(vt, hc, h, den_r, (float)__ldg(s + k - 1), (float)__ldg(cs + k - 1), zeta); };
-    int lo = 0, hi = nz + 1;            // z_lo <= zpar < z_hi (virtual ends)
+    auto zw = [&](int k) -> float {
+        return m_zlev(vt, hc, h, den_r, (float)__ldg(g.sw + k - 1), (float)__ldg(g.csw + k - 1), zeta);
+    };
+    auto zr = [&](int k) -> float {
+        return m_zlev(vt, hc, h, den_r, (float)__ldg(g.sr + k - 1), (float)__ldg(g.csr + k - 1), zeta);
+    };
+    int lo = 0, hi = N + 2;             // zw(lo) <= zpar < zw(hi) (virtual ends)
     while (hi - lo > 1) {
         const int mid = (lo + hi) >> 1;
-        if (zl(mid) > zpar) hi = mid; else lo = mid;
+        if (zw(mid) > zpar) hi = mid; else lo = mid;
     }
-    const int i = hi;                   // first level above zpar, nz+1 if none
-    if (i > nz) {
-        if (wlev) fl |= RP_FL_WTOP;
-        L.ibot = nz; L.itop = nz; L.z1 = 0.5f; L.z2 = 0.5f;
-    } else if (i == 1) {
-        if (wlev) fl |= RP_FL_WBOT;
-        L.ibot = 1; L.itop = 1; L.z1 = 0.5f; L.z2 = 0.5f;
+    const int iw = hi;                  // first w level above zpar, N+2 if none
+    int ir;                             // first rho level above zpar, N+1 if none
+    if (iw == 1) ir = 1;
+    else if (iw > N + 1) ir = N + 1;
+    else ir = (zr(iw - 1) > zpar) ? iw - 1 : iw;
+    if (iw > N + 1) {
+        fl |= RP_FL_WTOP;
+        Lw.ibot = N + 1; Lw.itop = N + 1; Lw.z1 = 0.5f; Lw.z2 = 0.5f;
+    } else if (iw == 1) {
+        fl |= RP_FL_WBOT;
+        Lw.ibot = 1; Lw.itop = 1; Lw.z1 = 0.5f; Lw.z2 = 0.5f;
     } else {
-        const float za = zl(i - 1), zb = zl(i);
+        const float za = zw(iw - 1), zb = zw(iw);
         const float Z = (zpar - za) / (zb - za);
-        L.ibot = i - 1; L.itop = i; L.z1 = 1.f - Z; L.z2 = Z;
+        Lw.ibot = iw - 1; Lw.itop = iw; Lw.z1 = 1.f - Z; Lw.z2 = Z;
+    }
+    if (ir > N) {
+        Lr.ibot = N; Lr.itop = N; Lr.z1 = 0.5f; Lr.z2 = 0.5f;
+    } else if (ir == 1) {
+        Lr.ibot = 1; Lr.itop = 1; Lr.z1 = 0.5f; Lr.z2 = 0.5f;
+    } else {
+        const float za = zr(ir - 1), zb = zr(ir);
+        const float Z = (zpar - za) / (zb - za);
+        Lr.ibot = ir - 1; Lr.itop = ir; Lr.z1 = 1.f - Z; Lr.z2 = Z;
     }
 }
 
-// one stored 16-bit field value (before its level scale): FP16, or int16
-// fixed point
-__device__ __forceinline__ float m_h(const __half* f, int64_t idx) { return __half2float(__ldg(f + idx)); }
-__device__ __forceinline__ float m_h(const int16_t* f, int64_t idx) { return (float)__ldg(f + idx); }
+// one stored 16-bit value (before its level scale): FP16, or int16 fixed point
+template <typename E>
+__device__ __forceinline__ float m_dec(uint32_t bits);
+template <>
+__device__ __forceinline__ float m_dec<__half>(uint32_t bits) {
+    return __half2float(__ushort_as_half((unsigned short)bits));
+}
+template <>
+__device__ __forceinline__ float m_dec<int16_t>(uint32_t bits) {
+    return (float)(int16_t)(uint16_t)bits;
+}
 
-// zcff1*zprof(Ibot) + zcff2*zprof(Itop) of one slot of an FP16 field
+// slot s (0..3, uniform) of the four 16-bit slots of one (point, level)
+template <typename E>
+__device__ __forceinline__ float m_slot(const uint2& v, int s) {
+    const uint32_t word = (s < 2) ? v.x : v.y;
+    return m_dec<E>((s & 1) ? (word >> 16) : (word & 0xffffu));
+}
+
+// sum over corners of cff * (time-interpolated, scaled value) at level lev
+template <typename E>
+__device__ __forceinline__ float m_level(const uint2* f, const float4* qs, const int64_t o[4], const float cff[4],
+                                         const bool use[4], int nlev, int lev, const MTime& t) {
+    const float4 sc = __ldg(qs + lev - 1);             // level scales [k][slot4]
+    const float wb = t.wb * m_pick4(sc, t.sb), wc = t.wc * m_pick4(sc, t.sc), wf = t.wf * m_pick4(sc, t.sf);
+    float acc = 0.f;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        if (use[q]) {
+            const uint2 v = __ldg(f + o[q] * nlev + lev - 1);
+            acc += cff[q] * (wb * m_slot<E>(v, t.sb) + wc * m_slot<E>(v, t.sc) + wf * m_slot<E>(v, t.sf));
+        }
+    }
+    return acc;
+}
+
+// zcff1*zprof(Ibot) + zcff2*zprof(Itop), time-interpolated
 template <typename E>
 __device__ __forceinline__ float m_col(const void* fv, const float* qs, const int64_t o[4], const float cff[4],
-                                       const bool use[4], int nlev, const MPick& L, int slot) {
-    const E* f = reinterpret_cast<const E*>(fv);
-    float pb = 0.f, pt = 0.f;
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-        const int64_t base = o[k] * nlev;
-        const float vb = use[k] ? m_h(f, (base + L.ibot - 1) * RP_SLOTS + slot) : 0.f;
-        const float vt = use[k] ? m_h(f, (base + L.itop - 1) * RP_SLOTS + slot) : 0.f;
-        pb += cff[k] * vb;
-        pt += cff[k] * vt;
-    }
-    pb *= __ldg(qs + slot * nlev + L.ibot - 1);
-    pt *= __ldg(qs + slot * nlev + L.itop - 1);
+                                       const bool use[4], int nlev, const MPick& L, const MTime& t) {
+    const uint2* f = reinterpret_cast<const uint2*>(fv);
+    const float4* q4 = reinterpret_cast<const float4*>(qs);
+    const float pb = m_level<E>(f, q4, o, cff, use, nlev, L.ibot, t);
+    const float pt = (L.itop == L.ibot) ? pb : m_level<E>(f, q4, o, cff, use, nlev, L.itop, t);
     return L.z1 * pb + L.z2 * pt;
-}
-
-struct MPol {
-    float d1, dns, b, r12, r01, r02;
-    int ns;
-};
-
-__device__ __forceinline__ MPol m_pol(const RpPolint& P) {
-    MPol m;
-    m.d1 = (float)P.d1; m.dns = (float)P.dns; m.b = (float)P.b;
-    m.r12 = (float)P.re12; m.r01 = (float)P.re01; m.r02 = (float)P.re02;
-    m.ns = P.ns;
-    return m;
-}
-
-__device__ __forceinline__ float m_polintd(const MPol& P, float y0, float y1, float y2) {
-    const float q12 = (y2 - y1) * P.r12;
-    const float q01 = (y1 - y0) * P.r01;
-    const float c = (P.d1 * q12 - P.d1 * q01) * P.r02;
-    const float a = (P.ns == 2) ? q12 : q01;
-    const float yns = (P.ns == 0) ? y0 : ((P.ns == 1) ? y1 : y2);
-    return yns + P.dns * a + P.b * c;
 }
 
 struct MStage {
     MRho rc;
-    float tdepth, zb, zc, zf, zeta;
+    float tdepth, zeta;
 };
 
-// find_currents (advection_module.f90:129-350) in FP32 on FP16 fields
-// depth and the three zeta values at the stage's cell S.rc
-__device__ __forceinline__ void m_stage_2d(const MPol& P, const RpGridDev& g, MStage& S) {
+// depth and time-interpolated zeta at the stage's cell S.rc
+__device__ __forceinline__ void m_stage_2d(const MTime& tz, const RpGridDev& g, MStage& S) {
     S.tdepth = -m_bil(g.h, S.rc);
-    S.zb = m_zeta(g, S.rc, g.sb);
-    S.zc = m_zeta(g, S.rc, g.sc);
-    S.zf = m_zeta(g, S.rc, g.sf);
-    S.zeta = m_polintd(P, S.zb, S.zc, S.zf);
+    S.zeta = m_zeta(g, S.rc, tz);
 }
 
-// with cell_ready the caller has already filled S.rc for (X, Y); E is the
-// 16-bit storage type of u, v, w (and AKs)
+__device__ __forceinline__ MTime m_time(const RpStepArgs& A, const RpGridDev& g, int which) {
+    MTime t;
+    t.wb = A.lw[which][0];
+    t.wc = A.lw[which][1];
+    t.wf = A.lw[which][2];
+    t.sb = g.sb;
+    t.sc = g.sc;
+    t.sf = g.sf;
+    return t;
+}
+
+// find_currents (advection_module.f90:129-350) in FP32 on 16-bit fields;
+// Z is INOUT.  E is the 16-bit storage type of u, v, w.
 template <typename E>
-__device__ __forceinline__ void m_find_currents(const RpStepArgs& A, const MPol& P, const RpGridDev& g, float X,
-                                                float Y, float& Z, float& U, float& V, float& Wv, MStage& S,
-                                                bool cell_ready, uint32_t& fl) {
-    if (!cell_ready) m_rho_cell(g, X, Y, S.rc, fl);
-    m_stage_2d(P, g, S);
+__device__ __forceinline__ void m_find_currents(const RpStepArgs& A, const RpGridDev& g, float X, float Y, float& Z,
+                                                float& U, float& V, float& Wv, uint32_t& fl) {
+    MStage S;
+    m_rho_cell(g, X, Y, S.rc, fl);
+    m_stage_2d(m_time(A, g, 0), g, S);
     if (Z < S.tdepth) Z = S.tdepth + 0.001f;
     if (Z > S.zeta) Z = S.zeta - 0.001f;
     MPick Lr, Lw;
-    const float hc = (float)g.hc;
-    m_walk(g.sr, g.csr, g.N, g.vtransform, hc, S.zeta, S.tdepth, Z, false, Lr, fl);
-    m_walk(g.sw, g.csw, g.N + 1, g.vtransform, hc, S.zeta, S.tdepth, Z, true, Lw, fl);
+    m_walk2(g, S.zeta, S.tdepth, Z, Lr, Lw, fl);
     const int N = g.N;
-    MUV cu, cv;
-    m_uv_cell(g, X, Y, true, cu, fl);
-    m_uv_cell(g, X, Y, false, cv, fl);
-    const float Ub = m_col<E>(g.u, g.qs_u, cu.o, cu.cff, cu.use, N, Lr, g.sb);
-    const float Uc = m_col<E>(g.u, g.qs_u, cu.o, cu.cff, cu.use, N, Lr, g.sc);
-    const float Vb = m_col<E>(g.v, g.qs_v, cv.o, cv.cff, cv.use, N, Lr, g.sb);
-    const float Vc = m_col<E>(g.v, g.qs_v, cv.o, cv.cff, cv.use, N, Lr, g.sc);
+    const MTime tv = m_time(A, g, 1);                  // (b, b, c) at ets == 1
+    {
+        MUV cu;
+        m_uv_cell(g, X, Y, true, cu, fl);
+        U = m_col<E>(g.u, g.qs_u, cu.o, cu.cff, cu.use, N, Lr, tv);
+    }
+    {
+        MUV cv;
+        m_uv_cell(g, X, Y, false, cv, fl);
+        V = m_col<E>(g.v, g.qs_v, cv.o, cv.cff, cv.use, N, Lr, tv);
+    }
     const bool all[4] = {true, true, true, true};
     const float* cw = S.rc.wet4 ? S.rc.cb : S.rc.ci;
-    const float Wb = m_col<E>(g.w, g.qs_w, S.rc.o, cw, all, N + 1, Lw, g.sb);
-    const float Wc = m_col<E>(g.w, g.qs_w, S.rc.o, cw, all, N + 1, Lw, g.sc);
-    if (A.ets == 1) {
-        U = m_polintd(P, Ub, Ub, Uc);
-        V = m_polintd(P, Vb, Vb, Vc);
-        Wv = m_polintd(P, Wb, Wb, Wc);
-    } else {
-        const float Uf = m_col<E>(g.u, g.qs_u, cu.o, cu.cff, cu.use, N, Lr, g.sf);
-        const float Vf = m_col<E>(g.v, g.qs_v, cv.o, cv.cff, cv.use, N, Lr, g.sf);
-        const float Wf = m_col<E>(g.w, g.qs_w, S.rc.o, cw, all, N + 1, Lw, g.sf);
-        U = m_polintd(P, Ub, Uc, Uf);
-        V = m_polintd(P, Vb, Vc, Vf);
-        Wv = m_polintd(P, Wb, Wc, Wf);
-    }
+    Wv = m_col<E>(g.w, g.qs_w, S.rc.o, cw, all, N + 1, Lw, tv);
 }
 
 // --------------------------------------------- spline with a warm start
@@ -323,18 +364,22 @@ __device__ __forceinline__ void m_find_currents(const RpStepArgs& A, const MPol&
 // traffic is three arrays written forward and read backward plus u written
 // backward.
 
-constexpr int kMixedArrays = 7;
+// Workspace: three FP64 arrays for chol1d, then four FP32 arrays for the
+// data (the column and the resampled values carry FP32 information only),
+// kMixedArrays (NPMAX+1) doubles in all.
+constexpr int kMixedArrays = 5;
 
 template <int NPMAX>
 struct MSpline {
-    double* base;                  // kMixedArrays (NPMAX+1) doubles
+    double* base;
     __device__ __forceinline__ double& s1(int i) const { return base[i]; }                  // ratio1(i)
     __device__ __forceinline__ double& s2(int i) const { return base[(NPMAX + 1) + i]; }    // ratio2(i)
     __device__ __forceinline__ double& u(int i) const { return base[2 * (NPMAX + 1) + i]; } // u(i)/v(i,1), then u(i)
-    __device__ __forceinline__ double& y(int i) const { return base[3 * (NPMAX + 1) + i]; }  // resampled data y(i)
-    __device__ __forceinline__ double& cz(int k) const { return base[4 * (NPMAX + 1) + k]; } // column z(k)
-    __device__ __forceinline__ double& cm(int k) const { return base[5 * (NPMAX + 1) + k]; } // slope on [z(k), z(k+1)]
-    __device__ __forceinline__ double& cb(int k) const { return base[6 * (NPMAX + 1) + k]; } // intercept
+    __device__ __forceinline__ float* fb() const { return reinterpret_cast<float*>(base + 3 * (NPMAX + 1)); }
+    __device__ __forceinline__ float& y(int i) const { return fb()[i]; }                     // resampled data y(i)
+    __device__ __forceinline__ float& cz(int k) const { return fb()[(NPMAX + 1) + k]; }      // column z(k)
+    __device__ __forceinline__ float& cm(int k) const { return fb()[2 * (NPMAX + 1) + k]; }  // slope on [z(k), z(k+1)]
+    __device__ __forceinline__ float& cb(int k) const { return fb()[3 * (NPMAX + 1) + k]; }  // intercept
 };
 
 struct MFit {
@@ -368,9 +413,11 @@ struct MWalk {
 
 // One chol1d pass at p: factorise, solve for u, form qu = Q u; returns
 // sum_i qu(i)^2 dy^2 and, on request, utru = sum v4 (u(i-1)(u(i-1)+u(i)) + u(i)^2).
-// With store_y the resampled values y(i) are also kept (for ppvalu).
+// With store_y the resampled values y(i) are also kept (for ppvalu); u is
+// written back only with store_u (a pass whose u may be the fit's).
 template <int NPMAX>
-__device__ double m_chol1d(const MSpline<NPMAX>& w, const MFit& f, double p, double* utru_out, bool store_y) {
+__device__ double m_chol1d(const MSpline<NPMAX>& w, const MFit& f, double p, double* utru_out, bool store_y,
+                           bool store_u) {
     const int np = f.np;
     const double r = f.serr * f.rh;
     const double r2 = r * r;
@@ -385,9 +432,9 @@ __device__ double m_chol1d(const MSpline<NPMAX>& w, const MFit& f, double p, dou
     double y0 = wk.at(w, f.sw, f.z1 + f.h);
     double yp = wk.at(w, f.sw, f.z1 + 2.0 * f.h);
     if (store_y) {
-        w.y(1) = ym;
-        w.y(2) = y0;
-        w.y(3) = yp;
+        w.y(1) = (float)ym;
+        w.y(2) = (float)y0;
+        w.y(3) = (float)yp;
     }
     double a1 = D, a2 = E, b1 = D;
     double uprev = 0.0, ucur = (yp - 2.0 * y0 + ym) * f.rh, r2prev = 0.0;
@@ -406,7 +453,7 @@ __device__ double m_chol1d(const MSpline<NPMAX>& w, const MFit& f, double p, dou
         ym = y0;
         y0 = yp;
         yp = wk.at(w, f.sw, f.z1 + (double)(i + 1) * f.h);
-        if (store_y) w.y(i + 2) = yp;
+        if (store_y) w.y(i + 2) = (float)yp;
         const double qn = (yp - 2.0 * y0 + ym) * f.rh;     // qty(i+1)
         const double unext = qn - ratio1 * ucur - r2prev * uprev;
         uprev = ucur;
@@ -424,10 +471,10 @@ __device__ double m_chol1d(const MSpline<NPMAX>& w, const MFit& f, double p, dou
     double up2 = 0.0;                                // u(np+1), unused
     double rawp = 0.0;                               // raw(np+1)
     double sum = 0.0, utru = 0.0;
-    w.u(np) = 0.0;
+    if (store_u) w.u(np) = 0.0;
     {
         const double ui = ucur / a1;                 // u(np-1)
-        w.u(np - 1) = ui;
+        if (store_u) w.u(np - 1) = ui;
         const double raw = (up1 - ui) * f.rh;        // raw(np)
         const double fin = rawp - raw;               // qu(np)
         sum = sum + fin * fin * dy2;
@@ -439,7 +486,7 @@ __device__ double m_chol1d(const MSpline<NPMAX>& w, const MFit& f, double p, dou
 #pragma unroll 2
     for (int i = np - 2; i >= 2; i--) {
         const double ui = w.u(i) - up1 * w.s1(i) - up2 * w.s2(i);
-        w.u(i) = ui;
+        if (store_u) w.u(i) = ui;
         const double raw = (up1 - ui) * f.rh;        // raw(i+1)
         const double fin = rawp - raw;               // qu(i+1)
         sum = sum + fin * fin * dy2;
@@ -454,15 +501,16 @@ __device__ double m_chol1d(const MSpline<NPMAX>& w, const MFit& f, double p, dou
         sum = sum + fin2 * fin2 * dy2 + raw * raw * dy2;   // qu(1) = raw(2)
         utru = utru + f.h * (up1 * up1);
     }
-    w.u(1) = 0.0;
+    if (store_u) w.u(1) = 0.0;
     if (utru_out) *utru_out = utru;
     return sum;
 }
 
 // SF(q) = 36 sum qu^2 dy^2 / (1+q)^2 of one chol1d pass at p = q/(1+q)
 template <int NPMAX>
-__device__ __forceinline__ double m_sf(const MSpline<NPMAX>& w, const MFit& f, double q, bool store_y = false) {
-    return 36.0 * m_chol1d(w, f, q / (1.0 + q), nullptr, store_y) / ((1.0 + q) * (1.0 + q));
+__device__ __forceinline__ double m_sf(const MSpline<NPMAX>& w, const MFit& f, double q, bool store_y,
+                                       bool store_u) {
+    return 36.0 * m_chol1d(w, f, q / (1.0 + q), nullptr, store_y, store_u) / ((1.0 + q) * (1.0 + q));
 }
 
 // smooth() (pppack.f90:5108-5317): the secant search for q = p/(1-p) on
@@ -475,22 +523,27 @@ __device__ __forceinline__ double m_sf(const MSpline<NPMAX>& w, const MFit& f, d
 template <int NPMAX>
 __device__ double m_smooth(const MSpline<NPMAX>& w, const MFit& f, double s, int max_iter, double& qstate,
                            double& gstate, uint32_t& fl) {
-    // the first pass of every path also stores y(i)
+    // the first pass of every path also stores y(i); passes that are
+    // rarely the last one (the warm-start check, p = 0) do not store u and
+    // are repeated with it when they are
     if (s <= 0.0) {
-        m_chol1d(w, f, 1.0, nullptr, true);
+        m_chol1d(w, f, 1.0, nullptr, true, true);
         return 1.0;
     }
     const double ooss = 1.0 / sqrt(s);
     double q = qstate;
     const bool warm = q > 0.0;
     if (warm) {
-        double sfq = m_sf(w, f, q, true);
-        if (fabs(sfq - s) <= 0.01 * s) return q / (1.0 + q);
+        double sfq = m_sf(w, f, q, true, false);
+        if (fabs(sfq - s) <= 0.01 * s) {
+            m_chol1d(w, f, q / (1.0 + q), nullptr, false, true);
+            return q / (1.0 + q);
+        }
         double prevq = q, prevsf = 1.0 / sqrt(sfq);
         const double qn = (gstate > 0.0) ? q + (ooss - prevsf) / gstate : 0.0;
         q = (qn > 0.0) ? qn : q * sqrt(sfq / s);
         for (int it = 0; it < 6 && q > 0.0; it++) {
-            sfq = m_sf(w, f, q);
+            sfq = m_sf(w, f, q, false, true);
             const double oosf = 1.0 / sqrt(sfq);
             const double g = (oosf - prevsf) / (q - prevq);
             if (fabs(sfq - s) <= 0.01 * s) {
@@ -506,8 +559,9 @@ __device__ double m_smooth(const MSpline<NPMAX>& w, const MFit& f, double s, int
     }
     // cold start: the reference's sequence
     double utru = 0.0;
-    double sfq = 36.0 * m_chol1d(w, f, 0.0, &utru, !warm);
+    double sfq = 36.0 * m_chol1d(w, f, 0.0, &utru, !warm, false);
     if (!(s < sfq)) {
+        m_chol1d(w, f, 0.0, nullptr, false, true);
         qstate = 0.0;
         gstate = 0.0;
         return 0.0;
@@ -517,7 +571,7 @@ __device__ double m_smooth(const MSpline<NPMAX>& w, const MFit& f, double s, int
     double prevq = 0.0, prevsf = oosf;
     int it = 0;
     for (;;) {
-        sfq = m_sf(w, f, q);
+        sfq = m_sf(w, f, q, false, true);
         oosf = 1.0 / sqrt(sfq);
         it++;
         const double g = (oosf - prevsf) / (q - prevq);
@@ -539,17 +593,16 @@ __device__ double m_smooth(const MSpline<NPMAX>& w, const MFit& f, double s, int
     return q / (1.0 + q);
 }
 
-// ppvalu (pppack.f90:4246-4362) of the fit at x, the one piece it needs
-// formed as smooth's epilogue forms a(:,1..4) (pppack.f90:5303-5316).
+// One piece of the fit: the coefficients a(i,1..4) smooth's epilogue forms
+// (pppack.f90:5303-5316) for piece i, from u and y.
+struct MPiece {
+    int i;                          // 0: none yet
+    double xi, c1, c2, c3, c4;
+};
+
 template <int NPMAX>
-__device__ __forceinline__ double m_ppvalu(const MSpline<NPMAX>& w, const MFit& f, double p, double x,
-                                           int jderiv) {
+__device__ __forceinline__ void m_piece(const MSpline<NPMAX>& w, const MFit& f, double p, int i, MPiece& pc) {
     const int np = f.np;
-    // interv on uniform breaks: piece 1 below the first break, np-1 at or
-    // above the last (also for a NaN x)
-    const double t = floor((x - f.z1) * f.rh);
-    const int i = (t >= 0.0 && t < (double)(np - 1)) ? (int)t + 1 : ((t >= (double)(np - 1)) ? np - 1 : 1);
-    const double xi = f.z1 + (double)(i - 1) * f.h;
     const double um = (i >= 2) ? w.u(i - 1) : 0.0;
     const double u0 = w.u(i), u1 = w.u(i + 1);
     const double u2 = (i + 2 <= np) ? w.u(i + 2) : 0.0;
@@ -557,22 +610,40 @@ __device__ __forceinline__ double m_ppvalu(const MSpline<NPMAX>& w, const MFit& 
     const double raw1 = (u1 - u0) * f.rh;                            // raw(i+1)
     const double raw2 = (i + 2 <= np) ? (u2 - u1) * f.rh : 0.0;      // raw(i+2)
     const double K1 = 6.0 * (1.0 - p) * f.dy2;
-    const double a1i = w.y(i) - K1 * (raw1 - raw0);
-    const double a1n = w.y(i + 1) - K1 * (raw2 - raw1);
+    const double a1i = (double)w.y(i) - K1 * (raw1 - raw0);
+    const double a1n = (double)w.y(i + 1) - K1 * (raw2 - raw1);
     const double a3i = u0 * 6.0 * p;
     const double a3n = u1 * 6.0 * p;
     const double a4i = (a3n - a3i) * f.rh;
-    const double a2i = (a1n - a1i) * f.rh - (a3i + a4i * (1.0 / 3.0) * f.h) * 0.5 * f.h;
-    const double hx = x - xi;
+    pc.i = i;
+    pc.xi = f.z1 + (double)(i - 1) * f.h;
+    pc.c1 = a1i;
+    pc.c2 = (a1n - a1i) * f.rh - (a3i + a4i * (1.0 / 3.0) * f.h) * 0.5 * f.h;
+    pc.c3 = a3i;
+    pc.c4 = a4i;
+}
+
+// ppvalu (pppack.f90:4246-4362) of the fit at x; the piece is kept in
+// registers between calls (consecutive sub-step positions mostly share it).
+template <int NPMAX>
+__device__ __forceinline__ double m_ppvalu(const MSpline<NPMAX>& w, const MFit& f, double p, double x, int jderiv,
+                                           MPiece& pc) {
+    const int np = f.np;
+    // interv on uniform breaks: piece 1 below the first break, np-1 at or
+    // above the last (also for a NaN x)
+    const double t = floor((x - f.z1) * f.rh);
+    const int i = (t >= 0.0 && t < (double)(np - 1)) ? (int)t + 1 : ((t >= (double)(np - 1)) ? np - 1 : 1);
+    if (i != pc.i) m_piece(w, f, p, i, pc);
+    const double hx = x - pc.xi;
     // Horner loop of ppvalu with k = 4: value = (value/fmmjdr)*h + coef(m)
-    if (jderiv == 0) return ((a4i * (1.0 / 3.0) * hx + a3i) * 0.5 * hx + a2i) * hx + a1i;
-    return (a4i * 0.5 * hx + a3i) * hx + a2i;
+    if (jderiv == 0) return ((pc.c4 * (1.0 / 3.0) * hx + pc.c3) * 0.5 * hx + pc.c2) * hx + pc.c1;
+    return (pc.c4 * 0.5 * hx + pc.c3) * hx + pc.c2;
 }
 
 // VTurb (ver_turb_module.f90:31-329): column in FP32 from FP16 AKs, fit and
 // random-displacement sub-steps in FP64
 template <typename E, int NPMAX>
-__device__ float m_vturb(const RpStepArgs& A, const MPol& P, const RpGridDev& g, const MStage& S, float Zpar,
+__device__ float m_vturb(const RpStepArgs& A, const RpGridDev& g, const MStage& S, float Zpar,
                          uint32_t pid, double& qstate, double& gstate, uint32_t& fl, const MSpline<NPMAX>& w) {
     const int sw = g.N + 1;
     MFit f;
@@ -585,34 +656,22 @@ __device__ float m_vturb(const RpStepArgs& A, const MPol& P, const RpGridDev& g,
     const float hc = (float)g.hc;
     const float den_r = 1.f / (hc + h);
     const float* cwt = S.rc.wet4 ? S.rc.cb : S.rc.ci;
-    const E* aks = reinterpret_cast<const E*>(g.aks);
-    const int slots[3] = {g.sb, g.sc, g.sf};
+    const uint2* aks = reinterpret_cast<const uint2*>(g.aks);
+    const float4* qs = reinterpret_cast<const float4*>(g.qs_aks);
+    const MTime tk = m_time(A, g, 0);
+    const bool all[4] = {true, true, true, true};
     double zprev = 0.0, kprev = 0.0;
     for (int k = 1; k <= sw; k++) {
-        const float s = (float)__ldg(g.sw + k - 1), cs = (float)__ldg(g.csw + k - 1);
-        double zk;
-        if (k == sw) {
-            zk = zeta;                                  // the top w level is zeta
-        } else {
-            const float zb = m_zlev(g.vtransform, hc, h, den_r, s, cs, S.zb);
-            const float zcv = m_zlev(g.vtransform, hc, h, den_r, s, cs, S.zc);
-            const float zf = m_zlev(g.vtransform, hc, h, den_r, s, cs, S.zf);
-            zk = (double)m_polintd(P, zb, zcv, zf);
-        }
-        float K[3];
-#pragma unroll
-        for (int t = 0; t < 3; t++) {
-            float a = 0.f;
-#pragma unroll
-            for (int q = 0; q < 4; q++) a += cwt[q] * m_h(aks, (S.rc.o[q] * sw + (k - 1)) * RP_SLOTS + slots[t]);
-            K[t] = a * __ldg(g.qs_aks + slots[t] * sw + k - 1);
-        }
-        const double kk = (double)m_polintd(P, K[0], K[1], K[2]);
-        w.cz(k) = zk;
+        // z_w(k) of the interpolated zeta (getWlevel is linear in zeta)
+        const double zk = (k == sw) ? zeta
+                                    : (double)m_zlev(g.vtransform, hc, h, den_r, (float)__ldg(g.sw + k - 1),
+                                                     (float)__ldg(g.csw + k - 1), S.zeta);
+        const double kk = (double)m_level<E>(aks, qs, S.rc.o, cwt, all, sw, k, tk);   // getInterpAKs
+        w.cz(k) = (float)zk;
         if (k >= 2) {
             const double m = (kk - kprev) / (zk - zprev);
-            w.cm(k - 1) = m;
-            w.cb(k - 1) = kprev - m * zprev;
+            w.cm(k - 1) = (float)m;
+            w.cb(k - 1) = (float)(kprev - m * zprev);
         }
         zprev = zk;
         kprev = kk;
@@ -623,16 +682,18 @@ __device__ float m_vturb(const RpStepArgs& A, const MPol& P, const RpGridDev& g,
     const double p = m_smooth(w, f, A.smth, A.spline_max_iter, qstate, gstate, fl);
     const double deltat = A.deltat;
     double ParZc = (double)Zpar;
+    MPiece pc;
+    pc.i = 0;
     for (int i = 1; i <= A.loop; i++) {
         double Kprimec = 0.0;
-        if (!(ParZc <= tdepth || ParZc >= zeta)) Kprimec = m_ppvalu(w, f, p, ParZc, 1);
+        if (!(ParZc <= tdepth || ParZc >= zeta)) Kprimec = m_ppvalu(w, f, p, ParZc, 1, pc);
         const double KprimeZc = Kprimec * deltat;
         const double Z3rdc = ParZc + 0.5 * KprimeZc;
         double KH3rdc;
         if (Z3rdc < tdepth || Z3rdc > zeta) {
             KH3rdc = A.aksback;
         } else {
-            KH3rdc = m_ppvalu(w, f, p, Z3rdc, 0);
+            KH3rdc = m_ppvalu(w, f, p, Z3rdc, 0, pc);
             if (KH3rdc < A.aksback) KH3rdc = A.aksback;
         }
         const double DEV = rp_normal(A, pid, (uint32_t)(1 + i));
@@ -653,12 +714,39 @@ __device__ __forceinline__ void m_kahan_add(float& p, float& c, float d) {
 
 // ----------------------------------------------------------- one particle
 
+// VTurb of one particle on its own (the first kernel of the split form),
+// with the stage-1 z clamp of find_currents applied first when RK4 runs
+// (advection_module.f90:171-183), as RKAdvect hands Zpar to VTurb.
 template <typename E, int NPMAX>
-__device__ void m_update_one(const RpStepArgs& A, int64_t n, const MSpline<NPMAX>& w) {
+__device__ void m_vturb_one(const RpStepArgs& A, int64_t n, const MSpline<NPMAX>& w, float* turbv) {
+    const RpParticlesDev& Pt = A.p;
+    if (!rp_active(A, n)) return;
+    uint32_t fl = 0;
+    const int gid = Pt.gid[n];
+    const RpGridDev& g = A.g[gid - 1];
+    const float Xpar = Pt.x32[n], Ypar = Pt.y32[n];
+    float Zpar = Pt.z32[n] - Pt.cz[n];
+    MStage S1;
+    m_rho_cell(g, Xpar, Ypar, S1.rc, fl);
+    m_stage_2d(m_time(A, g, 0), g, S1);
+    if (A.scheme == 1) {
+        if (Zpar < S1.tdepth) Zpar = S1.tdepth + 0.001f;
+        if (Zpar > S1.zeta) Zpar = S1.zeta - 0.001f;
+    }
+    double q = Pt.qwarm[n], gs = Pt.gwarm[n];
+    turbv[n] = m_vturb<E>(A, g, S1, Zpar, Pt.pid[n], q, gs, fl, w);
+    Pt.qwarm[n] = q;
+    Pt.gwarm[n] = gs;
+    if (fl) Pt.flags[n] |= fl;
+}
+
+// One particle of update_particles in the mixed form.  With turbv_in
+// non-null the VTurb displacement comes from the split form's first kernel.
+template <typename E, int NPMAX>
+__device__ void m_update_one(const RpStepArgs& A, int64_t n, const MSpline<NPMAX>& w, const float* turbv_in) {
     const RpParticlesDev& Pt = A.p;
     if (!rp_active(A, n)) return;
     Pt.age[n] = Pt.age[n] + (double)(float)A.idt;
-    const MPol P = m_pol(A.pi);
     uint32_t fl = 0;
     int gid = Pt.gid[n];
     const RpGridDev& g = A.g[gid - 1];
@@ -688,14 +776,13 @@ __device__ void m_update_one(const RpStepArgs& A, int64_t n, const MSpline<NPMAX
 #pragma unroll 1
         for (int st = 0; st < 4; st++) {
             float U, V, Wv;
-            MStage Sx;
             float xs = Xpar, ys = Ypar, zs = Zpar;
             if (st > 0) {
                 xs = Xpar + kx * half_dt;
                 ys = Ypar + ky * half_dt;
                 zs = Zpar + kz * half_dt;
             }
-            m_find_currents<E>(A, P, g, xs, ys, zs, U, V, Wv, Sx, false, fl);
+            m_find_currents<E>(A, g, xs, ys, zs, U, V, Wv, fl);
             if (st == 0) Zpar = zs;                    // Z is INOUT in find_currents
             kx = U * pm;
             ky = V * pn;
@@ -710,9 +797,9 @@ __device__ void m_update_one(const RpStepArgs& A, int64_t n, const MSpline<NPMAX
         AdvectZ = didt * (AdvectZ * (1.f / 6.f));
     }
     MStage S1;
-    if (A.vturb_on) {
+    if (A.vturb_on && !turbv_in) {
         m_rho_cell(g, Xpar, Ypar, S1.rc, fl);
-        m_stage_2d(P, g, S1);
+        m_stage_2d(m_time(A, g, 0), g, S1);
     }
     float TurbHx = 0.f, TurbHy = 0.f;
     if (A.hturb_on) {                                  // HTurb, hor_turb_module.f90:30-51
@@ -723,9 +810,11 @@ __device__ void m_update_one(const RpStepArgs& A, int64_t n, const MSpline<NPMAX
     TurbHx *= pm;
     TurbHy *= pn;
     float TurbV = 0.f;
-    if (A.vturb_on) {
+    if (A.vturb_on && turbv_in) {
+        TurbV = turbv_in[n];
+    } else if (A.vturb_on) {
         double q = Pt.qwarm[n], gs = Pt.gwarm[n];
-        TurbV = m_vturb<E>(A, P, g, S1, Zpar, pid, q, gs, fl, w);
+        TurbV = m_vturb<E>(A, g, S1, Zpar, pid, q, gs, fl, w);
         Pt.qwarm[n] = q;
         Pt.gwarm[n] = gs;
     }
@@ -752,7 +841,7 @@ __device__ void m_update_one(const RpStepArgs& A, int64_t n, const MSpline<NPMAX
     MRho rn;
     m_rho_cell(gn, tx, ty, rn, fl);
     const float tdepth = -m_bil(gn.h, rn);
-    const float P_zeta = m_polintd(P, m_zeta(gn, rn, gn.sb), m_zeta(gn, rn, gn.sc), m_zeta(gn, rn, gn.sf));
+    const float P_zeta = m_zeta(gn, rn, m_time(A, gn, 0));
     Pt.wd[n] = (double)(-tdepth + P_zeta);
     Pt.zeta[n] = (double)P_zeta;
     Pt.bath[n] = (double)(-tdepth);
