@@ -68,6 +68,9 @@ def parse():
     ap.add_argument("--form", default="mixed", choices=["mixed", "exact"],
                     help="headline form: mixed precision (default) or exact FP64 arithmetic on the workload's "
                          "field storage; the other forms are timed beside it")
+    ap.add_argument("--resort", type=int, default=12,
+                    help="re-sort the particle state by grid and cell every this many internal steps "
+                         "(0: never; results are unchanged)")
     ap.add_argument("--error-study", action="store_true",
                     help="instead of timing: run the exact and the mixed form in lockstep on the same "
                          "frames and noise and report the mixed form's position / profile error")
@@ -383,7 +386,7 @@ def main():
 
     def make_tracker(form):
         T = Tracker([spec], [grid], params, numpar=npart, field_dtype=form, stokes=spec.stokes, seed=7,
-                    device=local)
+                    device=local, resort=args.resort)
         T.set_id_base(rank * npart)     # global particle ids: rank r holds [r*npart, (r+1)*npart)
         for k, slot in enumerate((1, 2, 3)):
             T.upload_frame(1, slot, frames[k])
@@ -536,7 +539,9 @@ def main():
                        "form": FORM_DESC[head],
                        "l2": "inputs larger than L2 (frame ring 390 MB FP32 / 195 MB FP16, particle state "
                              "~80 MB, spline workspace in local memory ~0.5-1 GB)",
-                       "parallelism": f"replicas x{world}: particles split per rank, no data-path collective"},
+                       "parallelism": f"replicas x{world}: particles split per rank, no data-path collective",
+                       "resort": f"particle state re-sorted by grid and cell every {args.resort} internal steps "
+                                 f"(inside the timed region)" if args.resort else "off"},
             "forms": {f: {"value": r["value"], "ms_per_step": r["ms_per_step"],
                           "avg_launch_ms": r["avg_launch_ms"], "desc": FORM_DESC[f],
                           "speedup_vs_plain_fp64": (r["value"] / plain["value"]) if plain else None}

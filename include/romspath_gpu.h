@@ -88,7 +88,11 @@ typedef struct rp_params {
     uint64_t seed;                       /* Philox key of the turbulence noise */
     int32_t device;                      /* CUDA device ordinal               */
     int32_t reserved[7];                 /* [0]: kernel form, 0 fused (default),
-                                            1 split; others must be 0        */
+                                            1 split; [1]: re-sort the particle
+                                            state by grid and cell every that
+                                            many internal steps (0: never;
+                                            results are unchanged, gathers
+                                            coalesce); others must be 0      */
 } rp_params;
 
 /* One grid (GRIDS(ng), grid_module.f90:14-35).  Pointers are borrowed for
@@ -185,7 +189,9 @@ int rp_last_error(rp_ctx *ctx, char *buf, int32_t len);
 int rp_destroy(rp_ctx *ctx);
 
 /* Device-resident state, for callers that keep particles in HBM between
- * calls (pointers stay valid until rp_destroy).  In the mixed form the
+ * calls (pointers stay valid until rp_destroy).  With re-sorting on
+ * (rp_params.reserved[1]) the columns are in the library's order: pid[i]
+ * minus the id base of the particle set is particle i's index.  In the mixed form the
  * positions live in compensated FP32 columns: rp_device_state_get first
  * writes x, y, z from them (and waits), and the mixed step does not read
  * x, y, z back. */

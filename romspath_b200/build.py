@@ -28,6 +28,7 @@ UNITS = [
     ("rp_kernels.cu", ["-fmad=false"]),
     ("rp_noalloc.cu", ["-fmad=false"]),
     ("rp_mixed.cu", []),          # mixed-precision form: FMA contraction allowed
+    ("rp_sort.cu", []),           # re-sorting of the particle state (no arithmetic on values)
     ("rp_api.cu", []),
 ]
 

@@ -79,6 +79,12 @@ struct rp_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool timed = false;
     int last_kernels = 0;
+    // re-sorting by cell: every `resort` internal steps (0: never)
+    int resort = 0;
+    int64_t since_sort = 0;
+    bool permuted = false;                     // columns not in the caller's order
+    uint32_t state_base = 0;                   // id base of the current particle set
+    rp::SortBufs sb;
     int64_t launches = 0;
     std::string err;
 };
@@ -255,7 +261,7 @@ void free_ctx(rp_ctx* c) {
     void* ptrs[] = {c->x, c->y, c->z, c->age, c->dob, c->status, c->wd, c->zeta, c->bath,
                     c->gid, c->isin, c->pid, c->flags, c->tmp_gid, c->tmp_isin, c->hook, c->turbv,
                     c->dstage[0], c->dstage[1], c->x32, c->y32, c->z32, c->cx, c->cy, c->cz, c->qwarm, c->gwarm,
-                    c->ftmp, c->qmax};
+                    c->ftmp, c->qmax, c->sb.keys, c->sb.hist, c->sb.sums, c->sb.perm, c->sb.gbase};
     for (void* p : ptrs) if (p) cudaFree(p);
     for (int h = 0; h < 2; h++) {
         if (c->pin[h]) cudaFreeHost(c->pin[h]);
@@ -481,6 +487,21 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
         dalloc(&ctx->flags, cap * 4) || dalloc(&ctx->tmp_gid, cap * 8) || dalloc(&ctx->tmp_isin, cap * 4) ||
         dalloc(&ctx->turbv, cap * 8))
         return bail(RP_ERR_NOMEM, "particle state allocation");
+    ctx->resort = p.reserved[1] > 0 ? p.reserved[1] : 0;
+    if (ctx->resort) {
+        RpStepArgs A{};
+        A.ngrid = ngrid;
+        fill_grids(ctx, A, 1, 1, 1);
+        uint32_t gb[RP_MAXNGRID] = {};
+        ctx->sb.nkeys = rp::sort_key_count(A, gb);
+        if (ctx->sb.nkeys > rp::kSortMaxKeys)
+            return bail(RP_ERR_UNSUPPORTED, "re-sort: grids exceed 1,048,576 cells in all");
+        if (dalloc(&ctx->sb.keys, cap * 4) || dalloc(&ctx->sb.perm, cap * 4) ||
+            dalloc(&ctx->sb.hist, (size_t)ctx->sb.nkeys * 4) || dalloc(&ctx->sb.sums, 1024 * 4) ||
+            dalloc(&ctx->sb.gbase, sizeof(gb)))
+            return bail(RP_ERR_NOMEM, "re-sort buffers");
+        cudaMemcpy(ctx->sb.gbase, gb, sizeof(gb), cudaMemcpyHostToDevice);
+    }
     const size_t half = (size_t)kChunkElems * 8 * 2;
     for (int h = 0; h < 2; h++) {
         if (cudaHostAlloc(&ctx->pin[h], half, cudaHostAllocDefault) != cudaSuccess)
@@ -544,6 +565,9 @@ int rp_set_particles(rp_ctx* ctx, int64_t n, const double* x, const double* y, c
         (rc = h2d(ctx, ctx->tmp_isin, isin, (size_t)n * 4, s)))
         return rc;
     ctx->n = n;
+    ctx->permuted = false;
+    ctx->since_sort = ctx->resort;
+    ctx->state_base = ctx->pid_base;
     RpParticlesDev P = particles_dev(ctx);
     CK(rp::launch_state_from_host(P, ctx->tmp_gid, ctx->tmp_isin, ctx->pid_base, s));
     ctx->launches++;
@@ -578,6 +602,9 @@ int rp_locate_particles(rp_ctx* ctx, int64_t n, const double* ipos, const double
     if (!(rc = h2d(ctx, dip, ipos, nbg, s)) && !(rc = h2d(ctx, djp, jpos, nbg, s)) && !(rc = h2d(ctx, dz, z, nb, s)) &&
         !(rc = h2d(ctx, ddob, dob, nb, s))) {
         ctx->n = n;
+        ctx->permuted = false;
+        ctx->since_sort = ctx->resort;
+        ctx->state_base = ctx->pid_base;
         RpStepArgs A{};
         fill_params(ctx, A);
         fill_grids(ctx, A, t_b, t_b, t_b);
@@ -627,6 +654,12 @@ int rp_step(rp_ctx* ctx, const double ex[3], const double ix[3], int32_t ets, in
         for (int q = 0; q < 3; q++) CK(cudaStreamWaitEvent(s, G.slot_ready[used[q]], 0));
     }
     int nl = 0;
+    if (ctx->resort && ctx->n > 0 && ctx->since_sort >= ctx->resort) {
+        CK(rp::launch_sort(A, ctx->mixed, ctx->sb, ctx->turbv, s, &nl));
+        ctx->permuted = true;
+        ctx->since_sort = 0;
+    }
+    ctx->since_sort++;
     CK(cudaEventRecord(ctx->ev0, s));
     if (ctx->n > 0 && ctx->mixed)
         CK(rp::launch_step_mixed(A, ctx->npmax, ctx->i16, (float*)ctx->turbv, ctx->prm.reserved[0] == 1, s,
@@ -696,26 +729,34 @@ int rp_get_particles(rp_ctx* ctx, int64_t n, double* x, double* y, double* z, do
     if (n < 0 || n > ctx->n) return fail(ctx, RP_ERR_ARG, "rp_get_particles: n exceeds particle count");
     CK(cudaSetDevice(ctx->device));
     cudaStream_t s = ctx->s_comp;
-    int rc;
-    const size_t b8 = (size_t)n * 8;
+    // re-sorted columns are converted whole and returned in the caller's
+    // order (particle k = id - id base)
+    const int64_t nc = ctx->permuted ? ctx->n : n;
     if (ctx->mixed && (x || y || z)) {
         RpParticlesDev P = particles_dev(ctx);
-        P.n = n;
+        P.n = nc;
         CK(rp::launch_mixed_convert(P, 1, s));
         ctx->launches++;
     }
     if (gid || isin) {
         RpParticlesDev P = particles_dev(ctx);
-        P.n = n;
+        P.n = nc;
         CK(rp::launch_state_to_host(P, ctx->tmp_gid, ctx->tmp_isin, s));
         ctx->launches++;
     }
-    if ((x && (rc = d2h(ctx, x, ctx->x, b8, s))) || (y && (rc = d2h(ctx, y, ctx->y, b8, s))) ||
-        (z && (rc = d2h(ctx, z, ctx->z, b8, s))) || (age && (rc = d2h(ctx, age, ctx->age, b8, s))) ||
-        (status && (rc = d2h(ctx, status, ctx->status, b8, s))) || (gid && (rc = d2h(ctx, gid, ctx->tmp_gid, b8, s))) ||
-        (isin && (rc = d2h(ctx, isin, ctx->tmp_isin, (size_t)n * 4, s))) || (wd && (rc = d2h(ctx, wd, ctx->wd, b8, s))) ||
-        (zeta && (rc = d2h(ctx, zeta, ctx->zeta, b8, s))) || (bath && (rc = d2h(ctx, bath, ctx->bath, b8, s))) ||
-        (flags && (rc = d2h(ctx, flags, ctx->flags, (size_t)n * 4, s))))
+    auto col = [&](void* dst, const void* src, int elem) -> int {
+        if (!dst) return RP_OK;
+        const size_t bytes = (size_t)n * elem;
+        if (!ctx->permuted) return d2h(ctx, dst, src, bytes, s);
+        CK(rp::launch_unsort(elem, src, ctx->turbv, ctx->pid, ctx->state_base, ctx->n, n, s));
+        ctx->launches++;
+        return d2h(ctx, dst, ctx->turbv, bytes, s);
+    };
+    int rc;
+    if ((rc = col(x, ctx->x, 8)) || (rc = col(y, ctx->y, 8)) || (rc = col(z, ctx->z, 8)) ||
+        (rc = col(age, ctx->age, 8)) || (rc = col(status, ctx->status, 8)) || (rc = col(gid, ctx->tmp_gid, 8)) ||
+        (rc = col(isin, ctx->tmp_isin, 4)) || (rc = col(wd, ctx->wd, 8)) || (rc = col(zeta, ctx->zeta, 8)) ||
+        (rc = col(bath, ctx->bath, 8)) || (rc = col(flags, ctx->flags, 4)))
         return rc;
     return RP_OK;
 }

@@ -49,6 +49,24 @@ cudaError_t launch_quantize(const float* f, uint32_t* maxbits, float* qs, void* 
                             int i16, int num_sms, cudaStream_t s);
 cudaError_t launch_mixed_convert(const RpParticlesDev& P, int to_f64, cudaStream_t s);
 
+// Re-sorting of the particle state by (grid, tile of cells, cell) (rp_sort.cu)
+struct SortBufs {
+    uint32_t* keys = nullptr;      // n
+    uint32_t* hist = nullptr;      // nkeys counters, then offsets
+    uint32_t* sums = nullptr;      // scan block totals (<= 1024)
+    int32_t* perm = nullptr;       // n: new slot -> old index
+    uint32_t* gbase = nullptr;     // first key of each grid (RP_MAXNGRID_D)
+    int64_t nkeys = 0;
+};
+constexpr int64_t kSortMaxKeys = 1024 * 1024;
+int64_t sort_key_count(const RpStepArgs& A, uint32_t* gbase_host);
+// sorts A.p's columns in place; `scratch8` holds n 8-byte values
+cudaError_t launch_sort(const RpStepArgs& A, int mixed, const SortBufs& b, void* scratch8, cudaStream_t s,
+                        int* nlaunch);
+// dst[pid[i] - base] = src[i] for pid[i] - base < nout (elem = 8, 4 or 1 bytes)
+cudaError_t launch_unsort(int elem, const void* src, void* dst, const uint32_t* pid, uint32_t base, int64_t n,
+                          int64_t nout, cudaStream_t s);
+
 cudaError_t launch_locate(const RpStepArgs& A, int field_dtype, const double* ipos, const double* jpos,
                           const double* z, const double* dob, cudaStream_t s);
 cudaError_t launch_convert(int src_f32, int dst_f32, const void* src, const void* add, void* dst, int ni, int nj,

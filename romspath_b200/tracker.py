@@ -34,7 +34,7 @@ class Tracker:
     def __init__(self, specs, grids: Sequence[Dict[str, np.ndarray]], params: dict, numpar: int,
                  field_dtype: str = "f64", stokes: bool = False, seed: int = 0, device: int = 0,
                  scl: Optional[np.ndarray] = None, off: Optional[np.ndarray] = None,
-                 spline_max_iter: int = 100, variant: str = "fused"):
+                 spline_max_iter: int = 100, variant: str = "fused", resort: int = 0):
         L = _lib.load()
         self.L = L
         self.ng = len(grids)
@@ -68,6 +68,9 @@ class Tracker:
         # memory) or "split" (VTurb kernel with the spline workspace in
         # shared memory writing a scratch array, then the advection kernel)
         P.reserved[0] = {"fused": 0, "split": 1}[variant]
+        # re-sort the particle state by grid and cell every `resort` internal
+        # steps (0: never); results are unchanged
+        P.reserved[1] = int(resort)
         G = (_lib.RpGrid * self.ng)()
         for k, (sp, gr) in enumerate(zip(specs, grids)):
             g = G[k]

@@ -91,13 +91,13 @@ def _steps(case: Case, nsteps: int):
 
 def run_gpu(case: Case, nsteps: int, noise: str = "philox", seed: int = 7,
             hook: Optional[np.ndarray] = None, tracker=None, variant: str = "fused",
-            field_dtype: Optional[str] = None):
+            field_dtype: Optional[str] = None, resort: int = 0):
     """Run the CUDA path; ``field_dtype="mixed"`` selects the mixed-precision
     form (the frames it is given are the same)."""
     from romspath_b200 import Tracker
     T = tracker or Tracker(case.specs, case.grids, case.params, numpar=case.release.z.shape[0],
                            field_dtype=field_dtype or case.spec.field_dtype, stokes=case.spec.stokes, seed=seed,
-                           scl=case.scl, off=case.off, variant=variant)
+                           scl=case.scl, off=case.off, variant=variant, resort=resort)
     for (k, slot) in schedule.initial_loads():
         for ng in range(1, case.ngrid + 1):
             T.upload_frame(ng, slot, case.frame(k, ng))
