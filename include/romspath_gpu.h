@@ -235,6 +235,57 @@ int rp_device_state_get(rp_ctx *ctx, rp_device_state *out);
 int rp_step_noalloc(rp_ctx *ctx, const rp_device_state *state, const double ex[3], const double ix[3],
                     int32_t ets, int32_t t_b, int32_t t_c, int32_t t_f);
 
+/* ------------------------------------------------------------------------
+ * Adjoint pair.  No counterpart in the reference (ROMSPath has no
+ * derivative code): gradients of a loss of the final particle positions
+ * with respect to each particle's initial position and to a multiplier
+ * kappa of the vertical diffusivity AKs, for release attribution.
+ *
+ * The differentiated model is the FP64 step of update_particles
+ * (ROMSPath.f90:662-905) with kappa scaling the AKs data, the smoothing
+ * spline on uniform breaks, and frozen Philox noise.  rp_forward searches
+ * each fit's smoothing parameter as smooth() does (pppack.f90:5108-5317)
+ * and records it; rp_backward, rp_tangent and rp_adj_replay reuse the
+ * recorded values, so the derivatives are those of the trajectory's own
+ * piece (level brackets, reflections, land rejection and hand-off are taken
+ * on values as well).  Frames come from a store that holds the whole time
+ * window, since the backward sweep runs through it in reverse.
+ * ---------------------------------------------------------------------- */
+typedef struct rp_adj_step {
+    double ex[3];                        /* frame times, as rp_step          */
+    double ix[3];                        /* internal times, as rp_step       */
+    int32_t ets;
+    int32_t frame_b, frame_c, frame_f;   /* frames (1..nframes) in time slots b, c, f */
+    uint64_t step_index;                 /* Philox step counter               */
+} rp_adj_step;
+
+/* Allocate the frame store for `nframes` frames of every grid (FP64). */
+int rp_adj_frames(rp_ctx *ctx, int32_t nframes);
+/* Frame number `frame` of grid `ng` into the store (arrays as
+ * rp_upload_frame; Stokes added when params->stokes). */
+int rp_adj_set_frame(rp_ctx *ctx, int32_t ng, int32_t frame, const double *zeta, const double *u,
+                     const double *v, const double *w, const double *aks, const double *su,
+                     const double *sv);
+/* Run `nsteps` steps of the model from the current particle state
+ * (rp_set_particles / rp_locate_particles), keeping the state every
+ * `checkpoint_every` steps and the smoothing parameter of every fit.  The
+ * final state is the context's particle state (rp_get_particles). */
+int rp_forward(rp_ctx *ctx, int32_t nsteps, const rp_adj_step *steps, double kappa, int32_t checkpoint_every);
+/* Given dL/d(final x, y, z) per particle, the gradients with respect to the
+ * initial x, y, z (per particle) and to kappa (summed): reverse sweep over
+ * the checkpoint segments, each segment's step-start states recomputed from
+ * its checkpoint, each step's Jacobian applied transposed. */
+int rp_backward(rp_ctx *ctx, const double *dL_dx, const double *dL_dy, const double *dL_dz, double *dL_dx0,
+                double *dL_dy0, double *dL_dz0, double *dL_dkappa);
+/* Tangent-linear reference: d(final x, y, z)/d(x0, y0, z0, kappa) per
+ * particle by forward propagation, jac[n][3][4] (row x, y, z). */
+int rp_tangent(rp_ctx *ctx, double kappa, double *jac);
+/* The recorded run from other initial x, y, z (NULL: unchanged) and kappa,
+ * with the recorded smoothing parameters: final x, y, z (for finite
+ * differences). */
+int rp_adj_replay(rp_ctx *ctx, const double *x0, const double *y0, const double *z0, double kappa, double *xf,
+                  double *yf, double *zf);
+
 /* Timing of the last rp_step launch sequence on the compute stream, in ms
  * (CUDA events), and the number of kernels it launched. */
 int rp_last_step_stats(rp_ctx *ctx, float *ms, int32_t *kernels);

@@ -21,7 +21,8 @@ EXPORTS = [
     "rp_create", "rp_upload_frame", "rp_upload_frame_f32", "rp_set_particles", "rp_locate_particles",
     "rp_step", "rp_get_particles", "rp_set_id_base", "rp_set_step_index", "rp_set_noise_hook", "rp_synchronize",
     "rp_last_error", "rp_destroy", "rp_device_state_get", "rp_last_step_stats", "rp_kernel_launches",
-    "rp_step_noalloc", "rp_version",
+    "rp_step_noalloc", "rp_version", "rp_adj_frames", "rp_adj_set_frame", "rp_forward", "rp_backward",
+    "rp_tangent", "rp_adj_replay",
 ]
 
 PD = C.POINTER(C.c_double)
@@ -51,6 +52,13 @@ class RpGrid(C.Structure):
         ("mask_rho", PI32), ("mask_u", PI32), ("mask_v", PI32),
         ("s_rho", PD), ("cs_r", PD), ("s_w", PD), ("cs_w", PD),
         ("scl", PD), ("off", PD),
+    ]
+
+
+class RpAdjStep(C.Structure):
+    _fields_ = [
+        ("ex", C.c_double * 3), ("ix", C.c_double * 3), ("ets", C.c_int32),
+        ("frame_b", C.c_int32), ("frame_c", C.c_int32), ("frame_f", C.c_int32), ("step_index", C.c_uint64),
     ]
 
 
@@ -107,6 +115,12 @@ def _declare(L):
     L.rp_kernel_launches.argtypes = [P, C.POINTER(C.c_int64)]
     L.rp_step_noalloc.argtypes = [P, C.POINTER(RpDeviceState), PD, PD, C.c_int32, C.c_int32, C.c_int32,
                                   C.c_int32]
+    L.rp_adj_frames.argtypes = [P, C.c_int32]
+    L.rp_adj_set_frame.argtypes = [P, C.c_int32, C.c_int32] + [PD] * 7
+    L.rp_forward.argtypes = [P, C.c_int32, C.POINTER(RpAdjStep), C.c_double, C.c_int32]
+    L.rp_backward.argtypes = [P] + [PD] * 6 + [PD]
+    L.rp_tangent.argtypes = [P, C.c_double, PD]
+    L.rp_adj_replay.argtypes = [P, PD, PD, PD, C.c_double, PD, PD, PD]
     L.rp_version.restype = C.c_char_p
     for name in EXPORTS:
         if name != "rp_version":

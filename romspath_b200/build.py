@@ -29,6 +29,7 @@ UNITS = [
     ("rp_noalloc.cu", ["-fmad=false"]),
     ("rp_mixed.cu", []),          # mixed-precision form: FMA contraction allowed
     ("rp_sort.cu", []),           # re-sorting of the particle state (no arithmetic on values)
+    ("rp_adjoint.cu", ["-fmad=false"]),   # adjoint pair: double and dual instantiations agree
     ("rp_api.cu", []),
 ]
 

@@ -85,6 +85,23 @@ struct rp_ctx {
     bool permuted = false;                     // columns not in the caller's order
     uint32_t state_base = 0;                   // id base of the current particle set
     rp::SortBufs sb;
+    // adjoint pair: frame store, step table, checkpoints, recorded smoothing
+    // parameters and the backward sweep's buffers
+    struct Adj {
+        int nframes = 0;
+        double* fst[RP_MAXNGRID][5] = {};      // [frame][j][i][k] per field
+        size_t fsize[RP_MAXNGRID][5] = {};     // values per frame
+        std::vector<rp_adj_step> steps;
+        int ckpt = 0;
+        int64_t n = 0;                         // particles of the recorded run
+        double kappa = 1.0;
+        double* ck = nullptr;                  // checkpoints: (nsteps/ckpt + 1) state blocks
+        double* prec = nullptr;                // recorded p: nsteps x n
+        double* seg = nullptr;                 // one segment of step-start states: ckpt blocks
+        double* work = nullptr;                // working state block
+        double *lx = nullptr, *ly = nullptr, *lz = nullptr, *kbar = nullptr, *tan = nullptr;
+        size_t cap_steps = 0;
+    } adj;
     int64_t launches = 0;
     std::string err;
 };
@@ -261,7 +278,12 @@ void free_ctx(rp_ctx* c) {
     void* ptrs[] = {c->x, c->y, c->z, c->age, c->dob, c->status, c->wd, c->zeta, c->bath,
                     c->gid, c->isin, c->pid, c->flags, c->tmp_gid, c->tmp_isin, c->hook, c->turbv,
                     c->dstage[0], c->dstage[1], c->x32, c->y32, c->z32, c->cx, c->cy, c->cz, c->qwarm, c->gwarm,
-                    c->ftmp, c->qmax, c->sb.keys, c->sb.hist, c->sb.sums, c->sb.perm, c->sb.gbase};
+                    c->ftmp, c->qmax, c->sb.keys, c->sb.hist, c->sb.sums, c->sb.perm, c->sb.gbase,
+                    c->adj.ck, c->adj.prec, c->adj.seg, c->adj.work, c->adj.lx, c->adj.ly, c->adj.lz,
+                    c->adj.kbar, c->adj.tan};
+    for (int g = 0; g < RP_MAXNGRID; g++)
+        for (int f = 0; f < 5; f++)
+            if (c->adj.fst[g][f]) cudaFree(c->adj.fst[g][f]);
     for (void* p : ptrs) if (p) cudaFree(p);
     for (int h = 0; h < 2; h++) {
         if (c->pin[h]) cudaFreeHost(c->pin[h]);
@@ -353,6 +375,83 @@ int upload_frame(rp_ctx* ctx, int32_t ng, int32_t slot, const S* zeta, const S* 
         CK(cudaEventRecord(G.slot_free[old], ctx->s_comp));
         G.free_recorded[old] = true;
         G.slot_loaded[old] = false;
+    }
+    return RP_OK;
+}
+
+// An adjoint state block: x, y, z, age, status (doubles), gid (int32),
+// isin (int8) for n particles, laid out in one allocation of
+// adj_block_bytes(n).
+size_t adj_block_bytes(int64_t n) { return (size_t)n * (5 * 8 + 4 + 1) + 64; }
+
+rp::AdjStateDev adj_view(void* base, int64_t n) {
+    rp::AdjStateDev s;
+    char* p = (char*)base;
+    s.x = (double*)p;
+    s.y = s.x + n;
+    s.z = s.y + n;
+    s.age = s.z + n;
+    s.status = s.age + n;
+    s.gid = (int32_t*)(s.status + n);
+    s.isin = (int8_t*)(s.gid + n);
+    return s;
+}
+
+rp::AdjStateDev adj_ctx_state(rp_ctx* c) {
+    rp::AdjStateDev s;
+    s.x = c->x; s.y = c->y; s.z = c->z; s.age = c->age; s.status = c->status; s.gid = c->gid; s.isin = c->isin;
+    return s;
+}
+
+// copy state a -> b (n particles) on stream st
+cudaError_t adj_copy(const rp::AdjStateDev& a, const rp::AdjStateDev& b, int64_t n, cudaStream_t st) {
+    const size_t d = (size_t)n * 8;
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(b.x, a.x, d, cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(b.y, a.y, d, cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(b.z, a.z, d, cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(b.age, a.age, d, cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(b.status, a.status, d, cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(b.gid, a.gid, (size_t)n * 4, cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return e;
+    return cudaMemcpyAsync(b.isin, a.isin, (size_t)n, cudaMemcpyDeviceToDevice, st);
+}
+
+// the arguments of step s of the recorded table
+void adj_args(rp_ctx* ctx, const rp_adj_step& st, RpStepArgs& A, AdjFrames& F, int64_t n) {
+    A = RpStepArgs{};
+    fill_params(ctx, A);
+    fill_grids(ctx, A, 1, 1, 1);
+    A.p.n = n;
+    for (int q = 0; q < 3; q++) { A.ex[q] = st.ex[q]; A.ix[q] = st.ix[q]; }
+    A.pi = polint_consts(st.ex, st.ix[1]);
+    A.ets = st.ets;
+    A.step_index = st.step_index;
+    A.hook = nullptr;
+    const int fr[3] = {st.frame_b, st.frame_c, st.frame_f};
+    for (int g = 0; g < ctx->ngrid; g++)
+        for (int f = 0; f < 5; f++)
+            for (int t = 0; t < 3; t++)
+                F.f[g][f][t] = ctx->adj.fst[g][f] + (size_t)(fr[t] - 1) * ctx->adj.fsize[g][f];
+}
+
+int adj_upload_field(rp_ctx* ctx, const double* src, const double* add, double* dst, int ni, int nj, int nk) {
+    const int64_t total = (int64_t)ni * nj * nk;
+    for (int64_t e0 = 0; e0 < total; e0 += kChunkElems) {
+        const int64_t cnt = std::min<int64_t>(kChunkElems, total - e0);
+        const size_t nb = (size_t)cnt * 8;
+        const int h = ctx->pin_next;
+        ctx->pin_next ^= 1;
+        if (ctx->pin_used[h]) CK(cudaEventSynchronize(ctx->pin_done[h]));
+        char* pin = (char*)ctx->pin[h];
+        char* ds = (char*)ctx->dstage[h];
+        std::memcpy(pin, src + e0, nb);
+        if (add) std::memcpy(pin + (size_t)kChunkElems * 8, add + e0, nb);
+        CK(cudaMemcpyAsync(ds, pin, add ? (size_t)kChunkElems * 8 + nb : nb, cudaMemcpyHostToDevice, ctx->s_copy));
+        CK(rp::launch_adj_store((const double*)ds, add ? (const double*)(ds + (size_t)kChunkElems * 8) : nullptr,
+                                dst, ni, nj, nk, e0, cnt, ctx->s_copy));
+        ctx->launches++;
+        CK(cudaEventRecord(ctx->pin_done[h], ctx->s_copy));
+        ctx->pin_used[h] = true;
     }
     return RP_OK;
 }
@@ -759,6 +858,204 @@ int rp_get_particles(rp_ctx* ctx, int64_t n, double* x, double* y, double* z, do
         (rc = col(bath, ctx->bath, 8)) || (rc = col(flags, ctx->flags, 4)))
         return rc;
     return RP_OK;
+}
+
+// ------------------------------------------------------------ adjoint pair
+
+int rp_adj_frames(rp_ctx* ctx, int32_t nframes) {
+    if (!ctx) return RP_ERR_ARG;
+    if (nframes < 3) return fail(ctx, RP_ERR_ARG, "rp_adj_frames: at least 3 frames");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaDeviceSynchronize());
+    for (int g = 0; g < ctx->ngrid; g++) {
+        const GridBuf& G = ctx->g[g];
+        const size_t n2 = (size_t)G.nx * G.ny, nu = (size_t)(G.nx - 1) * G.ny, nv = (size_t)G.nx * (G.ny - 1);
+        const size_t sz[5] = {n2, nu * G.N, nv * G.N, n2 * (G.N + 1), n2 * (G.N + 1)};
+        for (int f = 0; f < 5; f++) {
+            if (ctx->adj.fst[g][f]) cudaFree(ctx->adj.fst[g][f]);
+            ctx->adj.fst[g][f] = nullptr;
+            ctx->adj.fsize[g][f] = sz[f];
+            if (dalloc(&ctx->adj.fst[g][f], sz[f] * 8 * (size_t)nframes))
+                return fail(ctx, RP_ERR_NOMEM, "rp_adj_frames: frame store allocation");
+        }
+    }
+    ctx->adj.nframes = nframes;
+    return RP_OK;
+}
+
+int rp_adj_set_frame(rp_ctx* ctx, int32_t ng, int32_t frame, const double* zeta, const double* u, const double* v,
+                     const double* w, const double* aks, const double* su, const double* sv) {
+    if (!ctx) return RP_ERR_ARG;
+    if (ng < 1 || ng > ctx->ngrid) return fail(ctx, RP_ERR_ARG, "rp_adj_set_frame: grid id out of range");
+    if (frame < 1 || frame > ctx->adj.nframes)
+        return fail(ctx, RP_ERR_ARG, "rp_adj_set_frame: frame out of the store (rp_adj_frames)");
+    if (!zeta || !u || !v || !w || !aks) return fail(ctx, RP_ERR_ARG, "rp_adj_set_frame: null field");
+    const bool stokes = ctx->prm.stokes != 0;
+    if (stokes && (!su || !sv)) return fail(ctx, RP_ERR_ARG, "rp_adj_set_frame: stokes on but su/sv null");
+    CK(cudaSetDevice(ctx->device));
+    const GridBuf& G = ctx->g[ng - 1];
+    auto dst = [&](int f) { return ctx->adj.fst[ng - 1][f] + (size_t)(frame - 1) * ctx->adj.fsize[ng - 1][f]; };
+    int rc;
+    if ((rc = adj_upload_field(ctx, zeta, nullptr, dst(0), G.nx, G.ny, 1)) ||
+        (rc = adj_upload_field(ctx, u, stokes ? su : nullptr, dst(1), G.nx - 1, G.ny, G.N)) ||
+        (rc = adj_upload_field(ctx, v, stokes ? sv : nullptr, dst(2), G.nx, G.ny - 1, G.N)) ||
+        (rc = adj_upload_field(ctx, w, nullptr, dst(3), G.nx, G.ny, G.N + 1)) ||
+        (rc = adj_upload_field(ctx, aks, nullptr, dst(4), G.nx, G.ny, G.N + 1)))
+        return rc;
+    CK(cudaStreamSynchronize(ctx->s_copy));
+    return RP_OK;
+}
+
+int rp_forward(rp_ctx* ctx, int32_t nsteps, const rp_adj_step* steps, double kappa, int32_t checkpoint_every) {
+    if (!ctx || !steps) return RP_ERR_ARG;
+    if (nsteps < 1 || checkpoint_every < 1) return fail(ctx, RP_ERR_ARG, "rp_forward: nsteps, checkpoint_every >= 1");
+    if (ctx->adj.nframes < 3) return fail(ctx, RP_ERR_STATE, "rp_forward: load the frame store first");
+    if (ctx->permuted) return fail(ctx, RP_ERR_STATE, "rp_forward: particle state is re-sorted; set it again");
+    if (ctx->hook) return fail(ctx, RP_ERR_STATE, "rp_forward: the noise hook is not used by the adjoint pair");
+    for (int s = 0; s < nsteps; s++) {
+        const rp_adj_step& st = steps[s];
+        const int fr[3] = {st.frame_b, st.frame_c, st.frame_f};
+        for (int t = 0; t < 3; t++)
+            if (fr[t] < 1 || fr[t] > ctx->adj.nframes) return fail(ctx, RP_ERR_ARG, "rp_forward: frame out of the store");
+    }
+    CK(cudaSetDevice(ctx->device));
+    auto& J = ctx->adj;
+    const int64_t n = ctx->n;
+    const int nseg = (nsteps + checkpoint_every - 1) / checkpoint_every;
+    const size_t blk = adj_block_bytes(n);
+    // (re)allocate for this run
+    double* bufs[] = {J.ck, J.prec, J.seg, J.work, J.lx, J.ly, J.lz, J.kbar, J.tan};
+    for (double* b : bufs) if (b) cudaFree(b);
+    J.ck = J.prec = J.seg = J.work = J.lx = J.ly = J.lz = J.kbar = J.tan = nullptr;
+    if (dalloc(&J.ck, blk * (size_t)(nseg + 1)) || dalloc(&J.prec, (size_t)nsteps * n * 8) ||
+        dalloc(&J.seg, blk * (size_t)checkpoint_every) || dalloc(&J.work, blk) || dalloc(&J.lx, (size_t)n * 8) ||
+        dalloc(&J.ly, (size_t)n * 8) || dalloc(&J.lz, (size_t)n * 8) || dalloc(&J.kbar, (size_t)n * 8) ||
+        dalloc(&J.tan, (size_t)n * 12 * 8))
+        return fail(ctx, RP_ERR_NOMEM, "rp_forward: checkpoint / record allocation");
+    J.steps.assign(steps, steps + nsteps);
+    J.ckpt = checkpoint_every;
+    J.n = n;
+    J.kappa = kappa;
+    cudaStream_t s = ctx->s_comp;
+    const rp::AdjStateDev cur = adj_ctx_state(ctx);
+    for (int k = 0; k < nsteps; k++) {
+        if (k % checkpoint_every == 0)
+            CK(adj_copy(cur, adj_view((char*)J.ck + blk * (size_t)(k / checkpoint_every), n), n, s));
+        RpStepArgs A;
+        AdjFrames F;
+        adj_args(ctx, J.steps[k], A, F, n);
+        CK(rp::launch_adj(0, A, F, cur, J.prec + (size_t)k * n, 1, kappa, nullptr, nullptr, nullptr, nullptr, nullptr,
+                          ctx->npmax, s, ctx->num_sms));
+        ctx->launches++;
+    }
+    CK(adj_copy(cur, adj_view((char*)J.ck + blk * (size_t)nseg, n), n, s));   // final state
+    CK(cudaStreamSynchronize(s));
+    return RP_OK;
+}
+
+int rp_backward(rp_ctx* ctx, const double* dL_dx, const double* dL_dy, const double* dL_dz, double* dL_dx0,
+                double* dL_dy0, double* dL_dz0, double* dL_dkappa) {
+    if (!ctx || !dL_dx || !dL_dy || !dL_dz) return RP_ERR_ARG;
+    auto& J = ctx->adj;
+    if (J.steps.empty() || !J.ck) return fail(ctx, RP_ERR_STATE, "rp_backward: call rp_forward first");
+    CK(cudaSetDevice(ctx->device));
+    const int64_t n = J.n;
+    const int nsteps = (int)J.steps.size();
+    const size_t blk = adj_block_bytes(n);
+    cudaStream_t s = ctx->s_comp;
+    int rc;
+    if ((rc = h2d(ctx, J.lx, dL_dx, (size_t)n * 8, s)) || (rc = h2d(ctx, J.ly, dL_dy, (size_t)n * 8, s)) ||
+        (rc = h2d(ctx, J.lz, dL_dz, (size_t)n * 8, s)))
+        return rc;
+    CK(cudaMemsetAsync(J.kbar, 0, (size_t)n * 8, s));
+    const int nseg = (nsteps + J.ckpt - 1) / J.ckpt;
+    const rp::AdjStateDev work = adj_view(J.work, n);
+    for (int sg = nseg - 1; sg >= 0; sg--) {
+        const int k0 = sg * J.ckpt, k1 = std::min(nsteps, k0 + J.ckpt);
+        // recompute the segment's step-start states from its checkpoint
+        CK(adj_copy(adj_view((char*)J.ck + blk * (size_t)sg, n), work, n, s));
+        for (int k = k0; k < k1; k++) {
+            CK(adj_copy(work, adj_view((char*)J.seg + blk * (size_t)(k - k0), n), n, s));
+            if (k + 1 < k1) {
+                RpStepArgs A;
+                AdjFrames F;
+                adj_args(ctx, J.steps[k], A, F, n);
+                CK(rp::launch_adj(0, A, F, work, J.prec + (size_t)k * n, 0, J.kappa, nullptr, nullptr, nullptr, nullptr,
+                                  nullptr, ctx->npmax, s, ctx->num_sms));
+                ctx->launches++;
+            }
+        }
+        // reverse steps of the segment
+        for (int k = k1 - 1; k >= k0; k--) {
+            RpStepArgs A;
+            AdjFrames F;
+            adj_args(ctx, J.steps[k], A, F, n);
+            CK(rp::launch_adj(2, A, F, adj_view((char*)J.seg + blk * (size_t)(k - k0), n), J.prec + (size_t)k * n, 0,
+                              J.kappa, nullptr, J.lx, J.ly, J.lz, J.kbar, ctx->npmax, s, ctx->num_sms));
+            ctx->launches++;
+        }
+    }
+    if ((dL_dx0 && (rc = d2h(ctx, dL_dx0, J.lx, (size_t)n * 8, s))) ||
+        (dL_dy0 && (rc = d2h(ctx, dL_dy0, J.ly, (size_t)n * 8, s))) ||
+        (dL_dz0 && (rc = d2h(ctx, dL_dz0, J.lz, (size_t)n * 8, s))))
+        return rc;
+    if (dL_dkappa) {
+        std::vector<double> kb((size_t)n);
+        if ((rc = d2h(ctx, kb.data(), J.kbar, (size_t)n * 8, s))) return rc;
+        double acc = 0.0;
+        for (double v : kb) acc += v;
+        *dL_dkappa = acc;
+    }
+    return RP_OK;
+}
+
+int rp_adj_replay(rp_ctx* ctx, const double* x0, const double* y0, const double* z0, double kappa, double* xf,
+                  double* yf, double* zf) {
+    if (!ctx) return RP_ERR_ARG;
+    auto& J = ctx->adj;
+    if (J.steps.empty() || !J.ck) return fail(ctx, RP_ERR_STATE, "rp_adj_replay: call rp_forward first");
+    CK(cudaSetDevice(ctx->device));
+    const int64_t n = J.n;
+    cudaStream_t s = ctx->s_comp;
+    const rp::AdjStateDev work = adj_view(J.work, n);
+    CK(adj_copy(adj_view(J.ck, n), work, n, s));
+    int rc;
+    if ((x0 && (rc = h2d(ctx, work.x, x0, (size_t)n * 8, s))) || (y0 && (rc = h2d(ctx, work.y, y0, (size_t)n * 8, s))) ||
+        (z0 && (rc = h2d(ctx, work.z, z0, (size_t)n * 8, s))))
+        return rc;
+    for (size_t k = 0; k < J.steps.size(); k++) {
+        RpStepArgs A;
+        AdjFrames F;
+        adj_args(ctx, J.steps[k], A, F, n);
+        CK(rp::launch_adj(0, A, F, work, J.prec + k * n, 0, kappa, nullptr, nullptr, nullptr, nullptr, nullptr,
+                          ctx->npmax, s, ctx->num_sms));
+        ctx->launches++;
+    }
+    if ((xf && (rc = d2h(ctx, xf, work.x, (size_t)n * 8, s))) || (yf && (rc = d2h(ctx, yf, work.y, (size_t)n * 8, s))) ||
+        (zf && (rc = d2h(ctx, zf, work.z, (size_t)n * 8, s))))
+        return rc;
+    return RP_OK;
+}
+
+int rp_tangent(rp_ctx* ctx, double kappa, double* jac) {
+    if (!ctx || !jac) return RP_ERR_ARG;
+    auto& J = ctx->adj;
+    if (J.steps.empty() || !J.ck) return fail(ctx, RP_ERR_STATE, "rp_tangent: call rp_forward first");
+    CK(cudaSetDevice(ctx->device));
+    const int64_t n = J.n;
+    cudaStream_t s = ctx->s_comp;
+    const rp::AdjStateDev work = adj_view(J.work, n);
+    CK(adj_copy(adj_view(J.ck, n), work, n, s));
+    CK(rp::launch_adj_tangent_init(J.tan, n, s));
+    for (size_t k = 0; k < J.steps.size(); k++) {
+        RpStepArgs A;
+        AdjFrames F;
+        adj_args(ctx, J.steps[k], A, F, n);
+        CK(rp::launch_adj(1, A, F, work, J.prec + k * n, 0, kappa, J.tan, nullptr, nullptr, nullptr, nullptr,
+                          ctx->npmax, s, ctx->num_sms));
+        ctx->launches++;
+    }
+    return d2h(ctx, jac, J.tan, (size_t)n * 12 * 8, s);
 }
 
 int rp_set_id_base(rp_ctx* ctx, uint32_t base) {

@@ -95,6 +95,13 @@ struct RpParticlesDev {
     double* gwarm;
 };
 
+// Frame-store pointers of the three time levels (b, c, f) of one step of the
+// adjoint model: f[grid][field][t], field 0 zeta [j][i], 1 u, 2 v, 3 w,
+// 4 AKs [j][i][k] (FP64, one frame each).
+struct AdjFrames {
+    const double* f[RP_MAXNGRID_D][5][3];
+};
+
 // polintd (interpolation_module.f90:72-109) at fixed nodes ex(3) and point
 // x: the node-only terms, identical to the reference's subexpressions.
 struct RpPolint {

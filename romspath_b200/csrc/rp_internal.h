@@ -67,6 +67,26 @@ cudaError_t launch_sort(const RpStepArgs& A, int mixed, const SortBufs& b, void*
 cudaError_t launch_unsort(int elem, const void* src, void* dst, const uint32_t* pid, uint32_t base, int64_t n,
                           int64_t nout, cudaStream_t s);
 
+// Adjoint pair (rp_adjoint.cu).  State columns of the adjoint model.
+struct AdjStateDev {
+    double* x;
+    double* y;
+    double* z;
+    double* age;
+    double* status;
+    int32_t* gid;
+    int8_t* isin;
+};
+// kind 0: step (find: search and record p in prec, else replay prec);
+// 1: tangent step (t: 12 derivatives per particle); 2: reverse step
+// (lx/ly/lz: lambda in/out, kbar: += dL/dkappa per particle)
+cudaError_t launch_adj(int kind, const RpStepArgs& A, const AdjFrames& F, const AdjStateDev& s, double* prec, int find,
+                       double kappa, double* t, double* lx, double* ly, double* lz, double* kbar, int npmax,
+                       cudaStream_t st, int num_sms);
+cudaError_t launch_adj_store(const double* src, const double* add, double* dst, int ni, int nj, int nk, int64_t e0,
+                             int64_t count, cudaStream_t s);
+cudaError_t launch_adj_tangent_init(double* t, int64_t n, cudaStream_t s);
+
 cudaError_t launch_locate(const RpStepArgs& A, int field_dtype, const double* ipos, const double* jpos,
                           const double* z, const double* dob, cudaStream_t s);
 cudaError_t launch_convert(int src_f32, int dst_f32, const void* src, const void* add, void* dst, int ni, int nj,
