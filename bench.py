@@ -62,6 +62,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="cfg2")
     ap.add_argument("--particles", type=int, default=None)
+    ap.add_argument("--scale", type=float, default=1.0, help="--batched: fraction of the particle counts")
     ap.add_argument("--cpu-sample", type=int, default=32768, help="particles in the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -75,6 +76,10 @@ def parse():
                     help="instead of timing: run the exact and the mixed form in lockstep on the same "
                          "frames and noise and report the mixed form's position / profile error")
     ap.add_argument("--days", type=float, default=10.0, help="error study length")
+    ap.add_argument("--batched", action="store_true",
+                    help="instead of the single-grid workload: batched nested grids (400x300x30 parent, 3x and 5x "
+                         "children; 3M / 800k / 200k particles + 16 release ensembles), one launch per internal "
+                         "step over all grids, frame intervals as CUDA graphs, launch settings autotuned")
     ap.add_argument("--adjoint", action="store_true",
                     help="instead of timing the step: the adjoint pair on the 130x98x20 grid (262,144 particles, "
                          "3 days, checkpoints every 48 steps): forward / backward / tangent times and the "
@@ -328,6 +333,88 @@ def error_study(args):
     print(json.dumps(out), flush=True)
 
 
+# ----------------------------------------------------- batched nested grids
+
+def batched_run(args):
+    """Config 4: every grid and ensemble advanced by one launch per internal
+    step (particles carry their grid id; hand-off moves them between
+    grids), each frame interval's 12 steps captured as one CUDA graph, the
+    re-sort interval and particles per thread autotuned on the run."""
+    import torch
+    from romspath_b200 import Tracker
+    from romspath_b200.autotune import tune
+    torch.cuda.set_device(0)
+    specs = synth.config_spec("cfg4")
+    grids = [synth.make_grid(sp) for sp in specs]
+    params = synth.config_params("cfg4")
+    scl, off = synth.nest_maps(specs)
+    counts = [max(1, int(c * args.scale)) for c in synth.CONFIG4_COUNTS]
+    rel = synth.batched_release(specs, grids, counts, n_ensembles=16, ens_min=max(1, int(1000 * args.scale)),
+                                ens_max=max(2, int(500_000 * args.scale)), seed=0)
+    n = rel.z.shape[0]
+    nframes = 4
+    frames = [[synth.make_frame(sp, gr, k * 3600.0) for k in range(nframes)] for sp, gr in zip(specs, grids)]
+    exts = list(schedule.external_steps(30.0, int(params["dt"]), int(params["idt"])))
+    out = {"mode": "batched", "workload": "cfg4: parent 400x300x30 (8% islands) + child A 240x180x30 (3x) + child "
+                                         "B 300x250x30 (5x), children with a 0.1 m/s eddy field; FP32 frames + "
+                                         "Stokes; Kh = 1 m^2/s; VTurb dt_turb = 30 s",
+           "particles": n, "released_over": {"child_B": counts[0], "child_A": counts[1], "parent": counts[2],
+                                             "ensembles": int(n - sum(counts))}}
+    forms = {}
+    for form in (args.mixed_kind, "f32"):
+        T = Tracker(specs, grids, params, numpar=n, field_dtype=form, stokes=True, seed=7, scl=scl, off=off,
+                    resort=12)
+        for k, slot in enumerate((1, 2, 3)):
+            for ng in range(1, len(specs) + 1):
+                T.upload_frame(ng, slot, frames[ng - 1][k])
+        T.locate(rel, t_b=1)
+        st0 = T.get_particles()
+        pos = [2]
+
+        def interval(graph=True):
+            e = exts[pos[0]]
+            for (k, slot) in e.loads:
+                for ng in range(1, len(specs) + 1):
+                    T.upload_frame(ng, slot, frames[ng - 1][(k - 1) % nframes])
+            if graph:
+                T.step_n(e.internal)
+                ms, _ = T.last_step_stats()
+            else:
+                ms = 0.0
+                for it in e.internal:
+                    T.step(it.ex, it.ix, it.ets, it.tb, it.tc, it.tf)
+                    ms += T.last_step_stats()[0]
+            active = int(sum(np.sum(rel.dob < it.ix[2]) for it in e.internal))
+            pos[0] += 1
+            return ms, active
+
+        r = {}
+        if form == args.mixed_kind:
+            r["autotune"] = tune(T, lambda: interval()[0])
+        interval()
+        ms_g, act, ms_p = [], 0, []
+        for _ in range(args.steps):
+            m, a = interval(graph=True)
+            ms_g.append(m)
+            act += a
+        for _ in range(2):
+            ms_p.append(interval(graph=False)[0])
+        st = T.get_particles()
+        T.close()
+        own0 = np.bincount(st0["gid"].astype(int), minlength=len(specs) + 1)[1:]
+        own = np.bincount(st["gid"].astype(int), minlength=len(specs) + 1)[1:]
+        r.update({"ms_per_interval_graph": float(np.median(ms_g)), "ms_per_interval_stepwise": float(np.median(ms_p)),
+                  "active_particle_steps_per_s": act / (sum(ms_g) / 1e3),
+                  "owned_by_grid_at_start": {"child_B": int(own0[0]), "child_A": int(own0[1]), "parent": int(own0[2])},
+                  "owned_by_grid_at_end": {"child_B": int(own[0]), "child_A": int(own[1]), "parent": int(own[2])},
+                  "grid_changes": int(np.sum(st["gid"] != st0["gid"]))})
+        forms[form] = r
+    out["forms"] = forms
+    out["speedup_mixed_over_exact"] = forms[args.mixed_kind]["active_particle_steps_per_s"] / \
+        forms["f32"]["active_particle_steps_per_s"]
+    print(json.dumps(out), flush=True)
+
+
 # ---------------------------------------------------------------- adjoint
 
 def adjoint_run(args):
@@ -459,6 +546,9 @@ def main():
         return
     if args.adjoint:
         adjoint_run(args)
+        return
+    if args.batched:
+        batched_run(args)
         return
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -92,7 +92,10 @@ typedef struct rp_params {
                                             state by grid and cell every that
                                             many internal steps (0: never;
                                             results are unchanged, gathers
-                                            coalesce); others must be 0      */
+                                            coalesce); [2]: cap on resident
+                                            blocks per SM of the step kernels
+                                            (0: the occupancy limit; sets the
+                                            particles per thread); others 0 */
 } rp_params;
 
 /* One grid (GRIDS(ng), grid_module.f90:14-35).  Pointers are borrowed for
@@ -154,6 +157,15 @@ int rp_locate_particles(rp_ctx *ctx, int64_t n, const double *ipos, const double
  * (ROMSPath.f90:465-546). */
 int rp_step(rp_ctx *ctx, const double ex[3], const double ix[3], int32_t ets, int32_t t_b,
             int32_t t_c, int32_t t_f);
+
+/* `nsteps` internal steps in one call (typically the 12 of one external
+ * step, run_Internal_Timestep's loop, ROMSPath.f90:517-530): ex, ix are
+ * [nsteps][3], ets and the slots [nsteps].  The steps' launches are
+ * captured into a CUDA graph and launched as one; the graph of the previous
+ * call is updated in place when it has the same shape.  Same results as
+ * nsteps calls of rp_step. */
+int rp_step_n(rp_ctx *ctx, int32_t nsteps, const double *ex, const double *ix, const int32_t *ets,
+              const int32_t *t_b, const int32_t *t_c, const int32_t *t_f);
 
 /* Read back par(:,pX/pY/pZ/pAge/pStatus/pGID), isIn, par(:,pWD/pZeta/pBath)
  * and the per-particle flag bits for particles 1..n.  Any pointer may be
@@ -285,6 +297,12 @@ int rp_tangent(rp_ctx *ctx, double kappa, double *jac);
  * differences). */
 int rp_adj_replay(rp_ctx *ctx, const double *x0, const double *y0, const double *z0, double kappa, double *xf,
                   double *yf, double *zf);
+
+/* Change the launch settings of rp_params.reserved[1] (re-sort interval,
+ * 0: never) and [2] (resident blocks per SM, 0: occupancy limit) between
+ * steps; results do not depend on them (an autotuner times real steps of
+ * the run under each setting).  No counterpart in the reference. */
+int rp_set_launch(rp_ctx *ctx, int32_t resort, int32_t blocks_per_sm);
 
 /* Timing of the last rp_step launch sequence on the compute stream, in ms
  * (CUDA events), and the number of kernels it launched. */

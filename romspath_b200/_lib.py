@@ -22,7 +22,7 @@ EXPORTS = [
     "rp_step", "rp_get_particles", "rp_set_id_base", "rp_set_step_index", "rp_set_noise_hook", "rp_synchronize",
     "rp_last_error", "rp_destroy", "rp_device_state_get", "rp_last_step_stats", "rp_kernel_launches",
     "rp_step_noalloc", "rp_version", "rp_adj_frames", "rp_adj_set_frame", "rp_forward", "rp_backward",
-    "rp_tangent", "rp_adj_replay",
+    "rp_tangent", "rp_adj_replay", "rp_step_n", "rp_set_launch",
 ]
 
 PD = C.POINTER(C.c_double)
@@ -115,6 +115,8 @@ def _declare(L):
     L.rp_kernel_launches.argtypes = [P, C.POINTER(C.c_int64)]
     L.rp_step_noalloc.argtypes = [P, C.POINTER(RpDeviceState), PD, PD, C.c_int32, C.c_int32, C.c_int32,
                                   C.c_int32]
+    L.rp_step_n.argtypes = [P, C.c_int32, PD, PD, PI32, PI32, PI32, PI32]
+    L.rp_set_launch.argtypes = [P, C.c_int32, C.c_int32]
     L.rp_adj_frames.argtypes = [P, C.c_int32]
     L.rp_adj_set_frame.argtypes = [P, C.c_int32, C.c_int32] + [PD] * 7
     L.rp_forward.argtypes = [P, C.c_int32, C.POINTER(RpAdjStep), C.c_double, C.c_int32]

@@ -79,6 +79,7 @@ struct rp_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool timed = false;
     int last_kernels = 0;
+    cudaGraphExec_t gexec = nullptr;           // rp_step_n's graph of one call's launches
     // re-sorting by cell: every `resort` internal steps (0: never)
     int resort = 0;
     int64_t since_sort = 0;
@@ -216,6 +217,7 @@ void fill_params(const rp_ctx* c, RpStepArgs& A) {
     A.idt = p.idt; A.scheme = p.scheme; A.nsb = p.nsb;
     A.vturb_on = p.vturb_on; A.hturb_on = p.hturb_on; A.oob = p.open_ocean_boundary;
     A.loop = p.idt / (int)p.deltat;
+    A.grid_cap = p.reserved[2] > 0 ? p.reserved[2] : 0;
     A.spline_max_iter = p.spline_max_iter > 0 ? p.spline_max_iter : 100;
     A.vertdist = p.vertdist; A.serr = p.serr; A.smth = p.smth; A.sub = p.sub;
     A.deltat = p.deltat; A.aksback = p.aksback;
@@ -289,6 +291,7 @@ void free_ctx(rp_ctx* c) {
         if (c->pin[h]) cudaFreeHost(c->pin[h]);
         if (c->pin_done[h]) cudaEventDestroy(c->pin_done[h]);
     }
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->s_comp) cudaStreamDestroy(c->s_comp);
@@ -376,6 +379,25 @@ int upload_frame(rp_ctx* ctx, int32_t ng, int32_t slot, const S* zeta, const S* 
         G.free_recorded[old] = true;
         G.slot_loaded[old] = false;
     }
+    return RP_OK;
+}
+
+// Buffers of the re-sort (once per context).
+int sort_buffers(rp_ctx* ctx) {
+    if (ctx->sb.keys) return RP_OK;
+    RpStepArgs A{};
+    A.ngrid = ctx->ngrid;
+    fill_grids(ctx, A, 1, 1, 1);
+    uint32_t gb[RP_MAXNGRID] = {};
+    ctx->sb.nkeys = rp::sort_key_count(A, gb);
+    if (ctx->sb.nkeys > rp::kSortMaxKeys)
+        return fail(ctx, RP_ERR_UNSUPPORTED, "re-sort: grids exceed 1,048,576 cells in all");
+    const size_t cap = (size_t)ctx->cap;
+    if (dalloc(&ctx->sb.keys, cap * 4) || dalloc(&ctx->sb.perm, cap * 4) ||
+        dalloc(&ctx->sb.hist, (size_t)ctx->sb.nkeys * 4) || dalloc(&ctx->sb.sums, 1024 * 4) ||
+        dalloc(&ctx->sb.gbase, sizeof(gb)))
+        return fail(ctx, RP_ERR_NOMEM, "re-sort buffers");
+    CK(cudaMemcpy(ctx->sb.gbase, gb, sizeof(gb), cudaMemcpyHostToDevice));
     return RP_OK;
 }
 
@@ -588,18 +610,8 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
         return bail(RP_ERR_NOMEM, "particle state allocation");
     ctx->resort = p.reserved[1] > 0 ? p.reserved[1] : 0;
     if (ctx->resort) {
-        RpStepArgs A{};
-        A.ngrid = ngrid;
-        fill_grids(ctx, A, 1, 1, 1);
-        uint32_t gb[RP_MAXNGRID] = {};
-        ctx->sb.nkeys = rp::sort_key_count(A, gb);
-        if (ctx->sb.nkeys > rp::kSortMaxKeys)
-            return bail(RP_ERR_UNSUPPORTED, "re-sort: grids exceed 1,048,576 cells in all");
-        if (dalloc(&ctx->sb.keys, cap * 4) || dalloc(&ctx->sb.perm, cap * 4) ||
-            dalloc(&ctx->sb.hist, (size_t)ctx->sb.nkeys * 4) || dalloc(&ctx->sb.sums, 1024 * 4) ||
-            dalloc(&ctx->sb.gbase, sizeof(gb)))
-            return bail(RP_ERR_NOMEM, "re-sort buffers");
-        cudaMemcpy(ctx->sb.gbase, gb, sizeof(gb), cudaMemcpyHostToDevice);
+        const int rc = sort_buffers(ctx);
+        if (rc != RP_OK) return bail(rc, ctx->err);
     }
     const size_t half = (size_t)kChunkElems * 8 * 2;
     for (int h = 0; h < 2; h++) {
@@ -724,19 +736,39 @@ int rp_locate_particles(rp_ctx* ctx, int64_t n, const double* ipos, const double
     return rc;
 }
 
-int rp_step(rp_ctx* ctx, const double ex[3], const double ix[3], int32_t ets, int32_t t_b, int32_t t_c,
-            int32_t t_f) {
-    if (!ctx || !ex || !ix) return RP_ERR_ARG;
+}  // extern "C"
+
+namespace {
+
+// Checks of one internal step's arguments (rp_step / rp_step_n).
+int step_check(rp_ctx* ctx, const double* ex, const double* ix, int32_t t_b, int32_t t_c, int32_t t_f, int64_t k) {
+    if (!ex || !ix) return RP_ERR_ARG;
     if (t_b < 1 || t_b > 3 || t_c < 1 || t_c > 3 || t_f < 1 || t_f > 3)
         return fail(ctx, RP_ERR_ARG, "rp_step: slots must be 1..3");
-    for (int k = 0; k < ctx->ngrid; k++) {
-        const GridBuf& G = ctx->g[k];
+    for (int g = 0; g < ctx->ngrid; g++) {
+        const GridBuf& G = ctx->g[g];
         if (G.map[t_b - 1] < 0 || G.map[t_c - 1] < 0 || G.map[t_f - 1] < 0)
             return fail(ctx, RP_ERR_STATE, "rp_step: a frame slot was never loaded");
     }
-    if (ctx->hook && ctx->hook_pos >= ctx->hook_steps)
+    if (ctx->hook && ctx->hook_pos + k >= ctx->hook_steps)
         return fail(ctx, RP_ERR_STATE, "rp_step: noise hook exhausted");
-    CK(cudaSetDevice(ctx->device));
+    return RP_OK;
+}
+
+// The compute stream waits for the uploads of the slots a step reads.
+int step_waits(rp_ctx* ctx, int32_t t_b, int32_t t_c, int32_t t_f) {
+    for (int g = 0; g < ctx->ngrid; g++) {
+        const GridBuf& G = ctx->g[g];
+        const int used[3] = {G.map[t_b - 1], G.map[t_c - 1], G.map[t_f - 1]};
+        for (int q = 0; q < 3; q++) CK(cudaStreamWaitEvent(ctx->s_comp, G.slot_ready[used[q]], 0));
+    }
+    return RP_OK;
+}
+
+// The launches of one internal step on the compute stream (re-sort when
+// due, then the step kernels); advances the step counter and the hook.
+int step_launch(rp_ctx* ctx, const double ex[3], const double ix[3], int32_t ets, int32_t t_b, int32_t t_c,
+                int32_t t_f, int* nl) {
     cudaStream_t s = ctx->s_comp;
     RpStepArgs A{};
     fill_params(ctx, A);
@@ -747,31 +779,92 @@ int rp_step(rp_ctx* ctx, const double ex[3], const double ix[3], int32_t ets, in
     A.ets = ets;
     A.step_index = ctx->step_index;
     A.hook = ctx->hook ? ctx->hook + ctx->hook_pos * ctx->n * ctx->ndraw : nullptr;
-    for (int k = 0; k < ctx->ngrid; k++) {
-        const GridBuf& G = ctx->g[k];
-        const int used[3] = {G.map[t_b - 1], G.map[t_c - 1], G.map[t_f - 1]};
-        for (int q = 0; q < 3; q++) CK(cudaStreamWaitEvent(s, G.slot_ready[used[q]], 0));
-    }
-    int nl = 0;
     if (ctx->resort && ctx->n > 0 && ctx->since_sort >= ctx->resort) {
-        CK(rp::launch_sort(A, ctx->mixed, ctx->sb, ctx->turbv, s, &nl));
+        CK(rp::launch_sort(A, ctx->mixed, ctx->sb, ctx->turbv, s, nl));
         ctx->permuted = true;
         ctx->since_sort = 0;
     }
     ctx->since_sort++;
-    CK(cudaEventRecord(ctx->ev0, s));
     if (ctx->n > 0 && ctx->mixed)
         CK(rp::launch_step_mixed(A, ctx->npmax, ctx->i16, (float*)ctx->turbv, ctx->prm.reserved[0] == 1, s,
-                                 ctx->num_sms, &nl));
+                                 ctx->num_sms, nl));
     else if (ctx->n > 0)
         CK(rp::launch_step(A, ctx->prm.field_dtype, ctx->npmax, ctx->turbv, ctx->prm.reserved[0] == 1 ? 0 : 1, s,
-                           ctx->num_sms, &nl));
+                           ctx->num_sms, nl));
+    ctx->step_index++;
+    if (ctx->hook) ctx->hook_pos++;
+    return RP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rp_step(rp_ctx* ctx, const double ex[3], const double ix[3], int32_t ets, int32_t t_b, int32_t t_c,
+            int32_t t_f) {
+    if (!ctx) return RP_ERR_ARG;
+    int rc;
+    if ((rc = step_check(ctx, ex, ix, t_b, t_c, t_f, 0)) != RP_OK) return rc;
+    CK(cudaSetDevice(ctx->device));
+    if ((rc = step_waits(ctx, t_b, t_c, t_f)) != RP_OK) return rc;
+    int nl = 0;
+    CK(cudaEventRecord(ctx->ev0, ctx->s_comp));
+    if ((rc = step_launch(ctx, ex, ix, ets, t_b, t_c, t_f, &nl)) != RP_OK) return rc;
+    CK(cudaEventRecord(ctx->ev1, ctx->s_comp));
+    ctx->timed = true;
+    ctx->last_kernels = nl;
+    ctx->launches += nl;
+    return RP_OK;
+}
+
+int rp_step_n(rp_ctx* ctx, int32_t nsteps, const double* ex, const double* ix, const int32_t* ets,
+              const int32_t* t_b, const int32_t* t_c, const int32_t* t_f) {
+    if (!ctx || !ex || !ix || !ets || !t_b || !t_c || !t_f) return RP_ERR_ARG;
+    if (nsteps < 1) return fail(ctx, RP_ERR_ARG, "rp_step_n: nsteps >= 1");
+    int rc;
+    for (int k = 0; k < nsteps; k++)
+        if ((rc = step_check(ctx, ex + 3 * k, ix + 3 * k, t_b[k], t_c[k], t_f[k], k)) != RP_OK) return rc;
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->s_comp;
+    for (int k = 0; k < nsteps; k++)
+        if ((rc = step_waits(ctx, t_b[k], t_c[k], t_f[k])) != RP_OK) return rc;
+    // capture this call's launches; the graph of the previous call is
+    // updated in place when its shape is the same
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    int nl = 0;
+    for (int k = 0; k < nsteps && rc == RP_OK; k++)
+        rc = step_launch(ctx, ex + 3 * k, ix + 3 * k, ets[k], t_b[k], t_c[k], t_f[k], &nl);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(s, &graph);
+    if (rc != RP_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (ec != cudaSuccess) return fail(ctx, RP_ERR_CUDA, std::string("rp_step_n: capture: ") + cudaGetErrorString(ec));
+    bool updated = false;
+    if (ctx->gexec) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(ctx->gexec, graph, &info) == cudaSuccess) {
+            updated = true;
+        } else {
+            cudaGetLastError();
+            cudaGraphExecDestroy(ctx->gexec);
+            ctx->gexec = nullptr;
+        }
+    }
+    cudaError_t e = cudaSuccess;
+    if (!updated) e = cudaGraphInstantiate(&ctx->gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        ctx->gexec = nullptr;
+        return fail(ctx, RP_ERR_CUDA, std::string("rp_step_n: instantiate: ") + cudaGetErrorString(e));
+    }
+    CK(cudaEventRecord(ctx->ev0, s));
+    CK(cudaGraphLaunch(ctx->gexec, s));
     CK(cudaEventRecord(ctx->ev1, s));
     ctx->timed = true;
     ctx->last_kernels = nl;
     ctx->launches += nl;
-    ctx->step_index++;
-    if (ctx->hook) ctx->hook_pos++;
     return RP_OK;
 }
 
@@ -1056,6 +1149,22 @@ int rp_tangent(rp_ctx* ctx, double kappa, double* jac) {
         ctx->launches++;
     }
     return d2h(ctx, jac, J.tan, (size_t)n * 12 * 8, s);
+}
+
+int rp_set_launch(rp_ctx* ctx, int32_t resort, int32_t blocks_per_sm) {
+    if (!ctx) return RP_ERR_ARG;
+    if (resort < 0 || blocks_per_sm < 0) return fail(ctx, RP_ERR_ARG, "rp_set_launch: values must be >= 0");
+    CK(cudaSetDevice(ctx->device));
+    if (resort > 0) {
+        CK(cudaStreamSynchronize(ctx->s_comp));
+        const int rc = sort_buffers(ctx);
+        if (rc != RP_OK) return rc;
+    }
+    ctx->resort = resort;
+    ctx->prm.reserved[1] = resort;
+    ctx->prm.reserved[2] = blocks_per_sm;
+    if (ctx->since_sort > resort) ctx->since_sort = resort;
+    return RP_OK;
 }
 
 int rp_set_id_base(rp_ctx* ctx, uint32_t base) {

@@ -126,6 +126,7 @@ struct RpStepArgs {
     int ngrid;
     int idt, scheme, nsb, vturb_on, hturb_on, oob;
     int loop;                      // idt / int(deltat)
+    int grid_cap;                  // resident blocks per SM of the step kernels (0: occupancy limit)
     int spline_max_iter;
     double vertdist, serr, smth, sub, deltat, aksback;
     double khturb[RP_MAXNGRID_D];

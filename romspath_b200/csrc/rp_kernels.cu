@@ -47,10 +47,11 @@ __global__ void __launch_bounds__(kStepBlock, kVturbMinBlocks) k_step_fused(cons
 }
 
 template <class K>
-static int64_t grid_for(K kernel, int block, size_t smem, int64_t n, int num_sms, cudaError_t* err) {
+static int64_t grid_for(K kernel, int block, size_t smem, int64_t n, int num_sms, cudaError_t* err, int cap = 0) {
     int occ = 0;
     *err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, block, smem);
     if (occ < 1) occ = 1;
+    if (cap > 0 && occ > cap) occ = cap;
     int64_t need = (n + block - 1) / block;
     int64_t blocks = (int64_t)num_sms * occ;
     if (need < blocks) blocks = need;
@@ -62,20 +63,20 @@ static cudaError_t launch_step_t(const RpStepArgs& A, double* turbv, int variant
                                  int* nlaunch) {
     cudaError_t e = cudaSuccess;
     if (variant == 1) {
-        const int64_t blocks = grid_for(k_step_fused<T, NPMAX>, kStepBlock, 0, A.p.n, num_sms, &e);
+        const int64_t blocks = grid_for(k_step_fused<T, NPMAX>, kStepBlock, 0, A.p.n, num_sms, &e, A.grid_cap);
         if (e != cudaSuccess) return e;
         k_step_fused<T, NPMAX><<<(unsigned)blocks, kStepBlock, 0, s>>>(A);
         *nlaunch += 1;
         return cudaGetLastError();
     }
     if (A.vturb_on) {
-        const int64_t blocks = grid_for(k_vturb_local<T, NPMAX>, kStepBlock, 0, A.p.n, num_sms, &e);
+        const int64_t blocks = grid_for(k_vturb_local<T, NPMAX>, kStepBlock, 0, A.p.n, num_sms, &e, A.grid_cap);
         if (e != cudaSuccess) return e;
         k_vturb_local<T, NPMAX><<<(unsigned)blocks, kStepBlock, 0, s>>>(A, turbv);
         *nlaunch += 1;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
-    const int64_t blocks = grid_for(k_advect<T>, kStepBlock, 0, A.p.n, num_sms, &e);
+    const int64_t blocks = grid_for(k_advect<T>, kStepBlock, 0, A.p.n, num_sms, &e, A.grid_cap);
     if (e != cudaSuccess) return e;
     k_advect<T><<<(unsigned)blocks, kStepBlock, 0, s>>>(A, A.vturb_on ? turbv : nullptr);
     *nlaunch += 1;

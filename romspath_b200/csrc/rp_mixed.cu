@@ -64,7 +64,7 @@ static cudaError_t launch_mixed_t(const RpStepArgs& A, float* turbv, int split, 
     int64_t blocks = 0;
     cudaError_t e;
     if (!split || !A.vturb_on) {
-        if ((e = resident_grid(k_step_mixed<E, NPMAX>, A.p.n, num_sms, 0, &blocks)) != cudaSuccess) return e;
+        if ((e = resident_grid(k_step_mixed<E, NPMAX>, A.p.n, num_sms, A.grid_cap, &blocks)) != cudaSuccess) return e;
         k_step_mixed<E, NPMAX><<<(unsigned)blocks, kStepBlock, 0, s>>>(A);
         *nlaunch += 1;
         return cudaGetLastError();
@@ -74,7 +74,7 @@ static cudaError_t launch_mixed_t(const RpStepArgs& A, float* turbv, int split, 
     k_vturb_mixed<E, NPMAX><<<(unsigned)blocks, kStepBlock, 0, s>>>(A, turbv);
     *nlaunch += 1;
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if ((e = resident_grid(k_advect_mixed<E>, A.p.n, num_sms, 0, &blocks)) != cudaSuccess) return e;
+    if ((e = resident_grid(k_advect_mixed<E>, A.p.n, num_sms, A.grid_cap, &blocks)) != cudaSuccess) return e;
     k_advect_mixed<E><<<(unsigned)blocks, kStepBlock, 0, s>>>(A, turbv);
     *nlaunch += 1;
     return cudaGetLastError();

@@ -373,6 +373,66 @@ def nested_release(specs: List[GridSpec], grids, frames1, n: int, seed: int = 0,
     return Release(ipos=ipos, jpos=jpos, z=z, dob=np.full(n, dob))
 
 
+def batched_release(specs: List[GridSpec], grids, counts: List[int], n_ensembles: int = 16,
+                    ens_min: int = 1000, ens_max: int = 500_000, seed: int = 0, ens_sigma: float = 3000.0,
+                    ens_spacing_s: float = 3 * 3600.0) -> Release:
+    """The batched nested release: counts[g] particles uniform over the
+    interior of grid g (specs finest first, parent last; a particle released
+    over the parent inside a child belongs to the child, as ini_ROMSPath's
+    first-in-grid rule gives), plus n_ensembles release ensembles of
+    log-uniform sizes in [ens_min, ens_max] (fixed seed): Gaussian patches
+    (ens_sigma m) at random wet points of the parent, ensemble e released
+    at e * ens_spacing_s.  ipos/jpos hold the indices in every grid."""
+    rng = np.random.default_rng(seed)
+    parent, pg = specs[-1], grids[-1]
+    mk = pg["mask_rho"]
+
+    def wet_parent(m):
+        xs, ys, got = [], [], 0
+        while got < m:
+            X = rng.uniform(2.0, parent.xi_rho - 1.0, 2 * (m - got) + 8)
+            Y = rng.uniform(2.0, parent.eta_rho - 1.0, 2 * (m - got) + 8)
+            I = np.clip(np.floor(X).astype(int) - 1, 0, parent.xi_rho - 2)
+            J = np.clip(np.floor(Y).astype(int) - 1, 0, parent.eta_rho - 2)
+            wet = (mk[I, J] + mk[I + 1, J] + mk[I, J + 1] + mk[I + 1, J + 1]) == 4
+            sel = np.nonzero(wet)[0][: m - got]
+            xs.append(parent.x0 + (X[sel] - 1.0) * parent.dx)
+            ys.append(parent.y0 + (Y[sel] - 1.0) * parent.dy)
+            got += len(sel)
+        return np.concatenate(xs), np.concatenate(ys)
+
+    xs, ys, dobs = [], [], []
+    for g, (sp, m) in enumerate(zip(specs, counts)):
+        if m <= 0:
+            continue
+        if g == len(specs) - 1:
+            x, y = wet_parent(m)
+        else:
+            x = sp.x0 + rng.uniform(2.0, sp.xi_rho - 2.0, m) * sp.dx
+            y = sp.y0 + rng.uniform(2.0, sp.eta_rho - 2.0, m) * sp.dy
+        xs.append(x)
+        ys.append(y)
+        dobs.append(np.zeros(m))
+    sizes = np.exp(rng.uniform(np.log(ens_min), np.log(ens_max), n_ensembles)).astype(np.int64)
+    cx, cy = wet_parent(n_ensembles)
+    lo_x, hi_x = parent.x0 + 2.0 * parent.dx, parent.x0 + (parent.xi_rho - 2.0) * parent.dx
+    lo_y, hi_y = parent.y0 + 2.0 * parent.dy, parent.y0 + (parent.eta_rho - 2.0) * parent.dy
+    for e, m in enumerate(sizes):
+        xs.append(np.clip(cx[e] + rng.normal(0.0, ens_sigma, m), lo_x, hi_x))
+        ys.append(np.clip(cy[e] + rng.normal(0.0, ens_sigma, m), lo_y, hi_y))
+        dobs.append(np.full(m, e * ens_spacing_s))
+    x = np.concatenate(xs)
+    y = np.concatenate(ys)
+    n = x.shape[0]
+    ipos = np.empty((len(specs), n))
+    jpos = np.empty((len(specs), n))
+    for g, sp in enumerate(specs):
+        ipos[g], jpos[g] = index_of(sp, x, y)
+    s = rng.uniform(-0.95, -0.05, n)
+    h = 20.0 + 180.0 * (1.0 - np.exp(-x / 30000.0))
+    return Release(ipos=ipos, jpos=jpos, z=h * s, dob=np.concatenate(dobs))
+
+
 # ------------------------------------------------------------------ configs
 
 def config_spec(name: str) -> List[GridSpec]:
@@ -423,4 +483,6 @@ def config_params(name: str) -> dict:
 
 CONFIG_PARTICLES = {"cfg1": 10_000, "cfg2": 1_048_576, "cfg3": 4_194_304,
                     "cfg5": 262_144, "tiny": 64}
-CONFIG_DAYS = {"cfg1": 2.0, "cfg2": 10.0, "cfg3": 10.0, "cfg5": 3.0, "tiny": 0.25}
+# config 4: per grid (finest first: child B, child A, parent) + 16 ensembles
+CONFIG4_COUNTS = [200_000, 800_000, 3_000_000]
+CONFIG_DAYS = {"cfg1": 2.0, "cfg2": 10.0, "cfg3": 10.0, "cfg4": 5.0, "cfg5": 3.0, "tiny": 0.25}

@@ -34,7 +34,7 @@ class Tracker:
     def __init__(self, specs, grids: Sequence[Dict[str, np.ndarray]], params: dict, numpar: int,
                  field_dtype: str = "f64", stokes: bool = False, seed: int = 0, device: int = 0,
                  scl: Optional[np.ndarray] = None, off: Optional[np.ndarray] = None,
-                 spline_max_iter: int = 100, variant: str = "fused", resort: int = 0):
+                 spline_max_iter: int = 100, variant: str = "fused", resort: int = 0, blocks_per_sm: int = 0):
         L = _lib.load()
         self.L = L
         self.ng = len(grids)
@@ -71,6 +71,9 @@ class Tracker:
         # re-sort the particle state by grid and cell every `resort` internal
         # steps (0: never); results are unchanged
         P.reserved[1] = int(resort)
+        # cap on resident blocks per SM of the step kernels (0: occupancy
+        # limit); fewer blocks mean more particles per thread
+        P.reserved[2] = int(blocks_per_sm)
         G = (_lib.RpGrid * self.ng)()
         for k, (sp, gr) in enumerate(zip(specs, grids)):
             g = G[k]
@@ -175,6 +178,23 @@ class Tracker:
         ixa = (C.c_double * 3)(*ix)
         rc = self.L.rp_step(self.h, exa, ixa, ets, tb, tc, tf)
         self._check(rc, "rp_step")
+
+    def step_n(self, steps):
+        """Several internal steps (objects with ex, ix, ets, tb, tc, tf) in
+        one call, launched as one CUDA graph."""
+        k = len(steps)
+        ex = np.ascontiguousarray([s.ex for s in steps], dtype=np.float64)
+        ix = np.ascontiguousarray([s.ix for s in steps], dtype=np.float64)
+        i32 = lambda v: np.ascontiguousarray(v, dtype=np.int32)
+        ets, tb, tc, tf = (i32([s.ets for s in steps]), i32([s.tb for s in steps]), i32([s.tc for s in steps]),
+                           i32([s.tf for s in steps]))
+        rc = self.L.rp_step_n(self.h, k, _pd(ex), _pd(ix), *[a.ctypes.data_as(_lib.PI32) for a in (ets, tb, tc, tf)])
+        self._check(rc, "rp_step_n")
+
+    def set_launch(self, resort: int, blocks_per_sm: int):
+        """Re-sort interval (0: never) and resident blocks per SM (0: the
+        occupancy limit) from the next step on; results are unchanged."""
+        self._check(self.L.rp_set_launch(self.h, int(resort), int(blocks_per_sm)), "rp_set_launch")
 
     def set_id_base(self, base: int):
         """Particle k of the next locate/set_particles gets id base + k."""
