@@ -79,6 +79,7 @@ struct rp_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool timed = false;
     int last_kernels = 0;
+    bool direct_pending = false;               // an upload read the caller's pinned arrays by DMA
     cudaGraphExec_t gexec = nullptr;           // rp_step_n's graph of one call's launches
     // re-sorting by cell: every `resort` internal steps (0: never)
     int resort = 0;
@@ -309,6 +310,11 @@ int upload_field(rp_ctx* ctx, const S* src, const S* add, void* dst, int ni, int
     const int64_t total = (int64_t)ni * nj * nk;
     const int dst_f32 = (ctx->elem == 4 || f32);
     const int src_f32 = (sizeof(S) == 4);
+    // a page-locked source is copied by DMA straight into the device
+    // staging (the call then waits for the copies before returning, since
+    // the caller may reuse its arrays); otherwise through our pinned halves
+    const bool direct = is_pinned(src) && (!add || is_pinned(add));
+    if (direct) ctx->direct_pending = true;
     for (int64_t e0 = 0; e0 < total; e0 += kChunkElems) {
         const int64_t cnt = std::min<int64_t>(kChunkElems, total - e0);
         const size_t nb = (size_t)cnt * sizeof(S);
@@ -317,12 +323,16 @@ int upload_field(rp_ctx* ctx, const S* src, const S* add, void* dst, int ni, int
         if (ctx->pin_used[h]) CK(cudaEventSynchronize(ctx->pin_done[h]));
         char* pin = (char*)ctx->pin[h];
         char* dst_stage = (char*)ctx->dstage[h];
-        std::memcpy(pin, src + e0, nb);
-        if (add) std::memcpy(pin + (size_t)kChunkElems * 8, add + e0, nb);
-        CK(cudaMemcpyAsync(dst_stage, pin, nb, cudaMemcpyHostToDevice, ctx->s_copy));
+        const char* from = direct ? (const char*)(src + e0) : pin;
+        const char* from_add = direct ? (const char*)(add ? add + e0 : nullptr) : pin + (size_t)kChunkElems * 8;
+        if (!direct) {
+            std::memcpy(pin, src + e0, nb);
+            if (add) std::memcpy(pin + (size_t)kChunkElems * 8, add + e0, nb);
+        }
+        CK(cudaMemcpyAsync(dst_stage, from, nb, cudaMemcpyHostToDevice, ctx->s_copy));
         if (add)
-            CK(cudaMemcpyAsync(dst_stage + (size_t)kChunkElems * 8, pin + (size_t)kChunkElems * 8, nb,
-                               cudaMemcpyHostToDevice, ctx->s_copy));
+            CK(cudaMemcpyAsync(dst_stage + (size_t)kChunkElems * 8, from_add, nb, cudaMemcpyHostToDevice,
+                               ctx->s_copy));
         if (qs)
             CK(rp::launch_stage_f32(src_f32, dst_stage, add ? dst_stage + (size_t)kChunkElems * 8 : nullptr,
                                     ctx->ftmp, e0, cnt, ctx->s_copy));
@@ -370,6 +380,10 @@ int upload_frame(rp_ctx* ctx, int32_t ng, int32_t slot, const S* zeta, const S* 
     if ((rc = upload_field<S>(ctx, w, nullptr, G.w, nx, ny, N + 1, phys, mx, G.qs_w)) != RP_OK) return rc;
     if ((rc = upload_field<S>(ctx, aks, nullptr, G.aks, nx, ny, N + 1, phys, mx, G.qs_aks)) != RP_OK) return rc;
     CK(cudaEventRecord(G.slot_ready[phys], ctx->s_copy));
+    if (ctx->direct_pending) {                 // the caller's arrays are free again once copied
+        CK(cudaEventSynchronize(G.slot_ready[phys]));
+        ctx->direct_pending = false;
+    }
     G.slot_loaded[phys] = true;
     const int old = G.map[slot - 1];
     G.map[slot - 1] = phys;
