@@ -80,6 +80,10 @@ def parse():
                     help="instead of the single-grid workload: batched nested grids (400x300x30 parent, 3x and 5x "
                          "children; 3M / 800k / 200k particles + 16 release ensembles), one launch per internal "
                          "step over all grids, frame intervals as CUDA graphs, launch settings autotuned")
+    ap.add_argument("--config1", action="store_true",
+                    help="instead of timing: the reference's CPU-runnable case end to end (130x98x20 grid, "
+                         "10,000 particles, 2 days), the exact GPU form against the CPU restatement of the "
+                         "reference on the host cores, final states compared bit for bit")
     ap.add_argument("--adjoint", action="store_true",
                     help="instead of timing the step: the adjoint pair on the 130x98x20 grid (262,144 particles, "
                          "3 days, checkpoints every 48 steps): forward / backward / tangent times and the "
@@ -415,6 +419,92 @@ def batched_run(args):
     print(json.dumps(out), flush=True)
 
 
+# ------------------------------------------------------------- config 1
+
+def config1_run(args):
+    """Config 1 end to end: hourly frames uploaded as the driver reads them,
+    576 internal steps of 10,000 particles; the exact GPU form (FP64) and
+    the oracle (FP64 C restatement of the reference, OpenMP over particles,
+    same Philox noise) from the same release; then the serial form of the
+    reference's noise (one MT19937 stream) on the oracle, single-threaded,
+    on a 1,000-particle sample."""
+    import torch
+    from romspath_b200 import Tracker
+    from oracle import oracle as O
+    torch.cuda.set_device(0)
+    spec = synth.config_spec("cfg1")[0]
+    grid = synth.make_grid(spec)
+    params = synth.config_params("cfg1")
+    npart = args.particles or synth.CONFIG_PARTICLES["cfg1"]
+    days = synth.CONFIG_DAYS["cfg1"]
+    frames = {}
+
+    def frame(k):
+        if k not in frames:
+            frames[k] = synth.make_frame(spec, grid, (k - 1) * float(params["dt"]))
+        return frames[k]
+
+    rel = synth.uniform_release(spec, grid, frame(1), npart, seed=0)
+    exts = list(schedule.external_steps(days, int(params["dt"]), int(params["idt"])))
+    for e in exts:                                   # frames made before the timed runs
+        for (k, _) in e.loads:
+            frame(k)
+    for k in (1, 2, 3):
+        frame(k)
+    T = Tracker([spec], [grid], params, numpar=npart, field_dtype="f64", seed=7)
+    T.synchronize()
+    t0 = time.perf_counter()
+    for (k, slot) in schedule.initial_loads():
+        T.upload_frame(1, slot, frame(k))
+    T.locate(rel, t_b=1)
+    nsteps = 0
+    for e in exts:
+        for (k, slot) in e.loads:
+            T.upload_frame(1, slot, frame(k))
+        for it in e.internal:
+            T.step(it.ex, it.ix, it.ets, it.tb, it.tc, it.tf)
+            nsteps += 1
+    g = T.get_particles()
+    t_gpu = time.perf_counter() - t0
+    T.close()
+    threads = os.cpu_count() or 1
+
+    def oracle_run(n, noise, nthreads):
+        m = O.OracleModel([spec], [grid], params)
+        r = synth.Release(ipos=rel.ipos[:, :n], jpos=rel.jpos[:, :n], z=rel.z[:n], dob=rel.dob[:n])
+        mt = O.MT19937(7) if noise == "mt" else None
+        t0 = time.perf_counter()
+        for (k, slot) in schedule.initial_loads():
+            m.set_frame(1, slot, frame(k))
+        m.init_particles(r, tb=1)
+        for e in exts:
+            for (k, slot) in e.loads:
+                m.set_frame(1, slot, frame(k))
+            for it in e.internal:
+                m.step(it.ex, it.ix, it.ets, it.tb, it.tc, it.tf, noise=noise, seed=7, step_index=it.step_index,
+                       mt=mt, nthreads=nthreads)
+        return m.state(), time.perf_counter() - t0
+
+    o, t_cpu = oracle_run(npart, "philox", threads)
+    nser = min(1000, npart)
+    _, t_ser = oracle_run(nser, "mt", 1)
+    same = {}
+    for k in ("x", "y", "z", "age", "status"):
+        a, b = np.asarray(g[k]), np.asarray(o[k]).astype(np.float64)
+        same[k] = int(np.sum(a.view(np.uint64) != b.view(np.uint64)))
+    out = {"mode": "config1", "workload": "cfg1: 130x98x20 grid, 10x10 land corner, VTurb on, HTurb off, 2 days",
+           "particles": npart, "internal_steps": nsteps,
+           "seconds": {"gpu_end_to_end": t_gpu, "cpu_oracle_openmp": t_cpu,
+                       f"cpu_oracle_serial_mt19937_{nser}_particles": t_ser},
+           "particle_steps_per_s": {"gpu_end_to_end": npart * nsteps / t_gpu,
+                                    "cpu_oracle_openmp": npart * nsteps / t_cpu,
+                                    "cpu_oracle_serial_mt19937": nser * nsteps / t_ser},
+           "cpu_threads": threads, "particles_differing_from_oracle": same,
+           "note": "GPU time includes every frame upload from host arrays, the initial lookup and the final "
+                   "read-back; the frames are made before either run"}
+    print(json.dumps(out), flush=True)
+
+
 # ---------------------------------------------------------------- adjoint
 
 def adjoint_run(args):
@@ -549,6 +639,10 @@ def main():
         return
     if args.batched:
         batched_run(args)
+        return
+    if args.config1:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        config1_run(args)
         return
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
