@@ -66,6 +66,13 @@ extern "C" {
  * 11; absolute rather than relative resolution below them). */
 #define RP_FIELD_MIXED_I16 3
 
+/* Diagnostics switches, rp_params.reserved[3] (namelist "other",
+ * ROMSPath.h:325-330; computed at the end of update_particles' particle
+ * loop, ROMSPath.f90:935-986).  F64 and F32 forms only. */
+#define RP_DIAG_SALTTEMP 1       /* SaltTempOn: P_Salt, P_Temp               */
+#define RP_DIAG_SALTTEMP_MEAN 2  /* SaltTempMean: their running sums         */
+#define RP_DIAG_BOTTOM 4         /* WriteBottom: P_HOB, P_bustr, P_bvstr     */
+
 /* Run parameters: the namelist values the hot path reads (ROMSPath.h:77-80
  * timeparam, 140-148 turbparam, 152-154 advectparam, 161-180 behavparam,
  * 304-319 other) plus device options. */
@@ -95,7 +102,9 @@ typedef struct rp_params {
                                             coalesce); [2]: cap on resident
                                             blocks per SM of the step kernels
                                             (0: the occupancy limit; sets the
-                                            particles per thread); others 0 */
+                                            particles per thread); [3]:
+                                            diagnostics, RP_DIAG_* bits;
+                                            others 0 */
 } rp_params;
 
 /* One grid (GRIDS(ng), grid_module.f90:14-35).  Pointers are borrowed for
@@ -138,6 +147,20 @@ int rp_upload_frame_f32(rp_ctx *ctx, int32_t ng, int32_t slot, const float *zeta
                         const float *v, const float *w, const float *aks, const float *su,
                         const float *sv);
 
+/* rp_upload_frame with the fields of the diagnostics: salt and temp
+ * (xi_rho,eta_rho,N) for RP_DIAG_SALTTEMP, bustr (xi_u,eta_u) and bvstr
+ * (xi_v,eta_v) for RP_DIAG_BOTTOM (hydrodynamic_module.f90:262-450; the
+ * caller adds TempOffset, as updateHydro does).  With a diagnostic on, its
+ * fields are required on every upload and rp_upload_frame refuses. */
+int rp_upload_frame_ext(rp_ctx *ctx, int32_t ng, int32_t slot, const double *zeta, const double *u,
+                        const double *v, const double *w, const double *aks, const double *su,
+                        const double *sv, const double *salt, const double *temp, const double *bustr,
+                        const double *bvstr);
+int rp_upload_frame_ext_f32(rp_ctx *ctx, int32_t ng, int32_t slot, const float *zeta, const float *u,
+                            const float *v, const float *w, const float *aks, const float *su,
+                            const float *sv, const float *salt, const float *temp, const float *bustr,
+                            const float *bvstr);
+
 /* Set the particle state: the par(:,pX/pY/pZ/pDOB/pAge/pStatus/pGID)
  * columns and isIn(:) of ROMSPath.f90:104-129 for particles 1..n. */
 int rp_set_particles(rp_ctx *ctx, int64_t n, const double *x, const double *y, const double *z,
@@ -173,6 +196,21 @@ int rp_step_n(rp_ctx *ctx, int32_t nsteps, const double *ex, const double *ix, c
 int rp_get_particles(rp_ctx *ctx, int64_t n, double *x, double *y, double *z, double *age,
                      double *status, double *gid, int32_t *isin, double *wd, double *zeta,
                      double *bath, uint32_t *flags);
+
+/* Read back the diagnostics for particles 1..n: P_Salt, P_Temp,
+ * mean_salt, mean_temp (the running sums: the writer divides them by its
+ * count mI, ROMSPath.f90:2010-2014), P_HOB, P_bustr, P_bvstr.  Any pointer
+ * may be NULL; asking for a diagnostic that is off is RP_ERR_STATE.  Waits
+ * for queued work.  rp_set_particles sets them as the particle read loop
+ * does (P_HOB 9999, the others 0); rp_locate_particles also computes the
+ * initial salinity and temperature from slot t_b % 3 + 1 (t_c), with
+ * par(:,pWD/pZeta/pBath), as ini_ROMSPath does (ROMSPath.f90:408-427). */
+int rp_get_diagnostics(rp_ctx *ctx, int64_t n, double *salt, double *temp, double *mean_salt,
+                       double *mean_temp, double *hob, double *bustr, double *bvstr);
+
+/* The writer's resets after an output record (ROMSPath.f90:2030-2035,
+ * 2064): mean_salt, mean_temp to 0 and P_HOB to 9999.  Stream-ordered. */
+int rp_reset_diagnostics(rp_ctx *ctx);
 
 /* First particle id of this context (default 0).  Particle k of the next
  * rp_set_particles / rp_locate_particles call gets id base + k; the id keys

@@ -53,6 +53,7 @@ class OrcGrid(C.Structure):
         ("s_rho", PD), ("cs_r", PD), ("s_w", PD), ("cs_w", PD),
         ("scl", (C.c_double * 2) * MAXNGRID), ("off", (C.c_double * 2) * MAXNGRID),
         ("zeta", PD * 3), ("u", PD * 3), ("v", PD * 3), ("w", PD * 3), ("aks", PD * 3),
+        ("salt", PD * 3), ("temp", PD * 3), ("bustr", PD * 3), ("bvstr", PD * 3),
     ]
 
 
@@ -64,6 +65,7 @@ class OrcParams(C.Structure):
         ("sub", C.c_double), ("deltat", C.c_double), ("aksback", C.c_double),
         ("constant_hturb", C.c_double * MAXNGRID),
         ("spline_max_iter", C.c_int),
+        ("salttemp_on", C.c_int), ("salttemp_mean", C.c_int), ("write_bottom", C.c_int),
     ]
 
 
@@ -74,6 +76,8 @@ class OrcParticles(C.Structure):
         ("gid", PI32), ("isin", C.POINTER(C.c_int8)),
         ("wd", PD), ("zeta", PD), ("bath", PD),
         ("flags", C.POINTER(C.c_uint32)), ("pid", C.POINTER(C.c_uint32)),
+        ("p_salt", PD), ("p_temp", PD), ("mean_salt", PD), ("mean_temp", PD),
+        ("p_hob", PD), ("p_bustr", PD), ("p_bvstr", PD),
     ]
 
 
@@ -127,8 +131,11 @@ def _declare(L):
                                        C.POINTER(OrcNoise), C.c_int]
     L.orc_update_particles.restype = C.c_int
     L.orc_init_particles.argtypes = [C.POINTER(OrcParams), C.POINTER(OrcGrid), C.POINTER(OrcParticles),
-                                     PD, PD, C.c_int]
+                                     PD, PD, C.c_int, C.c_int]
     L.orc_init_particles.restype = C.c_int
+    L.orc_getinterp_str.argtypes = [C.POINTER(OrcGrid), C.c_int, C.c_double, C.c_double, C.c_int,
+                                    C.POINTER(C.c_uint32)]
+    L.orc_getinterp_str.restype = C.c_double
     L.orc_last_stats.argtypes = [C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
 
 
@@ -269,6 +276,10 @@ class OracleModel:
         for i, v in enumerate(params["constant_hturb"][:MAXNGRID]):
             p.constant_hturb[i] = float(v)
         p.spline_max_iter = spline_max_iter
+        # diagnostics (ROMSPath.f90:935-986): SaltTempOn, SaltTempMean, WriteBottom
+        p.salttemp_on = int(params.get("salttemp_on", 0))
+        p.salttemp_mean = int(params.get("salttemp_mean", 0))
+        p.write_bottom = int(params.get("write_bottom", 0))
         self.params = p
         self.ndraw = 2 + int(params["idt"]) // int(params["deltat"])
         self.P: Optional[OrcParticles] = None
@@ -276,7 +287,9 @@ class OracleModel:
     def set_frame(self, ng: int, slot: int, frame: Dict[str, np.ndarray]):
         """Frame values exactly as stored (FP64 arrays, Stokes already added)."""
         G = self.g[ng - 1]
-        for name in ("zeta", "u", "v", "w", "aks"):
+        for name in ("zeta", "u", "v", "w", "aks", "salt", "temp", "bustr", "bvstr"):
+            if name not in frame:
+                continue
             a = _f64(frame[name])
             self.frames[(ng, slot, name)] = a
             getattr(G, name)[slot - 1] = _pd(a)
@@ -291,6 +304,10 @@ class OracleModel:
             "flags": np.zeros(n, dtype=np.uint32),
             "pid": (np.arange(n, dtype=np.uint32) if pid is None else np.asarray(pid, dtype=np.uint32).copy()),
         }
+        # diagnostics as the particle read loop leaves them (ROMSPath.f90:247-264, 353-355)
+        for k in ("p_salt", "p_temp", "mean_salt", "mean_temp", "p_bustr", "p_bvstr"):
+            self.st[k] = np.zeros(n)
+        self.st["p_hob"] = np.full(n, 9999.0)
         self._bind()
 
     def _bind(self):
@@ -303,17 +320,21 @@ class OracleModel:
         P.isin = s["isin"].ctypes.data_as(C.POINTER(C.c_int8))
         P.flags = s["flags"].ctypes.data_as(C.POINTER(C.c_uint32))
         P.pid = s["pid"].ctypes.data_as(C.POINTER(C.c_uint32))
+        for k in ("p_salt", "p_temp", "mean_salt", "mean_temp", "p_hob", "p_bustr", "p_bvstr"):
+            setattr(P, k, _pd(s[k]))
         self.P = P
 
-    def init_particles(self, release, tb: int = 1, pid=None):
-        """ini_ROMSPath ownership + zbounds (ROMSPath.f90:367-432)."""
+    def init_particles(self, release, tb: int = 1, pid=None, tc: Optional[int] = None):
+        """ini_ROMSPath ownership + zbounds (ROMSPath.f90:367-432); initial
+        diagnostics at slot tc (default: the slot after tb)."""
         n = release.z.shape[0]
         self.set_particles(np.ones(n), np.ones(n), release.z, release.dob, np.zeros(n),
                            np.full(n, 9.0), np.full(n, self.ng, dtype=np.int32), np.zeros(n, dtype=np.int8),
                            pid=pid)
         ip = np.ascontiguousarray(release.ipos, dtype=np.float64)
         jp = np.ascontiguousarray(release.jpos, dtype=np.float64)
-        lib().orc_init_particles(C.byref(self.params), self.g, C.byref(self.P), _pd(ip), _pd(jp), tb)
+        tc = (tb % 3) + 1 if tc is None else tc
+        lib().orc_init_particles(C.byref(self.params), self.g, C.byref(self.P), _pd(ip), _pd(jp), tb, tc)
 
     def step(self, ex, ix, ets, tb, tc, tf, noise="philox", seed=0, step_index=0,
              hook: Optional[np.ndarray] = None, mt: Optional[MT19937] = None, nthreads=1):

@@ -491,8 +491,11 @@ double orc_getinterp3d(const orc_grid *g, int var, double ipar, double jpar, dou
         }
         zero_dry = 1;
     } else {
-        /* w (interpolation_module.f90:917-939) and AKs (810-829) */
-        fld = (var == ORC_V_W) ? g->w[t - 1] : g->aks[t - 1];
+        /* w (interpolation_module.f90:917-939), AKs (810-829), salt and
+         * temp (769-809): bilinear, inverse-distance when a corner is dry */
+        fld = (var == ORC_V_W) ? g->w[t - 1]
+            : (var == ORC_V_AKS) ? g->aks[t - 1]
+            : (var == ORC_V_SALT) ? g->salt[t - 1] : g->temp[t - 1];
         fni = nx; fnj = ny;
         int i0 = clampi(Inode, 1, nx, flags), i1 = clampi(Inode + 1, 1, nx, flags);
         int j0 = clampi(Jnode, 1, ny, flags), j1 = clampi(Jnode + 1, 1, ny, flags);
@@ -527,6 +530,75 @@ double orc_getinterp3d(const orc_grid *g, int var, double ipar, double jpar, dou
         zprof[k] = cff[0] * v0 + cff[1] * v1 + cff[2] * v2 + cff[3] * v3;
     }
     return zcff1 * zprof[Ibot] + zcff2 * zprof[Itop];
+}
+
+/* getInterpStr, interpolation_module.f90:964-1174: bottom stress at a u
+ * (bustr) or v (bvstr) point set, with the u/v edge rules and the
+ * zero-the-dry-corners rule.  The rows Jnode+1 (bustr) and the columns
+ * Inode+1 (bvstr) are read unclamped by the reference; here clamped and
+ * flagged. */
+double orc_getinterp_str(const orc_grid *g, int var, double ipar, double jpar, int t, uint32_t *flags)
+{
+    const int nx = g->xi_rho, ny = g->eta_rho;
+    int Inode = ifloor(ipar), Jnode = ifloor(jpar);
+    double X = ipar - (double)Inode, Y = jpar - (double)Jnode;
+    double cff[4], v[4], m[4];
+    if (var == ORC_V_BUSTR) {
+        const int xi_u = nx - 1, eta_u = ny;
+        const double *f = g->bustr[t - 1];
+        double uvI = ipar - 0.5;
+        Inode = ifloor(uvI);
+        X = uvI - (double)Inode;
+        cff[0] = (1 - X) * (1 - Y);
+        cff[1] = X * (1 - Y);
+        cff[2] = X * Y;
+        cff[3] = (1 - X) * Y;
+        int j0 = clampi(Jnode, 1, eta_u, flags), j1 = clampi(Jnode + 1, 1, eta_u, flags);
+        if (Inode >= xi_u) {
+            v[0] = f[IX2(xi_u, j0, xi_u)]; v[1] = f[IX2(xi_u, j0, xi_u)];
+            v[2] = f[IX2(xi_u, j1, xi_u)]; v[3] = f[IX2(xi_u, j1, xi_u)];
+            m[0] = g->mask_u[IX2(xi_u, j0, xi_u)]; m[1] = 0; m[2] = 0; m[3] = g->mask_u[IX2(xi_u, j1, xi_u)];
+        } else if (Inode < 1) {
+            v[0] = f[IX2(1, j0, xi_u)]; v[1] = f[IX2(1, j0, xi_u)];
+            v[2] = f[IX2(1, j1, xi_u)]; v[3] = f[IX2(1, j1, xi_u)];
+            m[0] = 0; m[1] = g->mask_u[IX2(1, j0, xi_u)]; m[2] = g->mask_u[IX2(1, j1, xi_u)]; m[3] = 0;
+        } else {
+            v[0] = f[IX2(Inode, j0, xi_u)]; v[1] = f[IX2(Inode + 1, j0, xi_u)];
+            v[2] = f[IX2(Inode + 1, j1, xi_u)]; v[3] = f[IX2(Inode, j1, xi_u)];
+            m[0] = g->mask_u[IX2(Inode, j0, xi_u)]; m[1] = g->mask_u[IX2(Inode + 1, j0, xi_u)];
+            m[2] = g->mask_u[IX2(Inode + 1, j1, xi_u)]; m[3] = g->mask_u[IX2(Inode, j1, xi_u)];
+        }
+    } else {
+        const int xi_v = nx, eta_v = ny - 1;
+        const double *f = g->bvstr[t - 1];
+        double uvJ = jpar - 0.5;
+        Jnode = ifloor(uvJ);
+        if (Jnode < 1) Jnode = 1;
+        if (Jnode > eta_v) Inode = eta_v;                       /* the reference's line, as getInterp3D */
+        Y = uvJ - (double)Jnode;
+        cff[0] = (1 - X) * (1 - Y);
+        cff[1] = X * (1 - Y);
+        cff[2] = X * Y;
+        cff[3] = (1 - X) * Y;
+        int i0 = clampi(Inode, 1, xi_v, flags), i1 = clampi(Inode + 1, 1, xi_v, flags);
+        if (Jnode >= eta_v) {
+            v[0] = f[IX2(i0, eta_v, xi_v)]; v[1] = f[IX2(i1, eta_v, xi_v)];
+            v[2] = f[IX2(i1, eta_v, xi_v)]; v[3] = f[IX2(i0, eta_v, xi_v)];
+            m[0] = g->mask_v[IX2(i0, eta_v, xi_v)]; m[1] = g->mask_v[IX2(i1, eta_v, xi_v)]; m[2] = 0; m[3] = 0;
+        } else {
+            v[0] = f[IX2(i0, Jnode, xi_v)]; v[1] = f[IX2(i1, Jnode, xi_v)];
+            v[2] = f[IX2(i1, Jnode + 1, xi_v)]; v[3] = f[IX2(i0, Jnode + 1, xi_v)];
+            m[0] = g->mask_v[IX2(i0, Jnode, xi_v)]; m[1] = g->mask_v[IX2(i1, Jnode, xi_v)];
+            m[2] = g->mask_v[IX2(i1, Jnode + 1, xi_v)]; m[3] = g->mask_v[IX2(i0, Jnode + 1, xi_v)];
+        }
+    }
+    double nwater = m[0] + m[1] + m[2] + m[3];
+    if (nwater < 4.0 && nwater > 0.0) {
+        for (int k = 0; k < 4; k++) if (m[k] == 0.0) v[k] = 0.0;
+    } else if (nwater == 0.0) {
+        for (int k = 0; k < 4; k++) { cff[k] = 0.0; v[k] = 0.0; }
+    }
+    return cff[0] * v[0] + cff[1] * v[1] + cff[2] * v[2] + cff[3] * v[3];
 }
 
 /* getInterpAKs, interpolation_module.f90:1175-1229 (one w level) */
@@ -1121,6 +1193,42 @@ static void update_one(const step_env *e0, const orc_grid *grids, orc_particles 
         p->isin[n] = 1;
         p->status[n] = -9.0;
     }
+    if (prm->write_bottom) {                                     /* 935-952 */
+        const orc_grid *gd = &grids[p->gid[n] - 1];
+        double btemp = -1.0 * tdepth + p->z[n];
+        p->p_hob[n] = (btemp < p->p_hob[n]) ? btemp : p->p_hob[n];
+        if (btemp == p->p_hob[n]) {
+            double eb[3];
+            eb[0] = orc_getinterp_str(gd, ORC_V_BUSTR, p->x[n], p->y[n], e.tb, &fl);
+            eb[1] = orc_getinterp_str(gd, ORC_V_BUSTR, p->x[n], p->y[n], e.tc, &fl);
+            eb[2] = orc_getinterp_str(gd, ORC_V_BUSTR, p->x[n], p->y[n], e.tf, &fl);
+            p->p_bustr[n] = orc_polintd(e.ex, eb, e.ix[1]);
+            eb[0] = orc_getinterp_str(gd, ORC_V_BVSTR, p->x[n], p->y[n], e.tb, &fl);
+            eb[1] = orc_getinterp_str(gd, ORC_V_BVSTR, p->x[n], p->y[n], e.tc, &fl);
+            eb[2] = orc_getinterp_str(gd, ORC_V_BVSTR, p->x[n], p->y[n], e.tf, &fl);
+            p->p_bvstr[n] = orc_polintd(e.ex, eb, e.ix[1]);
+        }
+    }
+    if (prm->salttemp_on) {                                      /* 962-986 */
+        const orc_grid *gd = &grids[p->gid[n] - 1];
+        const double X = p->x[n], Y = p->y[n], Z = p->z[n];
+        double zetab = orc_getinterp2d(gd, ORC_V_ZETA, X, Y, e.tb, &fl);
+        double zetac = orc_getinterp2d(gd, ORC_V_ZETA, X, Y, e.tc, &fl);
+        double zetaf = orc_getinterp2d(gd, ORC_V_ZETA, X, Y, e.tf, &fl);
+        double es[3];
+        es[0] = orc_getinterp3d(gd, ORC_V_SALT, X, Y, Z, e.tb, 1, zetab, tdepth, &fl);
+        es[1] = orc_getinterp3d(gd, ORC_V_SALT, X, Y, Z, e.tc, 1, zetac, tdepth, &fl);
+        es[2] = orc_getinterp3d(gd, ORC_V_SALT, X, Y, Z, e.tf, 1, zetaf, tdepth, &fl);
+        p->p_salt[n] = orc_polintd(e.ex, es, e.ix[1]);
+        es[0] = orc_getinterp3d(gd, ORC_V_TEMP, X, Y, Z, e.tb, 1, zetab, tdepth, &fl);
+        es[1] = orc_getinterp3d(gd, ORC_V_TEMP, X, Y, Z, e.tc, 1, zetac, tdepth, &fl);
+        es[2] = orc_getinterp3d(gd, ORC_V_TEMP, X, Y, Z, e.tf, 1, zetaf, tdepth, &fl);
+        p->p_temp[n] = orc_polintd(e.ex, es, e.ix[1]);
+        if (prm->salttemp_mean) {
+            p->mean_salt[n] = p->mean_salt[n] + p->p_salt[n];
+            p->mean_temp[n] = p->mean_temp[n] + p->p_temp[n];
+        }
+    }
     if (p->flags) p->flags[n] |= fl;
 }
 
@@ -1166,7 +1274,7 @@ int orc_update_particles(const orc_params *prm, const orc_grid *grids, orc_parti
 /* ini_ROMSPath ownership loop, ROMSPath.f90:319-432 (positions already in
  * each grid's index space; LL2ij itself is init-time host work). */
 int orc_init_particles(const orc_params *prm, const orc_grid *grids, orc_particles *p,
-                       const double *ipos, const double *jpos, int tb)
+                       const double *ipos, const double *jpos, int tb, int tc)
 {
     for (int64_t n = 0; n < p->n; n++) {
         p->status[n] = 9.0;
@@ -1179,6 +1287,11 @@ int orc_init_particles(const orc_params *prm, const orc_grid *grids, orc_particl
         p->x[n] = 1.0;
         p->y[n] = 1.0;
         if (p->flags) p->flags[n] = 0;
+        if (prm->write_bottom) { p->p_hob[n] = 9999.0; p->p_bustr[n] = 0.0; p->p_bvstr[n] = 0.0; }  /* 260-264, 353-355 */
+        if (prm->salttemp_on) {                                                                  /* 247-257 */
+            p->p_salt[n] = 0.0; p->p_temp[n] = 0.0;
+            if (prm->salttemp_mean) { p->mean_salt[n] = 0.0; p->mean_temp[n] = 0.0; }
+        }
     }
     for (int ng = 1; ng <= prm->ngrid; ng++) {
         for (int64_t n = 0; n < p->n; n++) {
@@ -1196,6 +1309,22 @@ int orc_init_particles(const orc_params *prm, const orc_grid *grids, orc_particl
                 if (!inz) p->status[n] = 9.0;
                 if (p->flags) p->flags[n] |= fl;
             }
+        }
+    }
+    if (prm->salttemp_on) {                                      /* 408-427 */
+        for (int64_t n = 0; n < p->n; n++) {
+            if (!p->isin[n]) continue;
+            uint32_t fl = 0;
+            const orc_grid *gd = &grids[p->gid[n] - 1];
+            double tdepth = -1.0 * orc_getinterp2d(gd, ORC_V_DEPTH, p->x[n], p->y[n], tc, &fl);
+            double zeta = orc_getinterp2d(gd, ORC_V_ZETA, p->x[n], p->y[n], tc, &fl);
+            p->p_salt[n] = orc_getinterp3d(gd, ORC_V_SALT, p->x[n], p->y[n], p->z[n], tc, 1, zeta, tdepth, &fl);
+            p->p_temp[n] = orc_getinterp3d(gd, ORC_V_TEMP, p->x[n], p->y[n], p->z[n], tc, 1, zeta, tdepth, &fl);
+            p->wd[n] = (-1.0 * tdepth) + zeta;
+            p->zeta[n] = zeta;
+            p->bath[n] = -1.0 * tdepth;
+            if (prm->salttemp_mean) { p->mean_salt[n] = p->p_salt[n]; p->mean_temp[n] = p->p_temp[n]; }
+            if (p->flags) p->flags[n] |= fl;
         }
     }
     return 0;

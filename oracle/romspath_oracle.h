@@ -57,6 +57,9 @@ typedef struct {
     double off[ORC_MAXNGRID][2]; /* GRIDS(ng)%off(i,1:2)               */
     /* HYDRODATA(ng)%<field>(:,:,:,tind) for tind = 1..3 */
     const double *zeta[3], *u[3], *v[3], *w[3], *aks[3];
+    /* diagnostics fields (NULL unless used): salt, temp (xi_rho,eta_rho,N),
+     * bustr (xi_u,eta_u), bvstr (xi_v,eta_v) */
+    const double *salt[3], *temp[3], *bustr[3], *bvstr[3];
 } orc_grid;
 
 typedef struct {
@@ -68,6 +71,7 @@ typedef struct {
     double vertdist, serr, smth, sub, deltat, aksback;
     double constant_hturb[ORC_MAXNGRID];
     int spline_max_iter;         /* cap on smooth()'s secant loop (ref: none) */
+    int salttemp_on, salttemp_mean, write_bottom;   /* SaltTempOn, SaltTempMean, WriteBottom */
 } orc_params;
 
 typedef struct {
@@ -78,6 +82,9 @@ typedef struct {
     double *wd, *zeta, *bath;                /* par(:,pWD/pZeta/pBath) */
     uint32_t *flags;
     const uint32_t *pid;                     /* persistent particle id (noise) */
+    /* diagnostics (NULL unless used): P_Salt, P_Temp, mean_salt, mean_temp,
+     * P_HOB, P_bustr, P_bvstr (ROMSPath.f90:130-131) */
+    double *p_salt, *p_temp, *mean_salt, *mean_temp, *p_hob, *p_bustr, *p_bvstr;
 } orc_particles;
 
 /* MT19937 state, restated from random_module.f90:109-198. */
@@ -127,7 +134,10 @@ double orc_ppvalu(const double *brk, const double *coef, int l, int k,
 
 /* 2-D variable ids for orc_getinterp2d / 3-D ids for orc_getinterp3d */
 enum { ORC_V_DEPTH = 0, ORC_V_PM, ORC_V_PN, ORC_V_ZETA };
-enum { ORC_V_U = 0, ORC_V_V, ORC_V_W, ORC_V_AKS };
+enum { ORC_V_U = 0, ORC_V_V, ORC_V_W, ORC_V_AKS, ORC_V_SALT, ORC_V_TEMP };
+/* getInterpStr variables (interpolation_module.f90:964-1174) */
+enum { ORC_V_BUSTR = 0, ORC_V_BVSTR };
+double orc_getinterp_str(const orc_grid *g, int var, double ipar, double jpar, int t, uint32_t *flags);
 
 /* ---- the particle step (update_particles, ROMSPath.f90:608-1008) ---- */
 int orc_update_particles(const orc_params *prm, const orc_grid *grids,
@@ -138,10 +148,11 @@ int orc_update_particles(const orc_params *prm, const orc_grid *grids,
 /* Init-time ownership test of ini_ROMSPath (ROMSPath.f90:367-432): for
  * positions already in index space of each grid, first grid whose bounds()
  * says in-grid owns the particle; zbounds() fixes z.  ipos/jpos are
- * (ngrid, n) row-major: ipos[g*n + k]. */
+ * (ngrid, n) row-major: ipos[g*n + k].  With SaltTempOn the initial salt,
+ * temp (and pWD/pZeta/pBath) are taken at ring slot tc (408-427). */
 int orc_init_particles(const orc_params *prm, const orc_grid *grids,
                        orc_particles *p, const double *ipos,
-                       const double *jpos, int tb);
+                       const double *jpos, int tb, int tc);
 
 /* statistics of the last orc_update_particles call (secant iterations) */
 void orc_last_stats(int64_t *spline_calls, int64_t *secant_iters);

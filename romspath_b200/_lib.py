@@ -16,13 +16,15 @@ ERRORS = {-1: "RP_ERR_ARG", -2: "RP_ERR_CUDA", -3: "RP_ERR_STATE", -4: "RP_ERR_N
           -5: "RP_ERR_UNSUPPORTED", -6: "RP_ERR_NOEXT"}
 FIELD_F64, FIELD_F32, FIELD_MIXED, FIELD_MIXED_I16 = 0, 1, 2, 3
 FLAG_OOB, FLAG_NODE, FLAG_WBOT, FLAG_WTOP, FLAG_SPLINE = 1, 2, 4, 8, 16
+DIAG_SALTTEMP, DIAG_SALTTEMP_MEAN, DIAG_BOTTOM = 1, 2, 4
 
 EXPORTS = [
     "rp_create", "rp_upload_frame", "rp_upload_frame_f32", "rp_set_particles", "rp_locate_particles",
     "rp_step", "rp_get_particles", "rp_set_id_base", "rp_set_step_index", "rp_set_noise_hook", "rp_synchronize",
     "rp_last_error", "rp_destroy", "rp_device_state_get", "rp_last_step_stats", "rp_kernel_launches",
     "rp_step_noalloc", "rp_version", "rp_adj_frames", "rp_adj_set_frame", "rp_forward", "rp_backward",
-    "rp_tangent", "rp_adj_replay", "rp_step_n", "rp_set_launch",
+    "rp_tangent", "rp_adj_replay", "rp_step_n", "rp_set_launch", "rp_upload_frame_ext", "rp_upload_frame_ext_f32",
+    "rp_get_diagnostics", "rp_reset_diagnostics",
 ]
 
 PD = C.POINTER(C.c_double)
@@ -100,6 +102,10 @@ def _declare(L):
     L.rp_create.argtypes = [C.POINTER(RpParams), C.c_int32, C.POINTER(RpGrid), C.POINTER(P)]
     L.rp_upload_frame.argtypes = [P, C.c_int32, C.c_int32] + [PD] * 7
     L.rp_upload_frame_f32.argtypes = [P, C.c_int32, C.c_int32] + [PF] * 7
+    L.rp_upload_frame_ext.argtypes = [P, C.c_int32, C.c_int32] + [PD] * 11
+    L.rp_upload_frame_ext_f32.argtypes = [P, C.c_int32, C.c_int32] + [PF] * 11
+    L.rp_get_diagnostics.argtypes = [P, C.c_int64] + [PD] * 7
+    L.rp_reset_diagnostics.argtypes = [P]
     L.rp_set_particles.argtypes = [P, C.c_int64] + [PD] * 7 + [PI32]
     L.rp_locate_particles.argtypes = [P, C.c_int64, PD, PD, PD, PD, C.c_int32]
     L.rp_step.argtypes = [P, PD, PD, C.c_int32, C.c_int32, C.c_int32, C.c_int32]

@@ -24,6 +24,7 @@ struct GridBuf {
     double *sr = nullptr, *csr = nullptr, *sw = nullptr, *csw = nullptr;
     uint8_t *mrho = nullptr, *mu = nullptr, *mv = nullptr;
     void *zeta = nullptr, *u = nullptr, *v = nullptr, *w = nullptr, *aks = nullptr;
+    void *salt = nullptr, *temp = nullptr, *bustr = nullptr, *bvstr = nullptr;  // diagnostics only
     float *qs_u = nullptr, *qs_v = nullptr, *qs_w = nullptr, *qs_aks = nullptr;  // mixed form: [k][slot4]
     double scl[RP_MAXNGRID][2] = {}, off[RP_MAXNGRID][2] = {};
     int map[3] = {-1, -1, -1};                 // logical slot 1..3 -> physical 0..3
@@ -53,6 +54,10 @@ struct rp_ctx {
     int8_t* isin = nullptr;
     uint32_t *pid = nullptr, *flags = nullptr;
     double* turbv = nullptr;                   // scratch: VTurb displacement per particle
+    // diagnostics (RP_DIAG_* bits of reserved[3]); null when off
+    int diag = 0;
+    double *d_salt = nullptr, *d_temp = nullptr, *d_mean_salt = nullptr, *d_mean_temp = nullptr;
+    double *d_hob = nullptr, *d_bustr = nullptr, *d_bvstr = nullptr;
     // mixed form: compensated FP32 positions, spline warm start, and the
     // FP32 staging field plus per-level maxima of the FP16 quantisation
     float *x32 = nullptr, *y32 = nullptr, *z32 = nullptr, *cx = nullptr, *cy = nullptr, *cz = nullptr;
@@ -191,6 +196,8 @@ RpParticlesDev particles_dev(const rp_ctx* c) {
     P.gid = c->gid; P.isin = c->isin; P.pid = c->pid; P.flags = c->flags;
     P.x32 = c->x32; P.y32 = c->y32; P.z32 = c->z32; P.cx = c->cx; P.cy = c->cy; P.cz = c->cz;
     P.qwarm = c->qwarm; P.gwarm = c->gwarm;
+    P.salt = c->d_salt; P.temp = c->d_temp; P.mean_salt = c->d_mean_salt; P.mean_temp = c->d_mean_temp;
+    P.hob = c->d_hob; P.bustr = c->d_bustr; P.bvstr = c->d_bvstr;
     return P;
 }
 
@@ -203,6 +210,7 @@ void fill_grids(const rp_ctx* c, RpStepArgs& A, int tb, int tc, int tf) {
         d.mrho = G.mrho; d.mu = G.mu; d.mv = G.mv;
         d.sr = G.sr; d.csr = G.csr; d.sw = G.sw; d.csw = G.csw;
         d.zeta = G.zeta; d.u = G.u; d.v = G.v; d.w = G.w; d.aks = G.aks;
+        d.salt = G.salt; d.temp = G.temp; d.bustr = G.bustr; d.bvstr = G.bvstr;
         d.qs_u = G.qs_u; d.qs_v = G.qs_v; d.qs_w = G.qs_w; d.qs_aks = G.qs_aks;
         for (int i = 0; i < RP_MAXNGRID; i++)
             for (int q = 0; q < 2; q++) { d.scl[i][q] = G.scl[i][q]; d.off[i][q] = G.off[i][q]; }
@@ -220,6 +228,7 @@ void fill_params(const rp_ctx* c, RpStepArgs& A) {
     A.loop = p.idt / (int)p.deltat;
     A.grid_cap = p.reserved[2] > 0 ? p.reserved[2] : 0;
     A.spline_max_iter = p.spline_max_iter > 0 ? p.spline_max_iter : 100;
+    A.diag = c->diag;
     A.vertdist = p.vertdist; A.serr = p.serr; A.smth = p.smth; A.sub = p.sub;
     A.deltat = p.deltat; A.aksback = p.aksback;
     for (int i = 0; i < RP_MAXNGRID; i++) A.khturb[i] = p.constant_hturb[i];
@@ -271,7 +280,8 @@ void free_ctx(rp_ctx* c) {
     for (int k = 0; k < RP_MAXNGRID; k++) {
         GridBuf& G = c->g[k];
         void* ptrs[] = {G.h, G.pm, G.pn, G.sr, G.csr, G.sw, G.csw, G.mrho, G.mu, G.mv,
-                        G.zeta, G.u, G.v, G.w, G.aks, G.qs_u, G.qs_v, G.qs_w, G.qs_aks};
+                        G.zeta, G.u, G.v, G.w, G.aks, G.qs_u, G.qs_v, G.qs_w, G.qs_aks,
+                        G.salt, G.temp, G.bustr, G.bvstr};
         for (void* p : ptrs) if (p) cudaFree(p);
         for (int s = 0; s < RP_SLOTS; s++) {
             if (G.slot_free[s]) cudaEventDestroy(G.slot_free[s]);
@@ -283,7 +293,8 @@ void free_ctx(rp_ctx* c) {
                     c->dstage[0], c->dstage[1], c->x32, c->y32, c->z32, c->cx, c->cy, c->cz, c->qwarm, c->gwarm,
                     c->ftmp, c->qmax, c->sb.keys, c->sb.hist, c->sb.sums, c->sb.perm, c->sb.gbase,
                     c->adj.ck, c->adj.prec, c->adj.seg, c->adj.work, c->adj.lx, c->adj.ly, c->adj.lz,
-                    c->adj.kbar, c->adj.tan};
+                    c->adj.kbar, c->adj.tan, c->d_salt, c->d_temp, c->d_mean_salt, c->d_mean_temp,
+                    c->d_hob, c->d_bustr, c->d_bvstr};
     for (int g = 0; g < RP_MAXNGRID; g++)
         for (int f = 0; f < 5; f++)
             if (c->adj.fst[g][f]) cudaFree(c->adj.fst[g][f]);
@@ -352,11 +363,16 @@ int upload_field(rp_ctx* ctx, const S* src, const S* add, void* dst, int ni, int
 
 template <typename S>
 int upload_frame(rp_ctx* ctx, int32_t ng, int32_t slot, const S* zeta, const S* u, const S* v, const S* w,
-                 const S* aks, const S* su, const S* sv) {
+                 const S* aks, const S* su, const S* sv, const S* salt = nullptr, const S* temp = nullptr,
+                 const S* bustr = nullptr, const S* bvstr = nullptr) {
     if (!ctx) return RP_ERR_ARG;
     if (ng < 1 || ng > ctx->ngrid) return fail(ctx, RP_ERR_ARG, "rp_upload_frame: grid id out of range");
     if (slot < 1 || slot > 3) return fail(ctx, RP_ERR_ARG, "rp_upload_frame: slot must be 1..3");
     if (!zeta || !u || !v || !w || !aks) return fail(ctx, RP_ERR_ARG, "rp_upload_frame: null field");
+    if ((ctx->diag & RP_DIAG_SALTTEMP) && (!salt || !temp))
+        return fail(ctx, RP_ERR_ARG, "rp_upload_frame: SaltTempOn needs salt and temp (rp_upload_frame_ext)");
+    if ((ctx->diag & RP_DIAG_BOTTOM) && (!bustr || !bvstr))
+        return fail(ctx, RP_ERR_ARG, "rp_upload_frame: WriteBottom needs bustr and bvstr (rp_upload_frame_ext)");
     const bool stokes = ctx->prm.stokes != 0;
     if (stokes && (!su || !sv)) return fail(ctx, RP_ERR_ARG, "rp_upload_frame: stokes on but su/sv null");
     GridBuf& G = ctx->g[ng - 1];
@@ -379,6 +395,14 @@ int upload_frame(rp_ctx* ctx, int32_t ng, int32_t slot, const S* zeta, const S* 
         return rc;
     if ((rc = upload_field<S>(ctx, w, nullptr, G.w, nx, ny, N + 1, phys, mx, G.qs_w)) != RP_OK) return rc;
     if ((rc = upload_field<S>(ctx, aks, nullptr, G.aks, nx, ny, N + 1, phys, mx, G.qs_aks)) != RP_OK) return rc;
+    if (ctx->diag & RP_DIAG_SALTTEMP) {
+        if ((rc = upload_field<S>(ctx, salt, nullptr, G.salt, nx, ny, N, phys)) != RP_OK) return rc;
+        if ((rc = upload_field<S>(ctx, temp, nullptr, G.temp, nx, ny, N, phys)) != RP_OK) return rc;
+    }
+    if (ctx->diag & RP_DIAG_BOTTOM) {
+        if ((rc = upload_field<S>(ctx, bustr, nullptr, G.bustr, nx - 1, ny, 1, phys)) != RP_OK) return rc;
+        if ((rc = upload_field<S>(ctx, bvstr, nullptr, G.bvstr, nx, ny - 1, 1, phys)) != RP_OK) return rc;
+    }
     CK(cudaEventRecord(G.slot_ready[phys], ctx->s_copy));
     if (ctx->direct_pending) {                 // the caller's arrays are free again once copied
         CK(cudaEventSynchronize(G.slot_ready[phys]));
@@ -509,6 +533,9 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
     if (p.field_dtype != RP_FIELD_F64 && p.field_dtype != RP_FIELD_F32 && p.field_dtype != RP_FIELD_MIXED &&
         p.field_dtype != RP_FIELD_MIXED_I16)
         return RP_ERR_ARG;
+    if (p.reserved[3] & ~(RP_DIAG_SALTTEMP | RP_DIAG_SALTTEMP_MEAN | RP_DIAG_BOTTOM)) return RP_ERR_ARG;
+    if (p.reserved[3] && (p.field_dtype == RP_FIELD_MIXED || p.field_dtype == RP_FIELD_MIXED_I16))
+        return RP_ERR_UNSUPPORTED;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= p.device || p.device < 0) return RP_ERR_NOEXT;
     rp_ctx* ctx = new rp_ctx();
@@ -519,6 +546,10 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
     ctx->mixed = (p.field_dtype == RP_FIELD_MIXED || p.field_dtype == RP_FIELD_MIXED_I16);
     ctx->i16 = (p.field_dtype == RP_FIELD_MIXED_I16);
     ctx->ndraw = 2 + p.idt / (int)p.deltat;
+    // SaltTempMean applies only with SaltTempOn (ROMSPath.f90:247-257)
+    ctx->diag = p.reserved[3] & (RP_DIAG_SALTTEMP | RP_DIAG_BOTTOM);
+    if ((p.reserved[3] & RP_DIAG_SALTTEMP_MEAN) && (p.reserved[3] & RP_DIAG_SALTTEMP))
+        ctx->diag |= RP_DIAG_SALTTEMP_MEAN;
     auto bail = [&](int code, const std::string& m) {
         std::fprintf(stderr, "rp_create: %s\n", m.c_str());
         free_ctx(ctx);
@@ -587,6 +618,18 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
         cudaMemset(G.v, 0, nv * G.N * e);
         cudaMemset(G.w, 0, n2 * sw * e);
         cudaMemset(G.aks, 0, n2 * sw * e);
+        if (ctx->diag & RP_DIAG_SALTTEMP) {
+            if (dalloc(&G.salt, n2 * G.N * e) || dalloc(&G.temp, n2 * G.N * e))
+                return bail(RP_ERR_NOMEM, "salt/temp ring allocation");
+            cudaMemset(G.salt, 0, n2 * G.N * e);
+            cudaMemset(G.temp, 0, n2 * G.N * e);
+        }
+        if (ctx->diag & RP_DIAG_BOTTOM) {
+            if (dalloc(&G.bustr, nu * e) || dalloc(&G.bvstr, nv * e))
+                return bail(RP_ERR_NOMEM, "bottom stress ring allocation");
+            cudaMemset(G.bustr, 0, nu * e);
+            cudaMemset(G.bvstr, 0, nv * e);
+        }
         if (ctx->mixed) {
             const size_t qn = (size_t)RP_SLOTS * sw * 4;
             if (dalloc(&G.qs_u, qn) || dalloc(&G.qs_v, qn) || dalloc(&G.qs_w, qn) || dalloc(&G.qs_aks, qn))
@@ -622,6 +665,13 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
         dalloc(&ctx->flags, cap * 4) || dalloc(&ctx->tmp_gid, cap * 8) || dalloc(&ctx->tmp_isin, cap * 4) ||
         dalloc(&ctx->turbv, cap * 8))
         return bail(RP_ERR_NOMEM, "particle state allocation");
+    if ((ctx->diag & RP_DIAG_SALTTEMP) && (dalloc(&ctx->d_salt, cap * 8) || dalloc(&ctx->d_temp, cap * 8)))
+        return bail(RP_ERR_NOMEM, "diagnostics allocation");
+    if ((ctx->diag & RP_DIAG_SALTTEMP_MEAN) && (dalloc(&ctx->d_mean_salt, cap * 8) || dalloc(&ctx->d_mean_temp, cap * 8)))
+        return bail(RP_ERR_NOMEM, "diagnostics allocation");
+    if ((ctx->diag & RP_DIAG_BOTTOM) &&
+        (dalloc(&ctx->d_hob, cap * 8) || dalloc(&ctx->d_bustr, cap * 8) || dalloc(&ctx->d_bvstr, cap * 8)))
+        return bail(RP_ERR_NOMEM, "diagnostics allocation");
     ctx->resort = p.reserved[1] > 0 ? p.reserved[1] : 0;
     if (ctx->resort) {
         const int rc = sort_buffers(ctx);
@@ -669,6 +719,18 @@ int rp_upload_frame_f32(rp_ctx* ctx, int32_t ng, int32_t slot, const float* zeta
     return upload_frame<float>(ctx, ng, slot, zeta, u, v, w, aks, su, sv);
 }
 
+int rp_upload_frame_ext(rp_ctx* ctx, int32_t ng, int32_t slot, const double* zeta, const double* u, const double* v,
+                        const double* w, const double* aks, const double* su, const double* sv, const double* salt,
+                        const double* temp, const double* bustr, const double* bvstr) {
+    return upload_frame<double>(ctx, ng, slot, zeta, u, v, w, aks, su, sv, salt, temp, bustr, bvstr);
+}
+
+int rp_upload_frame_ext_f32(rp_ctx* ctx, int32_t ng, int32_t slot, const float* zeta, const float* u,
+                            const float* v, const float* w, const float* aks, const float* su, const float* sv,
+                            const float* salt, const float* temp, const float* bustr, const float* bvstr) {
+    return upload_frame<float>(ctx, ng, slot, zeta, u, v, w, aks, su, sv, salt, temp, bustr, bvstr);
+}
+
 int rp_set_particles(rp_ctx* ctx, int64_t n, const double* x, const double* y, const double* z,
                      const double* dob, const double* age, const double* status, const double* gid,
                      const int32_t* isin) {
@@ -713,8 +775,12 @@ int rp_locate_particles(rp_ctx* ctx, int64_t n, const double* ipos, const double
     if (n < 0 || n > ctx->cap) return fail(ctx, RP_ERR_ARG, "rp_locate_particles: n exceeds numpar");
     if (!ipos || !jpos || !z || !dob) return fail(ctx, RP_ERR_ARG, "rp_locate_particles: null array");
     if (t_b < 1 || t_b > 3) return fail(ctx, RP_ERR_ARG, "rp_locate_particles: slot must be 1..3");
+    // SaltTempOn reads the initial salinity and temperature from t_c, the
+    // slot after t_b (ROMSPath.f90:209-211, 408-427)
+    const int32_t t_c = (ctx->diag & RP_DIAG_SALTTEMP) ? t_b % 3 + 1 : t_b;
     for (int k = 0; k < ctx->ngrid; k++)
-        if (ctx->g[k].map[t_b - 1] < 0) return fail(ctx, RP_ERR_STATE, "rp_locate_particles: frame slot not loaded");
+        if (ctx->g[k].map[t_b - 1] < 0 || ctx->g[k].map[t_c - 1] < 0)
+            return fail(ctx, RP_ERR_STATE, "rp_locate_particles: frame slot not loaded");
     CK(cudaSetDevice(ctx->device));
     cudaStream_t s = ctx->s_comp;
     const size_t nb = (size_t)n * 8, nbg = nb * ctx->ngrid;
@@ -732,10 +798,10 @@ int rp_locate_particles(rp_ctx* ctx, int64_t n, const double* ipos, const double
         ctx->state_base = ctx->pid_base;
         RpStepArgs A{};
         fill_params(ctx, A);
-        fill_grids(ctx, A, t_b, t_b, t_b);
+        fill_grids(ctx, A, t_b, t_c, t_b);
         for (int k = 0; k < ctx->ngrid; k++) {
-            const int ph = ctx->g[k].map[t_b - 1];
-            cudaStreamWaitEvent(s, ctx->g[k].slot_ready[ph], 0);
+            cudaStreamWaitEvent(s, ctx->g[k].slot_ready[ctx->g[k].map[t_b - 1]], 0);
+            cudaStreamWaitEvent(s, ctx->g[k].slot_ready[ctx->g[k].map[t_c - 1]], 0);
         }
         cudaError_t e = rp::launch_locate(A, ctx->mixed ? RP_FIELD_F32 : ctx->prm.field_dtype, dip, djp, dz, ddob, s);
         ctx->launches++;
@@ -890,6 +956,7 @@ int rp_step_noalloc(rp_ctx* ctx, const rp_device_state* st, const double ex[3], 
     if (ctx->npmax > 128)
         return fail(ctx, RP_ERR_UNSUPPORTED, "rp_step_noalloc: int(s_w*sub) must be <= 128");
     if (ctx->mixed) return fail(ctx, RP_ERR_UNSUPPORTED, "rp_step_noalloc: not available in the mixed form");
+    if (ctx->diag) return fail(ctx, RP_ERR_UNSUPPORTED, "rp_step_noalloc: the diagnostics need the context's state");
     if (!st->x || !st->y || !st->z || !st->age || !st->dob || !st->status || !st->wd || !st->zeta || !st->bath ||
         !st->gid || !st->isin || !st->pid || !st->flags)
         return fail(ctx, RP_ERR_ARG, "rp_step_noalloc: null state column");
@@ -964,6 +1031,41 @@ int rp_get_particles(rp_ctx* ctx, int64_t n, double* x, double* y, double* z, do
         (rc = col(isin, ctx->tmp_isin, 4)) || (rc = col(wd, ctx->wd, 8)) || (rc = col(zeta, ctx->zeta, 8)) ||
         (rc = col(bath, ctx->bath, 8)) || (rc = col(flags, ctx->flags, 4)))
         return rc;
+    return RP_OK;
+}
+
+int rp_get_diagnostics(rp_ctx* ctx, int64_t n, double* salt, double* temp, double* mean_salt, double* mean_temp,
+                       double* hob, double* bustr, double* bvstr) {
+    if (!ctx) return RP_ERR_ARG;
+    if (n < 0 || n > ctx->n) return fail(ctx, RP_ERR_ARG, "rp_get_diagnostics: n exceeds particle count");
+    if (((salt || temp) && !ctx->d_salt) || ((mean_salt || mean_temp) && !ctx->d_mean_salt) ||
+        ((hob || bustr || bvstr) && !ctx->d_hob))
+        return fail(ctx, RP_ERR_STATE, "rp_get_diagnostics: that diagnostic is off in this context");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->s_comp;
+    auto col = [&](double* dst, const double* src) -> int {
+        if (!dst) return RP_OK;
+        const size_t bytes = (size_t)n * 8;
+        if (!ctx->permuted) return d2h(ctx, dst, src, bytes, s);
+        CK(rp::launch_unsort(8, src, ctx->turbv, ctx->pid, ctx->state_base, ctx->n, n, s));
+        ctx->launches++;
+        return d2h(ctx, dst, ctx->turbv, bytes, s);
+    };
+    int rc;
+    if ((rc = col(salt, ctx->d_salt)) || (rc = col(temp, ctx->d_temp)) || (rc = col(mean_salt, ctx->d_mean_salt)) ||
+        (rc = col(mean_temp, ctx->d_mean_temp)) || (rc = col(hob, ctx->d_hob)) || (rc = col(bustr, ctx->d_bustr)) ||
+        (rc = col(bvstr, ctx->d_bvstr)))
+        return rc;
+    return RP_OK;
+}
+
+int rp_reset_diagnostics(rp_ctx* ctx) {
+    if (!ctx) return RP_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    if (ctx->n > 0 && (ctx->d_mean_salt || ctx->d_hob)) {
+        CK(rp::launch_diag_reset(particles_dev(ctx), ctx->s_comp));
+        ctx->launches++;
+    }
     return RP_OK;
 }
 

@@ -57,6 +57,12 @@ struct RpGridDev {
     const void* v;
     const void* w;
     const void* aks;
+    // diagnostics only: salt, temp [j][i][k][slot4] (N levels); bustr on
+    // the u points, bvstr on the v points, [j][i][slot4]
+    const void* salt;
+    const void* temp;
+    const void* bustr;
+    const void* bvstr;
     double scl[RP_MAXNGRID_D][2];  // GRIDS(ng)%scl(i,1:2)
     double off[RP_MAXNGRID_D][2];
     int sb, sc, sf;                // physical ring slots of t_b, t_c, t_f
@@ -93,7 +99,21 @@ struct RpParticlesDev {
     float* cz;
     double* qwarm;
     double* gwarm;
+    // diagnostics (ROMSPath.f90:130-131): P_Salt, P_Temp, mean_salt,
+    // mean_temp (running sums), P_HOB, P_bustr, P_bvstr
+    double* salt;
+    double* temp;
+    double* mean_salt;
+    double* mean_temp;
+    double* hob;
+    double* bustr;
+    double* bvstr;
 };
+
+// RpStepArgs::diag bits (namelist "other", ROMSPath.h:325-330)
+#define RP_DIAG_SALTTEMP_D 1       // SaltTempOn
+#define RP_DIAG_MEAN_D 2           // SaltTempMean
+#define RP_DIAG_BOTTOM_D 4         // WriteBottom
 
 // Frame-store pointers of the three time levels (b, c, f) of one step of the
 // adjoint model: f[grid][field][t], field 0 zeta [j][i], 1 u, 2 v, 3 w,
@@ -128,6 +148,7 @@ struct RpStepArgs {
     int loop;                      // idt / int(deltat)
     int grid_cap;                  // resident blocks per SM of the step kernels (0: occupancy limit)
     int spline_max_iter;
+    int diag;                      // RP_DIAG_*_D bits
     double vertdist, serr, smth, sub, deltat, aksback;
     double khturb[RP_MAXNGRID_D];
     uint64_t seed, step_index;

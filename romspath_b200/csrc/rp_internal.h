@@ -94,5 +94,7 @@ cudaError_t launch_convert(int src_f32, int dst_f32, const void* src, const void
 cudaError_t launch_state_from_host(const RpParticlesDev& P, const double* gid_d, const int32_t* isin_i,
                                    uint32_t base, cudaStream_t s);
 cudaError_t launch_state_to_host(const RpParticlesDev& P, double* gid_d, int32_t* isin_i, cudaStream_t s);
+// the writer's resets of the diagnostics after an output record
+cudaError_t launch_diag_reset(const RpParticlesDev& P, cudaStream_t s);
 
 }  // namespace rp

@@ -99,7 +99,10 @@ cudaError_t launch_step(const RpStepArgs& A, int field_dtype, int npmax, double*
 
 // The grid loop of ini_ROMSPath (ROMSPath.f90:319-432): defaults, then for
 // ng = 1..Ngrid the first grid whose bounds() says in-grid takes the
-// particle, and zbounds() (boundary_module.f90:145-179) fixes z.
+// particle, and zbounds() (boundary_module.f90:145-179) fixes z.  With the
+// diagnostics on, their initial values (247-264, 353-355) and, for
+// SaltTempOn, salinity, temperature, water depth, zeta and bathymetry at
+// the particle from slot t_c (408-427).
 template <typename T>
 __global__ void k_locate(const __grid_constant__ RpStepArgs A, const double* ipos, const double* jpos,
                          const double* z, const double* dob) {
@@ -145,6 +148,33 @@ __global__ void k_locate(const __grid_constant__ RpStepArgs A, const double* ipo
             }
             P.z[n] = Z;
             if (!inz) P.status[n] = 9.0;
+        }
+    }
+    if (A.diag & RP_DIAG_BOTTOM_D) {
+        P.hob[n] = 9999.0;
+        P.bustr[n] = 0.0;
+        P.bvstr[n] = 0.0;
+    }
+    if (A.diag & RP_DIAG_SALTTEMP_D) {
+        double s = 0.0, t = 0.0;
+        if (P.isin[n]) {
+            const RpGridDev& g = A.g[P.gid[n] - 1];
+            const double X = P.x[n], Y = P.y[n], Z = P.z[n];
+            RhoCell rc;
+            rp_rho_cell(g, X, Y, rc, fl);
+            const double tdepth = -1.0 * rp_bil(g.h, rc);
+            const double zeta = rp_zeta_at<T>(g, rc, g.sc);
+            s = rp_tracer_at<T>(g, g.salt, rc, zeta, tdepth, Z, g.sc);
+            t = rp_tracer_at<T>(g, g.temp, rc, zeta, tdepth, Z, g.sc);
+            P.wd[n] = (-1.0 * tdepth) + zeta;
+            P.zeta[n] = zeta;
+            P.bath[n] = -1.0 * tdepth;
+        }
+        P.salt[n] = s;
+        P.temp[n] = t;
+        if (A.diag & RP_DIAG_MEAN_D) {
+            P.mean_salt[n] = s;
+            P.mean_temp[n] = t;
         }
     }
     P.flags[n] = fl;
@@ -213,6 +243,20 @@ __global__ void k_state_from_host(RpParticlesDev P, const double* gid_d, const i
     P.isin[n] = isin_i[n] ? 1 : 0;
     P.pid[n] = base + (uint32_t)n;
     P.flags[n] = 0u;
+    // diagnostics as the particle read loop leaves them (ROMSPath.f90:247-264, 353-355)
+    if (P.hob) {
+        P.hob[n] = 9999.0;
+        P.bustr[n] = 0.0;
+        P.bvstr[n] = 0.0;
+    }
+    if (P.salt) {
+        P.salt[n] = 0.0;
+        P.temp[n] = 0.0;
+    }
+    if (P.mean_salt) {
+        P.mean_salt[n] = 0.0;
+        P.mean_temp[n] = 0.0;
+    }
 }
 
 cudaError_t launch_state_from_host(const RpParticlesDev& P, const double* gid_d, const int32_t* isin_i,
@@ -236,6 +280,26 @@ cudaError_t launch_state_to_host(const RpParticlesDev& P, double* gid_d, int32_t
     const unsigned blocks = (unsigned)((P.n + block - 1) / block);
     if (blocks == 0) return cudaSuccess;
     k_state_to_host<<<blocks, block, 0, s>>>(P, gid_d, isin_i);
+    return cudaGetLastError();
+}
+
+// The writer's resets after an output record (ROMSPath.f90:2030-2035,
+// 2064): the running sums of salinity and temperature to 0, P_HOB to 9999.
+__global__ void k_diag_reset(RpParticlesDev P) {
+    const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= P.n) return;
+    if (P.mean_salt) {
+        P.mean_salt[n] = 0.0;
+        P.mean_temp[n] = 0.0;
+    }
+    if (P.hob) P.hob[n] = 9999.0;
+}
+
+cudaError_t launch_diag_reset(const RpParticlesDev& P, cudaStream_t s) {
+    const int block = 256;
+    const unsigned blocks = (unsigned)((P.n + block - 1) / block);
+    if (blocks == 0) return cudaSuccess;
+    k_diag_reset<<<blocks, block, 0, s>>>(P);
     return cudaGetLastError();
 }
 

@@ -435,6 +435,74 @@ __device__ void rp_vturb_one(const RpStepArgs& A, int64_t n, const W& w, double*
     if (fl) P.flags[n] |= fl;
 }
 
+// getInterpStr (interpolation_module.f90:964-1174) of one slot on the u or
+// v corner set: the same edge and dry-corner rules as u and v in getInterp3D.
+template <typename T>
+__device__ __forceinline__ double rp_str_at(const void* f, const UVCell& c, int slot) {
+    double v[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) v[k] = c.use[k] ? rp_ld<T>(f, c.o[k] * RP_SLOTS + slot) : 0.0;
+    return c.cff[0] * v[0] + c.cff[1] * v[1] + c.cff[2] * v[2] + c.cff[3] * v[3];
+}
+
+// getInterp3D of salt or temp, ztype 1 (interpolation_module.f90:529-558,
+// 769-809): the rho corner set (bilinear, inverse distance with a dry
+// corner) on the rho levels of the slot's own zeta.
+template <typename T>
+__device__ __forceinline__ double rp_tracer_at(const RpGridDev& g, const void* f, const RhoCell& c, double zeta,
+                                               double depth, double zpar, int slot) {
+    LevelPick L;
+    rp_walk_rho(g, zeta, depth, zpar, L);
+    return rp_col_rho<T>(f, c, c.wet4 ? c.cb : c.ci, g.N, L, slot);
+}
+
+// The diagnostics that close update_particles' particle loop
+// (ROMSPath.f90:935-986), at the particle's new position and grid, with
+// the step's tdepth: height above bottom and, where it reaches a new
+// minimum, the bottom stress (WriteBottom); salinity and temperature and
+// their running sums (SaltTempOn, SaltTempMean).  Out of line: the step's
+// registers are not spent on it when the diagnostics are off.
+template <typename T>
+__device__ __noinline__ void rp_diag_one(const RpStepArgs& A, int64_t n, double tdepth, uint32_t& fl) {
+    const RpParticlesDev& P = A.p;
+    const RpGridDev& g = A.g[P.gid[n] - 1];
+    const double X = P.x[n], Y = P.y[n], Z = P.z[n];
+    if (A.diag & RP_DIAG_BOTTOM_D) {                       // 935-952
+        const double btemp = -1.0 * tdepth + Z;
+        const double hob0 = P.hob[n];
+        const double hob = (btemp < hob0) ? btemp : hob0;
+        P.hob[n] = hob;
+        if (btemp == hob) {
+            UVCell c;
+            rp_u_cell(g, X, Y, c, fl);
+            P.bustr[n] = rp_polintd(A.pi, rp_str_at<T>(g.bustr, c, g.sb), rp_str_at<T>(g.bustr, c, g.sc),
+                                    rp_str_at<T>(g.bustr, c, g.sf));
+            rp_v_cell(g, X, Y, c, fl);
+            P.bvstr[n] = rp_polintd(A.pi, rp_str_at<T>(g.bvstr, c, g.sb), rp_str_at<T>(g.bvstr, c, g.sc),
+                                    rp_str_at<T>(g.bvstr, c, g.sf));
+        }
+    }
+    if (A.diag & RP_DIAG_SALTTEMP_D) {                     // 962-986
+        RhoCell c;
+        rp_rho_cell(g, X, Y, c, fl);
+        const double zb = rp_zeta_at<T>(g, c, g.sb);
+        const double zc = rp_zeta_at<T>(g, c, g.sc);
+        const double zf = rp_zeta_at<T>(g, c, g.sf);
+        const double s = rp_polintd(A.pi, rp_tracer_at<T>(g, g.salt, c, zb, tdepth, Z, g.sb),
+                                    rp_tracer_at<T>(g, g.salt, c, zc, tdepth, Z, g.sc),
+                                    rp_tracer_at<T>(g, g.salt, c, zf, tdepth, Z, g.sf));
+        const double t = rp_polintd(A.pi, rp_tracer_at<T>(g, g.temp, c, zb, tdepth, Z, g.sb),
+                                    rp_tracer_at<T>(g, g.temp, c, zc, tdepth, Z, g.sc),
+                                    rp_tracer_at<T>(g, g.temp, c, zf, tdepth, Z, g.sf));
+        P.salt[n] = s;
+        P.temp[n] = t;
+        if (A.diag & RP_DIAG_MEAN_D) {
+            P.mean_salt[n] = P.mean_salt[n] + s;
+            P.mean_temp[n] = P.mean_temp[n] + t;
+        }
+    }
+}
+
 // One particle of update_particles.  With turbv_in non-null the VTurb
 // displacement comes from the split kernel instead of being computed here.
 template <typename T, class W>
@@ -575,5 +643,6 @@ __device__ void rp_update_one(const RpStepArgs& A, int64_t n, const W& w, const 
         P.isin[n] = 1;
         P.status[n] = -9.0;
     }
+    if (A.diag) rp_diag_one<T>(A, n, tdepth, fl);
     if (fl) P.flags[n] |= fl;
 }

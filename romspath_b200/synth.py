@@ -52,6 +52,7 @@ class GridSpec:
     y0: float = 0.0
     gyre_lx: Optional[float] = None   # gyre domain size; default: this grid
     gyre_ly: Optional[float] = None
+    diag: bool = False            # frames also carry salt, temp, bustr, bvstr
 
     @property
     def xi_u(self) -> int:
@@ -205,6 +206,16 @@ def make_frame(spec: GridSpec, grid: Dict[str, np.ndarray], t: float) -> Dict[st
     aks = np.clip(aks, 0.0, None) * mask[..., None]
 
     out = {"zeta": zeta, "u": u, "v": v, "w": w, "aks": aks}
+    if spec.diag:
+        # stratified salinity and temperature advected by the tide, and a
+        # quadratic bottom stress of the bottom-level current (N/m^2 / rho0)
+        tide = np.sin(om * t - kx * x[:, None])[..., None]
+        out["salt"] = (33.0 + 2.0 * (1.0 - np.exp(z_r / 30.0)) + 0.3 * tide) * mask[..., None]
+        out["temp"] = (8.0 + 10.0 * np.exp(z_r / 40.0) - 0.5 * tide) * mask[..., None]
+        cd = 2.5e-3
+        ub, vb = u[:, :, 0], v[:, :, 0]
+        out["bustr"] = cd * ub * np.abs(ub)
+        out["bvstr"] = cd * vb * np.abs(vb)
     if spec.stokes:
         su = 0.05 * np.exp(zu / 5.0) * math.cos(math.radians(30.0)) * grid["mask_u"][..., None]
         sv = 0.05 * np.exp(zv / 5.0) * math.sin(math.radians(30.0)) * grid["mask_v"][..., None]
@@ -238,7 +249,9 @@ def stored_frame(frame: Dict[str, np.ndarray], field_dtype: str, stokes: bool) -
         f["u"] = f["u"] + f["su"]
         f["v"] = f["v"] + f["sv"]
     out = {}
-    for k in ("zeta", "u", "v", "w", "aks"):
+    for k in ("zeta", "u", "v", "w", "aks", "salt", "temp", "bustr", "bvstr"):
+        if k not in f:
+            continue
         a = f[k]
         if field_dtype == "f32":
             a = a.astype(np.float32).astype(np.float64)

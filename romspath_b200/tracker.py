@@ -74,6 +74,11 @@ class Tracker:
         # cap on resident blocks per SM of the step kernels (0: occupancy
         # limit); fewer blocks mean more particles per thread
         P.reserved[2] = int(blocks_per_sm)
+        # diagnostics (namelist "other"): SaltTempOn, SaltTempMean, WriteBottom
+        self.diag = ((_lib.DIAG_SALTTEMP if params.get("salttemp_on") else 0) |
+                     (_lib.DIAG_SALTTEMP_MEAN if params.get("salttemp_mean") else 0) |
+                     (_lib.DIAG_BOTTOM if params.get("write_bottom") else 0))
+        P.reserved[3] = self.diag
         G = (_lib.RpGrid * self.ng)()
         for k, (sp, gr) in enumerate(zip(specs, grids)):
             g = G[k]
@@ -130,9 +135,18 @@ class Tracker:
         sv = conv(frame["sv"]) if "sv" in frame else None
         if not self.params.stokes:
             su = sv = None
-        fn = self.L.rp_upload_frame_f32 if f32 else self.L.rp_upload_frame
         p = _pf if f32 else _pd
-        rc = fn(self.h, ng, slot, *[p(a) for a in arrs], p(su), p(sv))
+        if self.diag:
+            # salt/temp and bustr/bvstr of the diagnostics that are on
+            st = self.diag & _lib.DIAG_SALTTEMP
+            bt = self.diag & _lib.DIAG_BOTTOM
+            extra = [conv(frame[k]) if on else None
+                     for k, on in (("salt", st), ("temp", st), ("bustr", bt), ("bvstr", bt))]
+            fn = self.L.rp_upload_frame_ext_f32 if f32 else self.L.rp_upload_frame_ext
+            rc = fn(self.h, ng, slot, *[p(a) for a in arrs], p(su), p(sv), *[p(a) for a in extra])
+        else:
+            fn = self.L.rp_upload_frame_f32 if f32 else self.L.rp_upload_frame
+            rc = fn(self.h, ng, slot, *[p(a) for a in arrs], p(su), p(sv))
         self._check(rc, "rp_upload_frame")
 
     # --------------------------------------------------------- particles
@@ -171,6 +185,27 @@ class Tracker:
                                      flags.ctypes.data_as(_lib.PU32))
         self._check(rc, "rp_get_particles")
         return out
+
+    def get_diagnostics(self, n: Optional[int] = None) -> Dict[str, np.ndarray]:
+        """P_Salt, P_Temp, mean_salt, mean_temp (running sums), P_HOB,
+        P_bustr, P_bvstr of the diagnostics that are on."""
+        n = self.n if n is None else n
+        names = []
+        if self.diag & _lib.DIAG_SALTTEMP:
+            names += ["salt", "temp"]
+        if self.diag & _lib.DIAG_SALTTEMP_MEAN:
+            names += ["mean_salt", "mean_temp"]
+        if self.diag & _lib.DIAG_BOTTOM:
+            names += ["hob", "bustr", "bvstr"]
+        out = {k: np.empty(n) for k in names}
+        order = ("salt", "temp", "mean_salt", "mean_temp", "hob", "bustr", "bvstr")
+        rc = self.L.rp_get_diagnostics(self.h, n, *[_pd(out.get(k)) for k in order])
+        self._check(rc, "rp_get_diagnostics")
+        return out
+
+    def reset_diagnostics(self):
+        """The writer's resets after an output record (sums to 0, HOB to 9999)."""
+        self._check(self.L.rp_reset_diagnostics(self.h), "rp_reset_diagnostics")
 
     # --------------------------------------------------------------- step
     def step(self, ex, ix, ets: int, tb: int, tc: int, tf: int):

@@ -18,6 +18,10 @@ import numpy as np
 from romspath_b200 import schedule, synth
 
 FIELDS = ("x", "y", "z", "age", "status", "gid", "isin", "wd", "zeta", "bath", "flags")
+# diagnostics: Tracker.get_diagnostics names -> oracle state names
+DIAG_GPU_TO_ORACLE = {"salt": "p_salt", "temp": "p_temp", "mean_salt": "mean_salt", "mean_temp": "mean_temp",
+                      "hob": "p_hob", "bustr": "p_bustr", "bvstr": "p_bvstr"}
+DIAG_PARAMS = {"salttemp_on": 1, "salttemp_mean": 1, "write_bottom": 1}
 
 
 @dataclasses.dataclass
@@ -115,6 +119,8 @@ def run_gpu(case: Case, nsteps: int, noise: str = "philox", seed: int = 7,
             T.step(it.ex, it.ix, it.ets, it.tb, it.tc, it.tf)
             done += 1
     st = T.get_particles()
+    if T.diag:
+        st.update({DIAG_GPU_TO_ORACLE[k]: v for k, v in T.get_diagnostics().items()})
     return st, T
 
 
@@ -147,10 +153,10 @@ def run_oracle(case: Case, nsteps: int, noise: str = "philox", seed: int = 7,
     return st, m
 
 
-def compare(g: Dict[str, np.ndarray], o: Dict[str, np.ndarray]) -> Dict[str, int]:
+def compare(g: Dict[str, np.ndarray], o: Dict[str, np.ndarray], fields=FIELDS) -> Dict[str, int]:
     """Number of particles whose field differs bit-for-bit, per field."""
     out = {}
-    for f in FIELDS:
+    for f in fields:
         a = np.asarray(g[f])
         b = np.asarray(o[f]).astype(a.dtype)
         if a.dtype.kind == "f":
