@@ -212,6 +212,24 @@ int rp_get_diagnostics(rp_ctx *ctx, int64_t n, double *salt, double *temp, doubl
  * 2064): mean_salt, mean_temp to 0 and P_HOB to 9999.  Stream-ordered. */
 int rp_reset_diagnostics(rp_ctx *ctx);
 
+/* GRIDS(ng)%lon_rho, lat_rho (xi_rho,eta_rho) of grid ng, for the output
+ * records (grid_module.f90:209-300). */
+int rp_set_grid_lonlat(rp_ctx *ctx, int32_t ng, const double *lon_rho, const double *lat_rho);
+
+/* One output record: dataOutput (ROMSPath.f90:1012-1024) and the columns
+ * writeNetCDF puts (1924-2070), computed on the device for particles 1..n
+ * in the caller's order: lon, lat (getInterp2D "lon"/"lat", plain bilinear
+ * at pGID, pX, pY; rp_set_grid_lonlat first), zp = par(:,pZ), age, status,
+ * GID; salt and temp (mean_salt/mI, mean_temp/mI under SaltTempMean, else
+ * P_Salt/P_Temp); HOB, bustr, bvstr.  Then the writer's resets: the sums to
+ * 0 (SaltTempMean) and P_HOB to 9999 (WriteBottom), for every particle,
+ * whichever columns were asked for.  mI is the driver's step count since
+ * the last record (ROMSPath.f90:422, 533, 2035).  Any pointer may be NULL.
+ * Waits for queued work. */
+int rp_output_record(rp_ctx *ctx, int64_t n, int32_t mI, double *lon, double *lat, double *zp,
+                     double *age, double *status, double *gid, double *salt, double *temp,
+                     double *hob, double *bustr, double *bvstr);
+
 /* First particle id of this context (default 0).  Particle k of the next
  * rp_set_particles / rp_locate_particles call gets id base + k; the id keys
  * its Philox noise, so a run split over several contexts (one per GPU) with

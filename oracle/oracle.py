@@ -54,6 +54,7 @@ class OrcGrid(C.Structure):
         ("scl", (C.c_double * 2) * MAXNGRID), ("off", (C.c_double * 2) * MAXNGRID),
         ("zeta", PD * 3), ("u", PD * 3), ("v", PD * 3), ("w", PD * 3), ("aks", PD * 3),
         ("salt", PD * 3), ("temp", PD * 3), ("bustr", PD * 3), ("bvstr", PD * 3),
+        ("lon_rho", PD), ("lat_rho", PD),
     ]
 
 
@@ -137,6 +138,8 @@ def _declare(L):
                                     C.POINTER(C.c_uint32)]
     L.orc_getinterp_str.restype = C.c_double
     L.orc_last_stats.argtypes = [C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    L.orc_output_lonlat.argtypes = [C.POINTER(OrcGrid), C.POINTER(OrcParticles), PD, PD]
+    L.orc_output_lonlat.restype = None
 
 
 def _pd(a: np.ndarray):
@@ -257,6 +260,11 @@ class OracleModel:
                 a = _i32(gr[name])
                 self._keep.append(a)
                 setattr(G, name, a.ctypes.data_as(PI32))
+            for name in ("lon_rho", "lat_rho"):
+                if name in gr:
+                    a = _f64(gr[name])
+                    self._keep.append(a)
+                    setattr(G, name, _pd(a))
             for i in range(self.ng):
                 s = scl[k][i] if scl is not None else (1.0, 1.0)
                 o = off[k][i] if off is not None else (0.0, 0.0)
@@ -362,6 +370,34 @@ class OracleModel:
         a, b = C.c_int64(), C.c_int64()
         lib().orc_last_stats(C.byref(a), C.byref(b))
         return a.value, b.value
+
+    def output_record(self, mI: int) -> Dict[str, np.ndarray]:
+        """One output record of dataOutput / writeNetCDF (ROMSPath.f90:1012-1024,
+        1924-2070): lon, lat, zp, age, status, gid and the diagnostics that are
+        on (salt/temp as sum / mI under SaltTempMean), then the writer's resets
+        (sums to 0, P_HOB to 9999)."""
+        s = self.st
+        n = len(s["x"])
+        lon, lat = np.empty(n), np.empty(n)
+        lib().orc_output_lonlat(self.g, C.byref(self.P), _pd(lon), _pd(lat))
+        rec = {"lon": lon, "lat": lat, "zp": s["z"].copy(), "age": s["age"].copy(),
+               "status": s["status"].copy(), "gid": s["gid"].astype(np.float64)}
+        p = self.params
+        if p.salttemp_on:
+            if p.salttemp_mean:
+                rec["salt"] = s["mean_salt"] / float(mI)
+                rec["temp"] = s["mean_temp"] / float(mI)
+                s["mean_salt"][:] = 0.0
+                s["mean_temp"][:] = 0.0
+            else:
+                rec["salt"] = s["p_salt"].copy()
+                rec["temp"] = s["p_temp"].copy()
+        if p.write_bottom:
+            rec["hob"] = s["p_hob"].copy()
+            rec["bustr"] = s["p_bustr"].copy()
+            rec["bvstr"] = s["p_bvstr"].copy()
+            s["p_hob"][:] = 9999.0
+        return rec
 
     def state(self) -> Dict[str, np.ndarray]:
         return {k: v.copy() for k, v in self.st.items()}

@@ -371,6 +371,8 @@ double orc_getinterp2d(const orc_grid *g, int var, double ipar, double jpar, int
     case ORC_V_DEPTH: a = g->h; break;
     case ORC_V_PM: a = g->pm; break;
     case ORC_V_PN: a = g->pn; break;
+    case ORC_V_LON: a = g->lon_rho; break;                   /* 466-472 */
+    case ORC_V_LAT: a = g->lat_rho; break;                   /* 473-477 */
     default: a = g->zeta[t - 1]; break;
     }
     v[0] = a[IX2(i0, j0, nx)];
@@ -1328,4 +1330,15 @@ int orc_init_particles(const orc_params *prm, const orc_grid *grids, orc_particl
         }
     }
     return 0;
+}
+
+/* dataOutput, ROMSPath.f90:1012-1024 */
+void orc_output_lonlat(const orc_grid *grids, const orc_particles *p, double *lon, double *lat)
+{
+    for (int64_t n = 0; n < p->n; n++) {
+        uint32_t fl = 0;
+        const orc_grid *g = &grids[p->gid[n] - 1];
+        lon[n] = orc_getinterp2d(g, ORC_V_LON, p->x[n], p->y[n], 1, &fl);
+        lat[n] = orc_getinterp2d(g, ORC_V_LAT, p->x[n], p->y[n], 1, &fl);
+    }
 }

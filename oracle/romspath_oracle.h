@@ -60,6 +60,8 @@ typedef struct {
     /* diagnostics fields (NULL unless used): salt, temp (xi_rho,eta_rho,N),
      * bustr (xi_u,eta_u), bvstr (xi_v,eta_v) */
     const double *salt[3], *temp[3], *bustr[3], *bvstr[3];
+    /* GRIDS(ng)%lon_rho, lat_rho (xi_rho, eta_rho); NULL unless output is used */
+    const double *lon_rho, *lat_rho;
 } orc_grid;
 
 typedef struct {
@@ -133,7 +135,7 @@ double orc_ppvalu(const double *brk, const double *coef, int l, int k,
                   double x, int jderiv);
 
 /* 2-D variable ids for orc_getinterp2d / 3-D ids for orc_getinterp3d */
-enum { ORC_V_DEPTH = 0, ORC_V_PM, ORC_V_PN, ORC_V_ZETA };
+enum { ORC_V_DEPTH = 0, ORC_V_PM, ORC_V_PN, ORC_V_ZETA, ORC_V_LON, ORC_V_LAT };
 enum { ORC_V_U = 0, ORC_V_V, ORC_V_W, ORC_V_AKS, ORC_V_SALT, ORC_V_TEMP };
 /* getInterpStr variables (interpolation_module.f90:964-1174) */
 enum { ORC_V_BUSTR = 0, ORC_V_BVSTR };
@@ -153,6 +155,11 @@ int orc_update_particles(const orc_params *prm, const orc_grid *grids,
 int orc_init_particles(const orc_params *prm, const orc_grid *grids,
                        orc_particles *p, const double *ipos,
                        const double *jpos, int tb, int tc);
+
+/* dataOutput (ROMSPath.f90:1012-1024): pLon, pLat by getInterp2D("lon"/
+ * "lat", pGID, pX, pY, 1) for every particle (gather indices clamped; no
+ * flag is recorded, as the output step changes no particle state). */
+void orc_output_lonlat(const orc_grid *grids, const orc_particles *p, double *lon, double *lat);
 
 /* statistics of the last orc_update_particles call (secant iterations) */
 void orc_last_stats(int64_t *spline_calls, int64_t *secant_iters);

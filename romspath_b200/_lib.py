@@ -24,7 +24,7 @@ EXPORTS = [
     "rp_last_error", "rp_destroy", "rp_device_state_get", "rp_last_step_stats", "rp_kernel_launches",
     "rp_step_noalloc", "rp_version", "rp_adj_frames", "rp_adj_set_frame", "rp_forward", "rp_backward",
     "rp_tangent", "rp_adj_replay", "rp_step_n", "rp_set_launch", "rp_upload_frame_ext", "rp_upload_frame_ext_f32",
-    "rp_get_diagnostics", "rp_reset_diagnostics",
+    "rp_get_diagnostics", "rp_reset_diagnostics", "rp_set_grid_lonlat", "rp_output_record",
 ]
 
 PD = C.POINTER(C.c_double)
@@ -106,6 +106,8 @@ def _declare(L):
     L.rp_upload_frame_ext_f32.argtypes = [P, C.c_int32, C.c_int32] + [PF] * 11
     L.rp_get_diagnostics.argtypes = [P, C.c_int64] + [PD] * 7
     L.rp_reset_diagnostics.argtypes = [P]
+    L.rp_set_grid_lonlat.argtypes = [P, C.c_int32, PD, PD]
+    L.rp_output_record.argtypes = [P, C.c_int64, C.c_int32] + [PD] * 11
     L.rp_set_particles.argtypes = [P, C.c_int64] + [PD] * 7 + [PI32]
     L.rp_locate_particles.argtypes = [P, C.c_int64, PD, PD, PD, PD, C.c_int32]
     L.rp_step.argtypes = [P, PD, PD, C.c_int32, C.c_int32, C.c_int32, C.c_int32]

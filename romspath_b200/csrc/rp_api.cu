@@ -25,6 +25,7 @@ struct GridBuf {
     uint8_t *mrho = nullptr, *mu = nullptr, *mv = nullptr;
     void *zeta = nullptr, *u = nullptr, *v = nullptr, *w = nullptr, *aks = nullptr;
     void *salt = nullptr, *temp = nullptr, *bustr = nullptr, *bvstr = nullptr;  // diagnostics only
+    double *lon = nullptr, *lat = nullptr;     // lon_rho, lat_rho (output records only)
     float *qs_u = nullptr, *qs_v = nullptr, *qs_w = nullptr, *qs_aks = nullptr;  // mixed form: [k][slot4]
     double scl[RP_MAXNGRID][2] = {}, off[RP_MAXNGRID][2] = {};
     int map[3] = {-1, -1, -1};                 // logical slot 1..3 -> physical 0..3
@@ -58,6 +59,7 @@ struct rp_ctx {
     int diag = 0;
     double *d_salt = nullptr, *d_temp = nullptr, *d_mean_salt = nullptr, *d_mean_temp = nullptr;
     double *d_hob = nullptr, *d_bustr = nullptr, *d_bvstr = nullptr;
+    double* outbuf = nullptr;                  // packed output record: kOutCols x cap doubles
     // mixed form: compensated FP32 positions, spline warm start, and the
     // FP32 staging field plus per-level maxima of the FP16 quantisation
     float *x32 = nullptr, *y32 = nullptr, *z32 = nullptr, *cx = nullptr, *cy = nullptr, *cz = nullptr;
@@ -211,6 +213,7 @@ void fill_grids(const rp_ctx* c, RpStepArgs& A, int tb, int tc, int tf) {
         d.sr = G.sr; d.csr = G.csr; d.sw = G.sw; d.csw = G.csw;
         d.zeta = G.zeta; d.u = G.u; d.v = G.v; d.w = G.w; d.aks = G.aks;
         d.salt = G.salt; d.temp = G.temp; d.bustr = G.bustr; d.bvstr = G.bvstr;
+        d.lon = G.lon; d.lat = G.lat;
         d.qs_u = G.qs_u; d.qs_v = G.qs_v; d.qs_w = G.qs_w; d.qs_aks = G.qs_aks;
         for (int i = 0; i < RP_MAXNGRID; i++)
             for (int q = 0; q < 2; q++) { d.scl[i][q] = G.scl[i][q]; d.off[i][q] = G.off[i][q]; }
@@ -281,7 +284,7 @@ void free_ctx(rp_ctx* c) {
         GridBuf& G = c->g[k];
         void* ptrs[] = {G.h, G.pm, G.pn, G.sr, G.csr, G.sw, G.csw, G.mrho, G.mu, G.mv,
                         G.zeta, G.u, G.v, G.w, G.aks, G.qs_u, G.qs_v, G.qs_w, G.qs_aks,
-                        G.salt, G.temp, G.bustr, G.bvstr};
+                        G.salt, G.temp, G.bustr, G.bvstr, G.lon, G.lat};
         for (void* p : ptrs) if (p) cudaFree(p);
         for (int s = 0; s < RP_SLOTS; s++) {
             if (G.slot_free[s]) cudaEventDestroy(G.slot_free[s]);
@@ -294,7 +297,7 @@ void free_ctx(rp_ctx* c) {
                     c->ftmp, c->qmax, c->sb.keys, c->sb.hist, c->sb.sums, c->sb.perm, c->sb.gbase,
                     c->adj.ck, c->adj.prec, c->adj.seg, c->adj.work, c->adj.lx, c->adj.ly, c->adj.lz,
                     c->adj.kbar, c->adj.tan, c->d_salt, c->d_temp, c->d_mean_salt, c->d_mean_temp,
-                    c->d_hob, c->d_bustr, c->d_bvstr};
+                    c->d_hob, c->d_bustr, c->d_bvstr, c->outbuf};
     for (int g = 0; g < RP_MAXNGRID; g++)
         for (int f = 0; f < 5; f++)
             if (c->adj.fst[g][f]) cudaFree(c->adj.fst[g][f]);
@@ -1056,6 +1059,58 @@ int rp_get_diagnostics(rp_ctx* ctx, int64_t n, double* salt, double* temp, doubl
         (rc = col(mean_temp, ctx->d_mean_temp)) || (rc = col(hob, ctx->d_hob)) || (rc = col(bustr, ctx->d_bustr)) ||
         (rc = col(bvstr, ctx->d_bvstr)))
         return rc;
+    return RP_OK;
+}
+
+int rp_set_grid_lonlat(rp_ctx* ctx, int32_t ng, const double* lon_rho, const double* lat_rho) {
+    if (!ctx) return RP_ERR_ARG;
+    if (ng < 1 || ng > ctx->ngrid) return fail(ctx, RP_ERR_ARG, "rp_set_grid_lonlat: grid id out of range");
+    if (!lon_rho || !lat_rho) return fail(ctx, RP_ERR_ARG, "rp_set_grid_lonlat: null array");
+    CK(cudaSetDevice(ctx->device));
+    GridBuf& G = ctx->g[ng - 1];
+    const size_t bytes = (size_t)G.nx * G.ny * 8;
+    if (!G.lon && (dalloc(&G.lon, bytes) || dalloc(&G.lat, bytes)))
+        return fail(ctx, RP_ERR_NOMEM, "rp_set_grid_lonlat: allocation");
+    // the step kernels never read these; the copy is ordered before the
+    // next output record on the compute stream
+    int rc;
+    if ((rc = h2d(ctx, G.lon, lon_rho, bytes, ctx->s_comp)) || (rc = h2d(ctx, G.lat, lat_rho, bytes, ctx->s_comp)))
+        return rc;
+    CK(cudaStreamSynchronize(ctx->s_comp));
+    return RP_OK;
+}
+
+int rp_output_record(rp_ctx* ctx, int64_t n, int32_t mI, double* lon, double* lat, double* zp, double* age,
+                     double* status, double* gid, double* salt, double* temp, double* hob, double* bustr,
+                     double* bvstr) {
+    if (!ctx) return RP_ERR_ARG;
+    if (n < 0 || n > ctx->n) return fail(ctx, RP_ERR_ARG, "rp_output_record: n exceeds particle count");
+    if ((lon || lat))
+        for (int k = 0; k < ctx->ngrid; k++)
+            if (!ctx->g[k].lon) return fail(ctx, RP_ERR_STATE, "rp_output_record: lon/lat need rp_set_grid_lonlat");
+    if (((salt || temp) && !(ctx->diag & RP_DIAG_SALTTEMP)) || ((hob || bustr || bvstr) && !(ctx->diag & RP_DIAG_BOTTOM)))
+        return fail(ctx, RP_ERR_STATE, "rp_output_record: that diagnostic is off in this context");
+    if ((ctx->diag & RP_DIAG_SALTTEMP_MEAN) && mI < 1)
+        return fail(ctx, RP_ERR_ARG, "rp_output_record: SaltTempMean needs the step count mI >= 1");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->s_comp;
+    constexpr int kOutCols = 11;
+    if (!ctx->outbuf && dalloc(&ctx->outbuf, (size_t)kOutCols * ctx->cap * 8))
+        return fail(ctx, RP_ERR_NOMEM, "rp_output_record: record buffer");
+    double* host[kOutCols] = {lon, lat, zp, age, status, gid, salt, temp, hob, bustr, bvstr};
+    double* dev[kOutCols];
+    for (int c = 0; c < kOutCols; c++) dev[c] = host[c] ? ctx->outbuf + (size_t)c * ctx->cap : nullptr;
+    rp::OutCols o{dev[0], dev[1], dev[2], dev[3], dev[4], dev[5], dev[6], dev[7], dev[8], dev[9], dev[10]};
+    RpStepArgs A{};
+    fill_params(ctx, A);
+    fill_grids(ctx, A, 1, 1, 1);
+    CK(rp::launch_output(A, o, ctx->permuted ? 1 : 0, ctx->state_base, n, mI, s));
+    ctx->launches++;
+    for (int c = 0; c < kOutCols; c++) {
+        if (!host[c]) continue;
+        const int rc = d2h(ctx, host[c], dev[c], (size_t)n * 8, s);
+        if (rc != RP_OK) return rc;
+    }
     return RP_OK;
 }
 

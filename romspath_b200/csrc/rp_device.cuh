@@ -63,6 +63,8 @@ struct RpGridDev {
     const void* temp;
     const void* bustr;
     const void* bvstr;
+    const double* lon;             // lon_rho, lat_rho [j][i] (output only)
+    const double* lat;
     double scl[RP_MAXNGRID_D][2];  // GRIDS(ng)%scl(i,1:2)
     double off[RP_MAXNGRID_D][2];
     int sb, sc, sf;                // physical ring slots of t_b, t_c, t_f

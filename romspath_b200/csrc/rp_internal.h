@@ -97,4 +97,24 @@ cudaError_t launch_state_to_host(const RpParticlesDev& P, double* gid_d, int32_t
 // the writer's resets of the diagnostics after an output record
 cudaError_t launch_diag_reset(const RpParticlesDev& P, cudaStream_t s);
 
+// One output record (dataOutput / writeNetCDF): the requested columns
+// (null: not wanted) in the caller's particle order, each nout doubles.
+struct OutCols {
+    double* lon;
+    double* lat;
+    double* zp;
+    double* age;
+    double* status;
+    double* gid;
+    double* salt;
+    double* temp;
+    double* hob;
+    double* bustr;
+    double* bvstr;
+};
+// permuted: particle i goes to row pid[i] - base (rows >= nout dropped);
+// mI: the writer's step count dividing the sums (SaltTempMean)
+cudaError_t launch_output(const RpStepArgs& A, const OutCols& o, int permuted, uint32_t base, int64_t nout, int mI,
+                          cudaStream_t s);
+
 }  // namespace rp

@@ -295,6 +295,68 @@ __global__ void k_diag_reset(RpParticlesDev P) {
     if (P.hob) P.hob[n] = 9999.0;
 }
 
+// dataOutput and the record of writeNetCDF (ROMSPath.f90:1012-1024,
+// 1924-2070) for every particle: pLon, pLat by getInterp2D("lon"/"lat",
+// pGID, pX, pY) (plain bilinear, 466-477), zp, age, status, GID and the
+// diagnostics (salt/temp as sum / mI under SaltTempMean, 2010-2014), each
+// into its row of the packed record; then the writer's resets (2030-2035,
+// 2064).
+__global__ void k_output(const __grid_constant__ RpStepArgs A, const OutCols o, int permuted, uint32_t base,
+                         int64_t nout, int mI) {
+    const RpParticlesDev& P = A.p;
+    const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= P.n) return;
+    const int64_t r = permuted ? (int64_t)(P.pid[n] - base) : n;
+    if (r >= 0 && r < nout) {
+        if (o.lon || o.lat) {
+            const RpGridDev& g = A.g[P.gid[n] - 1];
+            const double ip = P.x[n], jp = P.y[n];
+            uint32_t fl = 0;                   // clamped, not recorded: output changes no state
+            const int I = rp_ifloor(ip), J = rp_ifloor(jp);
+            const double X = ip - (double)I, Y = jp - (double)J;
+            const int i0 = rp_clamp(I, 1, g.nx, fl), i1 = rp_clamp(I + 1, 1, g.nx, fl);
+            const int j0 = rp_clamp(J, 1, g.ny, fl), j1 = rp_clamp(J + 1, 1, g.ny, fl);
+            const int64_t o00 = (int64_t)(j0 - 1) * g.nx + (i0 - 1), o10 = (int64_t)(j0 - 1) * g.nx + (i1 - 1);
+            const int64_t o11 = (int64_t)(j1 - 1) * g.nx + (i1 - 1), o01 = (int64_t)(j1 - 1) * g.nx + (i0 - 1);
+            const double c0 = (1 - X) * (1 - Y), c1 = X * (1 - Y), c2 = X * Y, c3 = (1 - X) * Y;
+            if (o.lon)
+                o.lon[r] = c0 * __ldg(g.lon + o00) + c1 * __ldg(g.lon + o10) + c2 * __ldg(g.lon + o11) +
+                           c3 * __ldg(g.lon + o01);
+            if (o.lat)
+                o.lat[r] = c0 * __ldg(g.lat + o00) + c1 * __ldg(g.lat + o10) + c2 * __ldg(g.lat + o11) +
+                           c3 * __ldg(g.lat + o01);
+        }
+        if (o.zp) o.zp[r] = P.z[n];
+        if (o.age) o.age[r] = P.age[n];
+        if (o.status) o.status[r] = P.status[n];
+        if (o.gid) o.gid[r] = (double)P.gid[n];
+        if (A.diag & RP_DIAG_SALTTEMP_D) {
+            const bool mean = (A.diag & RP_DIAG_MEAN_D) != 0;
+            if (o.salt) o.salt[r] = mean ? P.mean_salt[n] / (double)mI : P.salt[n];
+            if (o.temp) o.temp[r] = mean ? P.mean_temp[n] / (double)mI : P.temp[n];
+        }
+        if (A.diag & RP_DIAG_BOTTOM_D) {
+            if (o.hob) o.hob[r] = P.hob[n];
+            if (o.bustr) o.bustr[r] = P.bustr[n];
+            if (o.bvstr) o.bvstr[r] = P.bvstr[n];
+        }
+    }
+    if (A.diag & RP_DIAG_MEAN_D) {
+        P.mean_salt[n] = 0.0;
+        P.mean_temp[n] = 0.0;
+    }
+    if (A.diag & RP_DIAG_BOTTOM_D) P.hob[n] = 9999.0;
+}
+
+cudaError_t launch_output(const RpStepArgs& A, const OutCols& o, int permuted, uint32_t base, int64_t nout, int mI,
+                          cudaStream_t s) {
+    const int block = 256;
+    const unsigned blocks = (unsigned)((A.p.n + block - 1) / block);
+    if (blocks == 0) return cudaSuccess;
+    k_output<<<blocks, block, 0, s>>>(A, o, permuted, base, nout, mI);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_diag_reset(const RpParticlesDev& P, cudaStream_t s) {
     const int block = 256;
     const unsigned blocks = (unsigned)((P.n + block - 1) / block);

@@ -118,7 +118,15 @@ def make_grid(spec: GridSpec) -> Dict[str, np.ndarray]:
     mask_u = np.asfortranarray((mask[:-1, :] * mask[1:, :]).astype(np.int32))
     mask_v = np.asfortranarray((mask[:, :-1] * mask[:, 1:]).astype(np.int32))
     s_rho, cs_r, s_w, cs_w = s_coordinate(N, spec.theta_s, spec.theta_b)
+    # geographic coordinates of the rho points: a grid rotated 10 degrees
+    # about (70.5 W, 41.2 N), the GRIDS(ng)%lon_rho / lat_rho of the output
+    Xg, Yg = np.meshgrid(x, y, indexing="ij")
+    th = math.radians(10.0)
+    lat0 = 41.2
+    lat = lat0 + (Xg * math.sin(th) + Yg * math.cos(th)) / 111_195.0
+    lon = -70.5 + (Xg * math.cos(th) - Yg * math.sin(th)) / (111_195.0 * math.cos(math.radians(lat0)))
     return {
+        "lon_rho": np.asfortranarray(lon), "lat_rho": np.asfortranarray(lat),
         "h": np.asfortranarray(h),
         "pm": np.asfortranarray(np.full((nx, ny), 1.0 / spec.dx)),
         "pn": np.asfortranarray(np.full((nx, ny), 1.0 / spec.dy)),

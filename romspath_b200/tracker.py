@@ -40,6 +40,7 @@ class Tracker:
         self.ng = len(grids)
         self.field_dtype = field_dtype
         self._keep: List[np.ndarray] = []
+        self._lonlat = []
         P = _lib.RpParams()
         P.numpar = int(numpar)
         P.idt = int(params["idt"])
@@ -92,6 +93,9 @@ class Tracker:
                 a = np.asfortranarray(gr[name], dtype=np.int32)
                 self._keep.append(a)
                 setattr(g, name, a.ctypes.data_as(_lib.PI32))
+            if "lon_rho" in gr:
+                self._lonlat.append((k + 1, np.asfortranarray(gr["lon_rho"], dtype=np.float64),
+                                     np.asfortranarray(gr["lat_rho"], dtype=np.float64)))
             if scl is not None:
                 s = np.asfortranarray(np.asarray(scl[k], dtype=np.float64).reshape(self.ng, 2))
                 o = np.asfortranarray(np.asarray(off[k], dtype=np.float64).reshape(self.ng, 2))
@@ -105,6 +109,9 @@ class Tracker:
             raise RomsPathError(f"rp_create failed: {_lib.ERRORS.get(rc, rc)}")
         self.h = h
         self.n = 0
+        for ng, lon, lat in self._lonlat:
+            self._check(L.rp_set_grid_lonlat(h, ng, _pd(lon), _pd(lat)), "rp_set_grid_lonlat")
+        self._lonlat = []
 
     # ------------------------------------------------------------ basics
     def _check(self, rc: int, what: str):
@@ -201,6 +208,24 @@ class Tracker:
         order = ("salt", "temp", "mean_salt", "mean_temp", "hob", "bustr", "bvstr")
         rc = self.L.rp_get_diagnostics(self.h, n, *[_pd(out.get(k)) for k in order])
         self._check(rc, "rp_get_diagnostics")
+        return out
+
+    RECORD = ("lon", "lat", "zp", "age", "status", "gid", "salt", "temp", "hob", "bustr", "bvstr")
+
+    def output_record(self, mI: int, n: Optional[int] = None, out: Optional[Dict[str, np.ndarray]] = None
+                      ) -> Dict[str, np.ndarray]:
+        """One output record (dataOutput + writeNetCDF's columns and resets);
+        ``out`` may hold preallocated (e.g. page-locked) arrays."""
+        n = self.n if n is None else n
+        if out is None:
+            names = ["lon", "lat", "zp", "age", "status", "gid"]
+            if self.diag & _lib.DIAG_SALTTEMP:
+                names += ["salt", "temp"]
+            if self.diag & _lib.DIAG_BOTTOM:
+                names += ["hob", "bustr", "bvstr"]
+            out = {k: np.empty(n) for k in names}
+        rc = self.L.rp_output_record(self.h, n, int(mI), *[_pd(out.get(k)) for k in self.RECORD])
+        self._check(rc, "rp_output_record")
         return out
 
     def reset_diagnostics(self):

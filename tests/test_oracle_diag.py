@@ -116,3 +116,34 @@ def test_off_leaves_diagnostics_alone():
     case = harness.make_case("tiny", 80, seed=3)
     o, _ = harness.run_oracle(case, 12)
     assert np.all(o["p_salt"] == 0.0) and np.all(o["p_hob"] == 9999.0) and np.all(o["mean_salt"] == 0.0)
+
+
+def test_output_record_lonlat_and_means():
+    """dataOutput's lon/lat are plain bilinear interpolants of lon_rho and
+    lat_rho; the record's salt/temp are the sums over mI; the writer then
+    resets the sums and P_HOB."""
+    case = _case(npart=100)
+    m = O.OracleModel(case.specs, case.grids, case.params, scl=case.scl, off=case.off)
+    from romspath_b200 import schedule
+    for (k, slot) in schedule.initial_loads():
+        m.set_frame(1, slot, case.stored(k))
+    m.init_particles(case.release, tb=1)
+    for it in list(harness._steps(case, 5))[0][1][:5]:
+        m.step(it.ex, it.ix, it.ets, it.tb, it.tc, it.tf, noise="philox", seed=7, step_index=it.step_index)
+    st = m.state()
+    rec = m.output_record(6)
+    g = case.grid
+    for n in range(100):
+        ip, jp = st["x"][n], st["y"][n]
+        I, J = int(np.floor(ip)), int(np.floor(jp))
+        X, Y = ip - I, jp - J
+        c = [(1 - X) * (1 - Y), X * (1 - Y), X * Y, (1 - X) * Y]
+        for name, key in (("lon_rho", "lon"), ("lat_rho", "lat")):
+            a = g[name]
+            v = [a[I - 1, J - 1], a[I, J - 1], a[I, J], a[I - 1, J]]
+            want = c[0] * v[0] + c[1] * v[1] + c[2] * v[2] + c[3] * v[3]
+            assert rec[key][n] == want
+    np.testing.assert_array_equal(rec["salt"], st["mean_salt"] / 6.0)
+    np.testing.assert_array_equal(rec["hob"], st["p_hob"])
+    after = m.state()
+    assert np.all(after["mean_salt"] == 0.0) and np.all(after["p_hob"] == 9999.0)
