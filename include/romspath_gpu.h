@@ -104,6 +104,10 @@ typedef struct rp_params {
                                             (0: the occupancy limit; sets the
                                             particles per thread); [3]:
                                             diagnostics, RP_DIAG_* bits;
+                                            [4]: 1 = WETDRY (the -DWETDRY
+                                            build: per-frame wet/dry masks
+                                            in getInterp3D and
+                                            getInterpStr; F64/F32 forms);
                                             others 0 */
 } rp_params;
 
@@ -160,6 +164,21 @@ int rp_upload_frame_ext_f32(rp_ctx *ctx, int32_t ng, int32_t slot, const float *
                             const float *v, const float *w, const float *aks, const float *su,
                             const float *sv, const float *salt, const float *temp, const float *bustr,
                             const float *bvstr);
+
+/* Every field of a frame in one descriptor: the pointers are const
+ * double * (f32 = 0) or const float * (f32 = 1); zeta..aks required,
+ * su/sv with params->stokes, salt..bvstr with the diagnostics, and the
+ * WETDRY masks HYDRODATA(ng)%wetdry_mask_rho/_u/_v(:,:,tind) (0/1 doubles,
+ * (xi_rho,eta_rho), (xi_u,eta_u), (xi_v,eta_v); hydrodynamic_module.f90:
+ * 510-570) with reserved[4] = 1.  NULL where unused. */
+typedef struct rp_frame {
+    int32_t f32;
+    const void *zeta, *u, *v, *w, *aks;
+    const void *su, *sv;
+    const void *salt, *temp, *bustr, *bvstr;
+    const double *wetdry_rho, *wetdry_u, *wetdry_v;
+} rp_frame;
+int rp_upload_frame_desc(rp_ctx *ctx, int32_t ng, int32_t slot, const rp_frame *frame);
 
 /* Set the particle state: the par(:,pX/pY/pZ/pDOB/pAge/pStatus/pGID)
  * columns and isIn(:) of ROMSPath.f90:104-129 for particles 1..n. */

@@ -55,6 +55,7 @@ class OrcGrid(C.Structure):
         ("zeta", PD * 3), ("u", PD * 3), ("v", PD * 3), ("w", PD * 3), ("aks", PD * 3),
         ("salt", PD * 3), ("temp", PD * 3), ("bustr", PD * 3), ("bvstr", PD * 3),
         ("lon_rho", PD), ("lat_rho", PD),
+        ("wd_rho", PD * 3), ("wd_u", PD * 3), ("wd_v", PD * 3),
     ]
 
 
@@ -289,6 +290,9 @@ class OracleModel:
         p.salttemp_mean = int(params.get("salttemp_mean", 0))
         p.write_bottom = int(params.get("write_bottom", 0))
         self.params = p
+        # -DWETDRY: the frames' wet/dry masks replace the static ones in
+        # getInterp3D and getInterpStr
+        self.wetdry = bool(params.get("wetdry", 0))
         self.ndraw = 2 + int(params["idt"]) // int(params["deltat"])
         self.P: Optional[OrcParticles] = None
 
@@ -301,6 +305,11 @@ class OracleModel:
             a = _f64(frame[name])
             self.frames[(ng, slot, name)] = a
             getattr(G, name)[slot - 1] = _pd(a)
+        if self.wetdry:
+            for name, field in (("wetdry_rho", "wd_rho"), ("wetdry_u", "wd_u"), ("wetdry_v", "wd_v")):
+                a = _f64(frame[name])
+                self.frames[(ng, slot, name)] = a
+                getattr(G, field)[slot - 1] = _pd(a)
 
     def set_particles(self, x, y, z, dob, age, status, gid, isin, pid=None):
         n = len(x)

@@ -383,6 +383,12 @@ double orc_getinterp2d(const orc_grid *g, int var, double ipar, double jpar, int
     return cff[0] * v[0] + cff[1] * v[1] + cff[2] * v[2] + cff[3] * v[3];
 }
 
+/* The mask getInterp3D / getInterpStr read: the frame's wetdry mask under
+ * WETDRY (interpolation_module.f90:628-671 and the like), else the grid's. */
+static double mk_u(const orc_grid *g, int t, int idx) { return g->wd_u[t - 1] ? g->wd_u[t - 1][idx] : (double)g->mask_u[idx]; }
+static double mk_v(const orc_grid *g, int t, int idx) { return g->wd_v[t - 1] ? g->wd_v[t - 1][idx] : (double)g->mask_v[idx]; }
+static double mk_r(const orc_grid *g, int t, int idx) { return g->wd_rho[t - 1] ? g->wd_rho[t - 1][idx] : (double)g->mask_rho[idx]; }
+
 /* getInterp3D, interpolation_module.f90:509-962 (u, v, w, AKs).  The full
  * column profile is formed as in the reference, then two levels blended. */
 double orc_getinterp3d(const orc_grid *g, int var, double ipar, double jpar, double zpar,
@@ -456,17 +462,17 @@ double orc_getinterp3d(const orc_grid *g, int var, double ipar, double jpar, dou
         if (Inode >= xi_u) {
             ci[0] = ci[1] = ci[2] = ci[3] = xi_u;
             cj[0] = j0; cj[1] = j0; cj[2] = j1; cj[3] = j1;
-            m[0] = g->mask_u[IX2(xi_u, j0, xi_u)]; m[1] = 0; m[2] = 0;
-            m[3] = g->mask_u[IX2(xi_u, j1, xi_u)];
+            m[0] = mk_u(g, t, IX2(xi_u, j0, xi_u)); m[1] = 0; m[2] = 0;
+            m[3] = mk_u(g, t, IX2(xi_u, j1, xi_u));
         } else if (Inode < 1) {
             ci[0] = ci[1] = ci[2] = ci[3] = 1;
             cj[0] = j0; cj[1] = j0; cj[2] = j1; cj[3] = j1;
-            m[0] = 0; m[1] = g->mask_u[IX2(1, j0, xi_u)];
-            m[2] = g->mask_u[IX2(1, j1, xi_u)]; m[3] = 0;
+            m[0] = 0; m[1] = mk_u(g, t, IX2(1, j0, xi_u));
+            m[2] = mk_u(g, t, IX2(1, j1, xi_u)); m[3] = 0;
         } else {
             ci[0] = Inode; ci[1] = Inode + 1; ci[2] = Inode + 1; ci[3] = Inode;
             cj[0] = j0; cj[1] = j0; cj[2] = j1; cj[3] = j1;
-            for (int k = 0; k < 4; k++) m[k] = g->mask_u[IX2(ci[k], cj[k], xi_u)];
+            for (int k = 0; k < 4; k++) m[k] = mk_u(g, t, IX2(ci[k], cj[k], xi_u));
         }
         zero_dry = 1;
     } else if (var == ORC_V_V) {
@@ -483,13 +489,13 @@ double orc_getinterp3d(const orc_grid *g, int var, double ipar, double jpar, dou
         if (Jnode >= eta_v) {
             ci[0] = i0; ci[1] = i1; ci[2] = i1; ci[3] = i0;
             cj[0] = cj[1] = cj[2] = cj[3] = eta_v;
-            m[0] = g->mask_v[IX2(i0, eta_v, xi_v)];
-            m[1] = g->mask_v[IX2(i1, eta_v, xi_v)];
+            m[0] = mk_v(g, t, IX2(i0, eta_v, xi_v));
+            m[1] = mk_v(g, t, IX2(i1, eta_v, xi_v));
             m[2] = 0; m[3] = 0;
         } else {
             ci[0] = i0; ci[1] = i1; ci[2] = i1; ci[3] = i0;
             cj[0] = Jnode; cj[1] = Jnode; cj[2] = Jnode + 1; cj[3] = Jnode + 1;
-            for (int k = 0; k < 4; k++) m[k] = g->mask_v[IX2(ci[k], cj[k], xi_v)];
+            for (int k = 0; k < 4; k++) m[k] = mk_v(g, t, IX2(ci[k], cj[k], xi_v));
         }
         zero_dry = 1;
     } else {
@@ -503,7 +509,7 @@ double orc_getinterp3d(const orc_grid *g, int var, double ipar, double jpar, dou
         int j0 = clampi(Jnode, 1, ny, flags), j1 = clampi(Jnode + 1, 1, ny, flags);
         ci[0] = i0; ci[1] = i1; ci[2] = i1; ci[3] = i0;
         cj[0] = j0; cj[1] = j0; cj[2] = j1; cj[3] = j1;
-        for (int k = 0; k < 4; k++) m[k] = g->mask_rho[IX2(ci[k], cj[k], nx)];
+        for (int k = 0; k < 4; k++) m[k] = mk_r(g, t, IX2(ci[k], cj[k], nx));
     }
 
     cff[0] = (1 - X) * (1 - Y);
@@ -559,16 +565,16 @@ double orc_getinterp_str(const orc_grid *g, int var, double ipar, double jpar, i
         if (Inode >= xi_u) {
             v[0] = f[IX2(xi_u, j0, xi_u)]; v[1] = f[IX2(xi_u, j0, xi_u)];
             v[2] = f[IX2(xi_u, j1, xi_u)]; v[3] = f[IX2(xi_u, j1, xi_u)];
-            m[0] = g->mask_u[IX2(xi_u, j0, xi_u)]; m[1] = 0; m[2] = 0; m[3] = g->mask_u[IX2(xi_u, j1, xi_u)];
+            m[0] = mk_u(g, t, IX2(xi_u, j0, xi_u)); m[1] = 0; m[2] = 0; m[3] = mk_u(g, t, IX2(xi_u, j1, xi_u));
         } else if (Inode < 1) {
             v[0] = f[IX2(1, j0, xi_u)]; v[1] = f[IX2(1, j0, xi_u)];
             v[2] = f[IX2(1, j1, xi_u)]; v[3] = f[IX2(1, j1, xi_u)];
-            m[0] = 0; m[1] = g->mask_u[IX2(1, j0, xi_u)]; m[2] = g->mask_u[IX2(1, j1, xi_u)]; m[3] = 0;
+            m[0] = 0; m[1] = mk_u(g, t, IX2(1, j0, xi_u)); m[2] = mk_u(g, t, IX2(1, j1, xi_u)); m[3] = 0;
         } else {
             v[0] = f[IX2(Inode, j0, xi_u)]; v[1] = f[IX2(Inode + 1, j0, xi_u)];
             v[2] = f[IX2(Inode + 1, j1, xi_u)]; v[3] = f[IX2(Inode, j1, xi_u)];
-            m[0] = g->mask_u[IX2(Inode, j0, xi_u)]; m[1] = g->mask_u[IX2(Inode + 1, j0, xi_u)];
-            m[2] = g->mask_u[IX2(Inode + 1, j1, xi_u)]; m[3] = g->mask_u[IX2(Inode, j1, xi_u)];
+            m[0] = mk_u(g, t, IX2(Inode, j0, xi_u)); m[1] = mk_u(g, t, IX2(Inode + 1, j0, xi_u));
+            m[2] = mk_u(g, t, IX2(Inode + 1, j1, xi_u)); m[3] = mk_u(g, t, IX2(Inode, j1, xi_u));
         }
     } else {
         const int xi_v = nx, eta_v = ny - 1;
@@ -586,12 +592,12 @@ double orc_getinterp_str(const orc_grid *g, int var, double ipar, double jpar, i
         if (Jnode >= eta_v) {
             v[0] = f[IX2(i0, eta_v, xi_v)]; v[1] = f[IX2(i1, eta_v, xi_v)];
             v[2] = f[IX2(i1, eta_v, xi_v)]; v[3] = f[IX2(i0, eta_v, xi_v)];
-            m[0] = g->mask_v[IX2(i0, eta_v, xi_v)]; m[1] = g->mask_v[IX2(i1, eta_v, xi_v)]; m[2] = 0; m[3] = 0;
+            m[0] = mk_v(g, t, IX2(i0, eta_v, xi_v)); m[1] = mk_v(g, t, IX2(i1, eta_v, xi_v)); m[2] = 0; m[3] = 0;
         } else {
             v[0] = f[IX2(i0, Jnode, xi_v)]; v[1] = f[IX2(i1, Jnode, xi_v)];
             v[2] = f[IX2(i1, Jnode + 1, xi_v)]; v[3] = f[IX2(i0, Jnode + 1, xi_v)];
-            m[0] = g->mask_v[IX2(i0, Jnode, xi_v)]; m[1] = g->mask_v[IX2(i1, Jnode, xi_v)];
-            m[2] = g->mask_v[IX2(i1, Jnode + 1, xi_v)]; m[3] = g->mask_v[IX2(i0, Jnode + 1, xi_v)];
+            m[0] = mk_v(g, t, IX2(i0, Jnode, xi_v)); m[1] = mk_v(g, t, IX2(i1, Jnode, xi_v));
+            m[2] = mk_v(g, t, IX2(i1, Jnode + 1, xi_v)); m[3] = mk_v(g, t, IX2(i0, Jnode + 1, xi_v));
         }
     }
     double nwater = m[0] + m[1] + m[2] + m[3];

@@ -62,6 +62,10 @@ typedef struct {
     const double *salt[3], *temp[3], *bustr[3], *bvstr[3];
     /* GRIDS(ng)%lon_rho, lat_rho (xi_rho, eta_rho); NULL unless output is used */
     const double *lon_rho, *lat_rho;
+    /* -DWETDRY: HYDRODATA(ng)%wetdry_mask_rho/_u/_v(:,:,tind); when set,
+     * getInterp3D and getInterpStr take their masks from these
+     * (hydrodynamic_module.f90:510-570); NULL: the static grid masks */
+    const double *wd_rho[3], *wd_u[3], *wd_v[3];
 } orc_grid;
 
 typedef struct {

@@ -24,7 +24,7 @@ EXPORTS = [
     "rp_last_error", "rp_destroy", "rp_device_state_get", "rp_last_step_stats", "rp_kernel_launches",
     "rp_step_noalloc", "rp_version", "rp_adj_frames", "rp_adj_set_frame", "rp_forward", "rp_backward",
     "rp_tangent", "rp_adj_replay", "rp_step_n", "rp_set_launch", "rp_upload_frame_ext", "rp_upload_frame_ext_f32",
-    "rp_get_diagnostics", "rp_reset_diagnostics", "rp_set_grid_lonlat", "rp_output_record",
+    "rp_get_diagnostics", "rp_reset_diagnostics", "rp_set_grid_lonlat", "rp_output_record", "rp_upload_frame_desc",
 ]
 
 PD = C.POINTER(C.c_double)
@@ -44,6 +44,12 @@ class RpParams(C.Structure):
         ("constant_hturb", C.c_double * MAXNGRID),
         ("seed", C.c_uint64), ("device", C.c_int32), ("reserved", C.c_int32 * 7),
     ]
+
+
+class RpFrame(C.Structure):
+    _fields_ = [("f32", C.c_int32)] + [(k, C.c_void_p) for k in (
+        "zeta", "u", "v", "w", "aks", "su", "sv", "salt", "temp", "bustr", "bvstr")] + [
+        (k, PD) for k in ("wetdry_rho", "wetdry_u", "wetdry_v")]
 
 
 class RpGrid(C.Structure):
@@ -107,6 +113,7 @@ def _declare(L):
     L.rp_get_diagnostics.argtypes = [P, C.c_int64] + [PD] * 7
     L.rp_reset_diagnostics.argtypes = [P]
     L.rp_set_grid_lonlat.argtypes = [P, C.c_int32, PD, PD]
+    L.rp_upload_frame_desc.argtypes = [P, C.c_int32, C.c_int32, C.POINTER(RpFrame)]
     L.rp_output_record.argtypes = [P, C.c_int64, C.c_int32] + [PD] * 11
     L.rp_set_particles.argtypes = [P, C.c_int64] + [PD] * 7 + [PI32]
     L.rp_locate_particles.argtypes = [P, C.c_int64, PD, PD, PD, PD, C.c_int32]

@@ -26,6 +26,7 @@ struct GridBuf {
     void *zeta = nullptr, *u = nullptr, *v = nullptr, *w = nullptr, *aks = nullptr;
     void *salt = nullptr, *temp = nullptr, *bustr = nullptr, *bvstr = nullptr;  // diagnostics only
     double *lon = nullptr, *lat = nullptr;     // lon_rho, lat_rho (output records only)
+    uint8_t *wd_rho = nullptr, *wd_u = nullptr, *wd_v = nullptr;  // WETDRY masks, [j][i][slot4]
     float *qs_u = nullptr, *qs_v = nullptr, *qs_w = nullptr, *qs_aks = nullptr;  // mixed form: [k][slot4]
     double scl[RP_MAXNGRID][2] = {}, off[RP_MAXNGRID][2] = {};
     int map[3] = {-1, -1, -1};                 // logical slot 1..3 -> physical 0..3
@@ -60,6 +61,8 @@ struct rp_ctx {
     double *d_salt = nullptr, *d_temp = nullptr, *d_mean_salt = nullptr, *d_mean_temp = nullptr;
     double *d_hob = nullptr, *d_bustr = nullptr, *d_bvstr = nullptr;
     double* outbuf = nullptr;                  // packed output record: kOutCols x cap doubles
+    bool wetdry = false;                       // WETDRY (reserved[4])
+    uint8_t* wd_stage = nullptr;               // one mask of a frame on its way into the ring
     // mixed form: compensated FP32 positions, spline warm start, and the
     // FP32 staging field plus per-level maxima of the FP16 quantisation
     float *x32 = nullptr, *y32 = nullptr, *z32 = nullptr, *cx = nullptr, *cy = nullptr, *cz = nullptr;
@@ -214,6 +217,7 @@ void fill_grids(const rp_ctx* c, RpStepArgs& A, int tb, int tc, int tf) {
         d.zeta = G.zeta; d.u = G.u; d.v = G.v; d.w = G.w; d.aks = G.aks;
         d.salt = G.salt; d.temp = G.temp; d.bustr = G.bustr; d.bvstr = G.bvstr;
         d.lon = G.lon; d.lat = G.lat;
+        d.wd_rho = G.wd_rho; d.wd_u = G.wd_u; d.wd_v = G.wd_v;
         d.qs_u = G.qs_u; d.qs_v = G.qs_v; d.qs_w = G.qs_w; d.qs_aks = G.qs_aks;
         for (int i = 0; i < RP_MAXNGRID; i++)
             for (int q = 0; q < 2; q++) { d.scl[i][q] = G.scl[i][q]; d.off[i][q] = G.off[i][q]; }
@@ -232,6 +236,7 @@ void fill_params(const rp_ctx* c, RpStepArgs& A) {
     A.grid_cap = p.reserved[2] > 0 ? p.reserved[2] : 0;
     A.spline_max_iter = p.spline_max_iter > 0 ? p.spline_max_iter : 100;
     A.diag = c->diag;
+    A.wetdry = c->wetdry ? 1 : 0;
     A.vertdist = p.vertdist; A.serr = p.serr; A.smth = p.smth; A.sub = p.sub;
     A.deltat = p.deltat; A.aksback = p.aksback;
     for (int i = 0; i < RP_MAXNGRID; i++) A.khturb[i] = p.constant_hturb[i];
@@ -284,7 +289,7 @@ void free_ctx(rp_ctx* c) {
         GridBuf& G = c->g[k];
         void* ptrs[] = {G.h, G.pm, G.pn, G.sr, G.csr, G.sw, G.csw, G.mrho, G.mu, G.mv,
                         G.zeta, G.u, G.v, G.w, G.aks, G.qs_u, G.qs_v, G.qs_w, G.qs_aks,
-                        G.salt, G.temp, G.bustr, G.bvstr, G.lon, G.lat};
+                        G.salt, G.temp, G.bustr, G.bvstr, G.lon, G.lat, G.wd_rho, G.wd_u, G.wd_v};
         for (void* p : ptrs) if (p) cudaFree(p);
         for (int s = 0; s < RP_SLOTS; s++) {
             if (G.slot_free[s]) cudaEventDestroy(G.slot_free[s]);
@@ -297,7 +302,7 @@ void free_ctx(rp_ctx* c) {
                     c->ftmp, c->qmax, c->sb.keys, c->sb.hist, c->sb.sums, c->sb.perm, c->sb.gbase,
                     c->adj.ck, c->adj.prec, c->adj.seg, c->adj.work, c->adj.lx, c->adj.ly, c->adj.lz,
                     c->adj.kbar, c->adj.tan, c->d_salt, c->d_temp, c->d_mean_salt, c->d_mean_temp,
-                    c->d_hob, c->d_bustr, c->d_bvstr, c->outbuf};
+                    c->d_hob, c->d_bustr, c->d_bvstr, c->outbuf, c->wd_stage};
     for (int g = 0; g < RP_MAXNGRID; g++)
         for (int f = 0; f < 5; f++)
             if (c->adj.fst[g][f]) cudaFree(c->adj.fst[g][f]);
@@ -364,10 +369,26 @@ int upload_field(rp_ctx* ctx, const S* src, const S* add, void* dst, int ni, int
     return RP_OK;
 }
 
+// A WETDRY mask of a frame (0/1 doubles, Fortran order, as HYDRODATA holds
+// it) into physical slot `phys` of its [j][i][slot4] ring.
+int upload_mask(rp_ctx* ctx, const double* src, uint8_t* dst, int64_t cnt, int phys) {
+    std::vector<uint8_t> m8((size_t)cnt);
+    for (int64_t i = 0; i < cnt; i++) {
+        if (src[i] != 0.0 && src[i] != 1.0) return fail(ctx, RP_ERR_ARG, "rp_upload_frame: wetdry masks must be 0 or 1");
+        m8[(size_t)i] = src[i] != 0.0 ? 1 : 0;
+    }
+    int rc;
+    if ((rc = h2d(ctx, ctx->wd_stage, m8.data(), (size_t)cnt, ctx->s_copy)) != RP_OK) return rc;
+    CK(rp::launch_mask_slot(ctx->wd_stage, dst, cnt, phys, ctx->s_copy));
+    ctx->launches++;
+    return RP_OK;
+}
+
 template <typename S>
 int upload_frame(rp_ctx* ctx, int32_t ng, int32_t slot, const S* zeta, const S* u, const S* v, const S* w,
                  const S* aks, const S* su, const S* sv, const S* salt = nullptr, const S* temp = nullptr,
-                 const S* bustr = nullptr, const S* bvstr = nullptr) {
+                 const S* bustr = nullptr, const S* bvstr = nullptr, const double* wd_rho = nullptr,
+                 const double* wd_u = nullptr, const double* wd_v = nullptr) {
     if (!ctx) return RP_ERR_ARG;
     if (ng < 1 || ng > ctx->ngrid) return fail(ctx, RP_ERR_ARG, "rp_upload_frame: grid id out of range");
     if (slot < 1 || slot > 3) return fail(ctx, RP_ERR_ARG, "rp_upload_frame: slot must be 1..3");
@@ -376,6 +397,8 @@ int upload_frame(rp_ctx* ctx, int32_t ng, int32_t slot, const S* zeta, const S* 
         return fail(ctx, RP_ERR_ARG, "rp_upload_frame: SaltTempOn needs salt and temp (rp_upload_frame_ext)");
     if ((ctx->diag & RP_DIAG_BOTTOM) && (!bustr || !bvstr))
         return fail(ctx, RP_ERR_ARG, "rp_upload_frame: WriteBottom needs bustr and bvstr (rp_upload_frame_ext)");
+    if (ctx->wetdry && (!wd_rho || !wd_u || !wd_v))
+        return fail(ctx, RP_ERR_ARG, "rp_upload_frame: WETDRY needs the frame's wetdry masks (rp_upload_frame_desc)");
     const bool stokes = ctx->prm.stokes != 0;
     if (stokes && (!su || !sv)) return fail(ctx, RP_ERR_ARG, "rp_upload_frame: stokes on but su/sv null");
     GridBuf& G = ctx->g[ng - 1];
@@ -405,6 +428,11 @@ int upload_frame(rp_ctx* ctx, int32_t ng, int32_t slot, const S* zeta, const S* 
     if (ctx->diag & RP_DIAG_BOTTOM) {
         if ((rc = upload_field<S>(ctx, bustr, nullptr, G.bustr, nx - 1, ny, 1, phys)) != RP_OK) return rc;
         if ((rc = upload_field<S>(ctx, bvstr, nullptr, G.bvstr, nx, ny - 1, 1, phys)) != RP_OK) return rc;
+    }
+    if (ctx->wetdry) {
+        if ((rc = upload_mask(ctx, wd_rho, G.wd_rho, (int64_t)nx * ny, phys)) != RP_OK) return rc;
+        if ((rc = upload_mask(ctx, wd_u, G.wd_u, (int64_t)(nx - 1) * ny, phys)) != RP_OK) return rc;
+        if ((rc = upload_mask(ctx, wd_v, G.wd_v, (int64_t)nx * (ny - 1), phys)) != RP_OK) return rc;
     }
     CK(cudaEventRecord(G.slot_ready[phys], ctx->s_copy));
     if (ctx->direct_pending) {                 // the caller's arrays are free again once copied
@@ -539,6 +567,9 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
     if (p.reserved[3] & ~(RP_DIAG_SALTTEMP | RP_DIAG_SALTTEMP_MEAN | RP_DIAG_BOTTOM)) return RP_ERR_ARG;
     if (p.reserved[3] && (p.field_dtype == RP_FIELD_MIXED || p.field_dtype == RP_FIELD_MIXED_I16))
         return RP_ERR_UNSUPPORTED;
+    if (p.reserved[4] != 0 && p.reserved[4] != 1) return RP_ERR_ARG;
+    if (p.reserved[4] && (p.field_dtype == RP_FIELD_MIXED || p.field_dtype == RP_FIELD_MIXED_I16))
+        return RP_ERR_UNSUPPORTED;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= p.device || p.device < 0) return RP_ERR_NOEXT;
     rp_ctx* ctx = new rp_ctx();
@@ -549,6 +580,7 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
     ctx->mixed = (p.field_dtype == RP_FIELD_MIXED || p.field_dtype == RP_FIELD_MIXED_I16);
     ctx->i16 = (p.field_dtype == RP_FIELD_MIXED_I16);
     ctx->ndraw = 2 + p.idt / (int)p.deltat;
+    ctx->wetdry = p.reserved[4] == 1;
     // SaltTempMean applies only with SaltTempOn (ROMSPath.f90:247-257)
     ctx->diag = p.reserved[3] & (RP_DIAG_SALTTEMP | RP_DIAG_BOTTOM);
     if ((p.reserved[3] & RP_DIAG_SALTTEMP_MEAN) && (p.reserved[3] & RP_DIAG_SALTTEMP))
@@ -627,6 +659,13 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
             cudaMemset(G.salt, 0, n2 * G.N * e);
             cudaMemset(G.temp, 0, n2 * G.N * e);
         }
+        if (ctx->wetdry) {
+            if (dalloc(&G.wd_rho, n2 * RP_SLOTS) || dalloc(&G.wd_u, nu * RP_SLOTS) || dalloc(&G.wd_v, nv * RP_SLOTS))
+                return bail(RP_ERR_NOMEM, "wetdry mask ring allocation");
+            cudaMemset(G.wd_rho, 0, n2 * RP_SLOTS);
+            cudaMemset(G.wd_u, 0, nu * RP_SLOTS);
+            cudaMemset(G.wd_v, 0, nv * RP_SLOTS);
+        }
         if (ctx->diag & RP_DIAG_BOTTOM) {
             if (dalloc(&G.bustr, nu * e) || dalloc(&G.bvstr, nv * e))
                 return bail(RP_ERR_NOMEM, "bottom stress ring allocation");
@@ -668,6 +707,11 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
         dalloc(&ctx->flags, cap * 4) || dalloc(&ctx->tmp_gid, cap * 8) || dalloc(&ctx->tmp_isin, cap * 4) ||
         dalloc(&ctx->turbv, cap * 8))
         return bail(RP_ERR_NOMEM, "particle state allocation");
+    if (ctx->wetdry) {
+        size_t mmax = 0;
+        for (int k = 0; k < ngrid; k++) mmax = std::max(mmax, (size_t)ctx->g[k].nx * ctx->g[k].ny);
+        if (dalloc(&ctx->wd_stage, mmax)) return bail(RP_ERR_NOMEM, "wetdry staging");
+    }
     if ((ctx->diag & RP_DIAG_SALTTEMP) && (dalloc(&ctx->d_salt, cap * 8) || dalloc(&ctx->d_temp, cap * 8)))
         return bail(RP_ERR_NOMEM, "diagnostics allocation");
     if ((ctx->diag & RP_DIAG_SALTTEMP_MEAN) && (dalloc(&ctx->d_mean_salt, cap * 8) || dalloc(&ctx->d_mean_temp, cap * 8)))
@@ -720,6 +764,19 @@ int rp_upload_frame(rp_ctx* ctx, int32_t ng, int32_t slot, const double* zeta, c
 int rp_upload_frame_f32(rp_ctx* ctx, int32_t ng, int32_t slot, const float* zeta, const float* u, const float* v,
                         const float* w, const float* aks, const float* su, const float* sv) {
     return upload_frame<float>(ctx, ng, slot, zeta, u, v, w, aks, su, sv);
+}
+
+int rp_upload_frame_desc(rp_ctx* ctx, int32_t ng, int32_t slot, const rp_frame* f) {
+    if (!ctx || !f) return RP_ERR_ARG;
+    if (f->f32)
+        return upload_frame<float>(ctx, ng, slot, (const float*)f->zeta, (const float*)f->u, (const float*)f->v,
+                                   (const float*)f->w, (const float*)f->aks, (const float*)f->su, (const float*)f->sv,
+                                   (const float*)f->salt, (const float*)f->temp, (const float*)f->bustr,
+                                   (const float*)f->bvstr, f->wetdry_rho, f->wetdry_u, f->wetdry_v);
+    return upload_frame<double>(ctx, ng, slot, (const double*)f->zeta, (const double*)f->u, (const double*)f->v,
+                                (const double*)f->w, (const double*)f->aks, (const double*)f->su, (const double*)f->sv,
+                                (const double*)f->salt, (const double*)f->temp, (const double*)f->bustr,
+                                (const double*)f->bvstr, f->wetdry_rho, f->wetdry_u, f->wetdry_v);
 }
 
 int rp_upload_frame_ext(rp_ctx* ctx, int32_t ng, int32_t slot, const double* zeta, const double* u, const double* v,
@@ -1176,6 +1233,7 @@ int rp_forward(rp_ctx* ctx, int32_t nsteps, const rp_adj_step* steps, double kap
     if (ctx->adj.nframes < 3) return fail(ctx, RP_ERR_STATE, "rp_forward: load the frame store first");
     if (ctx->permuted) return fail(ctx, RP_ERR_STATE, "rp_forward: particle state is re-sorted; set it again");
     if (ctx->hook) return fail(ctx, RP_ERR_STATE, "rp_forward: the noise hook is not used by the adjoint pair");
+    if (ctx->wetdry) return fail(ctx, RP_ERR_UNSUPPORTED, "rp_forward: the adjoint model has the static masks only");
     for (int s = 0; s < nsteps; s++) {
         const rp_adj_step& st = steps[s];
         const int fr[3] = {st.frame_b, st.frame_c, st.frame_f};

@@ -63,6 +63,10 @@ struct RpGridDev {
     const void* temp;
     const void* bustr;
     const void* bvstr;
+    // WETDRY: wetdry_mask_rho / _u / _v of the frames, [j][i][slot4] (0/1)
+    const uint8_t* wd_rho;
+    const uint8_t* wd_u;
+    const uint8_t* wd_v;
     const double* lon;             // lon_rho, lat_rho [j][i] (output only)
     const double* lat;
     double scl[RP_MAXNGRID_D][2];  // GRIDS(ng)%scl(i,1:2)
@@ -151,6 +155,7 @@ struct RpStepArgs {
     int grid_cap;                  // resident blocks per SM of the step kernels (0: occupancy limit)
     int spline_max_iter;
     int diag;                      // RP_DIAG_*_D bits
+    int wetdry;                    // WETDRY: time-varying masks in getInterp3D / getInterpStr
     double vertdist, serr, smth, sub, deltat, aksback;
     double khturb[RP_MAXNGRID_D];
     uint64_t seed, step_index;
@@ -293,6 +298,25 @@ __device__ __forceinline__ void rp_rho_cell(const RpGridDev& g, double ip, doubl
     rp_getcoeff(X, Y, m, c.ci, fl);
 }
 
+// getInterp3D's weights of a rho-point field under WETDRY (interpolation_
+// module.f90:769-939): the bilinear weights, or getcoeff's when a corner of
+// slot `slot`'s wetdry_mask_rho is dry.
+__device__ __forceinline__ void rp_rho_wd_weights(const RpGridDev& g, const RhoCell& c, int slot, double cff[4],
+                                                  uint32_t& fl) {
+    double m[4];
+    m[0] = (double)__ldg(g.wd_rho + c.o00 * RP_SLOTS + slot);
+    m[1] = (double)__ldg(g.wd_rho + c.o10 * RP_SLOTS + slot);
+    m[2] = (double)__ldg(g.wd_rho + c.o11 * RP_SLOTS + slot);
+    m[3] = (double)__ldg(g.wd_rho + c.o01 * RP_SLOTS + slot);
+    const double nwater = m[0] + m[1] + m[2] + m[3];
+    if (nwater < 4.0) {
+        rp_getcoeff(c.X, c.Y, m, cff, fl);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; k++) cff[k] = c.cb[k];
+    }
+}
+
 __device__ __forceinline__ double rp_bil(const double* a, const RhoCell& c) {
     return c.cb[0] * __ldg(a + c.o00) + c.cb[1] * __ldg(a + c.o10) + c.cb[2] * __ldg(a + c.o11) +
            c.cb[3] * __ldg(a + c.o01);
@@ -314,8 +338,12 @@ struct UVCell {
     bool use[4];
 };
 
+// The masks are mask_u (ms = 1, mo = 0) or, under WETDRY, the frame's
+// wetdry_mask_u of one ring slot (mk = the slot ring, ms = RP_SLOTS, mo =
+// the physical slot), hydrodynamic_module.f90:510-570.
 __device__ __forceinline__ void rp_u_cell(const RpGridDev& g, double ip, double jp, UVCell& c,
-                                          uint32_t& fl) {
+                                          uint32_t& fl, const uint8_t* mk = nullptr, int ms = 1, int mo = 0) {
+    if (!mk) mk = g.mu;
     const int xi_u = g.nx - 1, eta_u = g.ny;
     const int Jn = rp_ifloor(jp);
     const double Y = jp - (double)Jn;
@@ -340,12 +368,12 @@ __device__ __forceinline__ void rp_u_cell(const RpGridDev& g, double ip, double 
 #pragma unroll
     for (int k = 0; k < 4; k++) c.o[k] = (int64_t)(cj[k] - 1) * xi_u + (ci[k] - 1);
     if (In >= xi_u) {
-        m[0] = (double)__ldg(g.mu + c.o[0]); m[1] = 0; m[2] = 0; m[3] = (double)__ldg(g.mu + c.o[3]);
+        m[0] = (double)__ldg(mk + c.o[0] * ms + mo); m[1] = 0; m[2] = 0; m[3] = (double)__ldg(mk + c.o[3] * ms + mo);
     } else if (In < 1) {
-        m[0] = 0; m[1] = (double)__ldg(g.mu + c.o[1]); m[2] = (double)__ldg(g.mu + c.o[2]); m[3] = 0;
+        m[0] = 0; m[1] = (double)__ldg(mk + c.o[1] * ms + mo); m[2] = (double)__ldg(mk + c.o[2] * ms + mo); m[3] = 0;
     } else {
 #pragma unroll
-        for (int k = 0; k < 4; k++) m[k] = (double)__ldg(g.mu + c.o[k]);
+        for (int k = 0; k < 4; k++) m[k] = (double)__ldg(mk + c.o[k] * ms + mo);
     }
     const double nwater = m[0] + m[1] + m[2] + m[3];
 #pragma unroll
@@ -360,7 +388,8 @@ __device__ __forceinline__ void rp_u_cell(const RpGridDev& g, double ip, double 
 }
 
 __device__ __forceinline__ void rp_v_cell(const RpGridDev& g, double ip, double jp, UVCell& c,
-                                          uint32_t& fl) {
+                                          uint32_t& fl, const uint8_t* mk = nullptr, int ms = 1, int mo = 0) {
+    if (!mk) mk = g.mv;
     const int xi_v = g.nx, eta_v = g.ny - 1;
     int In = rp_ifloor(ip);
     const double X = ip - (double)In;
@@ -385,10 +414,10 @@ __device__ __forceinline__ void rp_v_cell(const RpGridDev& g, double ip, double 
 #pragma unroll
     for (int k = 0; k < 4; k++) c.o[k] = (int64_t)(cj[k] - 1) * xi_v + (ci[k] - 1);
     if (Jn >= eta_v) {
-        m[0] = (double)__ldg(g.mv + c.o[0]); m[1] = (double)__ldg(g.mv + c.o[1]); m[2] = 0; m[3] = 0;
+        m[0] = (double)__ldg(mk + c.o[0] * ms + mo); m[1] = (double)__ldg(mk + c.o[1] * ms + mo); m[2] = 0; m[3] = 0;
     } else {
 #pragma unroll
-        for (int k = 0; k < 4; k++) m[k] = (double)__ldg(g.mv + c.o[k]);
+        for (int k = 0; k < 4; k++) m[k] = (double)__ldg(mk + c.o[k] * ms + mo);
     }
     const double nwater = m[0] + m[1] + m[2] + m[3];
 #pragma unroll

@@ -94,6 +94,8 @@ cudaError_t launch_convert(int src_f32, int dst_f32, const void* src, const void
 cudaError_t launch_state_from_host(const RpParticlesDev& P, const double* gid_d, const int32_t* isin_i,
                                    uint32_t base, cudaStream_t s);
 cudaError_t launch_state_to_host(const RpParticlesDev& P, double* gid_d, int32_t* isin_i, cudaStream_t s);
+// dst[e * RP_SLOTS + slot] = src[e]: one WETDRY mask into its ring slot
+cudaError_t launch_mask_slot(const uint8_t* src, uint8_t* dst, int64_t n, int slot, cudaStream_t s);
 // the writer's resets of the diagnostics after an output record
 cudaError_t launch_diag_reset(const RpParticlesDev& P, cudaStream_t s);
 

@@ -164,8 +164,8 @@ __global__ void k_locate(const __grid_constant__ RpStepArgs A, const double* ipo
             rp_rho_cell(g, X, Y, rc, fl);
             const double tdepth = -1.0 * rp_bil(g.h, rc);
             const double zeta = rp_zeta_at<T>(g, rc, g.sc);
-            s = rp_tracer_at<T>(g, g.salt, rc, zeta, tdepth, Z, g.sc);
-            t = rp_tracer_at<T>(g, g.temp, rc, zeta, tdepth, Z, g.sc);
+            s = rp_tracer_at<T>(g, g.salt, rc, zeta, tdepth, Z, g.sc, A.wetdry, fl);
+            t = rp_tracer_at<T>(g, g.temp, rc, zeta, tdepth, Z, g.sc, A.wetdry, fl);
             P.wd[n] = (-1.0 * tdepth) + zeta;
             P.zeta[n] = zeta;
             P.bath[n] = -1.0 * tdepth;
@@ -231,6 +231,18 @@ cudaError_t launch_convert(int src_f32, int dst_f32, const void* src, const void
             k_convert<double, double><<<blocks, block, 0, s>>>((const double*)src, (const double*)add,
                                                                (double*)dst, ni, nj, nk, slot, e0, count);
     }
+    return cudaGetLastError();
+}
+
+__global__ void k_mask_slot(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst, int64_t n, int slot) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < n) dst[e * RP_SLOTS + slot] = src[e];
+}
+
+cudaError_t launch_mask_slot(const uint8_t* src, uint8_t* dst, int64_t n, int slot, cudaStream_t s) {
+    const unsigned blocks = (unsigned)((n + 255) / 256);
+    if (blocks == 0) return cudaSuccess;
+    k_mask_slot<<<blocks, 256, 0, s>>>(src, dst, n, slot);
     return cudaGetLastError();
 }
 

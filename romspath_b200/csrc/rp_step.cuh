@@ -28,6 +28,38 @@ struct StageState {
     double tdepth, zb, zc, zf, zeta;
 };
 
+// The u, v, w gathers of find_currents under WETDRY: each slot's value
+// with that slot's wetdry masks (interpolation_module.f90:628-671, 710-757,
+// 917-939).  Out of line: the step without WETDRY keeps its registers.
+template <typename T>
+__device__ __noinline__ void rp_gather_wd(const RpStepArgs& A, const RpGridDev& g, double X, double Y,
+                                          const LevelPick& Lr, const LevelPick& Lw, const RhoCell& rc, double& Uad,
+                                          double& Vad, double& Wad, uint32_t& fl) {
+    const int N = g.N;
+    const int ns = (A.ets == 1) ? 2 : 3;
+    const int sl[3] = {g.sb, g.sc, g.sf};
+    double u[3], v[3], w[3];
+    for (int q = 0; q < ns; q++) {
+        UVCell c;
+        rp_u_cell(g, X, Y, c, fl, g.wd_u, RP_SLOTS, sl[q]);
+        u[q] = rp_col_uv<T>(g.u, c, N, Lr, sl[q]);
+        rp_v_cell(g, X, Y, c, fl, g.wd_v, RP_SLOTS, sl[q]);
+        v[q] = rp_col_uv<T>(g.v, c, N, Lr, sl[q]);
+        double cw[4];
+        rp_rho_wd_weights(g, rc, sl[q], cw, fl);
+        w[q] = rp_col_rho<T>(g.w, rc, cw, N + 1, Lw, sl[q]);
+    }
+    if (A.ets == 1) {                                      // advection_module.f90:277-287
+        Uad = rp_polintd(A.pi, u[0], u[0], u[1]);
+        Vad = rp_polintd(A.pi, v[0], v[0], v[1]);
+        Wad = rp_polintd(A.pi, w[0], w[0], w[1]);
+    } else {
+        Uad = rp_polintd(A.pi, u[0], u[1], u[2]);
+        Vad = rp_polintd(A.pi, v[0], v[1], v[2]);
+        Wad = rp_polintd(A.pi, w[0], w[1], w[2]);
+    }
+}
+
 // find_currents (advection_module.f90:129-350); Z is INOUT.
 template <typename T>
 __device__ __forceinline__ void rp_find_currents(const RpStepArgs& A, const RpGridDev& g, double X, double Y,
@@ -45,6 +77,10 @@ __device__ __forceinline__ void rp_find_currents(const RpStepArgs& A, const RpGr
     LevelPick Lr, Lw;
     rp_walk_rho(g, S.zeta, S.tdepth, Z, Lr);
     rp_walk_w(g, S.zeta, S.tdepth, Z, Lw, fl);
+    if (A.wetdry) {
+        rp_gather_wd<T>(A, g, X, Y, Lr, Lw, S.rc, Uad, Vad, Wad, fl);
+        return;
+    }
     const int N = g.N;
     {
         UVCell cu;
@@ -450,9 +486,14 @@ __device__ __forceinline__ double rp_str_at(const void* f, const UVCell& c, int 
 // corner) on the rho levels of the slot's own zeta.
 template <typename T>
 __device__ __forceinline__ double rp_tracer_at(const RpGridDev& g, const void* f, const RhoCell& c, double zeta,
-                                               double depth, double zpar, int slot) {
+                                               double depth, double zpar, int slot, int wetdry, uint32_t& fl) {
     LevelPick L;
     rp_walk_rho(g, zeta, depth, zpar, L);
+    if (wetdry) {                                          // the slot's wetdry_mask_rho
+        double cff[4];
+        rp_rho_wd_weights(g, c, slot, cff, fl);
+        return rp_col_rho<T>(f, c, cff, g.N, L, slot);
+    }
     return rp_col_rho<T>(f, c, c.wet4 ? c.cb : c.ci, g.N, L, slot);
 }
 
@@ -473,13 +514,24 @@ __device__ __noinline__ void rp_diag_one(const RpStepArgs& A, int64_t n, double 
         const double hob = (btemp < hob0) ? btemp : hob0;
         P.hob[n] = hob;
         if (btemp == hob) {
+            const int sl[3] = {g.sb, g.sc, g.sf};
+            double su[3], sv[3];
             UVCell c;
-            rp_u_cell(g, X, Y, c, fl);
-            P.bustr[n] = rp_polintd(A.pi, rp_str_at<T>(g.bustr, c, g.sb), rp_str_at<T>(g.bustr, c, g.sc),
-                                    rp_str_at<T>(g.bustr, c, g.sf));
-            rp_v_cell(g, X, Y, c, fl);
-            P.bvstr[n] = rp_polintd(A.pi, rp_str_at<T>(g.bvstr, c, g.sb), rp_str_at<T>(g.bvstr, c, g.sc),
-                                    rp_str_at<T>(g.bvstr, c, g.sf));
+            if (A.wetdry) {                                // each slot's wetdry_mask_u / _v
+                for (int q = 0; q < 3; q++) {
+                    rp_u_cell(g, X, Y, c, fl, g.wd_u, RP_SLOTS, sl[q]);
+                    su[q] = rp_str_at<T>(g.bustr, c, sl[q]);
+                    rp_v_cell(g, X, Y, c, fl, g.wd_v, RP_SLOTS, sl[q]);
+                    sv[q] = rp_str_at<T>(g.bvstr, c, sl[q]);
+                }
+            } else {
+                rp_u_cell(g, X, Y, c, fl);
+                for (int q = 0; q < 3; q++) su[q] = rp_str_at<T>(g.bustr, c, sl[q]);
+                rp_v_cell(g, X, Y, c, fl);
+                for (int q = 0; q < 3; q++) sv[q] = rp_str_at<T>(g.bvstr, c, sl[q]);
+            }
+            P.bustr[n] = rp_polintd(A.pi, su[0], su[1], su[2]);
+            P.bvstr[n] = rp_polintd(A.pi, sv[0], sv[1], sv[2]);
         }
     }
     if (A.diag & RP_DIAG_SALTTEMP_D) {                     // 962-986
@@ -488,12 +540,13 @@ __device__ __noinline__ void rp_diag_one(const RpStepArgs& A, int64_t n, double 
         const double zb = rp_zeta_at<T>(g, c, g.sb);
         const double zc = rp_zeta_at<T>(g, c, g.sc);
         const double zf = rp_zeta_at<T>(g, c, g.sf);
-        const double s = rp_polintd(A.pi, rp_tracer_at<T>(g, g.salt, c, zb, tdepth, Z, g.sb),
-                                    rp_tracer_at<T>(g, g.salt, c, zc, tdepth, Z, g.sc),
-                                    rp_tracer_at<T>(g, g.salt, c, zf, tdepth, Z, g.sf));
-        const double t = rp_polintd(A.pi, rp_tracer_at<T>(g, g.temp, c, zb, tdepth, Z, g.sb),
-                                    rp_tracer_at<T>(g, g.temp, c, zc, tdepth, Z, g.sc),
-                                    rp_tracer_at<T>(g, g.temp, c, zf, tdepth, Z, g.sf));
+        const int wd = A.wetdry;
+        const double s = rp_polintd(A.pi, rp_tracer_at<T>(g, g.salt, c, zb, tdepth, Z, g.sb, wd, fl),
+                                    rp_tracer_at<T>(g, g.salt, c, zc, tdepth, Z, g.sc, wd, fl),
+                                    rp_tracer_at<T>(g, g.salt, c, zf, tdepth, Z, g.sf, wd, fl));
+        const double t = rp_polintd(A.pi, rp_tracer_at<T>(g, g.temp, c, zb, tdepth, Z, g.sb, wd, fl),
+                                    rp_tracer_at<T>(g, g.temp, c, zc, tdepth, Z, g.sc, wd, fl),
+                                    rp_tracer_at<T>(g, g.temp, c, zf, tdepth, Z, g.sf, wd, fl));
         P.salt[n] = s;
         P.temp[n] = t;
         if (A.diag & RP_DIAG_MEAN_D) {

@@ -53,6 +53,7 @@ class GridSpec:
     gyre_lx: Optional[float] = None   # gyre domain size; default: this grid
     gyre_ly: Optional[float] = None
     diag: bool = False            # frames also carry salt, temp, bustr, bvstr
+    wetdry: bool = False          # frames also carry wet/dry masks (an intertidal flat)
 
     @property
     def xi_u(self) -> int:
@@ -224,13 +225,29 @@ def make_frame(spec: GridSpec, grid: Dict[str, np.ndarray], t: float) -> Dict[st
         ub, vb = u[:, :, 0], v[:, :, 0]
         out["bustr"] = cd * ub * np.abs(ub)
         out["bvstr"] = cd * vb * np.abs(vb)
+    if spec.wetdry:
+        # an intertidal flat: wet points of a coastal band go dry while the
+        # tidal phase there is low; u/v masks from their rho neighbours, as
+        # ROMS forms them
+        Xg = x[:, None] * np.ones((1, ny))
+        Yg = np.ones((nx, 1)) * y[None, :]
+        Lx = (nx - 1) * spec.dx
+        Ly = (ny - 1) * spec.dy
+        band = (Xg > 0.3 * Lx) & (Xg < 0.7 * Lx) & (Yg > 0.25 * Ly) & (Yg < 0.75 * Ly)
+        patchy = np.sin(Xg / (3.0 * spec.dx)) * np.cos(Yg / (4.0 * spec.dy)) > 0.2
+        low = np.cos(phase_r) < 0.0
+        dry = band & patchy & low
+        wr = (mask.astype(bool) & ~dry).astype(np.float64)
+        out["wetdry_rho"] = wr
+        out["wetdry_u"] = wr[:-1, :] * wr[1:, :]
+        out["wetdry_v"] = wr[:, :-1] * wr[:, 1:]
     if spec.stokes:
         su = 0.05 * np.exp(zu / 5.0) * math.cos(math.radians(30.0)) * grid["mask_u"][..., None]
         sv = 0.05 * np.exp(zv / 5.0) * math.sin(math.radians(30.0)) * grid["mask_v"][..., None]
         out["su"] = su
         out["sv"] = sv
     dt = np.float32 if spec.field_dtype == "f32" else np.float64
-    return {k: np.asfortranarray(a.astype(dt)) for k, a in out.items()}
+    return {k: np.asfortranarray(a.astype(np.float64 if k.startswith("wetdry") else dt)) for k, a in out.items()}
 
 
 def frame_as_f64(frame: Dict[str, np.ndarray]) -> Dict[str, np.ndarray]:
@@ -257,7 +274,7 @@ def stored_frame(frame: Dict[str, np.ndarray], field_dtype: str, stokes: bool) -
         f["u"] = f["u"] + f["su"]
         f["v"] = f["v"] + f["sv"]
     out = {}
-    for k in ("zeta", "u", "v", "w", "aks", "salt", "temp", "bustr", "bvstr"):
+    for k in ("zeta", "u", "v", "w", "aks", "salt", "temp", "bustr", "bvstr", "wetdry_rho", "wetdry_u", "wetdry_v"):
         if k not in f:
             continue
         a = f[k]

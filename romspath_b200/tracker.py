@@ -80,6 +80,9 @@ class Tracker:
                      (_lib.DIAG_SALTTEMP_MEAN if params.get("salttemp_mean") else 0) |
                      (_lib.DIAG_BOTTOM if params.get("write_bottom") else 0))
         P.reserved[3] = self.diag
+        # WETDRY: per-frame wet/dry masks (frames then carry wetdry_rho/_u/_v)
+        self.wetdry = bool(params.get("wetdry", 0))
+        P.reserved[4] = int(self.wetdry)
         G = (_lib.RpGrid * self.ng)()
         for k, (sp, gr) in enumerate(zip(specs, grids)):
             g = G[k]
@@ -143,7 +146,29 @@ class Tracker:
         if not self.params.stokes:
             su = sv = None
         p = _pf if f32 else _pd
-        if self.diag:
+        if self.wetdry:
+            # every field through the frame descriptor
+            d = _lib.RpFrame()
+            d.f32 = int(f32)
+            keep = []
+            for k, a in zip(("zeta", "u", "v", "w", "aks"), arrs):
+                setattr(d, k, a.ctypes.data)
+            for k, a in (("su", su), ("sv", sv)):
+                if a is not None:
+                    setattr(d, k, a.ctypes.data)
+            st = self.diag & _lib.DIAG_SALTTEMP
+            bt = self.diag & _lib.DIAG_BOTTOM
+            for k, on in (("salt", st), ("temp", st), ("bustr", bt), ("bvstr", bt)):
+                if on:
+                    a = conv(frame[k])
+                    keep.append(a)
+                    setattr(d, k, a.ctypes.data)
+            for k in ("wetdry_rho", "wetdry_u", "wetdry_v"):
+                a = np.asfortranarray(frame[k], dtype=np.float64)
+                keep.append(a)
+                setattr(d, k, _pd(a))
+            rc = self.L.rp_upload_frame_desc(self.h, ng, slot, C.byref(d))
+        elif self.diag:
             # salt/temp and bustr/bvstr of the diagnostics that are on
             st = self.diag & _lib.DIAG_SALTTEMP
             bt = self.diag & _lib.DIAG_BOTTOM
