@@ -85,7 +85,9 @@ typedef struct rp_params {
     int32_t vturb_on;                    /* VTurbOn                           */
     int32_t hturb_on;                    /* HTurbOn                           */
     int32_t open_ocean_boundary;         /* OpenOceanBoundary                 */
-    int32_t behavior;                    /* Behavior; only 0 (passive)        */
+    int32_t behavior;                    /* Behavior: 0 passive, 1 swim, 10 Fuchs,
+                                            11 none (VA output); rp_set_behavior
+                                            for the others' parameters       */
     int32_t stokes;                      /* add ustokes/vstokes on upload     */
     int32_t field_dtype;                 /* RP_FIELD_F64 / _F32 / _MIXED      */
     int32_t spline_max_iter;             /* cap of smooth()'s secant loop (0: 100) */
@@ -177,6 +179,10 @@ typedef struct rp_frame {
     const void *su, *sv;
     const void *salt, *temp, *bustr, *bvstr;
     const double *wetdry_rho, *wetdry_u, *wetdry_v;
+    /* behave's fields, (xi_rho,eta_rho,N+1): Accelstd_t and Vortstd_t with
+     * Process_VA, Accelustd_w and Accelvstd_w with Process_WA
+     * (hydrodynamic_module.f90:662-760) */
+    const void *turbaccel, *turbvort, *waveaccelu, *waveaccelv;
 } rp_frame;
 int rp_upload_frame_desc(rp_ctx *ctx, int32_t ng, int32_t slot, const rp_frame *frame);
 
@@ -215,6 +221,30 @@ int rp_step_n(rp_ctx *ctx, int32_t nsteps, const double *ex, const double *ix, c
 int rp_get_particles(rp_ctx *ctx, int64_t n, double *x, double *y, double *z, double *age,
                      double *status, double *gid, int32_t *isin, double *wd, double *zeta,
                      double *bath, uint32_t *flags);
+
+/* behave (behavior_module.f90:186-393): the behavparam / fuchsparam
+ * namelists (ROMSPath.h:150-189) and par(:,pSize) = initsize (199, 342).
+ * behavior must equal rp_params.behavior.  Process_VA / Process_WA add
+ * their fields to every frame (rp_upload_frame_desc) and draw, per
+ * particle-step, 4 Laplace, 2 normal and 1 uniform deviates; Behavior 1
+ * adds swimfast*idt, Behavior 10 the Fuchs swim/sink velocity*idt to the
+ * vertical displacement.  Call before the first frame upload and before
+ * rp_set_noise_hook (the hook then holds 2 + idt/deltat + 7 draws per
+ * particle-step: behave's two normals, then its five uniforms in (0,1)).
+ * F64 and F32 forms. */
+typedef struct rp_behavior {
+    int32_t behavior, process_va, process_wa, va_flag;
+    double swimfast;                     /* m/s (Behavior 1)                  */
+    double initsize;                     /* larval size (um)                  */
+    double vort_cr, vort_sat, b0pv, b1pv, b0wv, b1w;
+    double acc_cr, acc_sat, b0pa, b1pa, b0wa;
+} rp_behavior;
+int rp_set_behavior(rp_ctx *ctx, const rp_behavior *b);
+
+/* Read back par(:,pAcc/pVort/pbehaveW/pSSF) (ROMSPath.f90:800-804) for
+ * particles 1..n; zeros without Process_VA / _WA.  Any pointer may be NULL.
+ * Waits for queued work. */
+int rp_get_behavior(rp_ctx *ctx, int64_t n, double *acc, double *vort, double *behavew, double *ssf);
 
 /* Read back the diagnostics for particles 1..n: P_Salt, P_Temp,
  * mean_salt, mean_temp (the running sums: the writer divides them by its

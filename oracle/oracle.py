@@ -44,6 +44,11 @@ PD = C.POINTER(C.c_double)
 PI32 = C.POINTER(C.c_int32)
 
 
+# the fuchsparam namelist (ROMSPath.h:165-189)
+FUCHS = ("vort_cr", "vort_sat", "b0pv", "b1pv", "b0wv", "b1w", "acc_cr", "acc_sat", "b0pa", "b1pa", "b0wa")
+BEHAVE_FIELDS = ("turbaccel", "turbvort", "waveaccelu", "waveaccelv")
+
+
 class OrcGrid(C.Structure):
     _fields_ = [
         ("xi_rho", C.c_int), ("eta_rho", C.c_int), ("N", C.c_int),
@@ -56,6 +61,7 @@ class OrcGrid(C.Structure):
         ("salt", PD * 3), ("temp", PD * 3), ("bustr", PD * 3), ("bvstr", PD * 3),
         ("lon_rho", PD), ("lat_rho", PD),
         ("wd_rho", PD * 3), ("wd_u", PD * 3), ("wd_v", PD * 3),
+        ("turbaccel", PD * 3), ("turbvort", PD * 3), ("waveaccelu", PD * 3), ("waveaccelv", PD * 3),
     ]
 
 
@@ -68,7 +74,9 @@ class OrcParams(C.Structure):
         ("constant_hturb", C.c_double * MAXNGRID),
         ("spline_max_iter", C.c_int),
         ("salttemp_on", C.c_int), ("salttemp_mean", C.c_int), ("write_bottom", C.c_int),
-    ]
+        ("behavior", C.c_int), ("process_va", C.c_int), ("process_wa", C.c_int), ("va_flag", C.c_int),
+        ("swimfast", C.c_double), ("initsize", C.c_double),
+    ] + [(k, C.c_double) for k in FUCHS]
 
 
 class OrcParticles(C.Structure):
@@ -80,6 +88,7 @@ class OrcParticles(C.Structure):
         ("flags", C.POINTER(C.c_uint32)), ("pid", C.POINTER(C.c_uint32)),
         ("p_salt", PD), ("p_temp", PD), ("mean_salt", PD), ("mean_temp", PD),
         ("p_hob", PD), ("p_bustr", PD), ("p_bvstr", PD),
+        ("p_acc", PD), ("p_vort", PD), ("p_behavew", PD), ("p_ssf", PD),
     ]
 
 
@@ -141,6 +150,12 @@ def _declare(L):
     L.orc_last_stats.argtypes = [C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.orc_output_lonlat.argtypes = [C.POINTER(OrcGrid), C.POINTER(OrcParticles), PD, PD]
     L.orc_output_lonlat.restype = None
+    L.orc_exp.argtypes = [C.c_double]
+    L.orc_exp.restype = C.c_double
+    L.orc_log.argtypes = [C.c_double]
+    L.orc_log.restype = C.c_double
+    L.orc_philox_uniform.argtypes = [C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint32]
+    L.orc_philox_uniform.restype = C.c_double
 
 
 def _pd(a: np.ndarray):
@@ -290,16 +305,27 @@ class OracleModel:
         p.salttemp_mean = int(params.get("salttemp_mean", 0))
         p.write_bottom = int(params.get("write_bottom", 0))
         self.params = p
+        # behave (behavior_module.f90:186-393)
+        p.behavior = int(params.get("behavior", 0))
+        p.process_va = int(params.get("process_va", 0))
+        p.process_wa = int(params.get("process_wa", 0))
+        p.va_flag = int(params.get("va_flag", 0))
+        p.swimfast = float(params.get("swimfast", 0.0))
+        p.initsize = float(params.get("initsize", 0.0))
+        for k in FUCHS:
+            setattr(p, k, float(params.get(k, 0.0)))
         # -DWETDRY: the frames' wet/dry masks replace the static ones in
         # getInterp3D and getInterpStr
         self.wetdry = bool(params.get("wetdry", 0))
-        self.ndraw = 2 + int(params["idt"]) // int(params["deltat"])
+        # draws per particle-step in a noise hook: HTurb 2, VTurb idt/deltat,
+        # then behave's 2 normals and 5 uniforms when Process_VA or _WA
+        self.ndraw = 2 + int(params["idt"]) // int(params["deltat"]) + (7 if (p.process_va or p.process_wa) else 0)
         self.P: Optional[OrcParticles] = None
 
     def set_frame(self, ng: int, slot: int, frame: Dict[str, np.ndarray]):
         """Frame values exactly as stored (FP64 arrays, Stokes already added)."""
         G = self.g[ng - 1]
-        for name in ("zeta", "u", "v", "w", "aks", "salt", "temp", "bustr", "bvstr"):
+        for name in ("zeta", "u", "v", "w", "aks", "salt", "temp", "bustr", "bvstr") + BEHAVE_FIELDS:
             if name not in frame:
                 continue
             a = _f64(frame[name])
@@ -322,7 +348,8 @@ class OracleModel:
             "pid": (np.arange(n, dtype=np.uint32) if pid is None else np.asarray(pid, dtype=np.uint32).copy()),
         }
         # diagnostics as the particle read loop leaves them (ROMSPath.f90:247-264, 353-355)
-        for k in ("p_salt", "p_temp", "mean_salt", "mean_temp", "p_bustr", "p_bvstr"):
+        for k in ("p_salt", "p_temp", "mean_salt", "mean_temp", "p_bustr", "p_bvstr",
+                  "p_acc", "p_vort", "p_behavew", "p_ssf"):          # 343-346
             self.st[k] = np.zeros(n)
         self.st["p_hob"] = np.full(n, 9999.0)
         self._bind()
@@ -337,7 +364,8 @@ class OracleModel:
         P.isin = s["isin"].ctypes.data_as(C.POINTER(C.c_int8))
         P.flags = s["flags"].ctypes.data_as(C.POINTER(C.c_uint32))
         P.pid = s["pid"].ctypes.data_as(C.POINTER(C.c_uint32))
-        for k in ("p_salt", "p_temp", "mean_salt", "mean_temp", "p_hob", "p_bustr", "p_bvstr"):
+        for k in ("p_salt", "p_temp", "mean_salt", "mean_temp", "p_hob", "p_bustr", "p_bvstr",
+                  "p_acc", "p_vort", "p_behavew", "p_ssf"):
             setattr(P, k, _pd(s[k]))
         self.P = P
 

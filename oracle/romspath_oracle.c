@@ -222,6 +222,64 @@ double orc_philox_normal(uint64_t seed, uint32_t pid, uint64_t step, uint32_t dr
     return sqrt(-2.0 * orc_log_pos(u1)) * orc_cos2pi(u2);
 }
 
+/* exp: x = k ln2 + r with |r| <= ln2/2 (k ln2 split so k * hi is exact),
+ * exp(r) by its Taylor series to r^13/13!, then 2^k in two factors. */
+#define ORC_LN2E_HI 0x1.62e42fee00000p-1    /* ln2 truncated to 32 bits */
+#define ORC_LN2E_LO 0x1.a39ef35793c76p-33   /* ln2 - ORC_LN2E_HI */
+#define ORC_INV_LN2 1.4426950408889634
+
+static double pow2i(int m)                  /* 2^m, -1022 <= m <= 1023 */
+{
+    uint64_t b = (uint64_t)(m + 1023) << 52;
+    double r;
+    memcpy(&r, &b, 8);
+    return r;
+}
+
+double orc_exp(double x)
+{
+    if (x != x) return x;
+    if (x > 709.782712893384) return INFINITY;
+    if (x < -745.1332191019412) return 0.0;
+    const double k = rint(x * ORC_INV_LN2);
+    const double r = (x - k * ORC_LN2E_HI) - k * ORC_LN2E_LO;
+    double p = 1.0 / 6227020800.0;                 /* 1/13! */
+    p = p * r + 1.0 / 479001600.0;                 /* 1/12! */
+    p = p * r + 1.0 / 39916800.0;
+    p = p * r + 1.0 / 3628800.0;
+    p = p * r + 1.0 / 362880.0;
+    p = p * r + 1.0 / 40320.0;
+    p = p * r + 1.0 / 5040.0;
+    p = p * r + 1.0 / 720.0;
+    p = p * r + 1.0 / 120.0;
+    p = p * r + 1.0 / 24.0;
+    p = p * r + 1.0 / 6.0;
+    p = p * r + 0.5;
+    p = p * r + 1.0;
+    p = p * r + 1.0;
+    const int ki = (int)k, k1 = ki / 2, k2 = ki - k1;
+    return (p * pow2i(k1)) * pow2i(k2);
+}
+
+double orc_log(double x)
+{
+    if (x != x || x < 0.0) return NAN;
+    if (x == 0.0) return -INFINITY;
+    if (x == INFINITY) return x;
+    if (x < 0x1p-1022)                              /* subnormal: scale by 2^54 */
+        return orc_log_pos(x * 0x1p54) - 54.0 * ORC_LN2_HI - 54.0 * ORC_LN2_LO;
+    return orc_log_pos(x);
+}
+
+double orc_philox_uniform(uint64_t seed, uint32_t pid, uint64_t step, uint32_t k)
+{
+    uint32_t ctr[4] = {pid, (uint32_t)step, (uint32_t)(step >> 32), 0x40000000u + (k >> 2)};
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    uint32_t o[4];
+    orc_philox4x32_10(ctr, key, o);
+    return ((double)o[k & 3u] + 0.5) / 4294967296.0;
+}
+
 typedef struct {
     const orc_noise *nz;
     uint32_t pid;
@@ -241,6 +299,30 @@ static double draw_normal(const noise_ctx *c, uint32_t d)
     default:
         return nz->hook[(int64_t)c->pid * nz->ndraw + d];
     }
+}
+
+/* Uniform k (0..4) of behave: genrand_real3 from the one stream, the
+ * Philox uniform, or the hook's entry d0 + 2 + k (d0 = first behave draw). */
+static double draw_uniform(const noise_ctx *c, uint32_t d0, uint32_t k)
+{
+    const orc_noise *nz = c->nz;
+    switch (nz->kind) {
+    case ORC_NOISE_MT:
+        return orc_mt_real3(nz->mt);
+    case ORC_NOISE_PHILOX:
+        return orc_philox_uniform(nz->seed, c->pid, nz->step, k);
+    default:
+        return nz->hook[(int64_t)c->pid * nz->ndraw + d0 + 2 + k];
+    }
+}
+
+/* laplace (pdf_module.f90:42-55) of one uniform */
+static double laplace_of(double u)
+{
+    const double dev1 = u - 0.5;
+    const double dev2 = -1.0 * orc_log(1.0 - (2.0 * fabs(dev1))) / sqrt(2.0);
+    const double mag = fabs(dev2);
+    return (dev1 >= 0.0) ? mag : -mag;                          /* sign(dev2, dev1) */
 }
 
 /* ======================= interpolation ======================= */
@@ -503,7 +585,12 @@ double orc_getinterp3d(const orc_grid *g, int var, double ipar, double jpar, dou
          * temp (769-809): bilinear, inverse-distance when a corner is dry */
         fld = (var == ORC_V_W) ? g->w[t - 1]
             : (var == ORC_V_AKS) ? g->aks[t - 1]
-            : (var == ORC_V_SALT) ? g->salt[t - 1] : g->temp[t - 1];
+            : (var == ORC_V_SALT) ? g->salt[t - 1]
+            : (var == ORC_V_TEMP) ? g->temp[t - 1]
+            : (var == ORC_V_TURBACCEL) ? g->turbaccel[t - 1]          /* 831-851 */
+            : (var == ORC_V_TURBVORT) ? g->turbvort[t - 1]            /* 852-872 */
+            : (var == ORC_V_WAVEACCELU) ? g->waveaccelu[t - 1]        /* 874-894 */
+            : g->waveaccelv[t - 1];                                   /* 896-916 */
         fni = nx; fnj = ny;
         int i0 = clampi(Inode, 1, nx, flags), i1 = clampi(Inode + 1, 1, nx, flags);
         int j0 = clampi(Jnode, 1, ny, flags), j1 = clampi(Jnode + 1, 1, ny, flags);
@@ -1121,6 +1208,97 @@ static double vturb(const step_env *e, double Xpar, double Ypar, double Zpar, co
 }
 
 /* One particle of update_particles, ROMSPath.f90:662-905 */
+/* behave, behavior_module.f90:186-393, at the step's (Xpar, Ypar, Zpar)
+ * (Zpar after find_currents' clamp) in the particle's grid.  Draws, in
+ * the reference's order, 4 laplace, 2 norm and 1 genrand_real3 whenever
+ * Process_VA or Process_WA; writes behout (par(:,pAcc/pVort/pbehaveW/pSSF),
+ * ROMSPath.f90:800-804) and returns ZBehav.  Real powers are pinned:
+ * x**2.0D0 = x*x, r**3.0D0 = (r*r)*r, x**0.5D0 = sqrt(x). */
+static double behave(const step_env *e, const orc_grid *g, double Xpar, double Ypar, double Zpar,
+                     const noise_ctx *nc, double behout[4], uint32_t *fl)
+{
+    const orc_params *b = e->prm;
+    const double G = 980.0, RHOF = 1.026, MU = 0.010260, RHOP = 1.06;   /* ROMSPath.h:15-19 */
+    double wb = 0.0;
+    behout[0] = behout[1] = behout[2] = behout[3] = 0.0;
+    if (b->process_va || b->process_wa) {                       /* 240 */
+        const double depth = -1.0 * orc_getinterp2d(g, ORC_V_DEPTH, Xpar, Ypar, e->tc, fl);
+        const double zt[3] = {orc_getinterp2d(g, ORC_V_ZETA, Xpar, Ypar, e->tb, fl),
+                              orc_getinterp2d(g, ORC_V_ZETA, Xpar, Ypar, e->tc, fl),
+                              orc_getinterp2d(g, ORC_V_ZETA, Xpar, Ypar, e->tf, fl)};
+        const int sl[3] = {e->tb, e->tc, e->tf};
+        double ey[3], stdaccturbu, stdvortturb, stdaccwaveu, stdaccwavev;
+        if (b->process_va) {                                    /* 249-264 */
+            for (int q = 0; q < 3; q++)
+                ey[q] = orc_getinterp3d(g, ORC_V_TURBACCEL, Xpar, Ypar, Zpar, sl[q], 2, zt[q], depth, fl);
+            stdaccturbu = orc_polintd(e->ex, ey, e->ix[1]);
+            for (int q = 0; q < 3; q++)
+                ey[q] = orc_getinterp3d(g, ORC_V_TURBVORT, Xpar, Ypar, Zpar, sl[q], 2, zt[q], depth, fl);
+            stdvortturb = orc_polintd(e->ex, ey, e->ix[1]);
+            stdaccturbu = stdaccturbu * 100.0;
+        } else {
+            stdaccturbu = 0.0;
+            stdvortturb = 0.0;
+        }
+        if (b->process_wa) {                                    /* 269-280 */
+            for (int q = 0; q < 3; q++)
+                ey[q] = orc_getinterp3d(g, ORC_V_WAVEACCELU, Xpar, Ypar, Zpar, sl[q], 2, zt[q], depth, fl);
+            stdaccwaveu = orc_polintd(e->ex, ey, e->ix[1]);
+            for (int q = 0; q < 3; q++)
+                ey[q] = orc_getinterp3d(g, ORC_V_WAVEACCELV, Xpar, Ypar, Zpar, sl[q], 2, zt[q], depth, fl);
+            stdaccwavev = orc_polintd(e->ex, ey, e->ix[1]);
+            stdaccwaveu = stdaccwaveu * 100.0;
+            stdaccwavev = stdaccwavev * 100.0;
+        } else {
+            stdaccwaveu = 0.0;
+            stdaccwavev = 0.0;
+        }
+        const uint32_t d0 = 2u + (uint32_t)(b->idt / (int)b->deltat);
+        const double vortturbu = stdvortturb * laplace_of(draw_uniform(nc, d0, 0));   /* 285-292 */
+        const double vortturbv = stdvortturb * laplace_of(draw_uniform(nc, d0, 1));
+        const double vorttot = sqrt(vortturbu * vortturbu + vortturbv * vortturbv);
+        const double accturbu = stdaccturbu * laplace_of(draw_uniform(nc, d0, 2));    /* 298-302 */
+        const double accturbv = stdaccturbu * laplace_of(draw_uniform(nc, d0, 3));
+        const double accwaveu = stdaccwaveu * draw_normal(nc, d0);                  /* 307-311 */
+        const double accwavev = stdaccwavev * draw_normal(nc, d0 + 1);
+        const double au = accturbu + accwaveu, av = accturbv + accwavev;
+        const double acctot = sqrt(au * au + av * av);
+        const double c1v = 2.0 / orc_log(b->vort_cr / b->vort_sat);                /* 322-326 */
+        const double c2v = c1v * orc_log(vorttot / sqrt(b->vort_cr * b->vort_sat));
+        const double c1a = 2.0 / orc_log(b->acc_cr / b->acc_sat);
+        const double c2a = c1a * orc_log(acctot / sqrt(b->acc_cr * b->acc_sat));
+        const double ev = orc_exp(-2.0 * c2v), ea = orc_exp(-2.0 * c2a);
+        const double pswimv = (b->b1pv - b->b0pv) / (1.0 + ev) + b->b0pv;          /* 329-330 */
+        const double pswima = (b->b1pa - b->b0pa) / (1.0 + ea) + b->b0pa;
+        double pswim;
+        if (b->va_flag == 1) pswim = pswimv;
+        else if (b->va_flag == 2) pswim = pswima;
+        else pswim = (pswima < pswimv) ? pswima : pswimv;                          /* min(pswima,pswimv) */
+        const double wswimv = ((b->b1w - b->b0wv) * 1.0 / (1.0 + ev)) + b->b0wv;   /* 341 */
+        const double wswima = ((b->b1w - b->b0wa) * 1.0 / (1.0 + ea)) + b->b0wa;   /* 344 */
+        double wswim;
+        if (b->va_flag == 1) wswim = wswimv;
+        else if (b->va_flag == 2) wswim = wswima;
+        else wswim = wswima + wswimv;
+        const double r = b->initsize / 2.0e4;                                       /* 359-360 */
+        const double wsink = ((3.0 * MU) - sqrt((4.0 / 3.0) * G * ((r * r) * r) * RHOF * (RHOP - RHOF) +
+                                                (9.0 * (MU * MU)))) / (r * RHOF);
+        behout[0] = acctot / 100.0;
+        behout[1] = vorttot;
+        if (draw_uniform(nc, d0, 4) < pswim) {                                     /* 366-375 */
+            wb = wswim;
+            behout[3] = 0.0;
+        } else {
+            wb = wsink;
+            behout[3] = 1.0;
+        }
+        behout[2] = wb;
+    }
+    if (b->behavior == 1) return b->swimfast * (double)b->idt;                    /* 381-391 */
+    if (b->behavior == 10) return wb * (double)b->idt / 100.0;
+    return 0.0;
+}
+
 static void update_one(const step_env *e0, const orc_grid *grids, orc_particles *p, int64_t n,
                        const orc_noise *noise, vt_work *w, int64_t *n_spline, int64_t *n_iter)
 {
@@ -1150,7 +1328,16 @@ static void update_one(const step_env *e0, const orc_grid *grids, orc_particles 
         TurbV = vturb(&e, Xpar, Ypar, Zpar, &nc, w, &fl, n_iter);
         (*n_spline)++;
     }
-    /* behave(): Behavior not in {1,10}, no VA/WA -> zero, no draws */
+    if (prm->behavior || prm->process_va || prm->process_wa) {     /* 800-804 */
+        double behout[4];
+        ZBehav = behave(&e, e.g, Xpar, Ypar, Zpar, &nc, behout, &fl);
+        if (p->p_acc) {
+            p->p_acc[n] = behout[0];
+            p->p_vort[n] = behout[1];
+            p->p_behavew[n] = behout[2];
+            p->p_ssf[n] = behout[3];
+        }
+    }
 
     double newXpos = p->x[n] + AdvectX + TurbHx;                 /* 821 */
     double newYpos = p->y[n] + AdvectY + TurbHy;

@@ -66,6 +66,9 @@ typedef struct {
      * getInterp3D and getInterpStr take their masks from these
      * (hydrodynamic_module.f90:510-570); NULL: the static grid masks */
     const double *wd_rho[3], *wd_u[3], *wd_v[3];
+    /* behaviour fields (Process_VA / Process_WA), (xi_rho,eta_rho,N+1):
+     * HYDRODATA(ng)%Accelstd_t, Vortstd_t, Accelustd_w, Accelvstd_w */
+    const double *turbaccel[3], *turbvort[3], *waveaccelu[3], *waveaccelv[3];
 } orc_grid;
 
 typedef struct {
@@ -78,6 +81,12 @@ typedef struct {
     double constant_hturb[ORC_MAXNGRID];
     int spline_max_iter;         /* cap on smooth()'s secant loop (ref: none) */
     int salttemp_on, salttemp_mean, write_bottom;   /* SaltTempOn, SaltTempMean, WriteBottom */
+    /* behave (behavior_module.f90:186-393): Behavior (0, 1 or 10),
+     * Process_VA, Process_WA, va_flag; swimfast (m/s); initsize =
+     * par(:,pSize); the fuchsparam namelist (ROMSPath.h:165-189) */
+    int behavior, process_va, process_wa, va_flag;
+    double swimfast, initsize;
+    double vort_cr, vort_sat, b0pv, b1pv, b0wv, b1w, acc_cr, acc_sat, b0pa, b1pa, b0wa;
 } orc_params;
 
 typedef struct {
@@ -91,6 +100,8 @@ typedef struct {
     /* diagnostics (NULL unless used): P_Salt, P_Temp, mean_salt, mean_temp,
      * P_HOB, P_bustr, P_bvstr (ROMSPath.f90:130-131) */
     double *p_salt, *p_temp, *mean_salt, *mean_temp, *p_hob, *p_bustr, *p_bvstr;
+    /* behave's outputs par(:,pAcc/pVort/pbehaveW/pSSF) (NULL unless used) */
+    double *p_acc, *p_vort, *p_behavew, *p_ssf;
 } orc_particles;
 
 /* MT19937 state, restated from random_module.f90:109-198. */
@@ -118,6 +129,13 @@ void     orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_
 double   orc_philox_normal(uint64_t seed, uint32_t pid, uint64_t step, uint32_t draw);
 double   orc_log_pos(double x);
 double   orc_cos2pi(double u);
+/* exp and log of any double from their series with exact argument
+ * reductions (own restatement; the device uses the same operations) */
+double   orc_exp(double x);
+double   orc_log(double x);
+/* the k-th uniform (k = 0..4) of behave's draws under Philox: counter
+ * (pid, step, 0x40000000 + k/4), word k%4, (r + 0.5) / 2^32 */
+double   orc_philox_uniform(uint64_t seed, uint32_t pid, uint64_t step, uint32_t k);
 
 double orc_polintd(const double xa[3], const double ya[3], double x);
 void   orc_linint(const double *xa, const double *ya, int n, double x, double *y, double *m);
@@ -140,7 +158,8 @@ double orc_ppvalu(const double *brk, const double *coef, int l, int k,
 
 /* 2-D variable ids for orc_getinterp2d / 3-D ids for orc_getinterp3d */
 enum { ORC_V_DEPTH = 0, ORC_V_PM, ORC_V_PN, ORC_V_ZETA, ORC_V_LON, ORC_V_LAT };
-enum { ORC_V_U = 0, ORC_V_V, ORC_V_W, ORC_V_AKS, ORC_V_SALT, ORC_V_TEMP };
+enum { ORC_V_U = 0, ORC_V_V, ORC_V_W, ORC_V_AKS, ORC_V_SALT, ORC_V_TEMP,
+       ORC_V_TURBACCEL, ORC_V_TURBVORT, ORC_V_WAVEACCELU, ORC_V_WAVEACCELV };
 /* getInterpStr variables (interpolation_module.f90:964-1174) */
 enum { ORC_V_BUSTR = 0, ORC_V_BVSTR };
 double orc_getinterp_str(const orc_grid *g, int var, double ipar, double jpar, int t, uint32_t *flags);

@@ -25,6 +25,7 @@ EXPORTS = [
     "rp_step_noalloc", "rp_version", "rp_adj_frames", "rp_adj_set_frame", "rp_forward", "rp_backward",
     "rp_tangent", "rp_adj_replay", "rp_step_n", "rp_set_launch", "rp_upload_frame_ext", "rp_upload_frame_ext_f32",
     "rp_get_diagnostics", "rp_reset_diagnostics", "rp_set_grid_lonlat", "rp_output_record", "rp_upload_frame_desc",
+    "rp_set_behavior", "rp_get_behavior",
 ]
 
 PD = C.POINTER(C.c_double)
@@ -49,7 +50,16 @@ class RpParams(C.Structure):
 class RpFrame(C.Structure):
     _fields_ = [("f32", C.c_int32)] + [(k, C.c_void_p) for k in (
         "zeta", "u", "v", "w", "aks", "su", "sv", "salt", "temp", "bustr", "bvstr")] + [
-        (k, PD) for k in ("wetdry_rho", "wetdry_u", "wetdry_v")]
+        (k, PD) for k in ("wetdry_rho", "wetdry_u", "wetdry_v")] + [
+        (k, C.c_void_p) for k in ("turbaccel", "turbvort", "waveaccelu", "waveaccelv")]
+
+
+FUCHS = ("vort_cr", "vort_sat", "b0pv", "b1pv", "b0wv", "b1w", "acc_cr", "acc_sat", "b0pa", "b1pa", "b0wa")
+
+
+class RpBehavior(C.Structure):
+    _fields_ = [(k, C.c_int32) for k in ("behavior", "process_va", "process_wa", "va_flag")] + [
+        ("swimfast", C.c_double), ("initsize", C.c_double)] + [(k, C.c_double) for k in FUCHS]
 
 
 class RpGrid(C.Structure):
@@ -114,6 +124,8 @@ def _declare(L):
     L.rp_reset_diagnostics.argtypes = [P]
     L.rp_set_grid_lonlat.argtypes = [P, C.c_int32, PD, PD]
     L.rp_upload_frame_desc.argtypes = [P, C.c_int32, C.c_int32, C.POINTER(RpFrame)]
+    L.rp_set_behavior.argtypes = [P, C.POINTER(RpBehavior)]
+    L.rp_get_behavior.argtypes = [P, C.c_int64] + [PD] * 4
     L.rp_output_record.argtypes = [P, C.c_int64, C.c_int32] + [PD] * 11
     L.rp_set_particles.argtypes = [P, C.c_int64] + [PD] * 7 + [PI32]
     L.rp_locate_particles.argtypes = [P, C.c_int64, PD, PD, PD, PD, C.c_int32]

@@ -27,6 +27,8 @@ struct GridBuf {
     void *salt = nullptr, *temp = nullptr, *bustr = nullptr, *bvstr = nullptr;  // diagnostics only
     double *lon = nullptr, *lat = nullptr;     // lon_rho, lat_rho (output records only)
     uint8_t *wd_rho = nullptr, *wd_u = nullptr, *wd_v = nullptr;  // WETDRY masks, [j][i][slot4]
+    void *turbaccel = nullptr, *turbvort = nullptr;      // behave's fields (Process_VA)
+    void *waveaccelu = nullptr, *waveaccelv = nullptr;   // (Process_WA)
     float *qs_u = nullptr, *qs_v = nullptr, *qs_w = nullptr, *qs_aks = nullptr;  // mixed form: [k][slot4]
     double scl[RP_MAXNGRID][2] = {}, off[RP_MAXNGRID][2] = {};
     int map[3] = {-1, -1, -1};                 // logical slot 1..3 -> physical 0..3
@@ -62,6 +64,10 @@ struct rp_ctx {
     double *d_hob = nullptr, *d_bustr = nullptr, *d_bvstr = nullptr;
     double* outbuf = nullptr;                  // packed output record: kOutCols x cap doubles
     bool wetdry = false;                       // WETDRY (reserved[4])
+    // behave: parameters (rp_set_behavior), its outputs per particle
+    bool beh_set = false;
+    RpBehaviorDev beh{};
+    double *b_acc = nullptr, *b_vort = nullptr, *b_behavew = nullptr, *b_ssf = nullptr;
     uint8_t* wd_stage = nullptr;               // one mask of a frame on its way into the ring
     // mixed form: compensated FP32 positions, spline warm start, and the
     // FP32 staging field plus per-level maxima of the FP16 quantisation
@@ -203,6 +209,7 @@ RpParticlesDev particles_dev(const rp_ctx* c) {
     P.qwarm = c->qwarm; P.gwarm = c->gwarm;
     P.salt = c->d_salt; P.temp = c->d_temp; P.mean_salt = c->d_mean_salt; P.mean_temp = c->d_mean_temp;
     P.hob = c->d_hob; P.bustr = c->d_bustr; P.bvstr = c->d_bvstr;
+    P.acc = c->b_acc; P.vort = c->b_vort; P.behavew = c->b_behavew; P.ssf = c->b_ssf;
     return P;
 }
 
@@ -218,6 +225,7 @@ void fill_grids(const rp_ctx* c, RpStepArgs& A, int tb, int tc, int tf) {
         d.salt = G.salt; d.temp = G.temp; d.bustr = G.bustr; d.bvstr = G.bvstr;
         d.lon = G.lon; d.lat = G.lat;
         d.wd_rho = G.wd_rho; d.wd_u = G.wd_u; d.wd_v = G.wd_v;
+        d.turbaccel = G.turbaccel; d.turbvort = G.turbvort; d.waveaccelu = G.waveaccelu; d.waveaccelv = G.waveaccelv;
         d.qs_u = G.qs_u; d.qs_v = G.qs_v; d.qs_w = G.qs_w; d.qs_aks = G.qs_aks;
         for (int i = 0; i < RP_MAXNGRID; i++)
             for (int q = 0; q < 2; q++) { d.scl[i][q] = G.scl[i][q]; d.off[i][q] = G.off[i][q]; }
@@ -237,6 +245,7 @@ void fill_params(const rp_ctx* c, RpStepArgs& A) {
     A.spline_max_iter = p.spline_max_iter > 0 ? p.spline_max_iter : 100;
     A.diag = c->diag;
     A.wetdry = c->wetdry ? 1 : 0;
+    A.beh = c->beh;
     A.vertdist = p.vertdist; A.serr = p.serr; A.smth = p.smth; A.sub = p.sub;
     A.deltat = p.deltat; A.aksback = p.aksback;
     for (int i = 0; i < RP_MAXNGRID; i++) A.khturb[i] = p.constant_hturb[i];
@@ -289,7 +298,8 @@ void free_ctx(rp_ctx* c) {
         GridBuf& G = c->g[k];
         void* ptrs[] = {G.h, G.pm, G.pn, G.sr, G.csr, G.sw, G.csw, G.mrho, G.mu, G.mv,
                         G.zeta, G.u, G.v, G.w, G.aks, G.qs_u, G.qs_v, G.qs_w, G.qs_aks,
-                        G.salt, G.temp, G.bustr, G.bvstr, G.lon, G.lat, G.wd_rho, G.wd_u, G.wd_v};
+                        G.salt, G.temp, G.bustr, G.bvstr, G.lon, G.lat, G.wd_rho, G.wd_u, G.wd_v,
+                        G.turbaccel, G.turbvort, G.waveaccelu, G.waveaccelv};
         for (void* p : ptrs) if (p) cudaFree(p);
         for (int s = 0; s < RP_SLOTS; s++) {
             if (G.slot_free[s]) cudaEventDestroy(G.slot_free[s]);
@@ -302,7 +312,8 @@ void free_ctx(rp_ctx* c) {
                     c->ftmp, c->qmax, c->sb.keys, c->sb.hist, c->sb.sums, c->sb.perm, c->sb.gbase,
                     c->adj.ck, c->adj.prec, c->adj.seg, c->adj.work, c->adj.lx, c->adj.ly, c->adj.lz,
                     c->adj.kbar, c->adj.tan, c->d_salt, c->d_temp, c->d_mean_salt, c->d_mean_temp,
-                    c->d_hob, c->d_bustr, c->d_bvstr, c->outbuf, c->wd_stage};
+                    c->d_hob, c->d_bustr, c->d_bvstr, c->outbuf, c->wd_stage, c->b_acc, c->b_vort,
+                    c->b_behavew, c->b_ssf};
     for (int g = 0; g < RP_MAXNGRID; g++)
         for (int f = 0; f < 5; f++)
             if (c->adj.fst[g][f]) cudaFree(c->adj.fst[g][f]);
@@ -388,7 +399,8 @@ template <typename S>
 int upload_frame(rp_ctx* ctx, int32_t ng, int32_t slot, const S* zeta, const S* u, const S* v, const S* w,
                  const S* aks, const S* su, const S* sv, const S* salt = nullptr, const S* temp = nullptr,
                  const S* bustr = nullptr, const S* bvstr = nullptr, const double* wd_rho = nullptr,
-                 const double* wd_u = nullptr, const double* wd_v = nullptr) {
+                 const double* wd_u = nullptr, const double* wd_v = nullptr, const S* turbaccel = nullptr,
+                 const S* turbvort = nullptr, const S* waveaccelu = nullptr, const S* waveaccelv = nullptr) {
     if (!ctx) return RP_ERR_ARG;
     if (ng < 1 || ng > ctx->ngrid) return fail(ctx, RP_ERR_ARG, "rp_upload_frame: grid id out of range");
     if (slot < 1 || slot > 3) return fail(ctx, RP_ERR_ARG, "rp_upload_frame: slot must be 1..3");
@@ -397,6 +409,10 @@ int upload_frame(rp_ctx* ctx, int32_t ng, int32_t slot, const S* zeta, const S* 
         return fail(ctx, RP_ERR_ARG, "rp_upload_frame: SaltTempOn needs salt and temp (rp_upload_frame_ext)");
     if ((ctx->diag & RP_DIAG_BOTTOM) && (!bustr || !bvstr))
         return fail(ctx, RP_ERR_ARG, "rp_upload_frame: WriteBottom needs bustr and bvstr (rp_upload_frame_ext)");
+    if (ctx->beh.va && (!turbaccel || !turbvort))
+        return fail(ctx, RP_ERR_ARG, "rp_upload_frame: Process_VA needs turbaccel and turbvort (rp_upload_frame_desc)");
+    if (ctx->beh.wa && (!waveaccelu || !waveaccelv))
+        return fail(ctx, RP_ERR_ARG, "rp_upload_frame: Process_WA needs waveaccelu and waveaccelv (rp_upload_frame_desc)");
     if (ctx->wetdry && (!wd_rho || !wd_u || !wd_v))
         return fail(ctx, RP_ERR_ARG, "rp_upload_frame: WETDRY needs the frame's wetdry masks (rp_upload_frame_desc)");
     const bool stokes = ctx->prm.stokes != 0;
@@ -428,6 +444,14 @@ int upload_frame(rp_ctx* ctx, int32_t ng, int32_t slot, const S* zeta, const S* 
     if (ctx->diag & RP_DIAG_BOTTOM) {
         if ((rc = upload_field<S>(ctx, bustr, nullptr, G.bustr, nx - 1, ny, 1, phys)) != RP_OK) return rc;
         if ((rc = upload_field<S>(ctx, bvstr, nullptr, G.bvstr, nx, ny - 1, 1, phys)) != RP_OK) return rc;
+    }
+    if (ctx->beh.va) {
+        if ((rc = upload_field<S>(ctx, turbaccel, nullptr, G.turbaccel, nx, ny, N + 1, phys)) != RP_OK) return rc;
+        if ((rc = upload_field<S>(ctx, turbvort, nullptr, G.turbvort, nx, ny, N + 1, phys)) != RP_OK) return rc;
+    }
+    if (ctx->beh.wa) {
+        if ((rc = upload_field<S>(ctx, waveaccelu, nullptr, G.waveaccelu, nx, ny, N + 1, phys)) != RP_OK) return rc;
+        if ((rc = upload_field<S>(ctx, waveaccelv, nullptr, G.waveaccelv, nx, ny, N + 1, phys)) != RP_OK) return rc;
     }
     if (ctx->wetdry) {
         if ((rc = upload_mask(ctx, wd_rho, G.wd_rho, (int64_t)nx * ny, phys)) != RP_OK) return rc;
@@ -558,7 +582,9 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
     *out = nullptr;
     const rp_params& p = *params;
     if (ngrid < 1 || ngrid > RP_MAXNGRID || p.numpar < 0 || p.idt <= 0 || p.dt <= 0) return RP_ERR_ARG;
-    if (p.behavior != 0) return RP_ERR_UNSUPPORTED;
+    if (p.behavior != 0 && p.behavior != 1 && p.behavior != 10 && p.behavior != 11) return RP_ERR_UNSUPPORTED;
+    if (p.behavior != 0 && (p.field_dtype == RP_FIELD_MIXED || p.field_dtype == RP_FIELD_MIXED_I16))
+        return RP_ERR_UNSUPPORTED;
     if (p.nsb < 0 || p.nsb > 2) return RP_ERR_ARG;
     if (!(p.deltat >= 1.0) || !(p.sub > 0.0)) return RP_ERR_ARG;
     if (p.field_dtype != RP_FIELD_F64 && p.field_dtype != RP_FIELD_F32 && p.field_dtype != RP_FIELD_MIXED &&
@@ -772,11 +798,15 @@ int rp_upload_frame_desc(rp_ctx* ctx, int32_t ng, int32_t slot, const rp_frame* 
         return upload_frame<float>(ctx, ng, slot, (const float*)f->zeta, (const float*)f->u, (const float*)f->v,
                                    (const float*)f->w, (const float*)f->aks, (const float*)f->su, (const float*)f->sv,
                                    (const float*)f->salt, (const float*)f->temp, (const float*)f->bustr,
-                                   (const float*)f->bvstr, f->wetdry_rho, f->wetdry_u, f->wetdry_v);
+                                   (const float*)f->bvstr, f->wetdry_rho, f->wetdry_u, f->wetdry_v,
+                                   (const float*)f->turbaccel, (const float*)f->turbvort, (const float*)f->waveaccelu,
+                                   (const float*)f->waveaccelv);
     return upload_frame<double>(ctx, ng, slot, (const double*)f->zeta, (const double*)f->u, (const double*)f->v,
                                 (const double*)f->w, (const double*)f->aks, (const double*)f->su, (const double*)f->sv,
                                 (const double*)f->salt, (const double*)f->temp, (const double*)f->bustr,
-                                (const double*)f->bvstr, f->wetdry_rho, f->wetdry_u, f->wetdry_v);
+                                (const double*)f->bvstr, f->wetdry_rho, f->wetdry_u, f->wetdry_v,
+                                (const double*)f->turbaccel, (const double*)f->turbvort, (const double*)f->waveaccelu,
+                                (const double*)f->waveaccelv);
 }
 
 int rp_upload_frame_ext(rp_ctx* ctx, int32_t ng, int32_t slot, const double* zeta, const double* u, const double* v,
@@ -892,6 +922,8 @@ int step_check(rp_ctx* ctx, const double* ex, const double* ix, int32_t t_b, int
     }
     if (ctx->hook && ctx->hook_pos + k >= ctx->hook_steps)
         return fail(ctx, RP_ERR_STATE, "rp_step: noise hook exhausted");
+    if (ctx->prm.behavior != 0 && !ctx->beh_set)
+        return fail(ctx, RP_ERR_STATE, "rp_step: Behavior needs rp_set_behavior first");
     return RP_OK;
 }
 
@@ -1017,6 +1049,8 @@ int rp_step_noalloc(rp_ctx* ctx, const rp_device_state* st, const double ex[3], 
         return fail(ctx, RP_ERR_UNSUPPORTED, "rp_step_noalloc: int(s_w*sub) must be <= 128");
     if (ctx->mixed) return fail(ctx, RP_ERR_UNSUPPORTED, "rp_step_noalloc: not available in the mixed form");
     if (ctx->diag) return fail(ctx, RP_ERR_UNSUPPORTED, "rp_step_noalloc: the diagnostics need the context's state");
+    if (ctx->prm.behavior != 0 || ctx->beh.va || ctx->beh.wa)
+        return fail(ctx, RP_ERR_UNSUPPORTED, "rp_step_noalloc: behave needs the context's state");
     if (!st->x || !st->y || !st->z || !st->age || !st->dob || !st->status || !st->wd || !st->zeta || !st->bath ||
         !st->gid || !st->isin || !st->pid || !st->flags)
         return fail(ctx, RP_ERR_ARG, "rp_step_noalloc: null state column");
@@ -1171,6 +1205,84 @@ int rp_output_record(rp_ctx* ctx, int64_t n, int32_t mI, double* lon, double* la
     return RP_OK;
 }
 
+int rp_set_behavior(rp_ctx* ctx, const rp_behavior* b) {
+    if (!ctx || !b) return RP_ERR_ARG;
+    if (ctx->mixed) return fail(ctx, RP_ERR_UNSUPPORTED, "rp_set_behavior: not available in the mixed form");
+    if (b->behavior != ctx->prm.behavior)
+        return fail(ctx, RP_ERR_ARG, "rp_set_behavior: behavior differs from rp_params.behavior");
+    if (b->va_flag < 0 || b->va_flag > 2) return fail(ctx, RP_ERR_ARG, "rp_set_behavior: va_flag must be 0, 1 or 2");
+    if ((b->process_va || b->process_wa) && !(b->initsize > 0.0))
+        return fail(ctx, RP_ERR_ARG, "rp_set_behavior: initsize must be > 0");
+    for (int k = 0; k < ctx->ngrid; k++)
+        for (int q = 0; q < 3; q++)
+            if (ctx->g[k].map[q] >= 0)
+                return fail(ctx, RP_ERR_STATE, "rp_set_behavior: call before the first frame upload");
+    if (ctx->hook) return fail(ctx, RP_ERR_STATE, "rp_set_behavior: call before rp_set_noise_hook");
+    CK(cudaSetDevice(ctx->device));
+    RpBehaviorDev d{};
+    d.behavior = b->behavior;
+    d.va = b->process_va ? 1 : 0;
+    d.wa = b->process_wa ? 1 : 0;
+    d.va_flag = b->va_flag;
+    d.swimfast = b->swimfast; d.initsize = b->initsize;
+    d.vort_cr = b->vort_cr; d.vort_sat = b->vort_sat; d.b0pv = b->b0pv; d.b1pv = b->b1pv; d.b0wv = b->b0wv;
+    d.b1w = b->b1w; d.acc_cr = b->acc_cr; d.acc_sat = b->acc_sat; d.b0pa = b->b0pa; d.b1pa = b->b1pa;
+    d.b0wa = b->b0wa;
+    const size_t e = (size_t)ctx->elem * RP_SLOTS;
+    for (int k = 0; k < ctx->ngrid; k++) {
+        GridBuf& G = ctx->g[k];
+        const size_t nw = (size_t)G.nx * G.ny * (G.N + 1) * e;
+        void** f[4] = {&G.turbaccel, &G.turbvort, &G.waveaccelu, &G.waveaccelv};
+        const bool need[4] = {d.va != 0, d.va != 0, d.wa != 0, d.wa != 0};
+        for (int q = 0; q < 4; q++) {
+            if (!need[q] || *f[q]) continue;
+            if (dalloc(f[q], nw)) return fail(ctx, RP_ERR_NOMEM, "rp_set_behavior: field ring allocation");
+            CK(cudaMemset(*f[q], 0, nw));
+        }
+    }
+    if ((d.va || d.wa) && !ctx->b_acc) {
+        const size_t cap = (size_t)ctx->cap * 8;
+        if (dalloc(&ctx->b_acc, cap) || dalloc(&ctx->b_vort, cap) || dalloc(&ctx->b_behavew, cap) ||
+            dalloc(&ctx->b_ssf, cap))
+            return fail(ctx, RP_ERR_NOMEM, "rp_set_behavior: output allocation");
+        CK(cudaMemset(ctx->b_acc, 0, cap));
+        CK(cudaMemset(ctx->b_vort, 0, cap));
+        CK(cudaMemset(ctx->b_behavew, 0, cap));
+        CK(cudaMemset(ctx->b_ssf, 0, cap));
+    }
+    ctx->beh = d;
+    ctx->beh_set = true;
+    // HTurb 2, VTurb idt/deltat, then behave's 2 normals and 5 uniforms
+    ctx->ndraw = 2 + ctx->prm.idt / (int)ctx->prm.deltat + ((d.va || d.wa) ? 7 : 0);
+    return RP_OK;
+}
+
+int rp_get_behavior(rp_ctx* ctx, int64_t n, double* acc, double* vort, double* behavew, double* ssf) {
+    if (!ctx) return RP_ERR_ARG;
+    if (n < 0 || n > ctx->n) return fail(ctx, RP_ERR_ARG, "rp_get_behavior: n exceeds particle count");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->s_comp;
+    double* host[4] = {acc, vort, behavew, ssf};
+    double* dev[4] = {ctx->b_acc, ctx->b_vort, ctx->b_behavew, ctx->b_ssf};
+    for (int c = 0; c < 4; c++) {
+        if (!host[c]) continue;
+        if (!dev[c]) {                       // no Process_VA / _WA: behout is 0 (behavior_module.f90:226-233)
+            std::memset(host[c], 0, (size_t)n * 8);
+            continue;
+        }
+        int rc;
+        if (!ctx->permuted) {
+            rc = d2h(ctx, host[c], dev[c], (size_t)n * 8, s);
+        } else {
+            CK(rp::launch_unsort(8, dev[c], ctx->turbv, ctx->pid, ctx->state_base, ctx->n, n, s));
+            ctx->launches++;
+            rc = d2h(ctx, host[c], ctx->turbv, (size_t)n * 8, s);
+        }
+        if (rc != RP_OK) return rc;
+    }
+    return RP_OK;
+}
+
 int rp_reset_diagnostics(rp_ctx* ctx) {
     if (!ctx) return RP_ERR_ARG;
     CK(cudaSetDevice(ctx->device));
@@ -1234,6 +1346,8 @@ int rp_forward(rp_ctx* ctx, int32_t nsteps, const rp_adj_step* steps, double kap
     if (ctx->permuted) return fail(ctx, RP_ERR_STATE, "rp_forward: particle state is re-sorted; set it again");
     if (ctx->hook) return fail(ctx, RP_ERR_STATE, "rp_forward: the noise hook is not used by the adjoint pair");
     if (ctx->wetdry) return fail(ctx, RP_ERR_UNSUPPORTED, "rp_forward: the adjoint model has the static masks only");
+    if (ctx->prm.behavior != 0 || ctx->beh.va || ctx->beh.wa)
+        return fail(ctx, RP_ERR_UNSUPPORTED, "rp_forward: the adjoint model is passive (Behavior 0)");
     for (int s = 0; s < nsteps; s++) {
         const rp_adj_step& st = steps[s];
         const int fr[3] = {st.frame_b, st.frame_c, st.frame_f};

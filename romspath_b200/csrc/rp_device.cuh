@@ -67,6 +67,12 @@ struct RpGridDev {
     const uint8_t* wd_rho;
     const uint8_t* wd_u;
     const uint8_t* wd_v;
+    // behave's fields (Process_VA / _WA): Accelstd_t, Vortstd_t,
+    // Accelustd_w, Accelvstd_w, [j][i][k][slot4] on the N+1 w levels
+    const void* turbaccel;
+    const void* turbvort;
+    const void* waveaccelu;
+    const void* waveaccelv;
     const double* lon;             // lon_rho, lat_rho [j][i] (output only)
     const double* lat;
     double scl[RP_MAXNGRID_D][2];  // GRIDS(ng)%scl(i,1:2)
@@ -114,6 +120,20 @@ struct RpParticlesDev {
     double* hob;
     double* bustr;
     double* bvstr;
+    // behave's outputs par(:,pAcc/pVort/pbehaveW/pSSF) (ROMSPath.f90:800-804)
+    double* acc;
+    double* vort;
+    double* behavew;
+    double* ssf;
+};
+
+// behave's switches and parameters (behavparam, fuchsparam; ROMSPath.h:
+// 150-189; initsize = par(:,pSize), 199)
+struct RpBehaviorDev {
+    int behavior;                  // 0, 1, 10 or 11
+    int va, wa, va_flag;           // Process_VA, Process_WA, va_flag
+    double swimfast, initsize;
+    double vort_cr, vort_sat, b0pv, b1pv, b0wv, b1w, acc_cr, acc_sat, b0pa, b1pa, b0wa;
 };
 
 // RpStepArgs::diag bits (namelist "other", ROMSPath.h:325-330)
@@ -156,6 +176,7 @@ struct RpStepArgs {
     int spline_max_iter;
     int diag;                      // RP_DIAG_*_D bits
     int wetdry;                    // WETDRY: time-varying masks in getInterp3D / getInterpStr
+    RpBehaviorDev beh;
     double vertdist, serr, smth, sub, deltat, aksback;
     double khturb[RP_MAXNGRID_D];
     uint64_t seed, step_index;
@@ -721,5 +742,51 @@ __device__ __forceinline__ double rp_cos2pi(double u) {
         r = RP_SUB(x, RP_MUL(x, p));                                     // x (1 - x^2/3! + ...)
     }
     return sign * r;
+}
+
+// exp: x = k ln2 + r with |r| <= ln2/2 (ln2 split so that k * hi is
+// exact), exp(r) by its Taylor series to r^13/13!, then 2^k in two factors;
+// the oracle's orc_exp runs the same operations.
+#define RP_LN2E_HI 0x1.62e42fee00000p-1    // ln2 truncated to 32 bits
+#define RP_LN2E_LO 0x1.a39ef35793c76p-33   // ln2 - RP_LN2E_HI
+#define RP_INV_LN2 1.4426950408889634
+
+__device__ __forceinline__ double rp_pow2i(int m) {            // 2^m, -1022 <= m <= 1023
+    return __longlong_as_double((long long)((unsigned long long)(m + 1023) << 52));
+}
+
+__device__ __forceinline__ double rp_exp(double x) {
+    if (x != x) return x;
+    if (x > 709.782712893384) return __longlong_as_double(0x7ff0000000000000ll);
+    if (x < -745.1332191019412) return 0.0;
+    const double k = rint(RP_MUL(x, RP_INV_LN2));
+    const double r = RP_SUB(RP_SUB(x, RP_MUL(k, RP_LN2E_HI)), RP_MUL(k, RP_LN2E_LO));
+    double p = 1.0 / 6227020800.0;                              // 1/13!
+    p = RP_ADD(RP_MUL(p, r), 1.0 / 479001600.0);
+    p = RP_ADD(RP_MUL(p, r), 1.0 / 39916800.0);
+    p = RP_ADD(RP_MUL(p, r), 1.0 / 3628800.0);
+    p = RP_ADD(RP_MUL(p, r), 1.0 / 362880.0);
+    p = RP_ADD(RP_MUL(p, r), 1.0 / 40320.0);
+    p = RP_ADD(RP_MUL(p, r), 1.0 / 5040.0);
+    p = RP_ADD(RP_MUL(p, r), 1.0 / 720.0);
+    p = RP_ADD(RP_MUL(p, r), 1.0 / 120.0);
+    p = RP_ADD(RP_MUL(p, r), 1.0 / 24.0);
+    p = RP_ADD(RP_MUL(p, r), 1.0 / 6.0);
+    p = RP_ADD(RP_MUL(p, r), 0.5);
+    p = RP_ADD(RP_MUL(p, r), 1.0);
+    p = RP_ADD(RP_MUL(p, r), 1.0);
+    const int ki = (int)k, k1 = ki / 2, k2 = ki - k1;
+    return RP_MUL(RP_MUL(p, rp_pow2i(k1)), rp_pow2i(k2));
+}
+
+// log of any double: rp_log_pos for positive normals, 2^54 scaling for
+// subnormals, and the special values
+__device__ __forceinline__ double rp_log(double x) {
+    if (x != x || x < 0.0) return __longlong_as_double(0x7ff8000000000000ll);
+    if (x == 0.0) return __longlong_as_double((long long)0xfff0000000000000ull);
+    if (x == __longlong_as_double(0x7ff0000000000000ll)) return x;
+    if (x < 0x1p-1022)
+        return RP_SUB(RP_SUB(rp_log_pos(RP_MUL(x, 0x1p54)), RP_MUL(54.0, RP_LN2_HI)), RP_MUL(54.0, RP_LN2_LO));
+    return rp_log_pos(x);
 }
 

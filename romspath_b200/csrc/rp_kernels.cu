@@ -150,6 +150,12 @@ __global__ void k_locate(const __grid_constant__ RpStepArgs A, const double* ipo
             if (!inz) P.status[n] = 9.0;
         }
     }
+    if (P.acc) {                           // par(:,pAcc/pVort/pbehaveW/pSSF), 343-346
+        P.acc[n] = 0.0;
+        P.vort[n] = 0.0;
+        P.behavew[n] = 0.0;
+        P.ssf[n] = 0.0;
+    }
     if (A.diag & RP_DIAG_BOTTOM_D) {
         P.hob[n] = 9999.0;
         P.bustr[n] = 0.0;
@@ -268,6 +274,12 @@ __global__ void k_state_from_host(RpParticlesDev P, const double* gid_d, const i
     if (P.mean_salt) {
         P.mean_salt[n] = 0.0;
         P.mean_temp[n] = 0.0;
+    }
+    if (P.acc) {                           // par(:,pAcc/pVort/pbehaveW/pSSF), 343-346
+        P.acc[n] = 0.0;
+        P.vort[n] = 0.0;
+        P.behavew[n] = 0.0;
+        P.ssf[n] = 0.0;
     }
 }
 

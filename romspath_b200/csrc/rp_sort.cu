@@ -139,7 +139,8 @@ cudaError_t launch_sort(const RpStepArgs& A, int mixed, const SortBufs& b, void*
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const RpParticlesDev& P = A.p;
     double* d8[] = {P.x, P.y, P.z, P.age, P.dob, P.status, P.wd, P.zeta, P.bath, mixed ? P.qwarm : nullptr,
-                    mixed ? P.gwarm : nullptr, P.salt, P.temp, P.mean_salt, P.mean_temp, P.hob, P.bustr, P.bvstr};
+                    mixed ? P.gwarm : nullptr, P.salt, P.temp, P.mean_salt, P.mean_temp, P.hob, P.bustr, P.bvstr,
+                    P.acc, P.vort, P.behavew, P.ssf};
     for (double* c : d8) {
         if ((e = permute_col(c, scratch8, b.perm, n, s)) != cudaSuccess) return e;
         if (c) *nlaunch += 1;

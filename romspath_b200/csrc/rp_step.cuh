@@ -21,6 +21,25 @@ __device__ __forceinline__ double rp_normal(const RpStepArgs& A, uint32_t pid, u
     return sqrt(-2.0 * rp_log_pos(u1)) * rp_cos2pi(u2);
 }
 
+// Uniform k (0..4) of behave's draws: the hook's entry d0 + 2 + k (d0 =
+// 2 + idt/deltat, after the HTurb and VTurb normals and behave's two), else
+// Philox4x32-10 at counter (pid, step, 0x40000000 + k/4), word k%4.
+__device__ __forceinline__ double rp_uniform(const RpStepArgs& A, uint32_t pid, uint32_t d0, uint32_t k) {
+    if (A.hook) return A.hook[(int64_t)(pid - A.pid_base) * A.ndraw + d0 + 2 + k];
+    uint32_t c[4] = {pid, (uint32_t)A.step_index, (uint32_t)(A.step_index >> 32), 0x40000000u + (k >> 2)};
+    rp_philox(c, (uint32_t)A.seed, (uint32_t)(A.seed >> 32));
+    return ((double)c[k & 3u] + 0.5) / 4294967296.0;
+}
+
+// laplace (pdf_module.f90:42-55) of one uniform: sign(dev2, dev1) with
+// dev1 = u - 0.5, dev2 = -log(1 - 2|dev1|) / sqrt(2)
+__device__ __forceinline__ double rp_laplace_of(double u) {
+    const double dev1 = RP_SUB(u, 0.5);
+    const double dev2 = RP_MUL(-1.0, rp_log(RP_SUB(1.0, RP_MUL(2.0, fabs(dev1))))) / sqrt(2.0);
+    const double mag = fabs(dev2);
+    return (dev1 >= 0.0) ? mag : -mag;
+}
+
 // ------------------------------------------------------- find_currents
 
 struct StageState {
@@ -556,6 +575,100 @@ __device__ __noinline__ void rp_diag_one(const RpStepArgs& A, int64_t n, double 
     }
 }
 
+// getInterp3D of a behave field, ztype 2 (the w levels) at one slot
+template <typename T>
+__device__ __forceinline__ double rp_wfield_at(const RpStepArgs& A, const RpGridDev& g, const void* f,
+                                               const RhoCell& c, double zeta, double depth, double zpar, int slot,
+                                               uint32_t& fl) {
+    LevelPick L;
+    rp_walk_w(g, zeta, depth, zpar, L, fl);
+    if (A.wetdry) {
+        double cff[4];
+        rp_rho_wd_weights(g, c, slot, cff, fl);
+        return rp_col_rho<T>(f, c, cff, g.N + 1, L, slot);
+    }
+    return rp_col_rho<T>(f, c, c.wet4 ? c.cb : c.ci, g.N + 1, L, slot);
+}
+
+// behave (behavior_module.f90:186-393) at the step's (Xpar, Ypar, Zpar) in
+// the particle's grid: with Process_VA / Process_WA the standard deviations
+// of turbulent acceleration and vorticity and of wave acceleration at the
+// particle (240-280), 4 laplace, 2 normal and 1 uniform draws (285-311,
+// 366), the Fuchs swim / sink response (322-375) into par(:,pAcc/pVort/
+// pbehaveW/pSSF); returns ZBehav (381-391).  Real powers are pinned as
+// x**2.0D0 = x*x, r**3.0D0 = (r*r)*r, x**0.5D0 = sqrt(x); exp and log are
+// this file's own.  Out of line: the passive step keeps its registers.
+template <typename T>
+__device__ __noinline__ double rp_behave(const RpStepArgs& A, int64_t n, const RpGridDev& g, double Xpar,
+                                         double Ypar, double Zpar, uint32_t pid, uint32_t& fl) {
+    const RpBehaviorDev& b = A.beh;
+    const double G = 980.0, RHOF = 1.026, MU = 0.010260, RHOP = 1.06;   // ROMSPath.h:15-19
+    double wb = 0.0;
+    if (b.va || b.wa) {
+        RhoCell c;
+        rp_rho_cell(g, Xpar, Ypar, c, fl);
+        const double depth = -1.0 * rp_bil(g.h, c);
+        const double zt[3] = {rp_zeta_at<T>(g, c, g.sb), rp_zeta_at<T>(g, c, g.sc), rp_zeta_at<T>(g, c, g.sf)};
+        const int sl[3] = {g.sb, g.sc, g.sf};
+        double ey[3], stdaccturbu = 0.0, stdvortturb = 0.0, stdaccwaveu = 0.0, stdaccwavev = 0.0;
+        if (b.va) {
+            for (int q = 0; q < 3; q++) ey[q] = rp_wfield_at<T>(A, g, g.turbaccel, c, zt[q], depth, Zpar, sl[q], fl);
+            stdaccturbu = rp_polintd(A.pi, ey[0], ey[1], ey[2]);
+            for (int q = 0; q < 3; q++) ey[q] = rp_wfield_at<T>(A, g, g.turbvort, c, zt[q], depth, Zpar, sl[q], fl);
+            stdvortturb = rp_polintd(A.pi, ey[0], ey[1], ey[2]);
+            stdaccturbu = RP_MUL(stdaccturbu, 100.0);
+        }
+        if (b.wa) {
+            for (int q = 0; q < 3; q++) ey[q] = rp_wfield_at<T>(A, g, g.waveaccelu, c, zt[q], depth, Zpar, sl[q], fl);
+            stdaccwaveu = rp_polintd(A.pi, ey[0], ey[1], ey[2]);
+            for (int q = 0; q < 3; q++) ey[q] = rp_wfield_at<T>(A, g, g.waveaccelv, c, zt[q], depth, Zpar, sl[q], fl);
+            stdaccwavev = rp_polintd(A.pi, ey[0], ey[1], ey[2]);
+            stdaccwaveu = RP_MUL(stdaccwaveu, 100.0);
+            stdaccwavev = RP_MUL(stdaccwavev, 100.0);
+        }
+        const uint32_t d0 = 2u + (uint32_t)A.loop;
+        const double vortturbu = RP_MUL(stdvortturb, rp_laplace_of(rp_uniform(A, pid, d0, 0)));
+        const double vortturbv = RP_MUL(stdvortturb, rp_laplace_of(rp_uniform(A, pid, d0, 1)));
+        const double vorttot = sqrt(RP_ADD(RP_MUL(vortturbu, vortturbu), RP_MUL(vortturbv, vortturbv)));
+        const double accturbu = RP_MUL(stdaccturbu, rp_laplace_of(rp_uniform(A, pid, d0, 2)));
+        const double accturbv = RP_MUL(stdaccturbu, rp_laplace_of(rp_uniform(A, pid, d0, 3)));
+        const double accwaveu = RP_MUL(stdaccwaveu, rp_normal(A, pid, d0));
+        const double accwavev = RP_MUL(stdaccwavev, rp_normal(A, pid, d0 + 1));
+        const double au = RP_ADD(accturbu, accwaveu), av = RP_ADD(accturbv, accwavev);
+        const double acctot = sqrt(RP_ADD(RP_MUL(au, au), RP_MUL(av, av)));
+        const double c1v = 2.0 / rp_log(b.vort_cr / b.vort_sat);
+        const double c2v = RP_MUL(c1v, rp_log(vorttot / sqrt(RP_MUL(b.vort_cr, b.vort_sat))));
+        const double c1a = 2.0 / rp_log(b.acc_cr / b.acc_sat);
+        const double c2a = RP_MUL(c1a, rp_log(acctot / sqrt(RP_MUL(b.acc_cr, b.acc_sat))));
+        const double ev = rp_exp(RP_MUL(-2.0, c2v)), ea = rp_exp(RP_MUL(-2.0, c2a));
+        const double pswimv = RP_ADD(RP_SUB(b.b1pv, b.b0pv) / RP_ADD(1.0, ev), b.b0pv);
+        const double pswima = RP_ADD(RP_SUB(b.b1pa, b.b0pa) / RP_ADD(1.0, ea), b.b0pa);
+        const double pswim = (b.va_flag == 1) ? pswimv : (b.va_flag == 2) ? pswima : ((pswima < pswimv) ? pswima : pswimv);
+        const double wswimv = RP_ADD(RP_MUL(RP_SUB(b.b1w, b.b0wv), 1.0) / RP_ADD(1.0, ev), b.b0wv);
+        const double wswima = RP_ADD(RP_MUL(RP_SUB(b.b1w, b.b0wa), 1.0) / RP_ADD(1.0, ea), b.b0wa);
+        const double wswim = (b.va_flag == 1) ? wswimv : (b.va_flag == 2) ? wswima : RP_ADD(wswima, wswimv);
+        const double r = b.initsize / 2.0e4;
+        const double t1 = RP_MUL(RP_MUL(RP_MUL(RP_MUL(4.0 / 3.0, G), RP_MUL(RP_MUL(r, r), r)), RHOF), RHOP - RHOF);
+        const double wsink = RP_SUB(RP_MUL(3.0, MU), sqrt(RP_ADD(t1, RP_MUL(9.0, RP_MUL(MU, MU))))) / RP_MUL(r, RHOF);
+        double ssf;
+        if (rp_uniform(A, pid, d0, 4) < pswim) {
+            wb = wswim;
+            ssf = 0.0;
+        } else {
+            wb = wsink;
+            ssf = 1.0;
+        }
+        const RpParticlesDev& P = A.p;
+        P.acc[n] = acctot / 100.0;
+        P.vort[n] = vorttot;
+        P.behavew[n] = wb;
+        P.ssf[n] = ssf;
+    }
+    if (b.behavior == 1) return RP_MUL(b.swimfast, (double)A.idt);
+    if (b.behavior == 10) return RP_MUL(wb, (double)A.idt) / 100.0;
+    return 0.0;
+}
+
 // One particle of update_particles.  With turbv_in non-null the VTurb
 // displacement comes from the split kernel instead of being computed here.
 template <typename T, class W>
@@ -643,7 +756,8 @@ __device__ void rp_update_one(const RpStepArgs& A, int64_t n, const W& w, const 
         }
         TurbV = rp_vturb<T>(A, g, S1, Zpar, pid, fl, w);
     }
-    const double ZBehav = 0.0;                             // behave(): passive
+    double ZBehav = 0.0;                                   // behave(), 800-804
+    if (A.beh.behavior || A.beh.va || A.beh.wa) ZBehav = rp_behave<T>(A, n, g, Xpar, Ypar, Zpar, pid, fl);
 
     // new position and nest hand-off (821-836)
     const double newXpos = P.x[n] + AdvectX + TurbHx;

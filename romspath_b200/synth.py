@@ -54,6 +54,7 @@ class GridSpec:
     gyre_ly: Optional[float] = None
     diag: bool = False            # frames also carry salt, temp, bustr, bvstr
     wetdry: bool = False          # frames also carry wet/dry masks (an intertidal flat)
+    behave: bool = False          # frames also carry behave's acceleration / vorticity fields
 
     @property
     def xi_u(self) -> int:
@@ -225,6 +226,16 @@ def make_frame(spec: GridSpec, grid: Dict[str, np.ndarray], t: float) -> Dict[st
         ub, vb = u[:, :, 0], v[:, :, 0]
         out["bustr"] = cd * ub * np.abs(ub)
         out["bvstr"] = cd * vb * np.abs(vb)
+    if spec.behave:
+        # standard deviations of turbulent acceleration (m/s^2) and vorticity
+        # (1/s) decaying from the surface, and of wave acceleration (m/s^2)
+        # decaying faster, tidally modulated; on the w levels
+        tw = np.cos(phase_r)[..., None]
+        mk = mask[..., None]
+        out["turbaccel"] = 0.05 * (1.0 + 0.5 * tw) * np.exp(z_w / 20.0) * mk
+        out["turbvort"] = 2.0 * (1.0 + 0.3 * tw) * np.exp(z_w / 15.0) * mk
+        out["waveaccelu"] = 0.08 * (1.0 + 0.4 * tw) * np.exp(z_w / 5.0) * mk
+        out["waveaccelv"] = 0.05 * (1.0 - 0.4 * tw) * np.exp(z_w / 5.0) * mk
     if spec.wetdry:
         # an intertidal flat: wet points of a coastal band go dry while the
         # tidal phase there is low; u/v masks from their rho neighbours, as
@@ -274,7 +285,8 @@ def stored_frame(frame: Dict[str, np.ndarray], field_dtype: str, stokes: bool) -
         f["u"] = f["u"] + f["su"]
         f["v"] = f["v"] + f["sv"]
     out = {}
-    for k in ("zeta", "u", "v", "w", "aks", "salt", "temp", "bustr", "bvstr", "wetdry_rho", "wetdry_u", "wetdry_v"):
+    for k in ("zeta", "u", "v", "w", "aks", "salt", "temp", "bustr", "bvstr", "wetdry_rho", "wetdry_u", "wetdry_v",
+              "turbaccel", "turbvort", "waveaccelu", "waveaccelv"):
         if k not in f:
             continue
         a = f[k]
@@ -502,6 +514,13 @@ def config_spec(name: str) -> List[GridSpec]:
         P.gyre_lx, P.gyre_ly = lx, ly
         return [B, A, P]
     raise KeyError(name)
+
+
+# The reference's sample behaviour settings (ROMSPath.data:56-57, 90-105,
+# 123-141, 154): Process_VA/WA on, the fuchsparam values, initsize 250.
+FUCHS_SAMPLE = {"process_va": 1, "process_wa": 1, "va_flag": 1, "initsize": 250.0, "swimfast": 0.0005,
+                "vort_cr": 1.0, "vort_sat": 10.0, "b0pv": 0.5, "b1pv": 1.0, "b0wv": 0.0, "b1w": 0.0,
+                "acc_cr": 10.0, "acc_sat": 1000.0, "b0pa": 0.5, "b1pa": 1.0, "b0wa": 0.2}
 
 
 def config_params(name: str) -> dict:

@@ -50,7 +50,10 @@ class Tracker:
         P.vturb_on = int(params["vturb_on"])
         P.hturb_on = int(params["hturb_on"])
         P.open_ocean_boundary = int(params["open_ocean_boundary"])
-        P.behavior = 0
+        # behave: Behavior (0, 1, 10, 11), Process_VA / Process_WA
+        P.behavior = int(params.get("behavior", 0))
+        self.va = bool(params.get("process_va", 0))
+        self.wa = bool(params.get("process_wa", 0))
         P.stokes = int(bool(stokes))
         # "f64" / "f32": fields stored at that width, FP64 arithmetic (exact);
         # "mixed": FP16 fields with per-level scales, FP32 positions with
@@ -115,6 +118,17 @@ class Tracker:
         for ng, lon, lat in self._lonlat:
             self._check(L.rp_set_grid_lonlat(h, ng, _pd(lon), _pd(lat)), "rp_set_grid_lonlat")
         self._lonlat = []
+        if P.behavior or self.va or self.wa:
+            b = _lib.RpBehavior()
+            b.behavior = P.behavior
+            b.process_va, b.process_wa = int(self.va), int(self.wa)
+            b.va_flag = int(params.get("va_flag", 0))
+            b.swimfast = float(params.get("swimfast", 0.0))
+            b.initsize = float(params.get("initsize", 0.0))
+            for k in _lib.FUCHS:
+                setattr(b, k, float(params.get(k, 0.0)))
+            self._check(L.rp_set_behavior(h, C.byref(b)), "rp_set_behavior")
+            self.ndraw += 7 if (self.va or self.wa) else 0
 
     # ------------------------------------------------------------ basics
     def _check(self, rc: int, what: str):
@@ -146,7 +160,7 @@ class Tracker:
         if not self.params.stokes:
             su = sv = None
         p = _pf if f32 else _pd
-        if self.wetdry:
+        if self.wetdry or self.va or self.wa:
             # every field through the frame descriptor
             d = _lib.RpFrame()
             d.f32 = int(f32)
@@ -159,14 +173,20 @@ class Tracker:
             st = self.diag & _lib.DIAG_SALTTEMP
             bt = self.diag & _lib.DIAG_BOTTOM
             for k, on in (("salt", st), ("temp", st), ("bustr", bt), ("bvstr", bt)):
-                if on:
+                if on and k in frame:
                     a = conv(frame[k])
                     keep.append(a)
                     setattr(d, k, a.ctypes.data)
-            for k in ("wetdry_rho", "wetdry_u", "wetdry_v"):
+            for k in ("wetdry_rho", "wetdry_u", "wetdry_v") if self.wetdry else ():
                 a = np.asfortranarray(frame[k], dtype=np.float64)
                 keep.append(a)
                 setattr(d, k, _pd(a))
+            for k, on in (("turbaccel", self.va), ("turbvort", self.va), ("waveaccelu", self.wa),
+                          ("waveaccelv", self.wa)):
+                if on and k in frame:
+                    a = conv(frame[k])
+                    keep.append(a)
+                    setattr(d, k, a.ctypes.data)
             rc = self.L.rp_upload_frame_desc(self.h, ng, slot, C.byref(d))
         elif self.diag:
             # salt/temp and bustr/bvstr of the diagnostics that are on
@@ -233,6 +253,14 @@ class Tracker:
         order = ("salt", "temp", "mean_salt", "mean_temp", "hob", "bustr", "bvstr")
         rc = self.L.rp_get_diagnostics(self.h, n, *[_pd(out.get(k)) for k in order])
         self._check(rc, "rp_get_diagnostics")
+        return out
+
+    def get_behavior(self, n: Optional[int] = None) -> Dict[str, np.ndarray]:
+        """par(:,pAcc/pVort/pbehaveW/pSSF) of behave."""
+        n = self.n if n is None else n
+        out = {k: np.empty(n) for k in ("acc", "vort", "behavew", "ssf")}
+        rc = self.L.rp_get_behavior(self.h, n, *[_pd(out[k]) for k in ("acc", "vort", "behavew", "ssf")])
+        self._check(rc, "rp_get_behavior")
         return out
 
     RECORD = ("lon", "lat", "zp", "age", "status", "gid", "salt", "temp", "hob", "bustr", "bvstr")

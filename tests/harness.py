@@ -22,6 +22,8 @@ FIELDS = ("x", "y", "z", "age", "status", "gid", "isin", "wd", "zeta", "bath", "
 DIAG_GPU_TO_ORACLE = {"salt": "p_salt", "temp": "p_temp", "mean_salt": "mean_salt", "mean_temp": "mean_temp",
                       "hob": "p_hob", "bustr": "p_bustr", "bvstr": "p_bvstr"}
 DIAG_PARAMS = {"salttemp_on": 1, "salttemp_mean": 1, "write_bottom": 1}
+# behave's outputs: Tracker.get_behavior names -> oracle state names
+BEHAVE_GPU_TO_ORACLE = {"acc": "p_acc", "vort": "p_vort", "behavew": "p_behavew", "ssf": "p_ssf"}
 
 
 @dataclasses.dataclass
@@ -78,9 +80,15 @@ def make_case(name: str, npart: int, seed: int = 0, spec_over: Optional[dict] = 
 
 
 def noise_array(case: Case, nsteps: int, seed: int = 123) -> np.ndarray:
+    """Hook draws [step][particle][draw]: normals, and with Process_VA/_WA
+    behave's 2 normals then 5 uniforms in (0, 1) last."""
     ndraw = 2 + int(case.params["idt"]) // int(case.params["deltat"])
+    beh = bool(case.params.get("process_va") or case.params.get("process_wa"))
     rng = np.random.default_rng(seed)
-    return rng.standard_normal((nsteps, case.release.z.shape[0], ndraw))
+    a = rng.standard_normal((nsteps, case.release.z.shape[0], ndraw + (7 if beh else 0)))
+    if beh:
+        a[..., ndraw + 2:] = (rng.integers(0, 2**32, a[..., ndraw + 2:].shape) + 0.5) / 2.0**32
+    return a
 
 
 def _steps(case: Case, nsteps: int):
@@ -121,6 +129,8 @@ def run_gpu(case: Case, nsteps: int, noise: str = "philox", seed: int = 7,
     st = T.get_particles()
     if T.diag:
         st.update({DIAG_GPU_TO_ORACLE[k]: v for k, v in T.get_diagnostics().items()})
+    if T.va or T.wa:
+        st.update({BEHAVE_GPU_TO_ORACLE[k]: v for k, v in T.get_behavior().items()})
     return st, T
 
 

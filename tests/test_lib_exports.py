@@ -62,7 +62,7 @@ def test_null_and_range_arguments_rejected():
     G = (_lib.RpGrid * 1)()
     assert L.rp_create(C.byref(P), 0, G, C.byref(h)) == -1
     assert L.rp_create(C.byref(P), 6, G, C.byref(h)) == -1
-    P.behavior = 1
+    P.behavior = 4          # the oyster-larva behaviours are outside the implemented path
     assert L.rp_create(C.byref(P), 1, G, C.byref(h)) == -5
     assert L.rp_step(None, None, None, 1, 1, 2, 3) == -1
     assert L.rp_destroy(None) == -1
