@@ -199,6 +199,33 @@ int rp_set_particles(rp_ctx *ctx, int64_t n, const double *x, const double *y, c
 int rp_locate_particles(rp_ctx *ctx, int64_t n, const double *ipos, const double *jpos,
                         const double *z, const double *dob, int32_t t_b);
 
+/* GRIDS(ng)%angle (xi_rho,eta_rho; radians, may be NULL for a Cartesian
+ * grid) and GRIDS(ng)%spherical (0 or 1) for rp_locate_lonlat
+ * (grid_module.f90:225-300). */
+int rp_set_grid_angle(rp_ctx *ctx, int32_t ng, const double *angle, int32_t spherical);
+
+/* rp_locate_particles from the particles' lon/lat (the parfile columns,
+ * ROMSPath.f90:319-356): LL2ij (interpolation_module.f90:110-268: a
+ * bisection of each grid with the point-in-polygon test inbox, then the
+ * Cartesian or spherical fractional index, GRIDS(1)%spherical deciding for
+ * every grid) of every particle in every grid on the device, then the
+ * ownership loop.  rp_set_grid_lonlat and rp_set_grid_angle first.
+ * ipos_out/jpos_out (may be NULL) receive the (n, Ngrid) Fortran-order
+ * indices LL2ij gave. */
+int rp_locate_lonlat(rp_ctx *ctx, int64_t n, const double *lon, const double *lat, const double *z,
+                     const double *dob, int32_t t_b, double *ipos_out, double *jpos_out);
+
+/* InitGrid's nest maps (grid_module.f90:437-481), host only: grefine(a,b) =
+ * refine(|a-b|)^|a-b|, and for every grid pair the first coincident lon/lat
+ * rho point in the reference's search order (found by hashing, O(points)
+ * instead of the reference's O(points^2)); scl and off receive, per grid
+ * ng, GRIDS(ng)%scl(Ngrid,2) and off(Ngrid,2) in Fortran order at
+ * scl + ng*2*Ngrid -- what rp_grid.scl/off take.  Without a coincident
+ * point the indices are those past the search loops' ends, as in the
+ * reference. */
+int rp_nest_maps(int32_t ngrid, const int32_t *xi_rho, const int32_t *eta_rho, const double *const *lon_rho,
+                 const double *const *lat_rho, const double *refine, double *scl, double *off);
+
 /* One internal step over all particles: update_particles
  * (ROMSPath.f90:608-1008) with ex(3), ix(3), ets and the ring slots
  * t_b/t_c/t_f from run_External_Timestep / run_Internal_Timestep

@@ -62,6 +62,7 @@ class OrcGrid(C.Structure):
         ("lon_rho", PD), ("lat_rho", PD),
         ("wd_rho", PD * 3), ("wd_u", PD * 3), ("wd_v", PD * 3),
         ("turbaccel", PD * 3), ("turbvort", PD * 3), ("waveaccelu", PD * 3), ("waveaccelv", PD * 3),
+        ("angle", PD),
     ]
 
 
@@ -156,6 +157,14 @@ def _declare(L):
     L.orc_log.restype = C.c_double
     L.orc_philox_uniform.argtypes = [C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint32]
     L.orc_philox_uniform.restype = C.c_double
+    L.orc_sincos.argtypes = [C.c_double, PD, PD]
+    L.orc_sincos.restype = None
+    L.orc_asin.argtypes = [C.c_double]
+    L.orc_asin.restype = C.c_double
+    L.orc_ll2ij.argtypes = [C.POINTER(OrcGrid), C.c_int, PD, PD, C.c_int64, PD, PD]
+    L.orc_ll2ij.restype = None
+    L.orc_nest_maps.argtypes = [C.c_int, C.POINTER(OrcGrid), PD, PD, PD]
+    L.orc_nest_maps.restype = None
 
 
 def _pd(a: np.ndarray):
@@ -204,6 +213,12 @@ def ppvalu(brk, coef_k_by_l, x, jderiv):
     coef = np.asfortranarray(coef_k_by_l, dtype=np.float64)
     k, l = coef.shape
     return lib().orc_ppvalu(_pd(brk), _pd(coef.ravel(order="F")), l, k, float(x), jderiv)
+
+
+def sincos(x):
+    s, c = C.c_double(), C.c_double()
+    lib().orc_sincos(float(x), C.byref(s), C.byref(c))
+    return s.value, c.value
 
 
 def inside(xb, yb, xo, yo) -> bool:
@@ -276,7 +291,7 @@ class OracleModel:
                 a = _i32(gr[name])
                 self._keep.append(a)
                 setattr(G, name, a.ctypes.data_as(PI32))
-            for name in ("lon_rho", "lat_rho"):
+            for name in ("lon_rho", "lat_rho", "angle"):
                 if name in gr:
                     a = _f64(gr[name])
                     self._keep.append(a)
@@ -407,6 +422,40 @@ class OracleModel:
         a, b = C.c_int64(), C.c_int64()
         lib().orc_last_stats(C.byref(a), C.byref(b))
         return a.value, b.value
+
+    def ll2ij(self, ng: int, lon, lat, spherical: int):
+        """LL2ij of grid ng (interpolation_module.f90:110-231)."""
+        lon = np.ascontiguousarray(lon, dtype=np.float64)
+        lat = np.ascontiguousarray(lat, dtype=np.float64)
+        ip, jp = np.empty(len(lon)), np.empty(len(lon))
+        lib().orc_ll2ij(C.byref(self.g[ng - 1]), int(spherical), _pd(lon), _pd(lat), len(lon), _pd(ip), _pd(jp))
+        return ip, jp
+
+    def locate_lonlat(self, lon, lat, z, dob, spherical: int, tb: int = 1, pid=None):
+        """ini_ROMSPath from particle lon/lat: LL2ij for every grid, then the
+        ownership loop (ROMSPath.f90:359-432)."""
+        n = len(lon)
+        ip = np.empty((self.ng, n))
+        jp = np.empty((self.ng, n))
+        for ng in range(1, self.ng + 1):
+            ip[ng - 1], jp[ng - 1] = self.ll2ij(ng, lon, lat, spherical)
+
+        class _R:
+            pass
+        r = _R()
+        r.ipos, r.jpos, r.z, r.dob = ip, jp, np.asarray(z, dtype=np.float64), np.asarray(dob, dtype=np.float64)
+        self.init_particles(r, tb=tb, pid=pid)
+        return ip, jp
+
+    def nest_maps(self, refine):
+        """scl, off of every grid (InitGrid's search, grid_module.f90:441-481):
+        arrays [ng][Ngrid][2] as GRIDS(ng)%scl(i, c)."""
+        ref = np.ascontiguousarray(list(refine) + [1.0] * MAXNGRID, dtype=np.float64)
+        scl = np.empty(self.ng * 2 * self.ng)
+        off = np.empty(self.ng * 2 * self.ng)
+        lib().orc_nest_maps(self.ng, self.g, _pd(ref), _pd(scl), _pd(off))
+        return (scl.reshape(self.ng, 2, self.ng).transpose(0, 2, 1).copy(),
+                off.reshape(self.ng, 2, self.ng).transpose(0, 2, 1).copy())
 
     def output_record(self, mI: int) -> Dict[str, np.ndarray]:
         """One output record of dataOutput / writeNetCDF (ROMSPath.f90:1012-1024,

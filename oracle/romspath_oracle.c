@@ -1535,3 +1535,248 @@ void orc_output_lonlat(const orc_grid *grids, const orc_particles *p, double *lo
         lat[n] = orc_getinterp2d(g, ORC_V_LAT, p->x[n], p->y[n], 1, &fl);
     }
 }
+
+/* ======================= init lookup (LL2ij) ======================= */
+
+#define ORC_PIO2_1 0x1.921fb54400000p+0     /* pi/2 in three parts; k * part */
+#define ORC_PIO2_2 0x1.0b4611a600000p-34    /* is exact for |k| < 2^19      */
+#define ORC_PIO2_3 0x1.3198a2e037073p-69
+#define ORC_PIO2_HI 0x1.921fb54442d18p+0    /* pi/2 = HI + LO                */
+#define ORC_PIO2_LO 0x1.1a62633145c07p-54
+#define ORC_2_OVER_PI 0.6366197723675814
+
+void orc_sincos(double x, double *s, double *c)
+{
+    const double k = rint(x * ORC_2_OVER_PI);
+    const double r = ((x - k * ORC_PIO2_1) - k * ORC_PIO2_2) - k * ORC_PIO2_3;
+    const double r2 = r * r;
+    double p = -1.0 / 121645100408832000.0;        /* -1/19! */
+    p = p * r2 + 1.0 / 355687428096000.0;           /*  1/17! */
+    p = p * r2 - 1.0 / 1307674368000.0;
+    p = p * r2 + 1.0 / 6227020800.0;
+    p = p * r2 - 1.0 / 39916800.0;
+    p = p * r2 + 1.0 / 362880.0;
+    p = p * r2 - 1.0 / 5040.0;
+    p = p * r2 + 1.0 / 120.0;
+    p = p * r2 - 1.0 / 6.0;
+    const double sr = r + (r * r2) * p;
+    double q = 1.0 / 2432902008176640000.0;        /*  1/20! */
+    q = q * r2 - 1.0 / 6402373705728000.0;
+    q = q * r2 + 1.0 / 20922789888000.0;
+    q = q * r2 - 1.0 / 87178291200.0;
+    q = q * r2 + 1.0 / 479001600.0;
+    q = q * r2 - 1.0 / 3628800.0;
+    q = q * r2 + 1.0 / 40320.0;
+    q = q * r2 - 1.0 / 720.0;
+    q = q * r2 + 1.0 / 24.0;
+    q = q * r2 - 0.5;
+    const double cr = 1.0 + r2 * q;
+    switch (((int)k) & 3) {
+    case 0: *s = sr; *c = cr; break;
+    case 1: *s = cr; *c = -sr; break;
+    case 2: *s = -sr; *c = -cr; break;
+    default: *s = -cr; *c = sr; break;
+    }
+}
+
+/* asin t for 0 <= t <= 0.5 by its series sum c_n t^(2n+1), n <= 25 */
+static double asin_series(double t)
+{
+    const double z = t * t;
+    double p = 5267108601573.0 / 2392537302040576.0;
+    p = p * z + 8061900920775.0 / 3448068464705536.0;
+    p = p * z + 514589420475.0 / 206708186021888.0;
+    p = p * z + 17534158031.0 / 6597069766656.0;
+    p = p * z + 67282234305.0 / 23639499997184.0;
+    p = p * z + 34461632205.0 / 11269994184704.0;
+    p = p * z + 1472719325.0 / 446676598784.0;
+    p = p * z + 2268783825.0 / 635655159808.0;
+    p = p * z + 116680311.0 / 30064771072.0;
+    p = p * z + 100180065.0 / 23622320128.0;
+    p = p * z + 9694845.0 / 2080374784.0;
+    p = p * z + 5014575.0 / 973078528.0;
+    p = p * z + 1300075.0 / 226492416.0;
+    p = p * z + 676039.0 / 104857600.0;
+    p = p * z + 88179.0 / 12058624.0;
+    p = p * z + 46189.0 / 5505024.0;
+    p = p * z + 12155.0 / 1245184.0;
+    p = p * z + 6435.0 / 557056.0;
+    p = p * z + 143.0 / 10240.0;
+    p = p * z + 231.0 / 13312.0;
+    p = p * z + 63.0 / 2816.0;
+    p = p * z + 35.0 / 1152.0;
+    p = p * z + 5.0 / 112.0;
+    p = p * z + 3.0 / 40.0;
+    p = p * z + 1.0 / 6.0;
+    return t + t * (z * p);
+}
+
+double orc_asin(double x)
+{
+    const double a = fabs(x);
+    if (!(a <= 1.0)) return NAN;
+    double r;
+    if (a <= 0.5) {
+        r = asin_series(a);
+    } else {                                          /* asin a = pi/2 - 2 asin sqrt((1-a)/2) */
+        const double t = sqrt((1.0 - a) * 0.5);
+        r = (ORC_PIO2_HI - 2.0 * asin_series(t)) + ORC_PIO2_LO;
+    }
+    return (x < 0.0) ? -r : r;
+}
+
+/* inbox, interpolation_module.f90:232-268: the box's boundary polygon,
+ * then inside() */
+static int inbox(const orc_grid *g, int Li, int Ui, int Lj, int Uj, double inlon, double inlat, double *lonb,
+                 double *latb)
+{
+    const int nx = g->xi_rho;
+    const int Nb = 2 * (Uj - Lj + Ui - Li);
+    int shft = 1 - Li;
+    for (int i = Li; i <= Ui - 1; i++) {
+        lonb[i + shft - 1] = g->lon_rho[IX2(i, Lj, nx)];
+        latb[i + shft - 1] = g->lat_rho[IX2(i, Lj, nx)];
+    }
+    shft = 1 - Lj + Ui - Li;
+    for (int j = Lj; j <= Uj - 1; j++) {
+        lonb[j + shft - 1] = g->lon_rho[IX2(Ui, j, nx)];
+        latb[j + shft - 1] = g->lat_rho[IX2(Ui, j, nx)];
+    }
+    shft = 1 + Uj - Lj + 2 * Ui - Li;
+    for (int i = Ui; i >= Li + 1; i--) {
+        lonb[shft - i - 1] = g->lon_rho[IX2(i, Uj, nx)];
+        latb[shft - i - 1] = g->lat_rho[IX2(i, Uj, nx)];
+    }
+    shft = 1 + 2 * Uj - Lj + 2 * (Ui - Li);
+    for (int j = Uj; j >= Lj + 1; j--) {
+        lonb[shft - j - 1] = g->lon_rho[IX2(Li, j, nx)];
+        latb[shft - j - 1] = g->lat_rho[IX2(Li, j, nx)];
+    }
+    return orc_inside(Nb, lonb, latb, inlon, inlat);
+}
+
+void orc_ll2ij(const orc_grid *g, int spherical, const double *inlon, const double *inlat, int64_t n,
+               double *ipar, double *jpar)
+{
+    const int nx = g->xi_rho, ny = g->eta_rho;
+    const double Eradius = 6371315.0, deg2rad = 3.14159265358979323846 / 180.0;   /* ROMSPath.h:11-13 */
+    const size_t nbmax = 2 * (size_t)(nx + ny) + 2;
+    double *lonb = (double *)malloc(nbmax * sizeof(double));
+    double *latb = (double *)malloc(nbmax * sizeof(double));
+    for (int64_t k = 0; k < n; k++) {
+        const double lo = inlon[k], la = inlat[k];
+        int Imin = 1, Imax = nx, Jmin = 1, Jmax = ny;
+        int found = inbox(g, Imin, Imax, Jmin, Jmax, lo, la, lonb, latb);
+        if (found) {                                             /* 138-159 */
+            while (((Imax - Imin) > 1) || ((Jmax - Jmin) > 1)) {
+                if ((Imax - Imin) > 1) {
+                    const int i0 = (Imin + Imax) / 2;
+                    if (inbox(g, Imin, i0, Jmin, Jmax, lo, la, lonb, latb)) Imax = i0;
+                    else Imin = i0;
+                }
+                if ((Jmax - Jmin) > 1) {
+                    const int j0 = (Jmin + Jmax) / 2;
+                    if (inbox(g, Imin, Imax, Jmin, j0, lo, la, lonb, latb)) Jmax = j0;
+                    else Jmin = j0;
+                }
+            }
+        }
+        found = inbox(g, Imin, Imax, Jmin, Jmax, lo, la, lonb, latb);   /* 166-168 */
+        if (spherical == 0) {                                    /* 173-183 */
+            const double xmin = g->lon_rho[IX2(Imin, Jmin, nx)], xmax = g->lon_rho[IX2(Imax, Jmax, nx)];
+            const double ymin = g->lat_rho[IX2(Imin, Jmin, nx)], ymax = g->lat_rho[IX2(Imax, Jmax, nx)];
+            const double xfac = ((double)Imax - (double)Imin) / (xmax - xmin);
+            const double yfac = ((double)Jmax - (double)Jmin) / (ymax - ymin);
+            const double dx = (lo - xmin) * xfac;
+            const double dy = (la - ymin) * yfac;
+            ipar[k] = (double)Imin + dx;
+            jpar[k] = (double)Jmin + dy;
+        } else if (found) {                                      /* 184-214 */
+            const double yfac = Eradius * deg2rad;
+            double sl, cl;
+            orc_sincos(la * deg2rad, &sl, &cl);
+            const double xfac = yfac * cl;
+            const double l00 = g->lon_rho[IX2(Imin, Jmin, nx)], t00 = g->lat_rho[IX2(Imin, Jmin, nx)];
+            const double l10 = g->lon_rho[IX2(Imin + 1, Jmin, nx)], t10 = g->lat_rho[IX2(Imin + 1, Jmin, nx)];
+            const double l01 = g->lon_rho[IX2(Imin, Jmin + 1, nx)], t01 = g->lat_rho[IX2(Imin, Jmin + 1, nx)];
+            const double xpp = (lo - l00) * xfac;
+            const double ypp = (la - t00) * yfac;
+            const double d1 = (l10 - l01) * xfac, d2 = (t10 - t01) * yfac;
+            const double diag2 = d1 * d1 + d2 * d2;
+            const double a1 = (l00 - l10) * xfac, a2 = (t00 - t10) * yfac;
+            const double aa2 = a1 * a1 + a2 * a2;
+            const double b1 = (l00 - l01) * xfac, b2 = (t00 - t01) * yfac;
+            const double bb2 = b1 * b1 + b2 * b2;
+            const double phi = orc_asin((diag2 - aa2 - bb2) / (2.0 * sqrt(aa2 * bb2)));
+            const double ang = g->angle[IX2(Imin, Jmin, nx)];
+            double sa, ca, sp, cp;
+            orc_sincos(ang, &sa, &ca);
+            orc_sincos(phi, &sp, &cp);
+            double dx = xpp * ca + ypp * sa;
+            double dy = ypp * ca - xpp * sa;
+            dx = dx + dy * (sp / cp);                            /* TAN(phi) */
+            dy = dy / cp;
+            dx = dx / sqrt(aa2);
+            dx = (dx > 0.0) ? dx : 0.0;                          /* MIN(MAX(0.0, .), 1.0) */
+            dx = (dx < 1.0) ? dx : 1.0;
+            dy = dy / sqrt(bb2);
+            dy = (dy > 0.0) ? dy : 0.0;
+            dy = (dy < 1.0) ? dy : 1.0;
+            ipar[k] = (double)Imin + dx;
+            jpar[k] = (double)Jmin + dy;
+        } else {
+            ipar[k] = -1.0;
+            jpar[k] = -1.0;
+        }
+    }
+    free(lonb);
+    free(latb);
+}
+
+void orc_nest_maps(int ngrid, const orc_grid *grids, const double *refine, double *scl, double *off)
+{
+    double grefine[ORC_MAXNGRID][ORC_MAXNGRID];
+    for (int a = 0; a < ngrid; a++)                              /* 437-450 */
+        for (int b = 0; b < ngrid; b++) {
+            grefine[a][b] = 1.0;
+            const int dng = abs(a - b);
+            for (int r = 1; r <= dng; r++) grefine[a][b] = refine[dng - 1] * grefine[a][b];
+        }
+    for (int k = 0; k < ngrid * 2 * ngrid; k++) { scl[k] = 1.0; off[k] = 0.0; }
+#define SCL(ng, c, i) scl[((ng) * 2 + (c)) * ngrid + (i)]
+#define OFF(ng, c, i) off[((ng) * 2 + (c)) * ngrid + (i)]
+    for (int ng2 = 0; ng2 < ngrid; ng2++) {                      /* 454-481 */
+        for (int ng = 0; ng < ngrid; ng++) {
+            const orc_grid *A = &grids[ng], *B = &grids[ng2];
+            int i, j = 1, ii = 1, jj = 1, hit = 0;
+            for (i = 1; i <= A->xi_rho && !hit; i++) {
+                for (j = 1; j <= A->eta_rho && !hit; j++) {
+                    for (ii = 1; ii <= B->xi_rho && !hit; ii++) {
+                        for (jj = 1; jj <= B->eta_rho; jj++) {
+                            if (A->lon_rho[IX2(i, j, A->xi_rho)] == B->lon_rho[IX2(ii, jj, B->xi_rho)] &&
+                                A->lat_rho[IX2(i, j, A->xi_rho)] == B->lat_rho[IX2(ii, jj, B->xi_rho)]) {
+                                hit = 1;
+                                break;
+                            }
+                        }
+                        if (hit) break;
+                    }
+                    if (hit) break;
+                }
+                if (hit) break;
+            }
+            /* no coincident point: the indices past the loops' ends, as
+             * Fortran leaves them after complete DO loops */
+            for (int c = 0; c < 2; c++) {
+                SCL(ng, c, ng2) = 1.0 / grefine[ng][ng2];
+                SCL(ng2, c, ng) = grefine[ng2][ng];
+            }
+            OFF(ng, 0, ng2) = (double)ii - SCL(ng, 0, ng2) * (double)i;
+            OFF(ng, 1, ng2) = (double)jj - SCL(ng, 1, ng2) * (double)j;
+            OFF(ng2, 0, ng) = (double)i - SCL(ng2, 0, ng) * (double)ii;
+            OFF(ng2, 1, ng) = (double)j - SCL(ng2, 1, ng) * (double)jj;
+        }
+    }
+#undef SCL
+#undef OFF
+}

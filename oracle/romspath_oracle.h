@@ -69,6 +69,8 @@ typedef struct {
     /* behaviour fields (Process_VA / Process_WA), (xi_rho,eta_rho,N+1):
      * HYDRODATA(ng)%Accelstd_t, Vortstd_t, Accelustd_w, Accelvstd_w */
     const double *turbaccel[3], *turbvort[3], *waveaccelu[3], *waveaccelv[3];
+    /* GRIDS(ng)%angle (xi_rho, eta_rho) for LL2ij (NULL unless used) */
+    const double *angle;
 } orc_grid;
 
 typedef struct {
@@ -183,6 +185,24 @@ int orc_init_particles(const orc_params *prm, const orc_grid *grids,
  * "lat", pGID, pX, pY, 1) for every particle (gather indices clamped; no
  * flag is recorded, as the output step changes no particle state). */
 void orc_output_lonlat(const orc_grid *grids, const orc_particles *p, double *lon, double *lat);
+
+/* sin, cos (|x| < 2^19 pi/2) and asin from their series with exact
+ * argument reductions (own restatement; the device runs the same ops) */
+void   orc_sincos(double x, double *s, double *c);
+double orc_asin(double x);
+
+/* LL2ij (interpolation_module.f90:110-231) for particles at (inlon,
+ * inlat) in grid g: bisection of the grid with inbox (232-268) and inside,
+ * then the Cartesian (spherical = 0) or spherical (1) fractional index;
+ * spherical is GRIDS(1)%spherical, as the reference reads it. */
+void orc_ll2ij(const orc_grid *g, int spherical, const double *inlon, const double *inlat, int64_t n,
+               double *ipar, double *jpar);
+
+/* The nest maps of InitGrid (grid_module.f90:441-481): grefine from
+ * refine(1..Ngrid-1), the first coincident lon/lat rho point of each grid
+ * pair by the reference's search order, and scl/off of every pair; scl and
+ * off are [ng][2][Ngrid] (GRIDS(ng)%scl(i,c) at [ng][c][i]). */
+void orc_nest_maps(int ngrid, const orc_grid *grids, const double *refine, double *scl, double *off);
 
 /* statistics of the last orc_update_particles call (secant iterations) */
 void orc_last_stats(int64_t *spline_calls, int64_t *secant_iters);

@@ -30,6 +30,7 @@ UNITS = [
     ("rp_mixed.cu", []),          # mixed-precision form: FMA contraction allowed
     ("rp_sort.cu", []),           # re-sorting of the particle state (no arithmetic on values)
     ("rp_adjoint.cu", ["-fmad=false"]),   # adjoint pair: double and dual instantiations agree
+    ("rp_init.cu", ["-fmad=false"]),      # LL2ij on the device, nest maps on the host
     ("rp_api.cu", []),
 ]
 

@@ -25,7 +25,9 @@ struct GridBuf {
     uint8_t *mrho = nullptr, *mu = nullptr, *mv = nullptr;
     void *zeta = nullptr, *u = nullptr, *v = nullptr, *w = nullptr, *aks = nullptr;
     void *salt = nullptr, *temp = nullptr, *bustr = nullptr, *bvstr = nullptr;  // diagnostics only
-    double *lon = nullptr, *lat = nullptr;     // lon_rho, lat_rho (output records only)
+    double *lon = nullptr, *lat = nullptr;     // lon_rho, lat_rho (output records, LL2ij)
+    double* angle = nullptr;                   // GRIDS(ng)%angle (LL2ij, spherical grids)
+    int spherical = -1;                        // GRIDS(ng)%spherical (-1: not set)
     uint8_t *wd_rho = nullptr, *wd_u = nullptr, *wd_v = nullptr;  // WETDRY masks, [j][i][slot4]
     void *turbaccel = nullptr, *turbvort = nullptr;      // behave's fields (Process_VA)
     void *waveaccelu = nullptr, *waveaccelv = nullptr;   // (Process_WA)
@@ -299,7 +301,7 @@ void free_ctx(rp_ctx* c) {
         void* ptrs[] = {G.h, G.pm, G.pn, G.sr, G.csr, G.sw, G.csw, G.mrho, G.mu, G.mv,
                         G.zeta, G.u, G.v, G.w, G.aks, G.qs_u, G.qs_v, G.qs_w, G.qs_aks,
                         G.salt, G.temp, G.bustr, G.bvstr, G.lon, G.lat, G.wd_rho, G.wd_u, G.wd_v,
-                        G.turbaccel, G.turbvort, G.waveaccelu, G.waveaccelv};
+                        G.turbaccel, G.turbvort, G.waveaccelu, G.waveaccelv, G.angle};
         for (void* p : ptrs) if (p) cudaFree(p);
         for (int s = 0; s < RP_SLOTS; s++) {
             if (G.slot_free[s]) cudaEventDestroy(G.slot_free[s]);
@@ -569,6 +571,82 @@ int adj_upload_field(rp_ctx* ctx, const double* src, const double* add, double* 
         ctx->pin_used[h] = true;
     }
     return RP_OK;
+}
+
+// ini_ROMSPath's particle set-up (ROMSPath.f90:319-432) on the device:
+// the particles' fractional indices in every grid, either given (ipos,
+// jpos; (n, Ngrid) Fortran order) or by LL2ij from lon/lat, then the
+// ownership loop with bounds/zbounds and the initial diagnostics.
+int locate(rp_ctx* ctx, int64_t n, const double* ipos, const double* jpos, const double* lon, const double* lat,
+           const double* z, const double* dob, int32_t t_b, double* ipos_out, double* jpos_out) {
+    if (n < 0 || n > ctx->cap) return fail(ctx, RP_ERR_ARG, "rp_locate_particles: n exceeds numpar");
+    if (!z || !dob) return fail(ctx, RP_ERR_ARG, "rp_locate_particles: null array");
+    if (t_b < 1 || t_b > 3) return fail(ctx, RP_ERR_ARG, "rp_locate_particles: slot must be 1..3");
+    // SaltTempOn reads the initial salinity and temperature from t_c, the
+    // slot after t_b (ROMSPath.f90:209-211, 408-427)
+    const int32_t t_c = (ctx->diag & RP_DIAG_SALTTEMP) ? t_b % 3 + 1 : t_b;
+    for (int k = 0; k < ctx->ngrid; k++)
+        if (ctx->g[k].map[t_b - 1] < 0 || ctx->g[k].map[t_c - 1] < 0)
+            return fail(ctx, RP_ERR_STATE, "rp_locate_particles: frame slot not loaded");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->s_comp;
+    const size_t nb = (size_t)n * 8, nbg = nb * ctx->ngrid;
+    double *dip = nullptr, *djp = nullptr, *dz = nullptr, *ddob = nullptr, *dlon = nullptr, *dlat = nullptr;
+    CK(cudaMalloc(&dip, std::max<size_t>(nbg, 8)));
+    CK(cudaMalloc(&djp, std::max<size_t>(nbg, 8)));
+    CK(cudaMalloc(&dz, std::max<size_t>(nb, 8)));
+    CK(cudaMalloc(&ddob, std::max<size_t>(nb, 8)));
+    if (lon) {
+        CK(cudaMalloc(&dlon, std::max<size_t>(nb, 8)));
+        CK(cudaMalloc(&dlat, std::max<size_t>(nb, 8)));
+    }
+    int rc = RP_OK;
+    cudaError_t e = cudaSuccess;
+    if (lon) {
+        if (!(rc = h2d(ctx, dlon, lon, nb, s)) && !(rc = h2d(ctx, dlat, lat, nb, s))) {
+            // LL2ij reads GRIDS(1)%spherical for every grid (interpolation_module.f90:171)
+            const int sph = ctx->g[0].spherical;
+            for (int k = 0; k < ctx->ngrid && e == cudaSuccess; k++) {
+                const GridBuf& G = ctx->g[k];
+                if (sph != 0 && !G.angle) {
+                    rc = fail(ctx, RP_ERR_STATE, "rp_locate_lonlat: spherical grids need their angle");
+                    break;
+                }
+                e = rp::launch_ll2ij(G.lon, G.lat, G.angle, G.nx, G.ny, sph, dlon, dlat, n, dip + (size_t)k * n,
+                                     djp + (size_t)k * n, ctx->num_sms, s);
+                ctx->launches++;
+            }
+            if (e == cudaSuccess && rc == RP_OK && ipos_out) rc = d2h(ctx, ipos_out, dip, nbg, s);
+            if (e == cudaSuccess && rc == RP_OK && jpos_out) rc = d2h(ctx, jpos_out, djp, nbg, s);
+        }
+    } else {
+        if (!(rc = h2d(ctx, dip, ipos, nbg, s))) rc = h2d(ctx, djp, jpos, nbg, s);
+    }
+    if (rc == RP_OK && e == cudaSuccess && !(rc = h2d(ctx, dz, z, nb, s)) && !(rc = h2d(ctx, ddob, dob, nb, s))) {
+        ctx->n = n;
+        ctx->permuted = false;
+        ctx->since_sort = ctx->resort;
+        ctx->state_base = ctx->pid_base;
+        RpStepArgs A{};
+        fill_params(ctx, A);
+        fill_grids(ctx, A, t_b, t_c, t_b);
+        for (int k = 0; k < ctx->ngrid; k++) {
+            cudaStreamWaitEvent(s, ctx->g[k].slot_ready[ctx->g[k].map[t_b - 1]], 0);
+            cudaStreamWaitEvent(s, ctx->g[k].slot_ready[ctx->g[k].map[t_c - 1]], 0);
+        }
+        e = rp::launch_locate(A, ctx->mixed ? RP_FIELD_F32 : ctx->prm.field_dtype, dip, djp, dz, ddob, s);
+        ctx->launches++;
+        if (e == cudaSuccess && ctx->mixed) {
+            e = rp::launch_mixed_convert(A.p, 0, s);
+            ctx->launches++;
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    }
+    if (e != cudaSuccess && rc == RP_OK) rc = fail(ctx, RP_ERR_CUDA, std::string("locate: ") + cudaGetErrorString(e));
+    cudaFree(dip); cudaFree(djp); cudaFree(dz); cudaFree(ddob);
+    if (dlon) cudaFree(dlon);
+    if (dlat) cudaFree(dlat);
+    return rc;
 }
 
 }  // namespace
@@ -862,48 +940,19 @@ int rp_set_particles(rp_ctx* ctx, int64_t n, const double* x, const double* y, c
 int rp_locate_particles(rp_ctx* ctx, int64_t n, const double* ipos, const double* jpos, const double* z,
                         const double* dob, int32_t t_b) {
     if (!ctx) return RP_ERR_ARG;
-    if (n < 0 || n > ctx->cap) return fail(ctx, RP_ERR_ARG, "rp_locate_particles: n exceeds numpar");
-    if (!ipos || !jpos || !z || !dob) return fail(ctx, RP_ERR_ARG, "rp_locate_particles: null array");
-    if (t_b < 1 || t_b > 3) return fail(ctx, RP_ERR_ARG, "rp_locate_particles: slot must be 1..3");
-    // SaltTempOn reads the initial salinity and temperature from t_c, the
-    // slot after t_b (ROMSPath.f90:209-211, 408-427)
-    const int32_t t_c = (ctx->diag & RP_DIAG_SALTTEMP) ? t_b % 3 + 1 : t_b;
-    for (int k = 0; k < ctx->ngrid; k++)
-        if (ctx->g[k].map[t_b - 1] < 0 || ctx->g[k].map[t_c - 1] < 0)
-            return fail(ctx, RP_ERR_STATE, "rp_locate_particles: frame slot not loaded");
-    CK(cudaSetDevice(ctx->device));
-    cudaStream_t s = ctx->s_comp;
-    const size_t nb = (size_t)n * 8, nbg = nb * ctx->ngrid;
-    double *dip = nullptr, *djp = nullptr, *dz = nullptr, *ddob = nullptr;
-    CK(cudaMalloc(&dip, std::max<size_t>(nbg, 8)));
-    CK(cudaMalloc(&djp, std::max<size_t>(nbg, 8)));
-    CK(cudaMalloc(&dz, std::max<size_t>(nb, 8)));
-    CK(cudaMalloc(&ddob, std::max<size_t>(nb, 8)));
-    int rc = RP_OK;
-    if (!(rc = h2d(ctx, dip, ipos, nbg, s)) && !(rc = h2d(ctx, djp, jpos, nbg, s)) && !(rc = h2d(ctx, dz, z, nb, s)) &&
-        !(rc = h2d(ctx, ddob, dob, nb, s))) {
-        ctx->n = n;
-        ctx->permuted = false;
-        ctx->since_sort = ctx->resort;
-        ctx->state_base = ctx->pid_base;
-        RpStepArgs A{};
-        fill_params(ctx, A);
-        fill_grids(ctx, A, t_b, t_c, t_b);
-        for (int k = 0; k < ctx->ngrid; k++) {
-            cudaStreamWaitEvent(s, ctx->g[k].slot_ready[ctx->g[k].map[t_b - 1]], 0);
-            cudaStreamWaitEvent(s, ctx->g[k].slot_ready[ctx->g[k].map[t_c - 1]], 0);
-        }
-        cudaError_t e = rp::launch_locate(A, ctx->mixed ? RP_FIELD_F32 : ctx->prm.field_dtype, dip, djp, dz, ddob, s);
-        ctx->launches++;
-        if (e == cudaSuccess && ctx->mixed) {
-            e = rp::launch_mixed_convert(A.p, 0, s);
-            ctx->launches++;
-        }
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess) rc = fail(ctx, RP_ERR_CUDA, std::string("locate: ") + cudaGetErrorString(e));
+    if (!ipos || !jpos) return fail(ctx, RP_ERR_ARG, "rp_locate_particles: null array");
+    return locate(ctx, n, ipos, jpos, nullptr, nullptr, z, dob, t_b, nullptr, nullptr);
+}
+
+int rp_locate_lonlat(rp_ctx* ctx, int64_t n, const double* lon, const double* lat, const double* z, const double* dob,
+                     int32_t t_b, double* ipos_out, double* jpos_out) {
+    if (!ctx) return RP_ERR_ARG;
+    if (!lon || !lat) return fail(ctx, RP_ERR_ARG, "rp_locate_lonlat: null array");
+    for (int k = 0; k < ctx->ngrid; k++) {
+        if (!ctx->g[k].lon) return fail(ctx, RP_ERR_STATE, "rp_locate_lonlat: lon/lat need rp_set_grid_lonlat");
+        if (ctx->g[k].spherical < 0) return fail(ctx, RP_ERR_STATE, "rp_locate_lonlat: rp_set_grid_angle first");
     }
-    cudaFree(dip); cudaFree(djp); cudaFree(dz); cudaFree(ddob);
-    return rc;
+    return locate(ctx, n, nullptr, nullptr, lon, lat, z, dob, t_b, ipos_out, jpos_out);
 }
 
 }  // extern "C"
@@ -1168,6 +1217,23 @@ int rp_set_grid_lonlat(rp_ctx* ctx, int32_t ng, const double* lon_rho, const dou
     if ((rc = h2d(ctx, G.lon, lon_rho, bytes, ctx->s_comp)) || (rc = h2d(ctx, G.lat, lat_rho, bytes, ctx->s_comp)))
         return rc;
     CK(cudaStreamSynchronize(ctx->s_comp));
+    return RP_OK;
+}
+
+int rp_set_grid_angle(rp_ctx* ctx, int32_t ng, const double* angle, int32_t spherical) {
+    if (!ctx) return RP_ERR_ARG;
+    if (ng < 1 || ng > ctx->ngrid) return fail(ctx, RP_ERR_ARG, "rp_set_grid_angle: grid id out of range");
+    if (spherical != 0 && spherical != 1) return fail(ctx, RP_ERR_ARG, "rp_set_grid_angle: spherical must be 0 or 1");
+    GridBuf& G = ctx->g[ng - 1];
+    if (angle) {
+        CK(cudaSetDevice(ctx->device));
+        const size_t bytes = (size_t)G.nx * G.ny * 8;
+        if (!G.angle && dalloc(&G.angle, bytes)) return fail(ctx, RP_ERR_NOMEM, "rp_set_grid_angle: allocation");
+        int rc;
+        if ((rc = h2d(ctx, G.angle, angle, bytes, ctx->s_comp)) != RP_OK) return rc;
+        CK(cudaStreamSynchronize(ctx->s_comp));
+    }
+    G.spherical = spherical;
     return RP_OK;
 }
 

@@ -87,6 +87,10 @@ cudaError_t launch_adj_store(const double* src, const double* add, double* dst, 
                              int64_t count, cudaStream_t s);
 cudaError_t launch_adj_tangent_init(double* t, int64_t n, cudaStream_t s);
 
+// LL2ij of n particles in one grid (rp_init.cu)
+cudaError_t launch_ll2ij(const double* lon, const double* lat, const double* angle, int nx, int ny, int spherical,
+                         const double* inlon, const double* inlat, int64_t n, double* ip, double* jp, int num_sms,
+                         cudaStream_t s);
 cudaError_t launch_locate(const RpStepArgs& A, int field_dtype, const double* ipos, const double* jpos,
                           const double* z, const double* dob, cudaStream_t s);
 cudaError_t launch_convert(int src_f32, int dst_f32, const void* src, const void* add, void* dst, int ni, int nj,

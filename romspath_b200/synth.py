@@ -129,6 +129,7 @@ def make_grid(spec: GridSpec) -> Dict[str, np.ndarray]:
     lon = -70.5 + (Xg * math.cos(th) - Yg * math.sin(th)) / (111_195.0 * math.cos(math.radians(lat0)))
     return {
         "lon_rho": np.asfortranarray(lon), "lat_rho": np.asfortranarray(lat),
+        "angle": np.asfortranarray(np.full((nx, ny), th)),
         "h": np.asfortranarray(h),
         "pm": np.asfortranarray(np.full((nx, ny), 1.0 / spec.dx)),
         "pn": np.asfortranarray(np.full((nx, ny), 1.0 / spec.dy)),

@@ -101,7 +101,8 @@ class Tracker:
                 setattr(g, name, a.ctypes.data_as(_lib.PI32))
             if "lon_rho" in gr:
                 self._lonlat.append((k + 1, np.asfortranarray(gr["lon_rho"], dtype=np.float64),
-                                     np.asfortranarray(gr["lat_rho"], dtype=np.float64)))
+                                     np.asfortranarray(gr["lat_rho"], dtype=np.float64),
+                                     np.asfortranarray(gr["angle"], dtype=np.float64) if "angle" in gr else None))
             if scl is not None:
                 s = np.asfortranarray(np.asarray(scl[k], dtype=np.float64).reshape(self.ng, 2))
                 o = np.asfortranarray(np.asarray(off[k], dtype=np.float64).reshape(self.ng, 2))
@@ -115,8 +116,11 @@ class Tracker:
             raise RomsPathError(f"rp_create failed: {_lib.ERRORS.get(rc, rc)}")
         self.h = h
         self.n = 0
-        for ng, lon, lat in self._lonlat:
+        # GRIDS(ng)%spherical: 1 for lon/lat grids (the default), 0 Cartesian
+        sph = int(params.get("spherical", 1))
+        for ng, lon, lat, ang in self._lonlat:
             self._check(L.rp_set_grid_lonlat(h, ng, _pd(lon), _pd(lat)), "rp_set_grid_lonlat")
+            self._check(L.rp_set_grid_angle(h, ng, _pd(ang), sph), "rp_set_grid_angle")
         self._lonlat = []
         if P.behavior or self.va or self.wa:
             b = _lib.RpBehavior()
@@ -219,6 +223,19 @@ class Tracker:
         rc = self.L.rp_locate_particles(self.h, n, _pd(ip), _pd(jp), _pd(z), _pd(dob), t_b)
         self._check(rc, "rp_locate_particles")
         self.n = n
+
+    def locate_lonlat(self, lon, lat, z, dob, t_b: int = 1):
+        """ini_ROMSPath from particle lon/lat: LL2ij of every grid on the
+        device, then the ownership loop; returns LL2ij's (ipos, jpos),
+        (Ngrid, n)."""
+        n = len(lon)
+        cols = [np.ascontiguousarray(a, dtype=np.float64) for a in (lon, lat, z, dob)]
+        ip = np.empty((self.ng, n))
+        jp = np.empty((self.ng, n))
+        rc = self.L.rp_locate_lonlat(self.h, n, *[_pd(a) for a in cols], t_b, _pd(ip), _pd(jp))
+        self._check(rc, "rp_locate_lonlat")
+        self.n = n
+        return ip, jp
 
     def get_particles(self, n: Optional[int] = None, out: Optional[Dict[str, np.ndarray]] = None
                       ) -> Dict[str, np.ndarray]:
@@ -365,3 +382,24 @@ class Tracker:
                 if max_steps is not None and done >= max_steps:
                     return done
         return done
+
+
+def nest_maps(grids: Sequence[Dict[str, np.ndarray]], refine: Sequence[float]):
+    """InitGrid's nest maps (rp_nest_maps) from the grids' lon_rho/lat_rho:
+    (scl, off), each (Ngrid, Ngrid, 2) as GRIDS(ng)%scl(i, c)."""
+    L = _lib.load()
+    ng = len(grids)
+    xi = np.array([g["lon_rho"].shape[0] for g in grids], dtype=np.int32)
+    eta = np.array([g["lon_rho"].shape[1] for g in grids], dtype=np.int32)
+    lons = [np.asfortranarray(g["lon_rho"], dtype=np.float64) for g in grids]
+    lats = [np.asfortranarray(g["lat_rho"], dtype=np.float64) for g in grids]
+    lp = (_lib.PD * ng)(*[_pd(a) for a in lons])
+    tp = (_lib.PD * ng)(*[_pd(a) for a in lats])
+    ref = np.ascontiguousarray(list(refine) + [1.0] * _lib.MAXNGRID, dtype=np.float64)
+    scl = np.empty(ng * 2 * ng)
+    off = np.empty(ng * 2 * ng)
+    rc = L.rp_nest_maps(ng, xi.ctypes.data_as(_lib.PI32), eta.ctypes.data_as(_lib.PI32), lp, tp, _pd(ref),
+                        _pd(scl), _pd(off))
+    if rc != 0:
+        raise RomsPathError(f"rp_nest_maps: {_lib.ERRORS.get(rc, rc)}")
+    return (scl.reshape(ng, 2, ng).transpose(0, 2, 1).copy(), off.reshape(ng, 2, ng).transpose(0, 2, 1).copy())
