@@ -35,6 +35,7 @@ the reported time is the max over ranks.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import math
 import os
@@ -88,6 +89,12 @@ def parse():
                     help="instead of timing the step: the adjoint pair on the 130x98x20 grid (262,144 particles, "
                          "3 days, checkpoints every 48 steps): forward / backward / tangent times and the "
                          "finite-difference agreement")
+    ap.add_argument("--features", action="store_true",
+                    help="cost of the diagnostics, WETDRY, behave and the output record on the exact step, "
+                         "and the init lookup (LL2ij, nest maps) against the oracle")
+    ap.add_argument("--variants", default=None,
+                    help="--features: comma-separated step variants to run (default all); 'none' skips the steps")
+    ap.add_argument("--no-init", action="store_true", help="--features: skip the LL2ij and nest-map timings")
     ap.add_argument("--deterministic", action="store_true", help="error study with turbulence off")
     ap.add_argument("--mixed-kind", default="mixed", choices=["mixed", "mixed-i16"],
                     help="16-bit field storage of the mixed form: FP16 (default) or int16 fixed point")
@@ -505,6 +512,137 @@ def config1_run(args):
     print(json.dumps(out), flush=True)
 
 
+# ---------------------------------------------------------------- features
+
+def features_run(args):
+    """The rows beyond the step on config 2's grid and 1,048,576 particles,
+    exact FP32-field form: the step with the diagnostics (SaltTempOn,
+    SaltTempMean, WriteBottom), WETDRY, behave 10 (Process_VA and _WA) and
+    all of them, device time per internal step (CUDA events on the
+    library's stream, median of K after W); one output record (device pack,
+    read-back into page-locked arrays); LL2ij of every particle from lon/lat
+    (rp_locate_lonlat, end to end) against the oracle's LL2ij on a
+    single-threaded sample; InitGrid's nest maps hashed against the
+    reference's search on a parent 400x300 / child 240x180 pair."""
+    import torch
+    from romspath_b200 import Tracker
+    from romspath_b200.tracker import nest_maps
+    from oracle import oracle as O
+    torch.cuda.set_device(0)
+    npart = args.particles or synth.CONFIG_PARTICLES["cfg2"]
+    base = synth.config_spec("cfg2")[0]
+    spec = dataclasses.replace(base, diag=True, wetdry=True, behave=True)
+    grid = synth.make_grid(spec)
+    params0 = synth.config_params("cfg2")
+    frames = [synth.make_frame(spec, grid, k * 3600.0) for k in range(4)]
+    rel = synth.uniform_release(spec, grid, frames[0], npart, seed=0)
+    exts = list(schedule.external_steps(2.0, int(params0["dt"]), int(params0["idt"])))
+    its = [it for e in exts for it in e.internal]
+    synth_diag = {"salttemp_on": 1, "salttemp_mean": 1, "write_bottom": 1}
+    variants = [
+        ("passive", {}),
+        ("diagnostics", dict(synth_diag)),
+        ("wetdry", {"wetdry": 1}),
+        ("behave10", dict(synth.FUCHS_SAMPLE, behavior=10, va_flag=0)),
+        ("diagnostics+behave10", dict(synth.FUCHS_SAMPLE, behavior=10, va_flag=0, **synth_diag)),
+        ("diagnostics+wetdry", dict(wetdry=1, **synth_diag)),
+        ("behave10+wetdry", dict(synth.FUCHS_SAMPLE, behavior=10, va_flag=0, wetdry=1)),
+        ("all", dict(synth.FUCHS_SAMPLE, behavior=10, va_flag=0, wetdry=1, **synth_diag)),
+    ]
+    variants += [("passive/split", {}), ("all/split", variants[-1][1])]
+    if args.variants:
+        keep = set(args.variants.split(","))
+        variants = [v for v in variants if v[0] in keep]
+    steps = {}
+    for name, pov in variants:
+        params = dict(params0, **pov)
+        T = Tracker([spec], [grid], params, numpar=npart, field_dtype=spec.field_dtype, stokes=spec.stokes,
+                    seed=7, resort=args.resort, variant="split" if name.endswith("/split") else "fused")
+        for k, slot in enumerate((1, 2, 3)):
+            T.upload_frame(1, slot, frames[k])
+        T.locate(rel, t_b=1)
+        ms = []
+        for i in range(args.warmup + args.steps):
+            it = its[i % 12]
+            T.step(it.ex, it.ix, it.ets, it.tb, it.tc, it.tf)
+            T.synchronize()
+            if i >= args.warmup:
+                ms.append(T.last_step_stats()[0])
+        rec_ms = None
+        if name == "all":
+            pins = {k: pinned_empty(npart, np.float64) for k in Tracker.RECORD}   # (array, owning tensor)
+            out = {k: v[0] for k, v in pins.items()}
+            T.synchronize()
+            t0 = time.perf_counter()
+            T.output_record(13, out=out)
+            rec_ms = (time.perf_counter() - t0) * 1e3
+        T.close()
+        steps[name] = {"ms_per_step": float(np.median(ms)), "particle_steps_per_s": npart / (np.median(ms) * 1e-3)}
+        if rec_ms is not None:
+            steps[name]["output_record_ms"] = rec_ms
+    for name in steps:
+        if "passive" in steps:
+            steps[name]["vs_passive"] = steps[name]["ms_per_step"] / steps["passive"]["ms_per_step"]
+    if args.no_init:
+        print(json.dumps({"mode": "features", "step": steps}), flush=True)
+        return
+
+    # LL2ij from lon/lat: every particle, end to end through the C ABI
+    lon = np.ascontiguousarray(synth_bilinear(grid["lon_rho"], rel.ipos[0], rel.jpos[0]))
+    lat = np.ascontiguousarray(synth_bilinear(grid["lat_rho"], rel.ipos[0], rel.jpos[0]))
+    T = Tracker([spec], [grid], params0, numpar=npart, field_dtype=spec.field_dtype, stokes=spec.stokes, seed=7)
+    for k, slot in enumerate((1, 2, 3)):
+        T.upload_frame(1, slot, frames[k])
+    T.locate_lonlat(lon[:4096], lat[:4096], rel.z[:4096], rel.dob[:4096])    # warm-up
+    T.synchronize()
+    t0 = time.perf_counter()
+    gi, gj = T.locate_lonlat(lon, lat, rel.z, rel.dob)
+    t_gpu = time.perf_counter() - t0
+    T.close()
+    m = O.OracleModel([spec], [grid], params0)
+    ns = min(args.cpu_sample, npart)
+    t0 = time.perf_counter()
+    oi, oj = m.ll2ij(1, lon[:ns], lat[:ns], spherical=1)
+    t_cpu = time.perf_counter() - t0
+    same = int(np.sum(oi.view(np.uint64) != gi[0, :ns].view(np.uint64)) +
+               np.sum(oj.view(np.uint64) != gj[0, :ns].view(np.uint64)))
+    ll2ij = {"particles": npart, "grid": f"{spec.xi_rho}x{spec.eta_rho}",
+             "gpu_end_to_end_s": t_gpu, "gpu_particles_per_s": npart / t_gpu,
+             "cpu_oracle_sample": ns, "cpu_oracle_s": t_cpu, "cpu_particles_per_s": ns / t_cpu, "cpu_threads": 1,
+             "sample_indices_differing": same,
+             "max_index_error_cells": float(max(np.max(np.abs(gi[0] - rel.ipos[0])),
+                                                np.max(np.abs(gj[0] - rel.jpos[0]))))}
+
+    # nest maps: a parent 400x300 at 1 km and a child 240x180 at 250 m whose
+    # rho point (1,1) sits on parent point (101, 76)
+    px, py = np.meshgrid(np.arange(400) * 1000.0, np.arange(300) * 1000.0, indexing="ij")
+    cx, cy = np.meshgrid(100000.0 + np.arange(240) * 250.0, 75000.0 + np.arange(180) * 250.0, indexing="ij")
+    specs = [synth.GridSpec(240, 180, 4), synth.GridSpec(400, 300, 4)]
+    grids = [synth.make_grid(s) for s in specs]
+    grids[0]["lon_rho"], grids[0]["lat_rho"] = np.asfortranarray(cx), np.asfortranarray(cy)
+    grids[1]["lon_rho"], grids[1]["lat_rho"] = np.asfortranarray(px), np.asfortranarray(py)
+    t0 = time.perf_counter()
+    sh, oh = nest_maps(grids, [4.0])
+    t_hash = time.perf_counter() - t0
+    mo = O.OracleModel(specs, grids, params0)
+    t0 = time.perf_counter()
+    so, oo = mo.nest_maps([4.0])
+    t_search = time.perf_counter() - t0
+    nest = {"grids": "child 240x180 (250 m) in parent 400x300 (1 km)", "hashed_s": t_hash,
+            "reference_search_s": t_search, "maps_equal": bool(np.array_equal(sh, so) and np.array_equal(oh, oo)),
+            "child_to_parent": {"scl": sh[0][1].tolist(), "off": oh[0][1].tolist()}}
+    print(json.dumps({"mode": "features", "workload": "cfg2 grid 512x384x30, FP32 fields, 1,048,576 particles",
+                      "step": steps, "ll2ij": ll2ij, "nest_maps": nest,
+                      "timing": f"median of {args.steps} steps after {args.warmup}, CUDA events"}), flush=True)
+
+
+def synth_bilinear(a, ip, jp):
+    I, J = np.floor(ip).astype(int), np.floor(jp).astype(int)
+    X, Y = ip - I, jp - J
+    return ((1 - X) * (1 - Y) * a[I - 1, J - 1] + X * (1 - Y) * a[I, J - 1] + X * Y * a[I, J]
+            + (1 - X) * Y * a[I - 1, J])
+
+
 # ---------------------------------------------------------------- adjoint
 
 def adjoint_run(args):
@@ -643,6 +781,9 @@ def main():
     if args.config1:
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         config1_run(args)
+        return
+    if args.features:
+        features_run(args)
         return
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
