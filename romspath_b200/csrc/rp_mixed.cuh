@@ -364,18 +364,39 @@ __device__ __forceinline__ void m_find_currents(const RpStepArgs& A, const RpGri
 // traffic is three arrays written forward and read backward plus u written
 // backward.
 
-// Workspace: three FP64 arrays for chol1d, then four FP32 arrays for the
-// data (the column and the resampled values carry FP32 information only),
-// kMixedArrays (NPMAX+1) doubles in all.
-constexpr int kMixedArrays = 5;
+// Workspace: the chol1d arrays (ratio1, ratio2 and u), then four FP32
+// arrays for the data (the column and the resampled values carry FP32
+// information only).  RP_MIXED_WS sets the chol1d arrays' storage: 0 all
+// FP64, 1 the factor ratios FP32 and u FP64, 2 all FP32 (the arithmetic
+// stays FP64 in registers).  kMixedArrays (NPMAX+1) doubles in all.
+#ifndef RP_MIXED_WS
+#define RP_MIXED_WS 2
+#endif
+#if RP_MIXED_WS == 0
+using MRatio = double;
+using MU = double;
+#elif RP_MIXED_WS == 1
+using MRatio = float;
+using MU = double;
+#else
+using MRatio = float;
+using MU = float;
+#endif
+constexpr int kMixedBytesPerPoint = 2 * (int)sizeof(MRatio) + (int)sizeof(MU) + 4 * 4;
+constexpr int kMixedArrays = (kMixedBytesPerPoint + 7) / 8;
 
 template <int NPMAX>
 struct MSpline {
     double* base;
-    __device__ __forceinline__ double& s1(int i) const { return base[i]; }                  // ratio1(i)
-    __device__ __forceinline__ double& s2(int i) const { return base[(NPMAX + 1) + i]; }    // ratio2(i)
-    __device__ __forceinline__ double& u(int i) const { return base[2 * (NPMAX + 1) + i]; } // u(i)/v(i,1), then u(i)
-    __device__ __forceinline__ float* fb() const { return reinterpret_cast<float*>(base + 3 * (NPMAX + 1)); }
+    __device__ __forceinline__ MU& u(int i) const { return reinterpret_cast<MU*>(base)[i]; }  // u(i)/v(i,1), then u(i)
+    __device__ __forceinline__ MRatio* rb() const {
+        return reinterpret_cast<MRatio*>(reinterpret_cast<char*>(base) + (NPMAX + 1) * sizeof(MU));
+    }
+    __device__ __forceinline__ MRatio& s1(int i) const { return rb()[i]; }                   // ratio1(i)
+    __device__ __forceinline__ MRatio& s2(int i) const { return rb()[(NPMAX + 1) + i]; }     // ratio2(i)
+    __device__ __forceinline__ float* fb() const {
+        return reinterpret_cast<float*>(reinterpret_cast<char*>(base) + (NPMAX + 1) * (sizeof(MU) + 2 * sizeof(MRatio)));
+    }
     __device__ __forceinline__ float& y(int i) const { return fb()[i]; }                     // resampled data y(i)
     __device__ __forceinline__ float& cz(int k) const { return fb()[(NPMAX + 1) + k]; }      // column z(k)
     __device__ __forceinline__ float& cm(int k) const { return fb()[2 * (NPMAX + 1) + k]; }  // slope on [z(k), z(k+1)]
@@ -447,9 +468,9 @@ __device__ double m_chol1d(const MSpline<NPMAX>& w, const MFit& f, double p, dou
         const double c2 = E - ratio1 * Fi;
         const double ratio2 = Fi * inv;
         const double c1 = D - ratio2 * Fi;
-        w.s1(i) = ratio1;
-        w.s2(i) = ratio2;
-        w.u(i) = ucur * inv;
+        w.s1(i) = (MRatio)ratio1;
+        w.s2(i) = (MRatio)ratio2;
+        w.u(i) = (MU)(ucur * inv);
         ym = y0;
         y0 = yp;
         yp = wk.at(w, f.sw, f.z1 + (double)(i + 1) * f.h);
@@ -474,7 +495,7 @@ __device__ double m_chol1d(const MSpline<NPMAX>& w, const MFit& f, double p, dou
     if (store_u) w.u(np) = 0.0;
     {
         const double ui = ucur / a1;                 // u(np-1)
-        if (store_u) w.u(np - 1) = ui;
+        if (store_u) w.u(np - 1) = (MU)ui;
         const double raw = (up1 - ui) * f.rh;        // raw(np)
         const double fin = rawp - raw;               // qu(np)
         sum = sum + fin * fin * dy2;
@@ -485,8 +506,8 @@ __device__ double m_chol1d(const MSpline<NPMAX>& w, const MFit& f, double p, dou
     }
 #pragma unroll 2
     for (int i = np - 2; i >= 2; i--) {
-        const double ui = w.u(i) - up1 * w.s1(i) - up2 * w.s2(i);
-        if (store_u) w.u(i) = ui;
+        const double ui = (double)w.u(i) - up1 * (double)w.s1(i) - up2 * (double)w.s2(i);
+        if (store_u) w.u(i) = (MU)ui;
         const double raw = (up1 - ui) * f.rh;        // raw(i+1)
         const double fin = rawp - raw;               // qu(i+1)
         sum = sum + fin * fin * dy2;
@@ -603,9 +624,9 @@ struct MPiece {
 template <int NPMAX>
 __device__ __forceinline__ void m_piece(const MSpline<NPMAX>& w, const MFit& f, double p, int i, MPiece& pc) {
     const int np = f.np;
-    const double um = (i >= 2) ? w.u(i - 1) : 0.0;
-    const double u0 = w.u(i), u1 = w.u(i + 1);
-    const double u2 = (i + 2 <= np) ? w.u(i + 2) : 0.0;
+    const double um = (i >= 2) ? (double)w.u(i - 1) : 0.0;
+    const double u0 = (double)w.u(i), u1 = (double)w.u(i + 1);
+    const double u2 = (i + 2 <= np) ? (double)w.u(i + 2) : 0.0;
     const double raw0 = (i >= 2) ? (u0 - um) * f.rh : 0.0;          // raw(i)
     const double raw1 = (u1 - u0) * f.rh;                            // raw(i+1)
     const double raw2 = (i + 2 <= np) ? (u2 - u1) * f.rh : 0.0;      // raw(i+2)
