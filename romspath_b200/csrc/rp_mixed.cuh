@@ -459,17 +459,44 @@ __device__ double m_chol1d(const MSpline<NPMAX>& w, const MFit& f, double p, dou
     }
     double a1 = D, a2 = E, b1 = D;
     double uprev = 0.0, ucur = (yp - 2.0 * y0 + ym) * f.rh, r2prev = 0.0;
+    // The bands are constant (uniform breaks), so the factor converges to
+    // a fixed point: once a row's ratios round to the previous row's in
+    // the storage precision, rows ks..np-3 reuse them (no division, no
+    // store); the last row (F = 0 there) is factorised from the held state.
+    int ks = np - 1;                                 // first reused row (np-1: none)
+    double hinv = 0.0, hr1 = 0.0, hr2 = 0.0;
+    MRatio pr1 = (MRatio)0, pr2 = (MRatio)0;
 #pragma unroll 2
     for (int i = 2; i <= np - 2; i++) {
-        const double Fi = (i <= np - 3) ? F : 0.0;
-        const double inv = 1.0 / a1;                 // one division per row
-        const double ratio1 = a2 * inv;
-        b1 = b1 - ratio1 * a2;
-        const double c2 = E - ratio1 * Fi;
-        const double ratio2 = Fi * inv;
-        const double c1 = D - ratio2 * Fi;
-        w.s1(i) = (MRatio)ratio1;
-        w.s2(i) = (MRatio)ratio2;
+        double inv, ratio1, ratio2;
+        if (i < ks || i == np - 2) {
+            const double Fi = (i <= np - 3) ? F : 0.0;
+            inv = 1.0 / a1;                          // one division per row
+            ratio1 = a2 * inv;
+            const double b1n = b1 - ratio1 * a2;
+            const double c2 = E - ratio1 * Fi;
+            ratio2 = Fi * inv;
+            const double c1 = D - ratio2 * Fi;
+            const MRatio q1 = (MRatio)ratio1, q2 = (MRatio)ratio2;
+            if (i > 2 && i < np - 2 && q1 == pr1 && q2 == pr2) {
+                ks = i;
+                hinv = inv;
+                hr1 = ratio1;
+                hr2 = ratio2;
+            } else {
+                w.s1(i) = q1;
+                w.s2(i) = q2;
+                a1 = b1n;
+                a2 = c2;
+                b1 = c1;
+            }
+            pr1 = q1;
+            pr2 = q2;
+        } else {
+            inv = hinv;
+            ratio1 = hr1;
+            ratio2 = hr2;
+        }
         w.u(i) = (MU)(ucur * inv);
         ym = y0;
         y0 = yp;
@@ -480,9 +507,6 @@ __device__ double m_chol1d(const MSpline<NPMAX>& w, const MFit& f, double p, dou
         uprev = ucur;
         ucur = unext;
         r2prev = ratio2;
-        a1 = b1;
-        a2 = c2;
-        b1 = c1;
     }
     // back substitution, descending, with qu and its sum of squares:
     // raw(k) = (u(k) - u(k-1))/h for 2 <= k <= np, raw(1) = raw(np+1) = 0,
@@ -506,7 +530,10 @@ __device__ double m_chol1d(const MSpline<NPMAX>& w, const MFit& f, double p, dou
     }
 #pragma unroll 2
     for (int i = np - 2; i >= 2; i--) {
-        const double ui = (double)w.u(i) - up1 * (double)w.s1(i) - up2 * (double)w.s2(i);
+        const bool held = (i >= ks && i <= np - 3);
+        const double s1v = held ? (double)(MRatio)hr1 : (double)w.s1(i);
+        const double s2v = held ? (double)(MRatio)hr2 : (double)w.s2(i);
+        const double ui = (double)w.u(i) - up1 * s1v - up2 * s2v;
         if (store_u) w.u(i) = (MU)ui;
         const double raw = (up1 - ui) * f.rh;        // raw(i+1)
         const double fin = rawp - raw;               // qu(i+1)
