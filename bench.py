@@ -523,7 +523,8 @@ def features_run(args):
     read-back into page-locked arrays); LL2ij of every particle from lon/lat
     (rp_locate_lonlat, end to end) against the oracle's LL2ij on a
     single-threaded sample; InitGrid's nest maps hashed against the
-    reference's search on a parent 400x300 / child 240x180 pair."""
+    reference's search on a parent 400x300 / child 240x180 pair.  The
+    "mixed/" variants run the mixed-precision form instead."""
     import torch
     from romspath_b200 import Tracker
     from romspath_b200.tracker import nest_maps
@@ -549,14 +550,16 @@ def features_run(args):
         ("behave10+wetdry", dict(synth.FUCHS_SAMPLE, behavior=10, va_flag=0, wetdry=1)),
         ("all", dict(synth.FUCHS_SAMPLE, behavior=10, va_flag=0, wetdry=1, **synth_diag)),
     ]
-    variants += [("passive/split", {}), ("all/split", variants[-1][1])]
+    variants += [("passive/split", {}), ("all/split", variants[-1][1]),
+                 ("mixed/passive", {}), ("mixed/diagnostics", dict(synth_diag))]
     if args.variants:
         keep = set(args.variants.split(","))
         variants = [v for v in variants if v[0] in keep]
     steps = {}
     for name, pov in variants:
         params = dict(params0, **pov)
-        T = Tracker([spec], [grid], params, numpar=npart, field_dtype=spec.field_dtype, stokes=spec.stokes,
+        form = "mixed" if name.startswith("mixed/") else spec.field_dtype
+        T = Tracker([spec], [grid], params, numpar=npart, field_dtype=form, stokes=spec.stokes,
                     seed=7, resort=args.resort, variant="split" if name.endswith("/split") else "fused")
         for k, slot in enumerate((1, 2, 3)):
             T.upload_frame(1, slot, frames[k])
@@ -581,8 +584,9 @@ def features_run(args):
         if rec_ms is not None:
             steps[name]["output_record_ms"] = rec_ms
     for name in steps:
-        if "passive" in steps:
-            steps[name]["vs_passive"] = steps[name]["ms_per_step"] / steps["passive"]["ms_per_step"]
+        ref = "mixed/passive" if name.startswith("mixed/") else "passive"
+        if ref in steps:
+            steps[name]["vs_passive"] = steps[name]["ms_per_step"] / steps[ref]["ms_per_step"]
     if args.no_init:
         print(json.dumps({"mode": "features", "step": steps}), flush=True)
         return

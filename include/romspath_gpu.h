@@ -68,7 +68,8 @@ extern "C" {
 
 /* Diagnostics switches, rp_params.reserved[3] (namelist "other",
  * ROMSPath.h:325-330; computed at the end of update_particles' particle
- * loop, ROMSPath.f90:935-986).  F64 and F32 forms only. */
+ * loop, ROMSPath.f90:935-986).  Every form; the mixed forms hold the
+ * diagnostics' fields in FP32. */
 #define RP_DIAG_SALTTEMP 1       /* SaltTempOn: P_Salt, P_Temp               */
 #define RP_DIAG_SALTTEMP_MEAN 2  /* SaltTempMean: their running sums         */
 #define RP_DIAG_BOTTOM 4         /* WriteBottom: P_HOB, P_bustr, P_bvstr     */

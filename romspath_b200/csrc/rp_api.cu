@@ -440,12 +440,12 @@ int upload_frame(rp_ctx* ctx, int32_t ng, int32_t slot, const S* zeta, const S* 
     if ((rc = upload_field<S>(ctx, w, nullptr, G.w, nx, ny, N + 1, phys, mx, G.qs_w)) != RP_OK) return rc;
     if ((rc = upload_field<S>(ctx, aks, nullptr, G.aks, nx, ny, N + 1, phys, mx, G.qs_aks)) != RP_OK) return rc;
     if (ctx->diag & RP_DIAG_SALTTEMP) {
-        if ((rc = upload_field<S>(ctx, salt, nullptr, G.salt, nx, ny, N, phys)) != RP_OK) return rc;
-        if ((rc = upload_field<S>(ctx, temp, nullptr, G.temp, nx, ny, N, phys)) != RP_OK) return rc;
+        if ((rc = upload_field<S>(ctx, salt, nullptr, G.salt, nx, ny, N, phys, mx)) != RP_OK) return rc;
+        if ((rc = upload_field<S>(ctx, temp, nullptr, G.temp, nx, ny, N, phys, mx)) != RP_OK) return rc;
     }
     if (ctx->diag & RP_DIAG_BOTTOM) {
-        if ((rc = upload_field<S>(ctx, bustr, nullptr, G.bustr, nx - 1, ny, 1, phys)) != RP_OK) return rc;
-        if ((rc = upload_field<S>(ctx, bvstr, nullptr, G.bvstr, nx, ny - 1, 1, phys)) != RP_OK) return rc;
+        if ((rc = upload_field<S>(ctx, bustr, nullptr, G.bustr, nx - 1, ny, 1, phys, mx)) != RP_OK) return rc;
+        if ((rc = upload_field<S>(ctx, bvstr, nullptr, G.bvstr, nx, ny - 1, 1, phys, mx)) != RP_OK) return rc;
     }
     if (ctx->beh.va) {
         if ((rc = upload_field<S>(ctx, turbaccel, nullptr, G.turbaccel, nx, ny, N + 1, phys)) != RP_OK) return rc;
@@ -669,8 +669,6 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
         p.field_dtype != RP_FIELD_MIXED_I16)
         return RP_ERR_ARG;
     if (p.reserved[3] & ~(RP_DIAG_SALTTEMP | RP_DIAG_SALTTEMP_MEAN | RP_DIAG_BOTTOM)) return RP_ERR_ARG;
-    if (p.reserved[3] && (p.field_dtype == RP_FIELD_MIXED || p.field_dtype == RP_FIELD_MIXED_I16))
-        return RP_ERR_UNSUPPORTED;
     if (p.reserved[4] != 0 && p.reserved[4] != 1) return RP_ERR_ARG;
     if (p.reserved[4] && (p.field_dtype == RP_FIELD_MIXED || p.field_dtype == RP_FIELD_MIXED_I16))
         return RP_ERR_UNSUPPORTED;
@@ -757,11 +755,13 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
         cudaMemset(G.v, 0, nv * G.N * e);
         cudaMemset(G.w, 0, n2 * sw * e);
         cudaMemset(G.aks, 0, n2 * sw * e);
+        // the diagnostics' fields: FP32 in the mixed form
+        const size_t ed = (size_t)(ctx->mixed ? 4 : ctx->elem) * RP_SLOTS;
         if (ctx->diag & RP_DIAG_SALTTEMP) {
-            if (dalloc(&G.salt, n2 * G.N * e) || dalloc(&G.temp, n2 * G.N * e))
+            if (dalloc(&G.salt, n2 * G.N * ed) || dalloc(&G.temp, n2 * G.N * ed))
                 return bail(RP_ERR_NOMEM, "salt/temp ring allocation");
-            cudaMemset(G.salt, 0, n2 * G.N * e);
-            cudaMemset(G.temp, 0, n2 * G.N * e);
+            cudaMemset(G.salt, 0, n2 * G.N * ed);
+            cudaMemset(G.temp, 0, n2 * G.N * ed);
         }
         if (ctx->wetdry) {
             if (dalloc(&G.wd_rho, n2 * RP_SLOTS) || dalloc(&G.wd_u, nu * RP_SLOTS) || dalloc(&G.wd_v, nv * RP_SLOTS))
@@ -771,10 +771,10 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
             cudaMemset(G.wd_v, 0, nv * RP_SLOTS);
         }
         if (ctx->diag & RP_DIAG_BOTTOM) {
-            if (dalloc(&G.bustr, nu * e) || dalloc(&G.bvstr, nv * e))
+            if (dalloc(&G.bustr, nu * ed) || dalloc(&G.bvstr, nv * ed))
                 return bail(RP_ERR_NOMEM, "bottom stress ring allocation");
-            cudaMemset(G.bustr, 0, nu * e);
-            cudaMemset(G.bvstr, 0, nv * e);
+            cudaMemset(G.bustr, 0, nu * ed);
+            cudaMemset(G.bvstr, 0, nv * ed);
         }
         if (ctx->mixed) {
             const size_t qn = (size_t)RP_SLOTS * sw * 4;
@@ -1261,6 +1261,10 @@ int rp_output_record(rp_ctx* ctx, int64_t n, int32_t mI, double* lon, double* la
     RpStepArgs A{};
     fill_params(ctx, A);
     fill_grids(ctx, A, 1, 1, 1);
+    if (ctx->mixed) {                          // the FP64 columns from the compensated FP32 positions
+        CK(rp::launch_mixed_convert(A.p, 1, s));
+        ctx->launches++;
+    }
     CK(rp::launch_output(A, o, ctx->permuted ? 1 : 0, ctx->state_base, n, mI, s));
     ctx->launches++;
     for (int c = 0; c < kOutCols; c++) {

@@ -760,6 +760,74 @@ __device__ __forceinline__ void m_kahan_add(float& p, float& c, float d) {
     p = t;
 }
 
+// ------------------------------------------------------- diagnostics
+
+// A field stored as FP32 for the four ring slots of each (point, level)
+// (the diagnostics' fields in this form): value at level lev of the corner
+// set, time-interpolated with the slot weights.
+__device__ __forceinline__ float m_f32_level(const float4* f, const int64_t o[4], const float cff[4],
+                                             const bool use[4], int nlev, int lev, const MTime& t) {
+    float acc = 0.f;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        if (use[q]) {
+            const float4 v = __ldg(f + o[q] * nlev + lev - 1);
+            acc += cff[q] * (t.wb * m_pick4(v, t.sb) + t.wc * m_pick4(v, t.sc) + t.wf * m_pick4(v, t.sf));
+        }
+    }
+    return acc;
+}
+
+// The diagnostics that close update_particles' particle loop
+// (ROMSPath.f90:935-986) in this form: at the particle's new position and
+// grid, with the step's tdepth; the bottom stress on the u / v corner sets
+// (getInterpStr's rules) and salt / temp on the rho levels bracketing z at
+// the time-interpolated zeta (as u and v are here), the b, c, f slots
+// folded as Lagrange weights.  Out of line: the step keeps its registers
+// when the diagnostics are off.
+__device__ __noinline__ void m_diag_one(const RpStepArgs& A, int64_t n, float tdepth, uint32_t& fl) {
+    const RpParticlesDev& P = A.p;
+    const RpGridDev& g = A.g[P.gid[n] - 1];
+    const float X = P.x32[n] - P.cx[n], Y = P.y32[n] - P.cy[n], Z = P.z32[n] - P.cz[n];
+    const MTime t = m_time(A, g, 0);
+    const bool all[4] = {true, true, true, true};
+    if (A.diag & RP_DIAG_BOTTOM_D) {                       // 935-952
+        const double btemp = -1.0 * (double)tdepth + (double)Z;
+        const double hob0 = P.hob[n];
+        const double hob = (btemp < hob0) ? btemp : hob0;
+        P.hob[n] = hob;
+        if (btemp == hob) {
+            MUV c;
+            m_uv_cell(g, X, Y, true, c, fl);
+            P.bustr[n] = (double)m_f32_level(reinterpret_cast<const float4*>(g.bustr), c.o, c.cff, c.use, 1, 1, t);
+            m_uv_cell(g, X, Y, false, c, fl);
+            P.bvstr[n] = (double)m_f32_level(reinterpret_cast<const float4*>(g.bvstr), c.o, c.cff, c.use, 1, 1, t);
+        }
+    }
+    if (A.diag & RP_DIAG_SALTTEMP_D) {                     // 962-986
+        MRho c;
+        m_rho_cell(g, X, Y, c, fl);
+        const float zeta = m_zeta(g, c, t);
+        MPick Lr, Lw;
+        uint32_t wfl = 0;                                  // the w bracket is not used here
+        m_walk2(g, zeta, tdepth, Z, Lr, Lw, wfl);
+        const float* cw = c.wet4 ? c.cb : c.ci;
+        const float4* fs = reinterpret_cast<const float4*>(g.salt);
+        const float4* ft = reinterpret_cast<const float4*>(g.temp);
+        const int N = g.N;
+        const float sb = m_f32_level(fs, c.o, cw, all, N, Lr.ibot, t), st = m_f32_level(fs, c.o, cw, all, N, Lr.itop, t);
+        const float tb = m_f32_level(ft, c.o, cw, all, N, Lr.ibot, t), tt = m_f32_level(ft, c.o, cw, all, N, Lr.itop, t);
+        const double s = (double)(Lr.z1 * sb + Lr.z2 * st);
+        const double tp = (double)(Lr.z1 * tb + Lr.z2 * tt);
+        P.salt[n] = s;
+        P.temp[n] = tp;
+        if (A.diag & RP_DIAG_MEAN_D) {
+            P.mean_salt[n] = P.mean_salt[n] + s;
+            P.mean_temp[n] = P.mean_temp[n] + tp;
+        }
+    }
+}
+
 // ----------------------------------------------------------- one particle
 
 // VTurb of one particle on its own (the first kernel of the split form),
@@ -923,5 +991,6 @@ __device__ void m_update_one(const RpStepArgs& A, int64_t n, const MSpline<NPMAX
         Pt.isin[n] = 1;
         Pt.status[n] = -9.0;
     }
+    if (A.diag) m_diag_one(A, n, tdepth, fl);
     if (fl) Pt.flags[n] |= fl;
 }

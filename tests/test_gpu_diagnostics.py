@@ -102,9 +102,6 @@ def test_output_reset_between_records():
 
 def test_refusals():
     case = harness.make_case("tiny", 50, seed=3, spec_over={"diag": True}, param_over=harness.DIAG_PARAMS)
-    # the mixed form has no diagnostics
-    with pytest.raises(RomsPathError, match="UNSUPPORTED"):
-        Tracker(case.specs, case.grids, case.params, numpar=50, field_dtype="mixed")
     T = Tracker(case.specs, case.grids, case.params, numpar=50)
     # an upload without the diagnostics' fields is refused
     f = {k: v for k, v in case.frame(1).items() if k not in ("salt", "temp", "bustr", "bvstr")}
