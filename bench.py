@@ -551,7 +551,8 @@ def features_run(args):
         ("all", dict(synth.FUCHS_SAMPLE, behavior=10, va_flag=0, wetdry=1, **synth_diag)),
     ]
     variants += [("passive/split", {}), ("all/split", variants[-1][1]),
-                 ("mixed/passive", {}), ("mixed/diagnostics", dict(synth_diag))]
+                 ("mixed/passive", {}), ("mixed/diagnostics", dict(synth_diag)),
+                 ("mixed/behave10", dict(synth.FUCHS_SAMPLE, behavior=10, va_flag=0))]
     if args.variants:
         keep = set(args.variants.split(","))
         variants = [v for v in variants if v[0] in keep]

@@ -259,7 +259,7 @@ int rp_get_particles(rp_ctx *ctx, int64_t n, double *x, double *y, double *z, do
  * vertical displacement.  Call before the first frame upload and before
  * rp_set_noise_hook (the hook then holds 2 + idt/deltat + 7 draws per
  * particle-step: behave's two normals, then its five uniforms in (0,1)).
- * F64 and F32 forms. */
+ * Every form; the mixed forms hold behave's fields in FP32. */
 typedef struct rp_behavior {
     int32_t behavior, process_va, process_wa, va_flag;
     double swimfast;                     /* m/s (Behavior 1)                  */

@@ -448,12 +448,12 @@ int upload_frame(rp_ctx* ctx, int32_t ng, int32_t slot, const S* zeta, const S* 
         if ((rc = upload_field<S>(ctx, bvstr, nullptr, G.bvstr, nx, ny - 1, 1, phys, mx)) != RP_OK) return rc;
     }
     if (ctx->beh.va) {
-        if ((rc = upload_field<S>(ctx, turbaccel, nullptr, G.turbaccel, nx, ny, N + 1, phys)) != RP_OK) return rc;
-        if ((rc = upload_field<S>(ctx, turbvort, nullptr, G.turbvort, nx, ny, N + 1, phys)) != RP_OK) return rc;
+        if ((rc = upload_field<S>(ctx, turbaccel, nullptr, G.turbaccel, nx, ny, N + 1, phys, mx)) != RP_OK) return rc;
+        if ((rc = upload_field<S>(ctx, turbvort, nullptr, G.turbvort, nx, ny, N + 1, phys, mx)) != RP_OK) return rc;
     }
     if (ctx->beh.wa) {
-        if ((rc = upload_field<S>(ctx, waveaccelu, nullptr, G.waveaccelu, nx, ny, N + 1, phys)) != RP_OK) return rc;
-        if ((rc = upload_field<S>(ctx, waveaccelv, nullptr, G.waveaccelv, nx, ny, N + 1, phys)) != RP_OK) return rc;
+        if ((rc = upload_field<S>(ctx, waveaccelu, nullptr, G.waveaccelu, nx, ny, N + 1, phys, mx)) != RP_OK) return rc;
+        if ((rc = upload_field<S>(ctx, waveaccelv, nullptr, G.waveaccelv, nx, ny, N + 1, phys, mx)) != RP_OK) return rc;
     }
     if (ctx->wetdry) {
         if ((rc = upload_mask(ctx, wd_rho, G.wd_rho, (int64_t)nx * ny, phys)) != RP_OK) return rc;
@@ -661,8 +661,6 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
     const rp_params& p = *params;
     if (ngrid < 1 || ngrid > RP_MAXNGRID || p.numpar < 0 || p.idt <= 0 || p.dt <= 0) return RP_ERR_ARG;
     if (p.behavior != 0 && p.behavior != 1 && p.behavior != 10 && p.behavior != 11) return RP_ERR_UNSUPPORTED;
-    if (p.behavior != 0 && (p.field_dtype == RP_FIELD_MIXED || p.field_dtype == RP_FIELD_MIXED_I16))
-        return RP_ERR_UNSUPPORTED;
     if (p.nsb < 0 || p.nsb > 2) return RP_ERR_ARG;
     if (!(p.deltat >= 1.0) || !(p.sub > 0.0)) return RP_ERR_ARG;
     if (p.field_dtype != RP_FIELD_F64 && p.field_dtype != RP_FIELD_F32 && p.field_dtype != RP_FIELD_MIXED &&
@@ -1277,7 +1275,6 @@ int rp_output_record(rp_ctx* ctx, int64_t n, int32_t mI, double* lon, double* la
 
 int rp_set_behavior(rp_ctx* ctx, const rp_behavior* b) {
     if (!ctx || !b) return RP_ERR_ARG;
-    if (ctx->mixed) return fail(ctx, RP_ERR_UNSUPPORTED, "rp_set_behavior: not available in the mixed form");
     if (b->behavior != ctx->prm.behavior)
         return fail(ctx, RP_ERR_ARG, "rp_set_behavior: behavior differs from rp_params.behavior");
     if (b->va_flag < 0 || b->va_flag > 2) return fail(ctx, RP_ERR_ARG, "rp_set_behavior: va_flag must be 0, 1 or 2");
@@ -1298,7 +1295,7 @@ int rp_set_behavior(rp_ctx* ctx, const rp_behavior* b) {
     d.vort_cr = b->vort_cr; d.vort_sat = b->vort_sat; d.b0pv = b->b0pv; d.b1pv = b->b1pv; d.b0wv = b->b0wv;
     d.b1w = b->b1w; d.acc_cr = b->acc_cr; d.acc_sat = b->acc_sat; d.b0pa = b->b0pa; d.b1pa = b->b1pa;
     d.b0wa = b->b0wa;
-    const size_t e = (size_t)ctx->elem * RP_SLOTS;
+    const size_t e = (size_t)(ctx->mixed ? 4 : ctx->elem) * RP_SLOTS;   // FP32 in the mixed form
     for (int k = 0; k < ctx->ngrid; k++) {
         GridBuf& G = ctx->g[k];
         const size_t nw = (size_t)G.nx * G.ny * (G.N + 1) * e;

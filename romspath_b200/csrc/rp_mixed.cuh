@@ -828,6 +828,46 @@ __device__ __noinline__ void m_diag_one(const RpStepArgs& A, int64_t n, float td
     }
 }
 
+// behave (behavior_module.f90:186-393) in this form: its four fields held
+// in FP32, gathered at the start position's rho cell on the w levels that
+// bracket Zpar at the time-interpolated zeta (as w is here), the slots
+// folded as Lagrange weights; then the response the exact form uses (FP64,
+// own exp/log, the same draws).  Out of line, as the diagnostics.
+__device__ __noinline__ double m_behave(const RpStepArgs& A, int64_t n, const RpGridDev& g, float Xpar, float Ypar,
+                                        float Zpar, uint32_t pid, uint32_t& fl) {
+    const RpBehaviorDev& b = A.beh;
+    double wb = 0.0;
+    if (b.va || b.wa) {
+        MRho c;
+        m_rho_cell(g, Xpar, Ypar, c, fl);
+        const MTime t = m_time(A, g, 0);
+        const float depth = -m_bil(g.h, c);
+        const float zeta = m_zeta(g, c, t);
+        MPick Lr, Lw;
+        m_walk2(g, zeta, depth, Zpar, Lr, Lw, fl);
+        const float* cw = c.wet4 ? c.cb : c.ci;
+        const bool all[4] = {true, true, true, true};
+        const int nl = g.N + 1;
+        auto col = [&](const void* f) -> double {
+            const float4* p4 = reinterpret_cast<const float4*>(f);
+            const float vb = m_f32_level(p4, c.o, cw, all, nl, Lw.ibot, t);
+            const float vt = (Lw.itop == Lw.ibot) ? vb : m_f32_level(p4, c.o, cw, all, nl, Lw.itop, t);
+            return (double)(Lw.z1 * vb + Lw.z2 * vt);
+        };
+        double sa = 0.0, sv = 0.0, su = 0.0, sw = 0.0;
+        if (b.va) {
+            sa = RP_MUL(col(g.turbaccel), 100.0);
+            sv = col(g.turbvort);
+        }
+        if (b.wa) {
+            su = RP_MUL(col(g.waveaccelu), 100.0);
+            sw = RP_MUL(col(g.waveaccelv), 100.0);
+        }
+        wb = rp_behave_swim(A, n, pid, sa, sv, su, sw);
+    }
+    return rp_behave_z(A, wb);
+}
+
 // ----------------------------------------------------------- one particle
 
 // VTurb of one particle on its own (the first kernel of the split form),
@@ -934,6 +974,8 @@ __device__ void m_update_one(const RpStepArgs& A, int64_t n, const MSpline<NPMAX
         Pt.qwarm[n] = q;
         Pt.gwarm[n] = gs;
     }
+    float ZBehav = 0.f;                                // behave(), ROMSPath.f90:800-804
+    if (A.beh.behavior || A.beh.va || A.beh.wa) ZBehav = (float)m_behave(A, n, g, Xpar, Ypar, Zpar, pid, fl);
     // new position (Kahan), nest hand-off
     float nx = x, ncx = cx, ny = y, ncy = cy;
     m_kahan_add(nx, ncx, AdvectX + TurbHx);
@@ -964,7 +1006,7 @@ __device__ void m_update_one(const RpStepArgs& A, int64_t n, const MSpline<NPMAX
     bool hbot = false, htop = false;
     float nz = z, ncz = cz;
     if (A.nsb == 0) {
-        m_kahan_add(nz, ncz, AdvectZ + TurbV);
+        m_kahan_add(nz, ncz, AdvectZ + TurbV + ZBehav);
         const float zv = nz - ncz;
         if (zv < tdepth) { nz = tdepth + fabsf(zv - tdepth); ncz = 0.f; hbot = true; }
         if (nz - ncz > P_zeta) { nz = P_zeta - fabsf(nz - ncz - P_zeta); ncz = 0.f; htop = true; }

@@ -575,6 +575,64 @@ __device__ __noinline__ void rp_diag_one(const RpStepArgs& A, int64_t n, double 
     }
 }
 
+// behave's response to the four standard deviations at the particle
+// (behavior_module.f90:285-375): 4 laplace, 2 normal and 1 uniform draws,
+// the Fuchs swim / sink choice into par(:,pAcc/pVort/pbehaveW/pSSF);
+// returns the vertical velocity wb (cm/s).  Real powers are pinned as
+// x**2.0D0 = x*x, r**3.0D0 = (r*r)*r, x**0.5D0 = sqrt(x); exp and log are
+// this project's own.  Shared by both forms of the step.
+__device__ __forceinline__ double rp_behave_swim(const RpStepArgs& A, int64_t n, uint32_t pid, double stdaccturbu,
+                                                 double stdvortturb, double stdaccwaveu, double stdaccwavev) {
+    const RpBehaviorDev& b = A.beh;
+    const double G = 980.0, RHOF = 1.026, MU = 0.010260, RHOP = 1.06;   // ROMSPath.h:15-19
+    double wb;
+    const uint32_t d0 = 2u + (uint32_t)A.loop;
+    const double vortturbu = RP_MUL(stdvortturb, rp_laplace_of(rp_uniform(A, pid, d0, 0)));
+    const double vortturbv = RP_MUL(stdvortturb, rp_laplace_of(rp_uniform(A, pid, d0, 1)));
+    const double vorttot = sqrt(RP_ADD(RP_MUL(vortturbu, vortturbu), RP_MUL(vortturbv, vortturbv)));
+    const double accturbu = RP_MUL(stdaccturbu, rp_laplace_of(rp_uniform(A, pid, d0, 2)));
+    const double accturbv = RP_MUL(stdaccturbu, rp_laplace_of(rp_uniform(A, pid, d0, 3)));
+    const double accwaveu = RP_MUL(stdaccwaveu, rp_normal(A, pid, d0));
+    const double accwavev = RP_MUL(stdaccwavev, rp_normal(A, pid, d0 + 1));
+    const double au = RP_ADD(accturbu, accwaveu), av = RP_ADD(accturbv, accwavev);
+    const double acctot = sqrt(RP_ADD(RP_MUL(au, au), RP_MUL(av, av)));
+    const double c1v = 2.0 / rp_log(b.vort_cr / b.vort_sat);
+    const double c2v = RP_MUL(c1v, rp_log(vorttot / sqrt(RP_MUL(b.vort_cr, b.vort_sat))));
+    const double c1a = 2.0 / rp_log(b.acc_cr / b.acc_sat);
+    const double c2a = RP_MUL(c1a, rp_log(acctot / sqrt(RP_MUL(b.acc_cr, b.acc_sat))));
+    const double ev = rp_exp(RP_MUL(-2.0, c2v)), ea = rp_exp(RP_MUL(-2.0, c2a));
+    const double pswimv = RP_ADD(RP_SUB(b.b1pv, b.b0pv) / RP_ADD(1.0, ev), b.b0pv);
+    const double pswima = RP_ADD(RP_SUB(b.b1pa, b.b0pa) / RP_ADD(1.0, ea), b.b0pa);
+    const double pswim = (b.va_flag == 1) ? pswimv : (b.va_flag == 2) ? pswima : ((pswima < pswimv) ? pswima : pswimv);
+    const double wswimv = RP_ADD(RP_MUL(RP_SUB(b.b1w, b.b0wv), 1.0) / RP_ADD(1.0, ev), b.b0wv);
+    const double wswima = RP_ADD(RP_MUL(RP_SUB(b.b1w, b.b0wa), 1.0) / RP_ADD(1.0, ea), b.b0wa);
+    const double wswim = (b.va_flag == 1) ? wswimv : (b.va_flag == 2) ? wswima : RP_ADD(wswima, wswimv);
+    const double r = b.initsize / 2.0e4;
+    const double t1 = RP_MUL(RP_MUL(RP_MUL(RP_MUL(4.0 / 3.0, G), RP_MUL(RP_MUL(r, r), r)), RHOF), RHOP - RHOF);
+    const double wsink = RP_SUB(RP_MUL(3.0, MU), sqrt(RP_ADD(t1, RP_MUL(9.0, RP_MUL(MU, MU))))) / RP_MUL(r, RHOF);
+    double ssf;
+    if (rp_uniform(A, pid, d0, 4) < pswim) {
+        wb = wswim;
+        ssf = 0.0;
+    } else {
+        wb = wsink;
+        ssf = 1.0;
+    }
+    const RpParticlesDev& P = A.p;
+    P.acc[n] = acctot / 100.0;
+    P.vort[n] = vorttot;
+    P.behavew[n] = wb;
+    P.ssf[n] = ssf;
+    return wb;
+}
+
+// ZBehav of behave (381-391) from the vertical velocity wb
+__device__ __forceinline__ double rp_behave_z(const RpStepArgs& A, double wb) {
+    if (A.beh.behavior == 1) return RP_MUL(A.beh.swimfast, (double)A.idt);
+    if (A.beh.behavior == 10) return RP_MUL(wb, (double)A.idt) / 100.0;
+    return 0.0;
+}
+
 // getInterp3D of a behave field, ztype 2 (the w levels) at one slot
 template <typename T>
 __device__ __forceinline__ double rp_wfield_at(const RpStepArgs& A, const RpGridDev& g, const void* f,
@@ -593,16 +651,12 @@ __device__ __forceinline__ double rp_wfield_at(const RpStepArgs& A, const RpGrid
 // behave (behavior_module.f90:186-393) at the step's (Xpar, Ypar, Zpar) in
 // the particle's grid: with Process_VA / Process_WA the standard deviations
 // of turbulent acceleration and vorticity and of wave acceleration at the
-// particle (240-280), 4 laplace, 2 normal and 1 uniform draws (285-311,
-// 366), the Fuchs swim / sink response (322-375) into par(:,pAcc/pVort/
-// pbehaveW/pSSF); returns ZBehav (381-391).  Real powers are pinned as
-// x**2.0D0 = x*x, r**3.0D0 = (r*r)*r, x**0.5D0 = sqrt(x); exp and log are
-// this file's own.  Out of line: the passive step keeps its registers.
+// particle (240-280), then the response; returns ZBehav.  Out of line: the
+// passive step keeps its registers.
 template <typename T>
 __device__ __noinline__ double rp_behave(const RpStepArgs& A, int64_t n, const RpGridDev& g, double Xpar,
                                          double Ypar, double Zpar, uint32_t pid, uint32_t& fl) {
     const RpBehaviorDev& b = A.beh;
-    const double G = 980.0, RHOF = 1.026, MU = 0.010260, RHOP = 1.06;   // ROMSPath.h:15-19
     double wb = 0.0;
     if (b.va || b.wa) {
         RhoCell c;
@@ -626,47 +680,9 @@ __device__ __noinline__ double rp_behave(const RpStepArgs& A, int64_t n, const R
             stdaccwaveu = RP_MUL(stdaccwaveu, 100.0);
             stdaccwavev = RP_MUL(stdaccwavev, 100.0);
         }
-        const uint32_t d0 = 2u + (uint32_t)A.loop;
-        const double vortturbu = RP_MUL(stdvortturb, rp_laplace_of(rp_uniform(A, pid, d0, 0)));
-        const double vortturbv = RP_MUL(stdvortturb, rp_laplace_of(rp_uniform(A, pid, d0, 1)));
-        const double vorttot = sqrt(RP_ADD(RP_MUL(vortturbu, vortturbu), RP_MUL(vortturbv, vortturbv)));
-        const double accturbu = RP_MUL(stdaccturbu, rp_laplace_of(rp_uniform(A, pid, d0, 2)));
-        const double accturbv = RP_MUL(stdaccturbu, rp_laplace_of(rp_uniform(A, pid, d0, 3)));
-        const double accwaveu = RP_MUL(stdaccwaveu, rp_normal(A, pid, d0));
-        const double accwavev = RP_MUL(stdaccwavev, rp_normal(A, pid, d0 + 1));
-        const double au = RP_ADD(accturbu, accwaveu), av = RP_ADD(accturbv, accwavev);
-        const double acctot = sqrt(RP_ADD(RP_MUL(au, au), RP_MUL(av, av)));
-        const double c1v = 2.0 / rp_log(b.vort_cr / b.vort_sat);
-        const double c2v = RP_MUL(c1v, rp_log(vorttot / sqrt(RP_MUL(b.vort_cr, b.vort_sat))));
-        const double c1a = 2.0 / rp_log(b.acc_cr / b.acc_sat);
-        const double c2a = RP_MUL(c1a, rp_log(acctot / sqrt(RP_MUL(b.acc_cr, b.acc_sat))));
-        const double ev = rp_exp(RP_MUL(-2.0, c2v)), ea = rp_exp(RP_MUL(-2.0, c2a));
-        const double pswimv = RP_ADD(RP_SUB(b.b1pv, b.b0pv) / RP_ADD(1.0, ev), b.b0pv);
-        const double pswima = RP_ADD(RP_SUB(b.b1pa, b.b0pa) / RP_ADD(1.0, ea), b.b0pa);
-        const double pswim = (b.va_flag == 1) ? pswimv : (b.va_flag == 2) ? pswima : ((pswima < pswimv) ? pswima : pswimv);
-        const double wswimv = RP_ADD(RP_MUL(RP_SUB(b.b1w, b.b0wv), 1.0) / RP_ADD(1.0, ev), b.b0wv);
-        const double wswima = RP_ADD(RP_MUL(RP_SUB(b.b1w, b.b0wa), 1.0) / RP_ADD(1.0, ea), b.b0wa);
-        const double wswim = (b.va_flag == 1) ? wswimv : (b.va_flag == 2) ? wswima : RP_ADD(wswima, wswimv);
-        const double r = b.initsize / 2.0e4;
-        const double t1 = RP_MUL(RP_MUL(RP_MUL(RP_MUL(4.0 / 3.0, G), RP_MUL(RP_MUL(r, r), r)), RHOF), RHOP - RHOF);
-        const double wsink = RP_SUB(RP_MUL(3.0, MU), sqrt(RP_ADD(t1, RP_MUL(9.0, RP_MUL(MU, MU))))) / RP_MUL(r, RHOF);
-        double ssf;
-        if (rp_uniform(A, pid, d0, 4) < pswim) {
-            wb = wswim;
-            ssf = 0.0;
-        } else {
-            wb = wsink;
-            ssf = 1.0;
-        }
-        const RpParticlesDev& P = A.p;
-        P.acc[n] = acctot / 100.0;
-        P.vort[n] = vorttot;
-        P.behavew[n] = wb;
-        P.ssf[n] = ssf;
+        wb = rp_behave_swim(A, n, pid, stdaccturbu, stdvortturb, stdaccwaveu, stdaccwavev);
     }
-    if (b.behavior == 1) return RP_MUL(b.swimfast, (double)A.idt);
-    if (b.behavior == 10) return RP_MUL(wb, (double)A.idt) / 100.0;
-    return 0.0;
+    return rp_behave_z(A, wb);
 }
 
 // One particle of update_particles.  With turbv_in non-null the VTurb

@@ -60,8 +60,6 @@ def test_behave_bit_exact(cid, name, npart, nsteps, noise, sov, pov, resort, var
 
 def test_behave_refusals():
     case = harness.make_case("tiny", 50, seed=3, spec_over={"behave": True}, param_over=F10)
-    with pytest.raises(RomsPathError, match="UNSUPPORTED"):
-        Tracker(case.specs, case.grids, case.params, numpar=50, field_dtype="mixed")
     T = Tracker(case.specs, case.grids, case.params, numpar=50)
     f = {k: v for k, v in case.frame(1).items() if k not in ("turbaccel", "turbvort")}
     with pytest.raises(RomsPathError, match="Process_VA"):
