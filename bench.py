@@ -552,7 +552,9 @@ def features_run(args):
     ]
     variants += [("passive/split", {}), ("all/split", variants[-1][1]),
                  ("mixed/passive", {}), ("mixed/diagnostics", dict(synth_diag)),
-                 ("mixed/behave10", dict(synth.FUCHS_SAMPLE, behavior=10, va_flag=0))]
+                 ("mixed/behave10", dict(synth.FUCHS_SAMPLE, behavior=10, va_flag=0)),
+                 ("mixed/wetdry", {"wetdry": 1}),
+                 ("mixed/all", dict(synth.FUCHS_SAMPLE, behavior=10, va_flag=0, wetdry=1, **synth_diag))]
     if args.variants:
         keep = set(args.variants.split(","))
         variants = [v for v in variants if v[0] in keep]

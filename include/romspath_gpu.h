@@ -110,7 +110,7 @@ typedef struct rp_params {
                                             [4]: 1 = WETDRY (the -DWETDRY
                                             build: per-frame wet/dry masks
                                             in getInterp3D and
-                                            getInterpStr; F64/F32 forms);
+                                            getInterpStr; every form);
                                             others 0 */
 } rp_params;
 

@@ -668,8 +668,6 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
         return RP_ERR_ARG;
     if (p.reserved[3] & ~(RP_DIAG_SALTTEMP | RP_DIAG_SALTTEMP_MEAN | RP_DIAG_BOTTOM)) return RP_ERR_ARG;
     if (p.reserved[4] != 0 && p.reserved[4] != 1) return RP_ERR_ARG;
-    if (p.reserved[4] && (p.field_dtype == RP_FIELD_MIXED || p.field_dtype == RP_FIELD_MIXED_I16))
-        return RP_ERR_UNSUPPORTED;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= p.device || p.device < 0) return RP_ERR_NOEXT;
     rp_ctx* ctx = new rp_ctx();

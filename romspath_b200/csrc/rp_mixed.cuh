@@ -125,7 +125,10 @@ struct MUV {
 };
 
 // u / v corner sets with the reference's edge rules (interpolation_module.f90:608-767)
-__device__ __forceinline__ void m_uv_cell(const RpGridDev& g, float ip, float jp, bool is_u, MUV& c, uint32_t& fl) {
+// The masks are mask_u / mask_v, or under WETDRY one ring slot's
+// wetdry_mask_u / _v (mk = the ring, ms = RP_SLOTS, mo = the physical slot).
+__device__ __forceinline__ void m_uv_cell(const RpGridDev& g, float ip, float jp, bool is_u, MUV& c, uint32_t& fl,
+                                          const uint8_t* mk = nullptr, int ms = 1, int mo = 0) {
     float X, Y;
     int ci[4], cj[4];
     float m[4];
@@ -143,8 +146,9 @@ __device__ __forceinline__ void m_uv_cell(const RpGridDev& g, float ip, float jp
         cj[0] = j0; cj[1] = j0; cj[2] = j1; cj[3] = j1;
 #pragma unroll
         for (int k = 0; k < 4; k++) c.o[k] = (int64_t)(cj[k] - 1) * xi_u + (ci[k] - 1);
+        const uint8_t* mm = mk ? mk : g.mu;
 #pragma unroll
-        for (int k = 0; k < 4; k++) m[k] = (float)__ldg(g.mu + c.o[k]);
+        for (int k = 0; k < 4; k++) m[k] = (float)__ldg(mm + c.o[k] * ms + mo);
         if (In >= xi_u) { m[1] = 0.f; m[2] = 0.f; }
         else if (In < 1) { m[0] = 0.f; m[3] = 0.f; }
     } else {
@@ -162,8 +166,9 @@ __device__ __forceinline__ void m_uv_cell(const RpGridDev& g, float ip, float jp
         else { cj[0] = Jn; cj[1] = Jn; cj[2] = Jn + 1; cj[3] = Jn + 1; }
 #pragma unroll
         for (int k = 0; k < 4; k++) c.o[k] = (int64_t)(cj[k] - 1) * xi_v + (ci[k] - 1);
+        const uint8_t* mm = mk ? mk : g.mv;
 #pragma unroll
-        for (int k = 0; k < 4; k++) m[k] = (float)__ldg(g.mv + c.o[k]);
+        for (int k = 0; k < 4; k++) m[k] = (float)__ldg(mm + c.o[k] * ms + mo);
         if (Jn >= eta_v) { m[2] = 0.f; m[3] = 0.f; }
     }
     c.cff[0] = (1.f - X) * (1.f - Y);
@@ -297,6 +302,75 @@ __device__ __forceinline__ float m_col(const void* fv, const float* qs, const in
     return L.z1 * pb + L.z2 * pt;
 }
 
+// ---------------------------------------------- WETDRY: one slot at a time
+//
+// Under WETDRY each ring slot has its own masks, so the corner weights
+// differ by slot and the three slots cannot share one weighted gather:
+// each slot's value is formed with its own weights, then the slot weights
+// are applied (interpolation_module.f90:628-939).
+
+// one slot's value at level lev of a 16-bit field
+template <typename E>
+__device__ __forceinline__ float m_level_slot(const uint2* f, const float4* qs, const int64_t o[4],
+                                              const float cff[4], const bool use[4], int nlev, int lev, int s) {
+    const float sc = m_pick4(__ldg(qs + lev - 1), s);
+    float acc = 0.f;
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+        if (use[q]) acc += cff[q] * m_slot<E>(__ldg(f + o[q] * nlev + lev - 1), s);
+    return acc * sc;
+}
+
+template <typename E>
+__device__ __forceinline__ float m_col_slot(const void* fv, const float* qs, const int64_t o[4], const float cff[4],
+                                            const bool use[4], int nlev, const MPick& L, int s) {
+    const uint2* f = reinterpret_cast<const uint2*>(fv);
+    const float4* q4 = reinterpret_cast<const float4*>(qs);
+    const float pb = m_level_slot<E>(f, q4, o, cff, use, nlev, L.ibot, s);
+    const float pt = (L.itop == L.ibot) ? pb : m_level_slot<E>(f, q4, o, cff, use, nlev, L.itop, s);
+    return L.z1 * pb + L.z2 * pt;
+}
+
+// rho-point weights of one slot: bilinear, or getcoeff's with that slot's
+// wetdry_mask_rho when a corner is dry
+__device__ __forceinline__ void m_rho_wd_cff(const RpGridDev& g, const MRho& c, int s, float cff[4], uint32_t& fl) {
+    float m[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) m[k] = (float)__ldg(g.wd_rho + c.o[k] * RP_SLOTS + s);
+    if (m[0] + m[1] + m[2] + m[3] < 4.f) {
+        m_getcoeff(c.X, c.Y, m, cff, fl);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; k++) cff[k] = c.cb[k];
+    }
+}
+
+// find_currents' u, v, w under WETDRY (out of line: the step keeps its
+// registers when WETDRY is off)
+template <typename E>
+__device__ __noinline__ void m_gather_wd(const RpStepArgs& A, const RpGridDev& g, float X, float Y, const MRho& rc,
+                                         const MPick& Lr, const MPick& Lw, float& U, float& V, float& Wv,
+                                         uint32_t& fl) {
+    const int N = g.N;
+    const bool all[4] = {true, true, true, true};
+    const float wt[3] = {A.lw[1][0], A.lw[1][1], A.lw[1][2]};   // (b, b, c) at ets == 1
+    const int sl[3] = {g.sb, g.sc, g.sf};
+    U = 0.f;
+    V = 0.f;
+    Wv = 0.f;
+    for (int q = 0; q < 3; q++) {
+        if (wt[q] == 0.f) continue;
+        MUV c;
+        m_uv_cell(g, X, Y, true, c, fl, g.wd_u, RP_SLOTS, sl[q]);
+        U += wt[q] * m_col_slot<E>(g.u, g.qs_u, c.o, c.cff, c.use, N, Lr, sl[q]);
+        m_uv_cell(g, X, Y, false, c, fl, g.wd_v, RP_SLOTS, sl[q]);
+        V += wt[q] * m_col_slot<E>(g.v, g.qs_v, c.o, c.cff, c.use, N, Lr, sl[q]);
+        float cw[4];
+        m_rho_wd_cff(g, rc, sl[q], cw, fl);
+        Wv += wt[q] * m_col_slot<E>(g.w, g.qs_w, rc.o, cw, all, N + 1, Lw, sl[q]);
+    }
+}
+
 struct MStage {
     MRho rc;
     float tdepth, zeta;
@@ -331,6 +405,10 @@ __device__ __forceinline__ void m_find_currents(const RpStepArgs& A, const RpGri
     if (Z > S.zeta) Z = S.zeta - 0.001f;
     MPick Lr, Lw;
     m_walk2(g, S.zeta, S.tdepth, Z, Lr, Lw, fl);
+    if (A.wetdry) {
+        m_gather_wd<E>(A, g, X, Y, S.rc, Lr, Lw, U, V, Wv, fl);
+        return;
+    }
     const int N = g.N;
     const MTime tv = m_time(A, g, 1);                  // (b, b, c) at ets == 1
     {
@@ -778,6 +856,63 @@ __device__ __forceinline__ float m_f32_level(const float4* f, const int64_t o[4]
     return acc;
 }
 
+// A field held in FP32 on a rho corner set, levels L, time-interpolated;
+// under WETDRY each slot with its own weights
+__device__ __forceinline__ float m_f32_col(const RpStepArgs& A, const RpGridDev& g, const void* fv, const MRho& c,
+                                           int nlev, const MPick& L, const MTime& t, uint32_t& fl) {
+    const float4* f = reinterpret_cast<const float4*>(fv);
+    const bool all[4] = {true, true, true, true};
+    if (!A.wetdry) {
+        const float* cw = c.wet4 ? c.cb : c.ci;
+        const float vb = m_f32_level(f, c.o, cw, all, nlev, L.ibot, t);
+        const float vt = (L.itop == L.ibot) ? vb : m_f32_level(f, c.o, cw, all, nlev, L.itop, t);
+        return L.z1 * vb + L.z2 * vt;
+    }
+    const float wt[3] = {t.wb, t.wc, t.wf};
+    const int sl[3] = {t.sb, t.sc, t.sf};
+    float acc = 0.f;
+    for (int q = 0; q < 3; q++) {
+        if (wt[q] == 0.f) continue;
+        float cw[4];
+        m_rho_wd_cff(g, c, sl[q], cw, fl);
+        float lv[2];
+        for (int h = 0; h < 2; h++) {
+            const int lev = h ? L.itop : L.ibot;
+            float a = 0.f;
+#pragma unroll
+            for (int k = 0; k < 4; k++) a += cw[k] * m_pick4(__ldg(f + c.o[k] * nlev + lev - 1), sl[q]);
+            lv[h] = a;
+        }
+        acc += wt[q] * (L.z1 * lv[0] + L.z2 * lv[1]);
+    }
+    return acc;
+}
+
+// A field held in FP32 on the u or v corner set (one level), time-
+// interpolated; under WETDRY each slot with its own masks
+__device__ __forceinline__ float m_f32_uv(const RpStepArgs& A, const RpGridDev& g, const void* fv, float X, float Y,
+                                          bool is_u, const MTime& t, uint32_t& fl) {
+    const float4* f = reinterpret_cast<const float4*>(fv);
+    MUV c;
+    if (!A.wetdry) {
+        m_uv_cell(g, X, Y, is_u, c, fl);
+        return m_f32_level(f, c.o, c.cff, c.use, 1, 1, t);
+    }
+    const float wt[3] = {t.wb, t.wc, t.wf};
+    const int sl[3] = {t.sb, t.sc, t.sf};
+    float acc = 0.f;
+    for (int q = 0; q < 3; q++) {
+        if (wt[q] == 0.f) continue;
+        m_uv_cell(g, X, Y, is_u, c, fl, is_u ? g.wd_u : g.wd_v, RP_SLOTS, sl[q]);
+        float a = 0.f;
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            if (c.use[k]) a += c.cff[k] * m_pick4(__ldg(f + c.o[k]), sl[q]);
+        acc += wt[q] * a;
+    }
+    return acc;
+}
+
 // The diagnostics that close update_particles' particle loop
 // (ROMSPath.f90:935-986) in this form: at the particle's new position and
 // grid, with the step's tdepth; the bottom stress on the u / v corner sets
@@ -790,18 +925,14 @@ __device__ __noinline__ void m_diag_one(const RpStepArgs& A, int64_t n, float td
     const RpGridDev& g = A.g[P.gid[n] - 1];
     const float X = P.x32[n] - P.cx[n], Y = P.y32[n] - P.cy[n], Z = P.z32[n] - P.cz[n];
     const MTime t = m_time(A, g, 0);
-    const bool all[4] = {true, true, true, true};
     if (A.diag & RP_DIAG_BOTTOM_D) {                       // 935-952
         const double btemp = -1.0 * (double)tdepth + (double)Z;
         const double hob0 = P.hob[n];
         const double hob = (btemp < hob0) ? btemp : hob0;
         P.hob[n] = hob;
         if (btemp == hob) {
-            MUV c;
-            m_uv_cell(g, X, Y, true, c, fl);
-            P.bustr[n] = (double)m_f32_level(reinterpret_cast<const float4*>(g.bustr), c.o, c.cff, c.use, 1, 1, t);
-            m_uv_cell(g, X, Y, false, c, fl);
-            P.bvstr[n] = (double)m_f32_level(reinterpret_cast<const float4*>(g.bvstr), c.o, c.cff, c.use, 1, 1, t);
+            P.bustr[n] = (double)m_f32_uv(A, g, g.bustr, X, Y, true, t, fl);
+            P.bvstr[n] = (double)m_f32_uv(A, g, g.bvstr, X, Y, false, t, fl);
         }
     }
     if (A.diag & RP_DIAG_SALTTEMP_D) {                     // 962-986
@@ -811,14 +942,8 @@ __device__ __noinline__ void m_diag_one(const RpStepArgs& A, int64_t n, float td
         MPick Lr, Lw;
         uint32_t wfl = 0;                                  // the w bracket is not used here
         m_walk2(g, zeta, tdepth, Z, Lr, Lw, wfl);
-        const float* cw = c.wet4 ? c.cb : c.ci;
-        const float4* fs = reinterpret_cast<const float4*>(g.salt);
-        const float4* ft = reinterpret_cast<const float4*>(g.temp);
-        const int N = g.N;
-        const float sb = m_f32_level(fs, c.o, cw, all, N, Lr.ibot, t), st = m_f32_level(fs, c.o, cw, all, N, Lr.itop, t);
-        const float tb = m_f32_level(ft, c.o, cw, all, N, Lr.ibot, t), tt = m_f32_level(ft, c.o, cw, all, N, Lr.itop, t);
-        const double s = (double)(Lr.z1 * sb + Lr.z2 * st);
-        const double tp = (double)(Lr.z1 * tb + Lr.z2 * tt);
+        const double s = (double)m_f32_col(A, g, g.salt, c, g.N, Lr, t, fl);
+        const double tp = (double)m_f32_col(A, g, g.temp, c, g.N, Lr, t, fl);
         P.salt[n] = s;
         P.temp[n] = tp;
         if (A.diag & RP_DIAG_MEAN_D) {
@@ -845,15 +970,8 @@ __device__ __noinline__ double m_behave(const RpStepArgs& A, int64_t n, const Rp
         const float zeta = m_zeta(g, c, t);
         MPick Lr, Lw;
         m_walk2(g, zeta, depth, Zpar, Lr, Lw, fl);
-        const float* cw = c.wet4 ? c.cb : c.ci;
-        const bool all[4] = {true, true, true, true};
         const int nl = g.N + 1;
-        auto col = [&](const void* f) -> double {
-            const float4* p4 = reinterpret_cast<const float4*>(f);
-            const float vb = m_f32_level(p4, c.o, cw, all, nl, Lw.ibot, t);
-            const float vt = (Lw.itop == Lw.ibot) ? vb : m_f32_level(p4, c.o, cw, all, nl, Lw.itop, t);
-            return (double)(Lw.z1 * vb + Lw.z2 * vt);
-        };
+        auto col = [&](const void* f) -> double { return (double)m_f32_col(A, g, f, c, nl, Lw, t, fl); };
         double sa = 0.0, sv = 0.0, su = 0.0, sw = 0.0;
         if (b.va) {
             sa = RP_MUL(col(g.turbaccel), 100.0);

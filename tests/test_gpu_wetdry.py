@@ -51,8 +51,6 @@ def test_wetdry_bit_exact(cid, name, npart, nsteps, sov, pov, resort, variant):
 
 def test_wetdry_refusals():
     case = harness.make_case("tiny", 50, seed=3, spec_over={"wetdry": True}, param_over=WD)
-    with pytest.raises(RomsPathError, match="UNSUPPORTED"):
-        Tracker(case.specs, case.grids, case.params, numpar=50, field_dtype="mixed")
     T = Tracker(case.specs, case.grids, case.params, numpar=50)
     f = case.frame(1)
     arrs = [np.asfortranarray(f[k]) for k in ("zeta", "u", "v", "w", "aks")]
