@@ -13,13 +13,15 @@
 namespace rp {
 
 // Fused form: one thread per particle for the whole step.
-template <typename E, int NPMAX>
+// FEAT: built with the options beyond the passive step (diagnostics,
+// WETDRY, behave); the passive variant is chosen when they are all off.
+template <typename E, int NPMAX, bool FEAT>
 __global__ void __launch_bounds__(kStepBlock, kMixedMinBlocks) k_step_mixed(const __grid_constant__ RpStepArgs A) {
     double buf[kMixedArrays * (NPMAX + 1)];
     const MSpline<NPMAX> w{buf};
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < A.p.n; n += stride)
-        m_update_one<E, NPMAX>(A, n, w, nullptr);
+        m_update_one<E, NPMAX, FEAT>(A, n, w, nullptr);
 }
 
 // Split form: VTurb alone at a resident-thread count whose spline
@@ -35,13 +37,13 @@ __global__ void __launch_bounds__(kStepBlock, kMixedVtMinBlocks) k_vturb_mixed(c
         m_vturb_one<E, NPMAX>(A, n, w, turbv);
 }
 
-template <typename E>
+template <typename E, bool FEAT>
 __global__ void __launch_bounds__(kStepBlock, kMixedMinBlocks) k_advect_mixed(const __grid_constant__ RpStepArgs A,
                                                              const float* __restrict__ turbv) {
     const MSpline<1> none{nullptr};
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < A.p.n; n += stride)
-        m_update_one<E, 1>(A, n, none, turbv);
+        m_update_one<E, 1, FEAT>(A, n, none, turbv);
 }
 
 template <class K>
@@ -58,14 +60,15 @@ static cudaError_t resident_grid(K kernel, int64_t n, int num_sms, int cap_per_s
     return cudaSuccess;
 }
 
-template <typename E, int NPMAX>
+template <typename E, int NPMAX, bool FEAT>
 static cudaError_t launch_mixed_t(const RpStepArgs& A, float* turbv, int split, cudaStream_t s, int num_sms,
                                   int* nlaunch) {
     int64_t blocks = 0;
     cudaError_t e;
     if (!split || !A.vturb_on) {
-        if ((e = resident_grid(k_step_mixed<E, NPMAX>, A.p.n, num_sms, A.grid_cap, &blocks)) != cudaSuccess) return e;
-        k_step_mixed<E, NPMAX><<<(unsigned)blocks, kStepBlock, 0, s>>>(A);
+        if ((e = resident_grid(k_step_mixed<E, NPMAX, FEAT>, A.p.n, num_sms, A.grid_cap, &blocks)) != cudaSuccess)
+            return e;
+        k_step_mixed<E, NPMAX, FEAT><<<(unsigned)blocks, kStepBlock, 0, s>>>(A);
         *nlaunch += 1;
         return cudaGetLastError();
     }
@@ -74,18 +77,26 @@ static cudaError_t launch_mixed_t(const RpStepArgs& A, float* turbv, int split, 
     k_vturb_mixed<E, NPMAX><<<(unsigned)blocks, kStepBlock, 0, s>>>(A, turbv);
     *nlaunch += 1;
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if ((e = resident_grid(k_advect_mixed<E>, A.p.n, num_sms, A.grid_cap, &blocks)) != cudaSuccess) return e;
-    k_advect_mixed<E><<<(unsigned)blocks, kStepBlock, 0, s>>>(A, turbv);
+    if ((e = resident_grid(k_advect_mixed<E, FEAT>, A.p.n, num_sms, A.grid_cap, &blocks)) != cudaSuccess) return e;
+    k_advect_mixed<E, FEAT><<<(unsigned)blocks, kStepBlock, 0, s>>>(A, turbv);
     *nlaunch += 1;
     return cudaGetLastError();
+}
+
+template <typename E, bool FEAT>
+static cudaError_t launch_mixed_f(const RpStepArgs& A, int npmax, float* turbv, int split, cudaStream_t s,
+                                  int num_sms, int* nlaunch) {
+    if (npmax <= 88) return launch_mixed_t<E, 88, FEAT>(A, turbv, split, s, num_sms, nlaunch);
+    if (npmax <= 128) return launch_mixed_t<E, 128, FEAT>(A, turbv, split, s, num_sms, nlaunch);
+    return launch_mixed_t<E, 144, FEAT>(A, turbv, split, s, num_sms, nlaunch);
 }
 
 template <typename E>
 static cudaError_t launch_mixed_e(const RpStepArgs& A, int npmax, float* turbv, int split, cudaStream_t s,
                                   int num_sms, int* nlaunch) {
-    if (npmax <= 88) return launch_mixed_t<E, 88>(A, turbv, split, s, num_sms, nlaunch);
-    if (npmax <= 128) return launch_mixed_t<E, 128>(A, turbv, split, s, num_sms, nlaunch);
-    return launch_mixed_t<E, 144>(A, turbv, split, s, num_sms, nlaunch);
+    const bool feat = A.diag || A.wetdry || A.beh.behavior || A.beh.va || A.beh.wa;
+    return feat ? launch_mixed_f<E, true>(A, npmax, turbv, split, s, num_sms, nlaunch)
+                : launch_mixed_f<E, false>(A, npmax, turbv, split, s, num_sms, nlaunch);
 }
 
 cudaError_t launch_step_mixed(const RpStepArgs& A, int npmax, int i16, float* turbv, int split, cudaStream_t s,

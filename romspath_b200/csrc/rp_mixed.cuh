@@ -394,8 +394,9 @@ __device__ __forceinline__ MTime m_time(const RpStepArgs& A, const RpGridDev& g,
 }
 
 // find_currents (advection_module.f90:129-350) in FP32 on 16-bit fields;
-// Z is INOUT.  E is the 16-bit storage type of u, v, w.
-template <typename E>
+// Z is INOUT.  E is the 16-bit storage type of u, v, w; FEAT: a kernel
+// built for the options beyond the passive step (here WETDRY).
+template <typename E, bool FEAT>
 __device__ __forceinline__ void m_find_currents(const RpStepArgs& A, const RpGridDev& g, float X, float Y, float& Z,
                                                 float& U, float& V, float& Wv, uint32_t& fl) {
     MStage S;
@@ -405,7 +406,7 @@ __device__ __forceinline__ void m_find_currents(const RpStepArgs& A, const RpGri
     if (Z > S.zeta) Z = S.zeta - 0.001f;
     MPick Lr, Lw;
     m_walk2(g, S.zeta, S.tdepth, Z, Lr, Lw, fl);
-    if (A.wetdry) {
+    if (FEAT && A.wetdry) {
         m_gather_wd<E>(A, g, X, Y, S.rc, Lr, Lw, U, V, Wv, fl);
         return;
     }
@@ -1016,7 +1017,10 @@ __device__ void m_vturb_one(const RpStepArgs& A, int64_t n, const MSpline<NPMAX>
 
 // One particle of update_particles in the mixed form.  With turbv_in
 // non-null the VTurb displacement comes from the split form's first kernel.
-template <typename E, int NPMAX>
+// FEAT: the kernel variant with the options beyond the passive step (the
+// diagnostics, WETDRY, behave); the passive variant carries none of their
+// code.
+template <typename E, int NPMAX, bool FEAT>
 __device__ void m_update_one(const RpStepArgs& A, int64_t n, const MSpline<NPMAX>& w, const float* turbv_in) {
     const RpParticlesDev& Pt = A.p;
     if (!rp_active(A, n)) return;
@@ -1056,7 +1060,7 @@ __device__ void m_update_one(const RpStepArgs& A, int64_t n, const MSpline<NPMAX
                 ys = Ypar + ky * half_dt;
                 zs = Zpar + kz * half_dt;
             }
-            m_find_currents<E>(A, g, xs, ys, zs, U, V, Wv, fl);
+            m_find_currents<E, FEAT>(A, g, xs, ys, zs, U, V, Wv, fl);
             if (st == 0) Zpar = zs;                    // Z is INOUT in find_currents
             kx = U * pm;
             ky = V * pn;
@@ -1093,7 +1097,8 @@ __device__ void m_update_one(const RpStepArgs& A, int64_t n, const MSpline<NPMAX
         Pt.gwarm[n] = gs;
     }
     float ZBehav = 0.f;                                // behave(), ROMSPath.f90:800-804
-    if (A.beh.behavior || A.beh.va || A.beh.wa) ZBehav = (float)m_behave(A, n, g, Xpar, Ypar, Zpar, pid, fl);
+    if (FEAT && (A.beh.behavior || A.beh.va || A.beh.wa))
+        ZBehav = (float)m_behave(A, n, g, Xpar, Ypar, Zpar, pid, fl);
     // new position (Kahan), nest hand-off
     float nx = x, ncx = cx, ny = y, ncy = cy;
     m_kahan_add(nx, ncx, AdvectX + TurbHx);
@@ -1151,6 +1156,6 @@ __device__ void m_update_one(const RpStepArgs& A, int64_t n, const MSpline<NPMAX
         Pt.isin[n] = 1;
         Pt.status[n] = -9.0;
     }
-    if (A.diag) m_diag_one(A, n, tdepth, fl);
+    if (FEAT && A.diag) m_diag_one(A, n, tdepth, fl);
     if (fl) Pt.flags[n] |= fl;
 }
