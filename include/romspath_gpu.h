@@ -307,6 +307,19 @@ int rp_output_record(rp_ctx *ctx, int64_t n, int32_t mI, double *lon, double *la
                      double *age, double *status, double *gid, double *salt, double *temp,
                      double *hob, double *bustr, double *bvstr);
 
+/* rp_output_record without waiting: the record is packed in stream order
+ * (after the steps queued so far, with the writer's resets) and its
+ * columns are copied into the caller's arrays, which must be page-locked,
+ * on a stream of their own while the steps queued next run.  The arrays
+ * may be read (or reused) only after rp_output_wait (or rp_synchronize).
+ * A later record waits for this one's copies before it is packed. */
+int rp_output_record_async(rp_ctx *ctx, int64_t n, int32_t mI, double *lon, double *lat, double *zp,
+                           double *age, double *status, double *gid, double *salt, double *temp,
+                           double *hob, double *bustr, double *bvstr);
+
+/* Wait for the copies of the last rp_output_record_async. */
+int rp_output_wait(rp_ctx *ctx);
+
 /* First particle id of this context (default 0).  Particle k of the next
  * rp_set_particles / rp_locate_particles call gets id base + k; the id keys
  * its Philox noise, so a run split over several contexts (one per GPU) with

@@ -26,6 +26,7 @@ EXPORTS = [
     "rp_tangent", "rp_adj_replay", "rp_step_n", "rp_set_launch", "rp_upload_frame_ext", "rp_upload_frame_ext_f32",
     "rp_get_diagnostics", "rp_reset_diagnostics", "rp_set_grid_lonlat", "rp_output_record", "rp_upload_frame_desc",
     "rp_set_behavior", "rp_get_behavior", "rp_set_grid_angle", "rp_locate_lonlat", "rp_nest_maps",
+    "rp_output_record_async", "rp_output_wait",
 ]
 
 PD = C.POINTER(C.c_double)
@@ -130,6 +131,8 @@ def _declare(L):
     L.rp_nest_maps.argtypes = [C.c_int32, PI32, PI32, C.POINTER(PD), C.POINTER(PD), PD, PD, PD]
     L.rp_get_behavior.argtypes = [P, C.c_int64] + [PD] * 4
     L.rp_output_record.argtypes = [P, C.c_int64, C.c_int32] + [PD] * 11
+    L.rp_output_record_async.argtypes = [P, C.c_int64, C.c_int32] + [PD] * 11
+    L.rp_output_wait.argtypes = [P]
     L.rp_set_particles.argtypes = [P, C.c_int64] + [PD] * 7 + [PI32]
     L.rp_locate_particles.argtypes = [P, C.c_int64, PD, PD, PD, PD, C.c_int32]
     L.rp_step.argtypes = [P, PD, PD, C.c_int32, C.c_int32, C.c_int32, C.c_int32]

@@ -87,6 +87,9 @@ struct rp_ctx {
     bool pin_used[2] = {false, false};
     int pin_next = 0;
     cudaStream_t s_comp = nullptr, s_copy = nullptr;
+    cudaStream_t s_out = nullptr;              // read-back of asynchronous output records
+    cudaEvent_t ev_packed = nullptr, ev_out_done = nullptr;
+    bool out_pending = false;                  // an asynchronous record's copies may be in flight
     // noise hook
     double* hook = nullptr;
     int64_t hook_steps = 0, hook_pos = 0;
@@ -329,6 +332,9 @@ void free_ctx(rp_ctx* c) {
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->s_comp) cudaStreamDestroy(c->s_comp);
     if (c->s_copy) cudaStreamDestroy(c->s_copy);
+    if (c->s_out) cudaStreamDestroy(c->s_out);
+    if (c->ev_packed) cudaEventDestroy(c->ev_packed);
+    if (c->ev_out_done) cudaEventDestroy(c->ev_out_done);
     delete c;
 }
 
@@ -649,6 +655,41 @@ int locate(rp_ctx* ctx, int64_t n, const double* ipos, const double* jpos, const
     return rc;
 }
 
+constexpr int kOutCols = 11;
+
+// Checks, then packs one output record into the device record buffer on
+// the compute stream (after the read-back of an earlier asynchronous
+// record, which shares the buffer); dev[c] receives each column's address.
+int output_pack(rp_ctx* ctx, int64_t n, int32_t mI, double* const host[kOutCols], double* dev[kOutCols]) {
+    const bool lon = host[0] || host[1];
+    if (n < 0 || n > ctx->n) return fail(ctx, RP_ERR_ARG, "rp_output_record: n exceeds particle count");
+    if (lon)
+        for (int k = 0; k < ctx->ngrid; k++)
+            if (!ctx->g[k].lon) return fail(ctx, RP_ERR_STATE, "rp_output_record: lon/lat need rp_set_grid_lonlat");
+    if (((host[6] || host[7]) && !(ctx->diag & RP_DIAG_SALTTEMP)) ||
+        ((host[8] || host[9] || host[10]) && !(ctx->diag & RP_DIAG_BOTTOM)))
+        return fail(ctx, RP_ERR_STATE, "rp_output_record: that diagnostic is off in this context");
+    if ((ctx->diag & RP_DIAG_SALTTEMP_MEAN) && mI < 1)
+        return fail(ctx, RP_ERR_ARG, "rp_output_record: SaltTempMean needs the step count mI >= 1");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->s_comp;
+    if (!ctx->outbuf && dalloc(&ctx->outbuf, (size_t)kOutCols * ctx->cap * 8))
+        return fail(ctx, RP_ERR_NOMEM, "rp_output_record: record buffer");
+    if (ctx->out_pending) CK(cudaStreamWaitEvent(s, ctx->ev_out_done, 0));
+    for (int c = 0; c < kOutCols; c++) dev[c] = host[c] ? ctx->outbuf + (size_t)c * ctx->cap : nullptr;
+    rp::OutCols o{dev[0], dev[1], dev[2], dev[3], dev[4], dev[5], dev[6], dev[7], dev[8], dev[9], dev[10]};
+    RpStepArgs A{};
+    fill_params(ctx, A);
+    fill_grids(ctx, A, 1, 1, 1);
+    if (ctx->mixed) {                          // the FP64 columns from the compensated FP32 positions
+        CK(rp::launch_mixed_convert(A.p, 1, s));
+        ctx->launches++;
+    }
+    CK(rp::launch_output(A, o, ctx->permuted ? 1 : 0, ctx->state_base, n, mI, s));
+    ctx->launches++;
+    return RP_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -834,6 +875,9 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
     }
     if (cudaStreamCreateWithFlags(&ctx->s_comp, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&ctx->s_copy, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->s_out, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->ev_packed, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->ev_out_done, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess)
         return bail(RP_ERR_CUDA, "stream/event creation");
     if (cudaDeviceSynchronize() != cudaSuccess) return bail(RP_ERR_CUDA, "initial upload");
@@ -1237,37 +1281,47 @@ int rp_output_record(rp_ctx* ctx, int64_t n, int32_t mI, double* lon, double* la
                      double* status, double* gid, double* salt, double* temp, double* hob, double* bustr,
                      double* bvstr) {
     if (!ctx) return RP_ERR_ARG;
-    if (n < 0 || n > ctx->n) return fail(ctx, RP_ERR_ARG, "rp_output_record: n exceeds particle count");
-    if ((lon || lat))
-        for (int k = 0; k < ctx->ngrid; k++)
-            if (!ctx->g[k].lon) return fail(ctx, RP_ERR_STATE, "rp_output_record: lon/lat need rp_set_grid_lonlat");
-    if (((salt || temp) && !(ctx->diag & RP_DIAG_SALTTEMP)) || ((hob || bustr || bvstr) && !(ctx->diag & RP_DIAG_BOTTOM)))
-        return fail(ctx, RP_ERR_STATE, "rp_output_record: that diagnostic is off in this context");
-    if ((ctx->diag & RP_DIAG_SALTTEMP_MEAN) && mI < 1)
-        return fail(ctx, RP_ERR_ARG, "rp_output_record: SaltTempMean needs the step count mI >= 1");
-    CK(cudaSetDevice(ctx->device));
-    cudaStream_t s = ctx->s_comp;
-    constexpr int kOutCols = 11;
-    if (!ctx->outbuf && dalloc(&ctx->outbuf, (size_t)kOutCols * ctx->cap * 8))
-        return fail(ctx, RP_ERR_NOMEM, "rp_output_record: record buffer");
     double* host[kOutCols] = {lon, lat, zp, age, status, gid, salt, temp, hob, bustr, bvstr};
     double* dev[kOutCols];
-    for (int c = 0; c < kOutCols; c++) dev[c] = host[c] ? ctx->outbuf + (size_t)c * ctx->cap : nullptr;
-    rp::OutCols o{dev[0], dev[1], dev[2], dev[3], dev[4], dev[5], dev[6], dev[7], dev[8], dev[9], dev[10]};
-    RpStepArgs A{};
-    fill_params(ctx, A);
-    fill_grids(ctx, A, 1, 1, 1);
-    if (ctx->mixed) {                          // the FP64 columns from the compensated FP32 positions
-        CK(rp::launch_mixed_convert(A.p, 1, s));
-        ctx->launches++;
-    }
-    CK(rp::launch_output(A, o, ctx->permuted ? 1 : 0, ctx->state_base, n, mI, s));
-    ctx->launches++;
+    int rc;
+    if ((rc = output_pack(ctx, n, mI, host, dev)) != RP_OK) return rc;
     for (int c = 0; c < kOutCols; c++) {
         if (!host[c]) continue;
-        const int rc = d2h(ctx, host[c], dev[c], (size_t)n * 8, s);
-        if (rc != RP_OK) return rc;
+        if ((rc = d2h(ctx, host[c], dev[c], (size_t)n * 8, ctx->s_comp)) != RP_OK) return rc;
     }
+    return RP_OK;
+}
+
+int rp_output_record_async(rp_ctx* ctx, int64_t n, int32_t mI, double* lon, double* lat, double* zp,
+                           double* age, double* status, double* gid, double* salt, double* temp, double* hob,
+                           double* bustr, double* bvstr) {
+    if (!ctx) return RP_ERR_ARG;
+    double* host[kOutCols] = {lon, lat, zp, age, status, gid, salt, temp, hob, bustr, bvstr};
+    for (int c = 0; c < kOutCols; c++)
+        if (host[c] && n > 0 && !is_pinned(host[c]))
+            return fail(ctx, RP_ERR_ARG, "rp_output_record_async: the arrays must be page-locked");
+    double* dev[kOutCols];
+    int rc;
+    if ((rc = output_pack(ctx, n, mI, host, dev)) != RP_OK) return rc;
+    // the copies run on their own stream once the record is packed; the
+    // steps enqueued next run meanwhile
+    CK(cudaEventRecord(ctx->ev_packed, ctx->s_comp));
+    CK(cudaStreamWaitEvent(ctx->s_out, ctx->ev_packed, 0));
+    for (int c = 0; c < kOutCols; c++) {
+        if (!host[c] || n == 0) continue;
+        CK(cudaMemcpyAsync(host[c], dev[c], (size_t)n * 8, cudaMemcpyDeviceToHost, ctx->s_out));
+    }
+    CK(cudaEventRecord(ctx->ev_out_done, ctx->s_out));
+    ctx->out_pending = true;
+    return RP_OK;
+}
+
+int rp_output_wait(rp_ctx* ctx) {
+    if (!ctx) return RP_ERR_ARG;
+    if (!ctx->out_pending) return RP_OK;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaEventSynchronize(ctx->ev_out_done));
+    ctx->out_pending = false;
     return RP_OK;
 }
 
@@ -1613,6 +1667,8 @@ int rp_synchronize(rp_ctx* ctx) {
     CK(cudaSetDevice(ctx->device));
     CK(cudaStreamSynchronize(ctx->s_copy));
     CK(cudaStreamSynchronize(ctx->s_comp));
+    CK(cudaStreamSynchronize(ctx->s_out));
+    ctx->out_pending = false;
     return RP_OK;
 }
 

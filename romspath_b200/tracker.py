@@ -298,6 +298,16 @@ class Tracker:
         self._check(rc, "rp_output_record")
         return out
 
+    def output_record_async(self, mI: int, out: Dict[str, np.ndarray], n: Optional[int] = None):
+        """rp_output_record_async into page-locked arrays ``out`` (names as
+        output_record); read them after output_wait()."""
+        n = self.n if n is None else n
+        rc = self.L.rp_output_record_async(self.h, n, int(mI), *[_pd(out.get(k)) for k in self.RECORD])
+        self._check(rc, "rp_output_record_async")
+
+    def output_wait(self):
+        self._check(self.L.rp_output_wait(self.h), "rp_output_wait")
+
     def reset_diagnostics(self):
         """The writer's resets after an output record (sums to 0, HOB to 9999)."""
         self._check(self.L.rp_reset_diagnostics(self.h), "rp_reset_diagnostics")
