@@ -908,32 +908,36 @@ def main():
                 keep.append(t)
                 d[k] = arr
             pframes.append(d)
-        out = {}
-        for k in ("x", "y", "z", "age", "status", "gid", "wd", "zeta", "bath"):
-            out[k], t = pinned_empty(npart, np.float64)
-            keep.append(t)
-        out["isin"], t = pinned_empty(npart, np.int32)
-        keep.append(t)
-        out["flags"], t = pinned_empty(npart, np.uint32)
-        keep.append(t)
+        # the dataOutput record (ROMSPath.f90:1012-1024, 1924-1995): lon,
+        # lat, zp, age, status, GID, double-buffered page-locked arrays
+        outs = []
+        for _ in range(2):
+            o = {}
+            for k in ("lon", "lat", "zp", "age", "status", "gid"):
+                o[k], t = pinned_empty(npart, np.float64)
+                keep.append(t)
+            outs.append(o)
         h2d = sum(pframes[0][k].nbytes for k in ("zeta", "u", "v", "w", "aks", "su", "sv") if k in pframes[0])
-        d2h = sum(v.nbytes for v in out.values())
+        d2h = sum(v.nbytes for v in outs[0].values())
 
         def e2e_run(es, f0):
             """The driver's frame intervals, pipelined: interval j's steps are
-            enqueued (one graph), then interval j+1's frame is uploaded into
-            the ring's spare slot while they run, then interval j's particle
-            columns are read back.  Each interval's frame crosses PCIe once
+            enqueued (one graph) with its output record behind them, then
+            interval j+1's frame is uploaded into the ring's spare slot while
+            they run; each record is copied into page-locked arrays while the
+            next interval runs (double-buffered; a record may be read after
+            rp_output_wait).  Each frame and each record crosses PCIe once,
             and the results equal the unpipelined order's (a step binds its
             ring slots when it is enqueued)."""
             for (kf, slot) in es[0].loads:
                 T.upload_frame(1, slot, pframes[f0 % nframes])
             for j, e in enumerate(es):
                 T.step_n(e.internal)
+                T.output_record_async(1, outs[j % 2])
                 if j + 1 < len(es):
                     for (kf, slot) in es[j + 1].loads:
                         T.upload_frame(1, slot, pframes[(f0 + j + 1) % nframes])
-                T.get_particles(npart, out=out)
+            T.output_wait()
 
         base = 2 + args.warmup + args.steps
         e2e_run(exts[base:base + args.warmup], 0)
@@ -950,9 +954,10 @@ def main():
                "ms_per_step": e2e_s * 1e3 / args.steps, "gpu_launches": T.kernel_launches() - l0,
                "form": head,
                "timing": "host clock between device synchronizations; every step uploads one frame "
-                         "(quantised on the device in the mixed form) and reads the particle columns "
-                         "back into page-locked host memory; the next interval's frame is uploaded "
-                         "while the current interval's steps run (one CUDA graph per interval)"}
+                         "(quantised on the device in the mixed form) and reads its dataOutput record "
+                         "(lon, lat, zp, age, status, GID) back into page-locked host memory; the next "
+                         "interval's frame is uploaded and each record copied back while the next "
+                         "steps run (one CUDA graph per interval)"}
     T.close()
 
     # ---------------- roofline of the headline step kernel (algorithmic bytes)
