@@ -857,13 +857,25 @@ __device__ __forceinline__ float m_f32_level(const float4* f, const int64_t o[4]
     return acc;
 }
 
+// Each ring slot's rho weights of a cell under WETDRY, formed once for all
+// the fields gathered there
+struct MRhoWD {
+    float cff[3][4];               // slots b, c, f
+};
+
+__device__ __forceinline__ void m_rho_wd_all(const RpGridDev& g, const MRho& c, const MTime& t, MRhoWD& wd,
+                                             uint32_t& fl) {
+    const int sl[3] = {t.sb, t.sc, t.sf};
+    for (int q = 0; q < 3; q++) m_rho_wd_cff(g, c, sl[q], wd.cff[q], fl);
+}
+
 // A field held in FP32 on a rho corner set, levels L, time-interpolated;
-// under WETDRY each slot with its own weights
+// under WETDRY (wd set) each slot with its own weights
 __device__ __forceinline__ float m_f32_col(const RpStepArgs& A, const RpGridDev& g, const void* fv, const MRho& c,
-                                           int nlev, const MPick& L, const MTime& t, uint32_t& fl) {
+                                           int nlev, const MPick& L, const MTime& t, const MRhoWD* wd) {
     const float4* f = reinterpret_cast<const float4*>(fv);
     const bool all[4] = {true, true, true, true};
-    if (!A.wetdry) {
+    if (!wd) {
         const float* cw = c.wet4 ? c.cb : c.ci;
         const float vb = m_f32_level(f, c.o, cw, all, nlev, L.ibot, t);
         const float vt = (L.itop == L.ibot) ? vb : m_f32_level(f, c.o, cw, all, nlev, L.itop, t);
@@ -874,8 +886,7 @@ __device__ __forceinline__ float m_f32_col(const RpStepArgs& A, const RpGridDev&
     float acc = 0.f;
     for (int q = 0; q < 3; q++) {
         if (wt[q] == 0.f) continue;
-        float cw[4];
-        m_rho_wd_cff(g, c, sl[q], cw, fl);
+        const float* cw = wd->cff[q];
         float lv[2];
         for (int h = 0; h < 2; h++) {
             const int lev = h ? L.itop : L.ibot;
@@ -943,8 +954,11 @@ __device__ __noinline__ void m_diag_one(const RpStepArgs& A, int64_t n, float td
         MPick Lr, Lw;
         uint32_t wfl = 0;                                  // the w bracket is not used here
         m_walk2(g, zeta, tdepth, Z, Lr, Lw, wfl);
-        const double s = (double)m_f32_col(A, g, g.salt, c, g.N, Lr, t, fl);
-        const double tp = (double)m_f32_col(A, g, g.temp, c, g.N, Lr, t, fl);
+        MRhoWD wd;
+        if (A.wetdry) m_rho_wd_all(g, c, t, wd, fl);
+        const MRhoWD* pw = A.wetdry ? &wd : nullptr;
+        const double s = (double)m_f32_col(A, g, g.salt, c, g.N, Lr, t, pw);
+        const double tp = (double)m_f32_col(A, g, g.temp, c, g.N, Lr, t, pw);
         P.salt[n] = s;
         P.temp[n] = tp;
         if (A.diag & RP_DIAG_MEAN_D) {
@@ -972,7 +986,10 @@ __device__ __noinline__ double m_behave(const RpStepArgs& A, int64_t n, const Rp
         MPick Lr, Lw;
         m_walk2(g, zeta, depth, Zpar, Lr, Lw, fl);
         const int nl = g.N + 1;
-        auto col = [&](const void* f) -> double { return (double)m_f32_col(A, g, f, c, nl, Lw, t, fl); };
+        MRhoWD wd;
+        if (A.wetdry) m_rho_wd_all(g, c, t, wd, fl);
+        const MRhoWD* pw = A.wetdry ? &wd : nullptr;
+        auto col = [&](const void* f) -> double { return (double)m_f32_col(A, g, f, c, nl, Lw, t, pw); };
         double sa = 0.0, sv = 0.0, su = 0.0, sw = 0.0;
         if (b.va) {
             sa = RP_MUL(col(g.turbaccel), 100.0);
