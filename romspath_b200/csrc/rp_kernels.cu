@@ -170,8 +170,10 @@ __global__ void k_locate(const __grid_constant__ RpStepArgs A, const double* ipo
             rp_rho_cell(g, X, Y, rc, fl);
             const double tdepth = -1.0 * rp_bil(g.h, rc);
             const double zeta = rp_zeta_at<T>(g, rc, g.sc);
-            s = rp_tracer_at<T>(g, g.salt, rc, zeta, tdepth, Z, g.sc, A.wetdry, fl);
-            t = rp_tracer_at<T>(g, g.temp, rc, zeta, tdepth, Z, g.sc, A.wetdry, fl);
+            double wcf[4];                                 // WETDRY: slot t_c's weights
+            if (A.wetdry) rp_rho_wd_weights(g, rc, g.sc, wcf, fl);
+            s = rp_tracer_at<T>(g, g.salt, rc, zeta, tdepth, Z, g.sc, A.wetdry ? wcf : nullptr);
+            t = rp_tracer_at<T>(g, g.temp, rc, zeta, tdepth, Z, g.sc, A.wetdry ? wcf : nullptr);
             P.wd[n] = (-1.0 * tdepth) + zeta;
             P.zeta[n] = zeta;
             P.bath[n] = -1.0 * tdepth;

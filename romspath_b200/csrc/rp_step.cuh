@@ -503,17 +503,14 @@ __device__ __forceinline__ double rp_str_at(const void* f, const UVCell& c, int 
 // getInterp3D of salt or temp, ztype 1 (interpolation_module.f90:529-558,
 // 769-809): the rho corner set (bilinear, inverse distance with a dry
 // corner) on the rho levels of the slot's own zeta.
+// wcf: under WETDRY the slot's weights from its wetdry_mask_rho
+// (rp_rho_wd_weights, formed once per cell by the caller), else null.
 template <typename T>
 __device__ __forceinline__ double rp_tracer_at(const RpGridDev& g, const void* f, const RhoCell& c, double zeta,
-                                               double depth, double zpar, int slot, int wetdry, uint32_t& fl) {
+                                               double depth, double zpar, int slot, const double* wcf) {
     LevelPick L;
     rp_walk_rho(g, zeta, depth, zpar, L);
-    if (wetdry) {                                          // the slot's wetdry_mask_rho
-        double cff[4];
-        rp_rho_wd_weights(g, c, slot, cff, fl);
-        return rp_col_rho<T>(f, c, cff, g.N, L, slot);
-    }
-    return rp_col_rho<T>(f, c, c.wet4 ? c.cb : c.ci, g.N, L, slot);
+    return rp_col_rho<T>(f, c, wcf ? wcf : (c.wet4 ? c.cb : c.ci), g.N, L, slot);
 }
 
 // The diagnostics that close update_particles' particle loop
@@ -559,13 +556,21 @@ __device__ __noinline__ void rp_diag_one(const RpStepArgs& A, int64_t n, double 
         const double zb = rp_zeta_at<T>(g, c, g.sb);
         const double zc = rp_zeta_at<T>(g, c, g.sc);
         const double zf = rp_zeta_at<T>(g, c, g.sf);
-        const int wd = A.wetdry;
-        const double s = rp_polintd(A.pi, rp_tracer_at<T>(g, g.salt, c, zb, tdepth, Z, g.sb, wd, fl),
-                                    rp_tracer_at<T>(g, g.salt, c, zc, tdepth, Z, g.sc, wd, fl),
-                                    rp_tracer_at<T>(g, g.salt, c, zf, tdepth, Z, g.sf, wd, fl));
-        const double t = rp_polintd(A.pi, rp_tracer_at<T>(g, g.temp, c, zb, tdepth, Z, g.sb, wd, fl),
-                                    rp_tracer_at<T>(g, g.temp, c, zc, tdepth, Z, g.sc, wd, fl),
-                                    rp_tracer_at<T>(g, g.temp, c, zf, tdepth, Z, g.sf, wd, fl));
+        double wcf[3][4];                                  // WETDRY: each slot's weights, once
+        if (A.wetdry) {
+            rp_rho_wd_weights(g, c, g.sb, wcf[0], fl);
+            rp_rho_wd_weights(g, c, g.sc, wcf[1], fl);
+            rp_rho_wd_weights(g, c, g.sf, wcf[2], fl);
+        }
+        const double* wb = A.wetdry ? wcf[0] : nullptr;
+        const double* wc = A.wetdry ? wcf[1] : nullptr;
+        const double* wf = A.wetdry ? wcf[2] : nullptr;
+        const double s = rp_polintd(A.pi, rp_tracer_at<T>(g, g.salt, c, zb, tdepth, Z, g.sb, wb),
+                                    rp_tracer_at<T>(g, g.salt, c, zc, tdepth, Z, g.sc, wc),
+                                    rp_tracer_at<T>(g, g.salt, c, zf, tdepth, Z, g.sf, wf));
+        const double t = rp_polintd(A.pi, rp_tracer_at<T>(g, g.temp, c, zb, tdepth, Z, g.sb, wb),
+                                    rp_tracer_at<T>(g, g.temp, c, zc, tdepth, Z, g.sc, wc),
+                                    rp_tracer_at<T>(g, g.temp, c, zf, tdepth, Z, g.sf, wf));
         P.salt[n] = s;
         P.temp[n] = t;
         if (A.diag & RP_DIAG_MEAN_D) {
@@ -633,19 +638,14 @@ __device__ __forceinline__ double rp_behave_z(const RpStepArgs& A, double wb) {
     return 0.0;
 }
 
-// getInterp3D of a behave field, ztype 2 (the w levels) at one slot
+// getInterp3D of a behave field, ztype 2 (the w levels) at one slot; wcf
+// as for rp_tracer_at
 template <typename T>
-__device__ __forceinline__ double rp_wfield_at(const RpStepArgs& A, const RpGridDev& g, const void* f,
-                                               const RhoCell& c, double zeta, double depth, double zpar, int slot,
-                                               uint32_t& fl) {
+__device__ __forceinline__ double rp_wfield_at(const RpGridDev& g, const void* f, const RhoCell& c, double zeta,
+                                               double depth, double zpar, int slot, const double* wcf, uint32_t& fl) {
     LevelPick L;
     rp_walk_w(g, zeta, depth, zpar, L, fl);
-    if (A.wetdry) {
-        double cff[4];
-        rp_rho_wd_weights(g, c, slot, cff, fl);
-        return rp_col_rho<T>(f, c, cff, g.N + 1, L, slot);
-    }
-    return rp_col_rho<T>(f, c, c.wet4 ? c.cb : c.ci, g.N + 1, L, slot);
+    return rp_col_rho<T>(f, c, wcf ? wcf : (c.wet4 ? c.cb : c.ci), g.N + 1, L, slot);
 }
 
 // behave (behavior_module.f90:186-393) at the step's (Xpar, Ypar, Zpar) in
@@ -664,18 +664,22 @@ __device__ __noinline__ double rp_behave(const RpStepArgs& A, int64_t n, const R
         const double depth = -1.0 * rp_bil(g.h, c);
         const double zt[3] = {rp_zeta_at<T>(g, c, g.sb), rp_zeta_at<T>(g, c, g.sc), rp_zeta_at<T>(g, c, g.sf)};
         const int sl[3] = {g.sb, g.sc, g.sf};
+        double wcf[3][4];                                  // WETDRY: each slot's weights, once
+        if (A.wetdry)
+            for (int q = 0; q < 3; q++) rp_rho_wd_weights(g, c, sl[q], wcf[q], fl);
+        auto wq = [&](int q) -> const double* { return A.wetdry ? wcf[q] : nullptr; };
         double ey[3], stdaccturbu = 0.0, stdvortturb = 0.0, stdaccwaveu = 0.0, stdaccwavev = 0.0;
         if (b.va) {
-            for (int q = 0; q < 3; q++) ey[q] = rp_wfield_at<T>(A, g, g.turbaccel, c, zt[q], depth, Zpar, sl[q], fl);
+            for (int q = 0; q < 3; q++) ey[q] = rp_wfield_at<T>(g, g.turbaccel, c, zt[q], depth, Zpar, sl[q], wq(q), fl);
             stdaccturbu = rp_polintd(A.pi, ey[0], ey[1], ey[2]);
-            for (int q = 0; q < 3; q++) ey[q] = rp_wfield_at<T>(A, g, g.turbvort, c, zt[q], depth, Zpar, sl[q], fl);
+            for (int q = 0; q < 3; q++) ey[q] = rp_wfield_at<T>(g, g.turbvort, c, zt[q], depth, Zpar, sl[q], wq(q), fl);
             stdvortturb = rp_polintd(A.pi, ey[0], ey[1], ey[2]);
             stdaccturbu = RP_MUL(stdaccturbu, 100.0);
         }
         if (b.wa) {
-            for (int q = 0; q < 3; q++) ey[q] = rp_wfield_at<T>(A, g, g.waveaccelu, c, zt[q], depth, Zpar, sl[q], fl);
+            for (int q = 0; q < 3; q++) ey[q] = rp_wfield_at<T>(g, g.waveaccelu, c, zt[q], depth, Zpar, sl[q], wq(q), fl);
             stdaccwaveu = rp_polintd(A.pi, ey[0], ey[1], ey[2]);
-            for (int q = 0; q < 3; q++) ey[q] = rp_wfield_at<T>(A, g, g.waveaccelv, c, zt[q], depth, Zpar, sl[q], fl);
+            for (int q = 0; q < 3; q++) ey[q] = rp_wfield_at<T>(g, g.waveaccelv, c, zt[q], depth, Zpar, sl[q], wq(q), fl);
             stdaccwavev = rp_polintd(A.pi, ey[0], ey[1], ey[2]);
             stdaccwaveu = RP_MUL(stdaccwaveu, 100.0);
             stdaccwavev = RP_MUL(stdaccwavev, 100.0);
