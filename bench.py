@@ -128,6 +128,25 @@ def profile_traffic(workload, kernel):
     return None
 
 
+def profile_fp64(workload, kernel):
+    """FP64 arithmetic of one launch of `kernel` from the committed ncu
+    counts of the same workload (DADD + DMUL + 2 DFMA thread instructions,
+    fp64 pipe activity), or None when no summary covers that kernel."""
+    p = os.path.join(ROOT, "profiles", f"step_{workload}_fp64.json")
+    if os.path.exists(p):
+        try:
+            d = json.load(open(p))
+        except Exception:
+            return None
+        return d.get("kernels", {}).get(kernel)
+    return None
+
+
+# B200 FP64 (vector and tensor core) nominal peak: 296 TFLOP/s per 8-GPU
+# DGX B200 system; no measured FP64 peak exists for this pool
+FP64_PEAK_NOMINAL_TFLOPS = 37.0
+
+
 class ClockSampler:
     """nvidia-smi clock / throttle sampling during the timed region."""
 
@@ -882,12 +901,24 @@ def main():
         return {"region_ms": region_ms, "avg_launch_ms": kern, "launches": T.kernel_launches() - l0,
                 "clocks": clocks}
 
+    def spline_counts(T):
+        """One frame interval after the timed region, with VTurb's
+        smoothing-spline fits and their chol1d passes counted (outside every
+        timed region; counting changes no result)."""
+        T.count_spline_passes(True)
+        for it in exts[1].internal:
+            T.step(it.ex, it.ix, it.ets, 1, 2, 3)
+        f, p = T.spline_pass_counts()
+        T.count_spline_passes(False)
+        return f, p
+
     results = {}
     e2e = None
     head_T = None
     for form in forms:
         T = make_tracker(form)
         r = time_resident(T, form == head)
+        r["spline_fits"], r["spline_passes"] = spline_counts(T)
         r["value"] = npart * 12 * args.steps * world / (r["region_ms"] / 1e3)
         r["ms_per_step"] = r["region_ms"] / args.steps
         results[form] = r
@@ -976,6 +1007,32 @@ def main():
                 "avg_launch_ms": hr["avg_launch_ms"],
                 "algorithmic_bytes": f"{balg} B/particle-step x {npart} particles per launch"}
 
+    # ---------------- the smoothing-spline fit: passes per fit, FP64 rate
+    np_fit = int((spec.N + 1) * params["sub"])
+
+    def spline_of(form):
+        r = results[form]
+        f, p = r["spline_fits"], r["spline_passes"]
+        d = {"fits_per_particle_step": f / (npart * 12), "chol1d_passes_per_fit": (p / f) if f else None,
+             "np": np_fit}
+        prof = profile_fp64(wl, KERNEL[form])
+        if prof and prof.get("form") == form:
+            fl = prof["fp64_flop_per_launch"] / prof["particles"]
+            d.update({"fp64_flop_per_particle_step": fl,
+                      "fp64_tflops": fl * npart / (r["avg_launch_ms"] / 1e3) / 1e12,
+                      "fp64_pipe_active_pct": prof.get("fp64_pipe_active_pct"),
+                      "fp64_source": prof.get("source")})
+        return d
+
+    spline = {"form": head, **spline_of(head),
+              "forms": {f: spline_of(f) for f in results if f != head},
+              "fp64_peak_tflops": FP64_PEAK_NOMINAL_TFLOPS, "fp64_peak_source": "nominal (296 TFLOP/s per DGX B200 / 8)",
+              "note": "fits and chol1d passes counted on the device over one frame interval after the timed region "
+                      "(rp_count_spline_passes); FP64 flops = DADD + DMUL + 2 DFMA per launch from ncu counts of the "
+                      "same workload, scaled per particle-step, over the live-timed launch"}
+    if "fp64_tflops" in spline:
+        spline["fp64_frac"] = spline["fp64_tflops"] / FP64_PEAK_NOMINAL_TFLOPS
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -1005,7 +1062,7 @@ def main():
                           "avg_launch_ms": r["avg_launch_ms"], "desc": FORM_DESC[f],
                           "speedup_vs_plain_fp64": (r["value"] / plain["value"]) if plain else None}
                       for f, r in results.items()},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": hr["clocks"],
+            "roofline": roofline, "spline": spline, "cpu_baseline": cpu, "e2e": e2e, "clocks": hr["clocks"],
             "gpu_launches": int(hr["launches"]),
         }
         print(json.dumps(line), flush=True)

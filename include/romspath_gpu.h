@@ -454,6 +454,18 @@ int rp_set_launch(rp_ctx *ctx, int32_t resort, int32_t blocks_per_sm);
  * (CUDA events), and the number of kernels it launched. */
 int rp_last_step_stats(rp_ctx *ctx, float *ms, int32_t *kernels);
 
+/* Counting of VTurb's smoothing-spline fits (smooth, ver_turb_module.f90:182;
+ * pppack.f90:5108-5317) and of the chol1d passes they make (pppack.f90:1428;
+ * one per evaluation of SF in the secant search on p, plus the final u):
+ * on = 1 zeroes the counts and counts the steps launched from then on,
+ * on = 0 stops.  Counting adds one pair of atomic adds per warp and step;
+ * it changes no result.  Every form; not in rp_forward/rp_backward. */
+int rp_count_spline_passes(rp_ctx *ctx, int32_t on);
+
+/* The counts since counting was last started (synchronises the compute
+ * stream).  RP_ERR_STATE if it was never started. */
+int rp_spline_pass_counts(rp_ctx *ctx, int64_t *fits, int64_t *passes);
+
 /* Total number of kernels this context has launched since creation. */
 int rp_kernel_launches(rp_ctx *ctx, int64_t *count);
 

@@ -26,7 +26,7 @@ EXPORTS = [
     "rp_tangent", "rp_adj_replay", "rp_step_n", "rp_set_launch", "rp_upload_frame_ext", "rp_upload_frame_ext_f32",
     "rp_get_diagnostics", "rp_reset_diagnostics", "rp_set_grid_lonlat", "rp_output_record", "rp_upload_frame_desc",
     "rp_set_behavior", "rp_get_behavior", "rp_set_grid_angle", "rp_locate_lonlat", "rp_nest_maps",
-    "rp_output_record_async", "rp_output_wait",
+    "rp_output_record_async", "rp_output_wait", "rp_count_spline_passes", "rp_spline_pass_counts",
 ]
 
 PD = C.POINTER(C.c_double)
@@ -146,6 +146,8 @@ def _declare(L):
     L.rp_device_state_get.argtypes = [P, C.POINTER(RpDeviceState)]
     L.rp_last_step_stats.argtypes = [P, C.POINTER(C.c_float), C.POINTER(C.c_int32)]
     L.rp_kernel_launches.argtypes = [P, C.POINTER(C.c_int64)]
+    L.rp_count_spline_passes.argtypes = [P, C.c_int32]
+    L.rp_spline_pass_counts.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.rp_step_noalloc.argtypes = [P, C.POINTER(RpDeviceState), PD, PD, C.c_int32, C.c_int32, C.c_int32,
                                   C.c_int32]
     L.rp_step_n.argtypes = [P, C.c_int32, PD, PD, PI32, PI32, PI32, PI32]

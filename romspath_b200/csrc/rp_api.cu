@@ -126,6 +126,9 @@ struct rp_ctx {
         size_t cap_steps = 0;
     } adj;
     int64_t launches = 0;
+    // smoothing-spline fits and chol1d passes counted by the step kernels
+    unsigned long long* d_spl = nullptr;
+    bool spl_on = false;
     std::string err;
 };
 
@@ -257,6 +260,7 @@ void fill_params(const rp_ctx* c, RpStepArgs& A) {
     A.seed = p.seed;
     A.ndraw = c->ndraw;
     A.pid_base = c->pid_base;
+    A.spl = c->spl_on ? c->d_spl : nullptr;
     A.p = particles_dev(c);
 }
 
@@ -318,7 +322,7 @@ void free_ctx(rp_ctx* c) {
                     c->adj.ck, c->adj.prec, c->adj.seg, c->adj.work, c->adj.lx, c->adj.ly, c->adj.lz,
                     c->adj.kbar, c->adj.tan, c->d_salt, c->d_temp, c->d_mean_salt, c->d_mean_temp,
                     c->d_hob, c->d_bustr, c->d_bvstr, c->outbuf, c->wd_stage, c->b_acc, c->b_vort,
-                    c->b_behavew, c->b_ssf};
+                    c->b_behavew, c->b_ssf, c->d_spl};
     for (int g = 0; g < RP_MAXNGRID; g++)
         for (int f = 0; f < 5; f++)
             if (c->adj.fst[g][f]) cudaFree(c->adj.fst[g][f]);
@@ -1691,6 +1695,27 @@ int rp_device_state_get(rp_ctx* ctx, rp_device_state* out) {
 int rp_kernel_launches(rp_ctx* ctx, int64_t* count) {
     if (!ctx || !count) return RP_ERR_ARG;
     *count = ctx->launches;
+    return RP_OK;
+}
+
+int rp_count_spline_passes(rp_ctx* ctx, int32_t on) {
+    if (!ctx) return RP_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    if (on && !ctx->d_spl) CK(cudaMalloc(&ctx->d_spl, 2 * sizeof(unsigned long long)));
+    if (on) CK(cudaMemsetAsync(ctx->d_spl, 0, 2 * sizeof(unsigned long long), ctx->s_comp));
+    ctx->spl_on = on != 0;
+    return RP_OK;
+}
+
+int rp_spline_pass_counts(rp_ctx* ctx, int64_t* fits, int64_t* passes) {
+    if (!ctx) return RP_ERR_ARG;
+    if (!ctx->d_spl) return fail(ctx, RP_ERR_STATE, "rp_spline_pass_counts: counting was never started");
+    cudaSetDevice(ctx->device);
+    unsigned long long h[2] = {0, 0};
+    CK(cudaMemcpyAsync(h, ctx->d_spl, sizeof h, cudaMemcpyDeviceToHost, ctx->s_comp));
+    CK(cudaStreamSynchronize(ctx->s_comp));
+    if (fits) *fits = (int64_t)h[0];
+    if (passes) *passes = (int64_t)h[1];
     return RP_OK;
 }
 

@@ -181,6 +181,7 @@ struct RpStepArgs {
     double khturb[RP_MAXNGRID_D];
     uint64_t seed, step_index;
     const double* hook;            // noise hook for this step, or nullptr
+    unsigned long long* spl;       // [0] smoothing-spline fits, [1] chol1d passes; nullptr: not counted
     int ndraw;
     uint32_t pid_base;             // hook row of particle id p is p - pid_base
     RpGridDev g[RP_MAXNGRID_D];
@@ -188,6 +189,19 @@ struct RpStepArgs {
 };
 
 // ------------------------------------------------------------------ basics
+
+// Adds one fit of `passes` chol1d passes per calling thread to c[0], c[1]:
+// the converged threads of the warp sum theirs and one lane adds the totals.
+__device__ __forceinline__ void rp_count_fit(unsigned long long* c, int passes) {
+    const unsigned m = __activemask();
+    const unsigned tot = __reduce_add_sync(m, (unsigned)passes);
+    unsigned lane;
+    asm volatile("mov.u32 %0, %%laneid;" : "=r"(lane));
+    if (lane == (unsigned)(__ffs(m) - 1)) {
+        atomicAdd(c, (unsigned long long)__popc(m));
+        atomicAdd(c + 1, (unsigned long long)tot);
+    }
+}
 
 __device__ __forceinline__ int rp_ifloor(double x) {
     double f = floor(x);

@@ -646,13 +646,14 @@ __device__ __forceinline__ double m_sf(const MSpline<NPMAX>& w, const MFit& f, d
 // g of 1/sqrt(SF) in q found there, which gives a Newton step when it does
 // not; then secant steps.  Falls back to the reference's cold start (p = 0,
 // utru) when that does not converge.  q and g are returned in qstate and
-// gstate (q = 0 for p = 0; g <= 0 when unknown).
+// gstate (q = 0 for p = 0; g <= 0 when unknown); passes = chol1d passes made.
 template <int NPMAX>
 __device__ double m_smooth(const MSpline<NPMAX>& w, const MFit& f, double s, int max_iter, double& qstate,
-                           double& gstate, uint32_t& fl) {
+                           double& gstate, uint32_t& fl, int& passes) {
     // the first pass of every path also stores y(i); passes that are
     // rarely the last one (the warm-start check, p = 0) do not store u and
     // are repeated with it when they are
+    passes = 1;
     if (s <= 0.0) {
         m_chol1d(w, f, 1.0, nullptr, true, true);
         return 1.0;
@@ -664,6 +665,7 @@ __device__ double m_smooth(const MSpline<NPMAX>& w, const MFit& f, double s, int
         double sfq = m_sf(w, f, q, true, false);
         if (fabs(sfq - s) <= 0.01 * s) {
             m_chol1d(w, f, q / (1.0 + q), nullptr, false, true);
+            passes = 2;
             return q / (1.0 + q);
         }
         double prevq = q, prevsf = 1.0 / sqrt(sfq);
@@ -671,6 +673,7 @@ __device__ double m_smooth(const MSpline<NPMAX>& w, const MFit& f, double s, int
         q = (qn > 0.0) ? qn : q * sqrt(sfq / s);
         for (int it = 0; it < 6 && q > 0.0; it++) {
             sfq = m_sf(w, f, q, false, true);
+            passes++;
             const double oosf = 1.0 / sqrt(sfq);
             const double g = (oosf - prevsf) / (q - prevq);
             if (fabs(sfq - s) <= 0.01 * s) {
@@ -687,8 +690,10 @@ __device__ double m_smooth(const MSpline<NPMAX>& w, const MFit& f, double s, int
     // cold start: the reference's sequence
     double utru = 0.0;
     double sfq = 36.0 * m_chol1d(w, f, 0.0, &utru, !warm, false);
+    passes += warm ? 1 : 0;
     if (!(s < sfq)) {
         m_chol1d(w, f, 0.0, nullptr, false, true);
+        passes++;
         qstate = 0.0;
         gstate = 0.0;
         return 0.0;
@@ -701,6 +706,7 @@ __device__ double m_smooth(const MSpline<NPMAX>& w, const MFit& f, double s, int
         sfq = m_sf(w, f, q, false, true);
         oosf = 1.0 / sqrt(sfq);
         it++;
+        passes++;
         const double g = (oosf - prevsf) / (q - prevq);
         if (fabs(sfq - s) <= 0.01 * s) {
             gstate = g;
@@ -806,7 +812,9 @@ __device__ float m_vturb(const RpStepArgs& A, const RpGridDev& g, const MStage& 
     f.z1 = w.cz(1);
     f.h = (zeta - f.z1) / (double)(f.np - 1);
     f.rh = 1.0 / f.h;
-    const double p = m_smooth(w, f, A.smth, A.spline_max_iter, qstate, gstate, fl);
+    int passes;
+    const double p = m_smooth(w, f, A.smth, A.spline_max_iter, qstate, gstate, fl, passes);
+    if (A.spl) rp_count_fit(A.spl, passes);
     const double deltat = A.deltat;
     double ParZc = (double)Zpar;
     MPiece pc;

@@ -264,10 +264,10 @@ __device__ __forceinline__ double rp_chol1d(const W& w, int np, double p, double
 }
 
 // smooth (pppack.f90:5108-5317) on fitz/y already in w; dy(i) = serr for
-// all i.  Returns p; w.u holds the final u.
+// all i.  Returns p; w.u holds the final u; passes = chol1d passes made.
 template <class W>
 __device__ __forceinline__ double rp_smooth(const W& w, int np, double serr, double s, int max_iter,
-                                            uint32_t& fl) {
+                                            uint32_t& fl, int& passes) {
     const double dy2 = serr * serr;
     // setupq's Q'y (pppack.f90:4816-4822)
     {
@@ -279,6 +279,7 @@ __device__ __forceinline__ double rp_smooth(const W& w, int np, double serr, dou
         }
     }
     double p, q, sfq;
+    passes = 1;
     if (s <= 0.0) {
         p = 1.0;
         rp_chol1d(w, np, p, serr, dy2, nullptr);
@@ -296,6 +297,7 @@ __device__ __forceinline__ double rp_smooth(const W& w, int np, double serr, dou
                 const double sum = rp_chol1d(w, np, q / (1.0 + q), serr, dy2, nullptr);
                 sfq = 36.0 * sum / ((1.0 + q) * (1.0 + q));
                 it++;
+                passes++;
                 if (fabs(sfq - s) <= 0.01 * s) break;
                 if (it >= max_iter) { fl |= RP_FL_SPLINE; break; }
                 oosf = 1.0 / sqrt(sfq);
@@ -424,7 +426,9 @@ __device__ double rp_vturb(const RpStepArgs& A, const RpGridDev& g, const StageS
         const double b = kh(jlo) - m * zc(jlo);
         w.y(i) = m * x + b;
     }
-    const double p = rp_smooth(w, np, A.serr, A.smth, A.spline_max_iter, fl);
+    int passes;
+    const double p = rp_smooth(w, np, A.serr, A.smth, A.spline_max_iter, fl, passes);
+    if (A.spl) rp_count_fit(A.spl, passes);
 
     // random displacement sub-steps (ver_turb_module.f90:231-293)
     const double deltat = A.deltat;

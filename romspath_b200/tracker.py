@@ -365,6 +365,18 @@ class Tracker:
         self._check(self.L.rp_kernel_launches(self.h, C.byref(c)), "rp_kernel_launches")
         return c.value
 
+    def count_spline_passes(self, on: bool = True):
+        """Start (counts zeroed) or stop counting VTurb's smoothing-spline
+        fits and their chol1d passes in the steps launched afterwards."""
+        self._check(self.L.rp_count_spline_passes(self.h, 1 if on else 0), "rp_count_spline_passes")
+
+    def spline_pass_counts(self):
+        """(fits, chol1d passes) since counting was last started."""
+        f = C.c_int64()
+        p = C.c_int64()
+        self._check(self.L.rp_spline_pass_counts(self.h, C.byref(f), C.byref(p)), "rp_spline_pass_counts")
+        return f.value, p.value
+
     def device_state(self) -> _lib.RpDeviceState:
         st = _lib.RpDeviceState()
         self._check(self.L.rp_device_state_get(self.h, C.byref(st)), "rp_device_state_get")

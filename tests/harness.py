@@ -135,7 +135,9 @@ def run_gpu(case: Case, nsteps: int, noise: str = "philox", seed: int = 7,
 
 
 def run_oracle(case: Case, nsteps: int, noise: str = "philox", seed: int = 7,
-               hook: Optional[np.ndarray] = None, nthreads: int = 8):
+               hook: Optional[np.ndarray] = None, nthreads: int = 8, spline_stats: Optional[list] = None):
+    """The oracle's run of the same steps; ``spline_stats`` (a list) gets
+    each step's (smoothing-spline fits, secant iterations)."""
     from oracle import oracle as O
     m = O.OracleModel(case.specs, case.grids, case.params, scl=case.scl, off=case.off)
     for (k, slot) in schedule.initial_loads():
@@ -156,6 +158,8 @@ def run_oracle(case: Case, nsteps: int, noise: str = "philox", seed: int = 7,
             else:
                 m.step(it.ex, it.ix, it.ets, it.tb, it.tc, it.tf, noise="philox", seed=seed,
                        step_index=it.step_index, nthreads=nthreads)
+            if spline_stats is not None:
+                spline_stats.append(m.stats())
             done += 1
     st = m.state()
     st["gid"] = st["gid"].astype(np.float64)
