@@ -158,6 +158,14 @@ struct SplineView {
     __device__ __forceinline__ double& u(int i) const { return at(5, i); }     // u(i)/v(i,1), then u(i)
 };
 
+// The breaks fitz(1..np) as VTurb's resampling forms them
+// (ver_turb_module.f90:126-136): fitz(1) = z1, fitz(k) = fitz(k-1) + dz for
+// k = 2..np-1, fitz(np) = zend.  The chol1d passes re-form them by the same
+// additions, ascending, instead of reading them back from the workspace.
+struct RpBreaks {
+    double z1, dz, zend;
+};
+
 // chol1d (pppack.f90:1428-1566) for p.  The setupq bands are rebuilt on the
 // fly: with all data weights dy(i) = serr, v(i,1) = r(i-1),
 // v(i,2) = -r(i) - r(i-1), v(i,3) = r(i) where r(k) = serr / v(k,4) and
@@ -167,13 +175,20 @@ struct SplineView {
 // descending; then Q u and sum_i qu(i)^2 dy(i)^2 are formed ascending (the
 // reference's summation order), with utru (pppack.f90:5219-5223) on request.
 template <class W>
-__device__ __forceinline__ double rp_chol1d(const W& w, int np, double p, double serr, double dy2,
-                                            double* utru_out) {
+__device__ __forceinline__ double rp_chol1d(const W& w, int np, const RpBreaks& B, double p, double serr,
+                                            double dy2, double* utru_out) {
     const double six1mp = 6.0 * (1.0 - p);
     const double twop = 2.0 * p;
-    double v4a = w.fitz(2) - w.fitz(1);          // v4(1)
-    double v4b = w.fitz(3) - w.fitz(2);          // v4(2)
-    double v4c = w.fitz(4) - w.fitz(3);          // v4(3)
+    double acc = B.z1;                           // the running sum of the breaks
+    auto brk = [&](int k) -> double {            // fitz(k), k = 2, 3, ... in turn
+        acc = acc + B.dz;
+        return (k == np) ? B.zend : acc;
+    };
+    const double f2 = brk(2), f3 = brk(3), f4 = brk(4);
+    double v4a = f2 - B.z1;                      // v4(1)
+    double v4b = f3 - f2;                        // v4(2)
+    double v4c = f4 - f3;                        // v4(3)
+    double fprev = f4;                           // fitz(i+2)
     const double r1_ = serr / v4a;               // r(1)
     double ri = serr / v4b;                      // r(i),   i = 2
     double rn = serr / v4c;                      // r(i+1)
@@ -199,8 +214,12 @@ __device__ __forceinline__ double rp_chol1d(const W& w, int np, double p, double
     for (int i = 2; i <= np - 2; i++) {
         // r(i+2), v4(i+2) (used while i+2 <= np-1)
         const bool has2 = (i + 2 <= np - 1);
-        const int i3 = has2 ? i + 3 : np;
-        const double v4nn = w.fitz(i3) - w.fitz(i3 - 1);
+        double v4nn = v4n;                        // past the end: discarded by the selects
+        if (has2) {
+            const double f = brk(i + 3);
+            v4nn = f - fprev;
+            fprev = f;
+        }
         const double rnn = serr / v4nn;
         const double qn = w.qty(i + 1);
         const double V3i = six1mp * ((i <= np - 3) ? (ri * rn) : 0.0);
@@ -243,11 +262,12 @@ __device__ __forceinline__ double rp_chol1d(const W& w, int np, double p, double
     // qu = Q u and the weighted sum of squares, i = 1..np in order
     double prev = 0.0, sum = 0.0, utru = 0.0;
     double ulast = 0.0;                           // u(1)
-    double flast = w.fitz(1);
+    double flast = B.z1;
+    acc = B.z1;
 #pragma unroll 4
     for (int i = 2; i <= np; i++) {
         const double ui = w.u(i);
-        const double fi = w.fitz(i);
+        const double fi = brk(i);
         const double v4i = fi - flast;
         const double raw = (ui - ulast) / v4i;
         const double fin = raw - prev;
@@ -266,8 +286,8 @@ __device__ __forceinline__ double rp_chol1d(const W& w, int np, double p, double
 // smooth (pppack.f90:5108-5317) on fitz/y already in w; dy(i) = serr for
 // all i.  Returns p; w.u holds the final u; passes = chol1d passes made.
 template <class W>
-__device__ __forceinline__ double rp_smooth(const W& w, int np, double serr, double s, int max_iter,
-                                            uint32_t& fl, int& passes) {
+__device__ __forceinline__ double rp_smooth(const W& w, int np, const RpBreaks& B, double serr, double s,
+                                            int max_iter, uint32_t& fl, int& passes) {
     const double dy2 = serr * serr;
     // setupq's Q'y (pppack.f90:4816-4822)
     {
@@ -282,11 +302,11 @@ __device__ __forceinline__ double rp_smooth(const W& w, int np, double serr, dou
     passes = 1;
     if (s <= 0.0) {
         p = 1.0;
-        rp_chol1d(w, np, p, serr, dy2, nullptr);
+        rp_chol1d(w, np, B, p, serr, dy2, nullptr);
     } else {
         p = 0.0;
         double utru = 0.0;
-        sfq = 36.0 * rp_chol1d(w, np, p, serr, dy2, &utru);
+        sfq = 36.0 * rp_chol1d(w, np, B, p, serr, dy2, &utru);
         if (s < sfq) {
             const double ooss = 1.0 / sqrt(s);
             double oosf = 1.0 / sqrt(sfq);
@@ -294,7 +314,7 @@ __device__ __forceinline__ double rp_smooth(const W& w, int np, double serr, dou
             double prevq = 0.0, prevsf = oosf;
             int it = 0;
             for (;;) {
-                const double sum = rp_chol1d(w, np, q / (1.0 + q), serr, dy2, nullptr);
+                const double sum = rp_chol1d(w, np, B, q / (1.0 + q), serr, dy2, nullptr);
                 sfq = 36.0 * sum / ((1.0 + q) * (1.0 + q));
                 it++;
                 passes++;
@@ -427,7 +447,8 @@ __device__ double rp_vturb(const RpStepArgs& A, const RpGridDev& g, const StageS
         w.y(i) = m * x + b;
     }
     int passes;
-    const double p = rp_smooth(w, np, A.serr, A.smth, A.spline_max_iter, fl, passes);
+    const RpBreaks B{zc(1), dz, zc(sw)};
+    const double p = rp_smooth(w, np, B, A.serr, A.smth, A.spline_max_iter, fl, passes);
     if (A.spl) rp_count_fit(A.spl, passes);
 
     // random displacement sub-steps (ver_turb_module.f90:231-293)

@@ -1,6 +1,8 @@
 """Multi-rank path on CPU: two gloo ranks each step their shard of the
 particles (the oracle stands in for the GPU step) with global particle ids,
-gather to all ranks, and must reproduce a one-rank run bit for bit."""
+gather to all ranks, and must reproduce a one-rank run bit for bit; the
+output-time reductions (the vertical concentration profile, a quantity
+summed over particles as dL/dkappa is) equal the one-rank values."""
 import os
 import socket
 
@@ -45,8 +47,11 @@ def _rank(rank, world, port, out):
                        step_index=it.step_index, nthreads=1)
         st = m.state()
         g = replicas.gather({k: st[k] for k in ("x", "y", "z", "status", "gid", "pid")}, world)
+        prof = replicas.global_profile(st)
+        # a per-particle additive quantity stands in for dL/dkappa's shares
+        gk = replicas.kappa_gradient(float(np.sum(st["x"])))
         if rank == 0:
-            np.savez(out, **g)
+            np.savez(out, prof=prof, gk=np.array(gk), **g)
     finally:
         dist.destroy_process_group()
 
@@ -69,3 +74,7 @@ def test_two_gloo_ranks_match_one_rank(tmp_path):
     for k in ("x", "y", "z", "status"):
         assert np.array_equal(g[k].view(np.uint64), o[k].view(np.uint64)), k
     assert np.array_equal(g["gid"], o["gid"].astype(np.int32))
+    prof = replicas.column_profile(o)
+    assert prof.sum() > 100
+    assert np.array_equal(g["prof"], prof)
+    assert abs(float(g["gk"]) - float(np.sum(o["x"]))) <= 1e-12 * abs(float(np.sum(o["x"])))
