@@ -54,6 +54,12 @@ from romspath_b200 import schedule, synth  # noqa: E402
 
 WORKLOAD_DESC = ("cfg2: 512x384x30 ROMS grid, 8% islands, FP32 u/v/w/AKs/zeta frames + Stokes, "
                  "Kh=1 m^2/s, VTurb dt_turb=30 s, RK4 idt=300 s")
+WORKLOAD_DESCS = {
+    "cfg2": WORKLOAD_DESC,
+    "cfg1": "cfg1: 130x98x20 ROMS grid, land corner, FP64 frames, HTurb off, VTurb dt_turb=30 s, RK4 idt=300 s",
+    "cfg3": "cfg3: config 1's 130x98x20 grid (FP64 frames; FP16 in the mixed form), HTurb off, VTurb dt_turb=30 s, "
+            "RK4 idt=300 s, 4,194,304 particles",
+}
 
 
 def parse():
@@ -266,7 +272,7 @@ def run_reference(args):
         "impl": "reference", "metric": "particle-steps/s", "value": val, "unit": "particle-steps/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": WORKLOAD_DESC,
+        "data": "synthetic", "config": {"workload": WORKLOAD_DESCS.get(args.workload, args.workload),
                                         "step": "one frame interval = 12 internal steps",
                                         "sample_particles": npart},
         "cpu_baseline": {"value": val, "unit": "particle-steps/s", "cores": threads, "kind": "port",
@@ -1058,11 +1064,13 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f16/f32/f64 (mixed)" if head.startswith("mixed") else "f64",
             "data": "synthetic (analytic ROMS-shaped fields, seeded release)",
-            "config": {"workload": WORKLOAD_DESC, "particles_per_gpu": npart,
+            "config": {"workload": WORKLOAD_DESCS.get(wl, wl), "particles_per_gpu": npart,
                        "step": "one hydro frame interval = 12 internal steps (idt=300 s)",
                        "form": FORM_DESC[head],
-                       "l2": "inputs larger than L2 (frame ring 390 MB FP32 / 195 MB FP16, particle state "
-                             "~80 MB, spline workspace in local memory ~0.5-1 GB)",
+                       "l2": ("inputs larger than L2 (frame ring 390 MB FP32 / 195 MB FP16, particle state "
+                              "~80 MB, spline workspace in local memory ~0.5-1 GB)") if wl == "cfg2" else
+                             ("frames L2-resident (8.4 MB per FP64 frame), particle state and spline workspace "
+                              "larger than L2"),
                        "parallelism": f"replicas x{world}: particles split per rank, no data-path collective",
                        "resort": f"particle state re-sorted by grid and cell every {args.resort} internal steps "
                                  f"(inside the timed region)" if args.resort else "off"},
