@@ -489,23 +489,34 @@ struct MFit {
 };
 
 // linint of the column at ascending points: the current piece j (slope,
-// intercept and upper end) is held in registers and advanced as needed
+// intercept and upper end) is held in registers and advanced as needed;
+// the next piece is loaded one piece ahead, so an advance waits on no load
 template <int NPMAX>
 struct MWalk {
     int j;
     double zn, m, b;               // cz(j+1), cm(j), cb(j)
-    __device__ __forceinline__ void init(const MSpline<NPMAX>& w) {
+    float zn2, m2, b2;             // cz(j+2), cm(j+1), cb(j+1) while j + 1 < sw
+    __device__ __forceinline__ void ahead(const MSpline<NPMAX>& w, int sw) {
+        if (j + 1 < sw) {
+            zn2 = w.cz(j + 2);
+            m2 = w.cm(j + 1);
+            b2 = w.cb(j + 1);
+        }
+    }
+    __device__ __forceinline__ void init(const MSpline<NPMAX>& w, int sw) {
         j = 1;
         zn = w.cz(2);
         m = w.cm(1);
         b = w.cb(1);
+        ahead(w, sw);
     }
     __device__ __forceinline__ double at(const MSpline<NPMAX>& w, int sw, double x) {
         while (j < sw - 1 && zn <= x) {
             j++;
-            zn = w.cz(j + 1);
-            m = w.cm(j);
-            b = w.cb(j);
+            zn = zn2;
+            m = m2;
+            b = b2;
+            ahead(w, sw);
         }
         return m * x + b;
     }
@@ -527,7 +538,7 @@ __device__ double m_chol1d(const MSpline<NPMAX>& w, const MFit& f, double p, dou
     const double F = six1mp * r2;
     // Q'y on the fly: qty(i) = (y(i+1) - 2 y(i) + y(i-1)) / h
     MWalk<NPMAX> wk;
-    wk.init(w);
+    wk.init(w, f.sw);
     double ym = wk.at(w, f.sw, f.z1);
     double y0 = wk.at(w, f.sw, f.z1 + f.h);
     double yp = wk.at(w, f.sw, f.z1 + 2.0 * f.h);
@@ -607,12 +618,20 @@ __device__ double m_chol1d(const MSpline<NPMAX>& w, const MFit& f, double p, dou
         up2 = up1;
         up1 = ui;
     }
+    // u(i) is loaded four rows ahead of its use (index 1 stands in past
+    // the start; that value is never used)
+    MU q0 = w.u(np - 2), q1 = w.u(max(np - 3, 1)), q2 = w.u(max(np - 4, 1)), q3 = w.u(max(np - 5, 1));
 #pragma unroll 2
     for (int i = np - 2; i >= 2; i--) {
+        const double uq = (double)q0;
+        q0 = q1;
+        q1 = q2;
+        q2 = q3;
+        q3 = w.u(max(i - 4, 1));
         const bool held = (i >= ks && i <= np - 3);
         const double s1v = held ? (double)(MRatio)hr1 : (double)w.s1(i);
         const double s2v = held ? (double)(MRatio)hr2 : (double)w.s2(i);
-        const double ui = (double)w.u(i) - up1 * s1v - up2 * s2v;
+        const double ui = uq - up1 * s1v - up2 * s2v;
         if (store_u) w.u(i) = (MU)ui;
         const double raw = (up1 - ui) * f.rh;        // raw(i+1)
         const double fin = rawp - raw;               // qu(i+1)
