@@ -119,9 +119,10 @@ def measured_peaks():
     return 6650.0, "fallback (6.65 TB/s)"
 
 
-def profile_traffic(workload, kernel):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary of
-    the same workload, or None when no summary covers that kernel."""
+def profile_traffic(workload, kernel, key="dram_bytes_per_launch"):
+    """DRAM (or, with key="lts_bytes_per_launch", L2) bytes per launch of
+    `kernel` from the committed ncu summary of the same workload, or None
+    when no summary covers that kernel."""
     p = os.path.join(ROOT, "profiles", f"step_{workload}_traffic.json")
     if os.path.exists(p):
         try:
@@ -130,7 +131,7 @@ def profile_traffic(workload, kernel):
             return None
         k = d.get("kernels", {}).get(kernel)
         if k:
-            return k.get("dram_bytes_per_launch")
+            return k.get(key)
     return None
 
 
@@ -1011,9 +1012,12 @@ def main():
     balg = B_ALG_FORM.get((wl, head), 1872)
     achieved = balg * npart / (hr["avg_launch_ms"] / 1e3) / 1e9
     traffic = profile_traffic(wl, KERNEL[head])
+    l2_traffic = profile_traffic(wl, KERNEL[head], "lts_bytes_per_launch")
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                 "dram_gbs_from_traffic": (traffic / (hr["avg_launch_ms"] / 1e3) / 1e9) if traffic else None,
+                "l2_traffic": l2_traffic,
+                "l2_gbs_from_traffic": (l2_traffic / (hr["avg_launch_ms"] / 1e3) / 1e9) if l2_traffic else None,
                 "note": "achieved counts the field and particle bytes the reference arithmetic consumes at the "
                         "form's storage widths; DRAM traffic is dominated by the smoothing-spline workspace in "
                         "local memory (see profiles/)",
