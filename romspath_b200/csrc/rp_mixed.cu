@@ -169,26 +169,41 @@ __device__ __forceinline__ void m_store16(int16_t* d, float v) {
 }
 
 // FP32 field (Fortran order) -> 16-bit device layout [j][i][k][slot4] and
-// the per-level scales qs[k][slot4]
+// the per-level scales qs[k][slot4].  A block takes 32 points of row j
+// with all their levels: it reads level by level (coalesced along i) into
+// shared memory and writes point by point, the levels of a point adjacent
+// as the ring holds them, so a warp's stores cover one contiguous run of
+// the ring instead of one sector per value.
+constexpr int kQuantMaxLevels = kMaxNp;     // s_w <= int(s_w*sub) <= kMaxNp
 template <typename E>
-__global__ void k_quantize(const float* __restrict__ f, const uint32_t* __restrict__ maxbits, float* __restrict__ qs,
-                           E* __restrict__ dst, int ni, int nj, int nk, int slot) {
+__global__ void __launch_bounds__(256) k_quantize(const float* __restrict__ f, const uint32_t* __restrict__ maxbits,
+                                                  float* __restrict__ qs, E* __restrict__ dst, int ni, int nj, int nk,
+                                                  int slot) {
     constexpr bool i16 = sizeof(E) == 2 && !std::is_same<E, __half>::value;
+    __shared__ float tile[kQuantMaxLevels][33];
+    __shared__ float sc[kQuantMaxLevels];
+    const int i0 = blockIdx.x * 32, j = blockIdx.y;
     const int64_t plane = (int64_t)ni * nj;
-    const int64_t total = plane * nk;
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e < nk) qs[e * RP_SLOTS + slot] = m_level_scale(maxbits[e], i16);
-    if (e >= total) return;
-    const int k = (int)(e / plane);
-    const int64_t r = e - (int64_t)k * plane;
-    const int j = (int)(r / ni);
-    const int i = (int)(r - (int64_t)j * ni);
-    const float sc = m_level_scale(maxbits[k], i16);
-    m_store16(dst + (((int64_t)j * ni + i) * nk + k) * RP_SLOTS + slot, i16 ? f[e] / sc : f[e] * (1.0f / sc));
+    for (int k = threadIdx.x; k < nk; k += blockDim.x) {
+        sc[k] = m_level_scale(maxbits[k], i16);
+        if (blockIdx.x == 0 && j == 0) qs[k * RP_SLOTS + slot] = sc[k];
+    }
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int npt = min(32, ni - i0);                 // points of this tile
+    for (int k = threadIdx.x >> 5; k < nk; k += nw)
+        if (lane < npt) tile[k][lane] = f[(int64_t)k * plane + (int64_t)j * ni + i0 + lane];
+    __syncthreads();
+    E* out = dst + ((int64_t)j * ni + i0) * nk * RP_SLOTS + slot;
+    for (int t = threadIdx.x; t < npt * nk; t += blockDim.x) {
+        const int il = t / nk, k = t - il * nk;
+        const float v = tile[k][il], s = sc[k];
+        m_store16(out + (int64_t)t * RP_SLOTS, i16 ? v / s : v * (1.0f / s));
+    }
 }
 
 cudaError_t launch_quantize(const float* f, uint32_t* maxbits, float* qs, void* dst, int ni, int nj, int nk, int slot,
                             int i16, int num_sms, cudaStream_t s) {
+    if (nk > kQuantMaxLevels || ni < 1 || nj < 1 || nj > 65535) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(maxbits, 0, sizeof(uint32_t) * nk, s);
     if (e != cudaSuccess) return e;
     const int64_t plane = (int64_t)ni * nj;
@@ -198,10 +213,9 @@ cudaError_t launch_quantize(const float* f, uint32_t* maxbits, float* qs, void* 
     if (bx > cap) bx = cap;
     k_level_maxabs<<<dim3((unsigned)bx, (unsigned)nk), block, 0, s>>>(f, plane, maxbits);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    const int64_t total = plane * nk;
-    const unsigned blocks = (unsigned)((total + block - 1) / block);
-    if (i16) k_quantize<int16_t><<<blocks, block, 0, s>>>(f, maxbits, qs, (int16_t*)dst, ni, nj, nk, slot);
-    else k_quantize<__half><<<blocks, block, 0, s>>>(f, maxbits, qs, (__half*)dst, ni, nj, nk, slot);
+    const dim3 grid((unsigned)((ni + 31) / 32), (unsigned)nj);
+    if (i16) k_quantize<int16_t><<<grid, 256, 0, s>>>(f, maxbits, qs, (int16_t*)dst, ni, nj, nk, slot);
+    else k_quantize<__half><<<grid, 256, 0, s>>>(f, maxbits, qs, (__half*)dst, ni, nj, nk, slot);
     return cudaGetLastError();
 }
 
