@@ -986,8 +986,13 @@ def main():
             T.output_wait()
 
         base = 2 + args.warmup + args.steps
+        # warm-up intervals (untimed) with the fit's passes counted: the
+        # frames change every interval here, unlike the resident leg's
+        T.count_spline_passes(True)
         e2e_run(exts[base:base + args.warmup], 0)
         T.synchronize()
+        e2e_fits, e2e_passes = T.spline_pass_counts()
+        T.count_spline_passes(False)
         barrier()
         l0 = T.kernel_launches()
         t0 = time.perf_counter()
@@ -998,6 +1003,7 @@ def main():
         e2e = {"value": npart * 12 * args.steps * world / e2e_s, "unit": "particle-steps/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "ms_per_step": e2e_s * 1e3 / args.steps, "gpu_launches": T.kernel_launches() - l0,
+               "chol1d_passes_per_fit": (e2e_passes / e2e_fits) if e2e_fits else None,
                "form": head,
                "timing": "host clock between device synchronizations; every step uploads one frame "
                          "(quantised on the device in the mixed form) and reads its dataOutput record "
