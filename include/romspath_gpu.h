@@ -5,7 +5,7 @@
  * frame hand-off of updateHydro (hydrodynamic_module.f90:112-760).  The
  * Fortran driver, its namelists (ROMSPath.h:59-345) and its NetCDF reader
  * stay as they are; the driver binds these entry points with ISO_C_BINDING
- * (see the interface module in INTEGRATION.md).
+ * (one bind(C) interface per entry point, arguments by value or as arrays).
  *
  * Conventions
  *  - Every array argument is a host pointer in the reference's own layout:
@@ -42,8 +42,9 @@ extern "C" {
 #define RP_ERR_UNSUPPORTED (-5)/* option outside the implemented path        */
 #define RP_ERR_NOEXT (-6)      /* no CUDA device / kernels not loadable      */
 
-/* per-particle flag bits returned by rp_get_particles (deviations where the
- * reference is undefined) */
+/* per-particle flag bits returned by rp_get_particles: each marks a particle
+ * that met, in its steps, a case where the reference's result is undefined
+ * and this library pins one (the bits below say which) */
 #define RP_FLAG_OOB 0x01u      /* a gather index left its array (clamped)      */
 #define RP_FLAG_NODE 0x02u     /* inverse-distance weight at an exact node      */
 #define RP_FLAG_WBOT 0x04u     /* w-level bracket below level 1                 */
