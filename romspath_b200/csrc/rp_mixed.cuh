@@ -489,34 +489,23 @@ struct MFit {
 };
 
 // linint of the column at ascending points: the current piece j (slope,
-// intercept and upper end) is held in registers and advanced as needed;
-// the next piece is loaded one piece ahead, so an advance waits on no load
+// intercept and upper end) is held in registers and advanced as needed
 template <int NPMAX>
 struct MWalk {
     int j;
     double zn, m, b;               // cz(j+1), cm(j), cb(j)
-    float zn2, m2, b2;             // cz(j+2), cm(j+1), cb(j+1) while j + 1 < sw
-    __device__ __forceinline__ void ahead(const MSpline<NPMAX>& w, int sw) {
-        if (j + 1 < sw) {
-            zn2 = w.cz(j + 2);
-            m2 = w.cm(j + 1);
-            b2 = w.cb(j + 1);
-        }
-    }
-    __device__ __forceinline__ void init(const MSpline<NPMAX>& w, int sw) {
+    __device__ __forceinline__ void init(const MSpline<NPMAX>& w) {
         j = 1;
         zn = w.cz(2);
         m = w.cm(1);
         b = w.cb(1);
-        ahead(w, sw);
     }
     __device__ __forceinline__ double at(const MSpline<NPMAX>& w, int sw, double x) {
         while (j < sw - 1 && zn <= x) {
             j++;
-            zn = zn2;
-            m = m2;
-            b = b2;
-            ahead(w, sw);
+            zn = w.cz(j + 1);
+            m = w.cm(j);
+            b = w.cb(j);
         }
         return m * x + b;
     }
@@ -538,7 +527,7 @@ __device__ double m_chol1d(const MSpline<NPMAX>& w, const MFit& f, double p, dou
     const double F = six1mp * r2;
     // Q'y on the fly: qty(i) = (y(i+1) - 2 y(i) + y(i-1)) / h
     MWalk<NPMAX> wk;
-    wk.init(w, f.sw);
+    wk.init(w);
     double ym = wk.at(w, f.sw, f.z1);
     double y0 = wk.at(w, f.sw, f.z1 + f.h);
     double yp = wk.at(w, f.sw, f.z1 + 2.0 * f.h);
