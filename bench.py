@@ -111,11 +111,24 @@ def parse():
     return ap.parse_args()
 
 
-def measured_peaks():
-    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+def measured_peaks(path=None):
+    """HBM copy bandwidth (GB/s) for the roofline: `hbm_gbs` of the measured
+    peaks file (top level, or in a nested object), else the pool's earlier
+    measurement of 6.65 TB/s."""
+    p = path or os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
-        d = json.load(open(p))
-        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+        try:
+            d = json.load(open(p))
+        except Exception:
+            d = None
+        stack = [d]
+        while stack:
+            x = stack.pop()
+            if isinstance(x, dict):
+                v = x.get("hbm_gbs")
+                if isinstance(v, (int, float)) and v > 0:
+                    return float(v), "measured (MEASURED_PEAKS.json hbm_gbs)"
+                stack.extend(x.values())
     return 6650.0, "fallback (6.65 TB/s)"
 
 

@@ -72,3 +72,14 @@ def test_measured_peaks_fallback_or_file():
         assert peak == float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
     else:
         assert (peak, src) == (6650.0, "fallback (6.65 TB/s)")
+
+
+def test_measured_peaks_file_forms(tmp_path):
+    p = tmp_path / "peaks.json"
+    p.write_text(json.dumps({"hbm_gbs": 6549.5, "bf16_tflops": 1590.0}))
+    assert bench.measured_peaks(str(p)) == (6549.5, "measured (MEASURED_PEAKS.json hbm_gbs)")
+    p.write_text(json.dumps({"gpu0": {"hbm_gbs": 6400.0}}))
+    assert bench.measured_peaks(str(p))[0] == 6400.0
+    p.write_text("not json")
+    assert bench.measured_peaks(str(p)) == (6650.0, "fallback (6.65 TB/s)")
+    assert bench.measured_peaks(str(tmp_path / "absent.json"))[1].startswith("fallback")
