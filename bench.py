@@ -113,8 +113,8 @@ def parse():
 
 def measured_peaks(path=None):
     """HBM copy bandwidth (GB/s) for the roofline: `hbm_gbs` of the measured
-    peaks file (top level, or in a nested object), else the pool's earlier
-    measurement of 6.65 TB/s."""
+    peaks file (top level, or in nested objects and lists; a positive number,
+    not a boolean), else the pool's earlier measurement of 6.65 TB/s."""
     p = path or os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
         try:
@@ -126,9 +126,11 @@ def measured_peaks(path=None):
             x = stack.pop()
             if isinstance(x, dict):
                 v = x.get("hbm_gbs")
-                if isinstance(v, (int, float)) and v > 0:
+                if isinstance(v, (int, float)) and not isinstance(v, bool) and v > 0:
                     return float(v), "measured (MEASURED_PEAKS.json hbm_gbs)"
-                stack.extend(x.values())
+                stack.extend(reversed(list(x.values())))
+            elif isinstance(x, list):
+                stack.extend(reversed(x))
     return 6650.0, "fallback (6.65 TB/s)"
 
 

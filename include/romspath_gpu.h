@@ -370,8 +370,8 @@ int rp_device_state_get(rp_ctx *ctx, rp_device_state *out);
 
 /* One internal step exactly like rp_step (same results, bit for bit), on
  * particle columns that live in the caller's own device memory
- * (state->x ... state->flags, state->n particles; `stream` is ignored), and
- * without allocating any device memory.  No counterpart in the reference.
+ * (state->x ... state->flags, state->n particles), and without allocating
+ * any device memory.  No counterpart in the reference.
  *
  * For callers that cannot allocate at step time: a Fortran driver that keeps
  * its particle arrays on the device itself (OpenACC / CUDA Fortran data
@@ -383,8 +383,16 @@ int rp_device_state_get(rp_ctx *ctx, rp_device_state *out);
  * that loads the library until the process exits.
  *  - state->n must be <= RP_NOALLOC_MAX_PARTICLES and int(s_w*sub) <= 128
  *    (RP_ERR_ARG / RP_ERR_UNSUPPORTED otherwise, with a message).
+ *  - state->stream is the caller's stream that orders its own reads and
+ *    writes of the columns (NULL: the legacy default stream).  The step
+ *    runs on the context's compute stream after the work queued on
+ *    state->stream so far, and work queued on state->stream after the call
+ *    runs after the step; with state->stream equal to the compute stream
+ *    (as rp_device_state_get returns it) nothing extra is ordered.
  *  - The first call on a device looks up the buffer's device address; make
- *    that first call before any stream capture.
+ *    that first call before any stream capture.  A process that resets the
+ *    device (cudaDeviceReset) between calls is not supported: the address
+ *    is kept for the life of the process.
  *  - Calls share the buffer: calls that overlap on the GPU (other streams or
  *    threads) race and must be serialised by the caller.  Its contents are
  *    never read before the same call writes them, so nothing is cleared.

@@ -77,7 +77,7 @@ class OrcParams(C.Structure):
         ("salttemp_on", C.c_int), ("salttemp_mean", C.c_int), ("write_bottom", C.c_int),
         ("behavior", C.c_int), ("process_va", C.c_int), ("process_wa", C.c_int), ("va_flag", C.c_int),
         ("swimfast", C.c_double), ("initsize", C.c_double),
-    ] + [(k, C.c_double) for k in FUCHS]
+    ] + [(k, C.c_double) for k in FUCHS] + [("vt_variant", C.c_int), ("vt_dy_end", C.c_double)]
 
 
 class OrcParticles(C.Structure):
@@ -329,6 +329,10 @@ class OracleModel:
         p.initsize = float(params.get("initsize", 0.0))
         for k in FUCHS:
             setattr(p, k, float(params.get(k, 0.0)))
+        # VTurb experiment variants (well-mixed-condition attribution);
+        # defaults are the reference's algorithm
+        p.vt_variant = int(params.get("vt_variant", 0))
+        p.vt_dy_end = float(params.get("vt_dy_end", float("nan")))
         # -DWETDRY: the frames' wet/dry masks replace the static ones in
         # getInterp3D and getInterpStr
         self.wetdry = bool(params.get("wetdry", 0))

@@ -1173,13 +1173,28 @@ static double vturb(const step_env *e, double Xpar, double Ypar, double Zpar, co
      * (ver_turb_module.f90:131-136); they are taken as serr. */
     dy[1] = prm->serr;
     dy[np] = prm->serr;
-    int iters = 0;
-    orc_smooth(&fitz[1], &fitkh[1], &dy[1], np, prm->smth, w->v, w->a, prm->spline_max_iter, &iters);
-    if (iters < 0) { *fl |= ORC_FLAG_SPLINE; iters = -iters; }
-    *n_iter += iters;
-    for (int i = 1; i <= np; i++)
-        for (int j = 1; j <= 4; j++)
-            w->coefsm[(j - 1) + (int64_t)(i - 1) * 4] = w->a[(i - 1) + (int64_t)(j - 1) * np];
+    if (prm->vt_dy_end == prm->vt_dy_end) { dy[1] = prm->vt_dy_end; dy[np] = prm->vt_dy_end; }
+    /* experiment variant 1: K = c 4 xi (1 - xi) fitted to the column */
+    double pc = 0.0;
+    const double hcol = zeta - tdepth;
+    if (prm->vt_variant == 1) {
+        double num = 0.0, den = 0.0;
+        for (int k = 1; k <= sw; k++) {
+            const double xi = (z[k] - tdepth) / hcol;
+            const double phi = 4.0 * xi * (1.0 - xi);
+            num += kh[k] * phi;
+            den += phi * phi;
+        }
+        pc = den > 0.0 ? num / den : 0.0;
+    } else {
+        int iters = 0;
+        orc_smooth(&fitz[1], &fitkh[1], &dy[1], np, prm->smth, w->v, w->a, prm->spline_max_iter, &iters);
+        if (iters < 0) { *fl |= ORC_FLAG_SPLINE; iters = -iters; }
+        *n_iter += iters;
+        for (int i = 1; i <= np; i++)
+            for (int j = 1; j <= 4; j++)
+                w->coefsm[(j - 1) + (int64_t)(i - 1) * 4] = w->a[(i - 1) + (int64_t)(j - 1) * np];
+    }
 
     const double deltat = prm->deltat;
     const int loop = prm->idt / (int)deltat;
@@ -1187,13 +1202,19 @@ static double vturb(const step_env *e, double Xpar, double Ypar, double Zpar, co
     for (int i = 1; i <= loop; i++) {
         double Kprimec = 0.0, KprimeZc, Z3rdc, KH3rdc, DEV, r, dTz, newZc;
         if (ParZc <= tdepth || ParZc >= zeta) Kprimec = 0.0;
+        else if (prm->vt_variant == 1) Kprimec = pc * 4.0 * (1.0 - 2.0 * ((ParZc - tdepth) / hcol)) / hcol;
         else Kprimec = orc_ppvalu(&fitz[1], w->coefsm, np - 1, 4, ParZc, 1);
         KprimeZc = Kprimec * deltat;
         Z3rdc = ParZc + 0.5 * KprimeZc;
         if (Z3rdc < tdepth || Z3rdc > zeta) {
             KH3rdc = prm->aksback;
         } else {
-            KH3rdc = orc_ppvalu(&fitz[1], w->coefsm, np - 1, 4, Z3rdc, 0);
+            if (prm->vt_variant == 1) {
+                const double xi = (Z3rdc - tdepth) / hcol;
+                KH3rdc = pc * 4.0 * xi * (1.0 - xi);
+            } else {
+                KH3rdc = orc_ppvalu(&fitz[1], w->coefsm, np - 1, 4, Z3rdc, 0);
+            }
             if (KH3rdc < prm->aksback) KH3rdc = prm->aksback;
         }
         DEV = draw_normal(nc, (uint32_t)(1 + i));

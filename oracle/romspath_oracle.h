@@ -89,6 +89,15 @@ typedef struct {
     int behavior, process_va, process_wa, va_flag;
     double swimfast, initsize;
     double vort_cr, vort_sat, b0pv, b1pv, b0wv, b1w, acc_cr, acc_sat, b0pa, b1pa, b0wa;
+    /* Experiment variants of VTurb for attributing well-mixed-condition
+     * results (0 / NaN: the reference's algorithm).  vt_variant 1 replaces
+     * the smoothing-spline fit by the parabola K = c 4 xi (1 - xi),
+     * xi = (z - tdepth) / (zeta - tdepth), with c the least-squares fit to
+     * the column, and K' its exact derivative; vt_dy_end, when not NaN, is
+     * the value of dy(1) and dy(np) (never set by the reference,
+     * ver_turb_module.f90:131-136; pinned to serr otherwise). */
+    int vt_variant;
+    double vt_dy_end;
 } orc_params;
 
 typedef struct {

@@ -89,6 +89,7 @@ struct rp_ctx {
     cudaStream_t s_comp = nullptr, s_copy = nullptr;
     cudaStream_t s_out = nullptr;              // read-back of asynchronous output records
     cudaEvent_t ev_packed = nullptr, ev_out_done = nullptr;
+    cudaEvent_t ev_na_in = nullptr, ev_na_out = nullptr;   // rp_step_noalloc: caller stream <-> compute stream
     bool out_pending = false;                  // an asynchronous record's copies may be in flight
     // noise hook
     double* hook = nullptr;
@@ -338,6 +339,8 @@ void free_ctx(rp_ctx* c) {
     if (c->s_copy) cudaStreamDestroy(c->s_copy);
     if (c->s_out) cudaStreamDestroy(c->s_out);
     if (c->ev_packed) cudaEventDestroy(c->ev_packed);
+    if (c->ev_na_in) cudaEventDestroy(c->ev_na_in);
+    if (c->ev_na_out) cudaEventDestroy(c->ev_na_out);
     if (c->ev_out_done) cudaEventDestroy(c->ev_out_done);
     delete c;
 }
@@ -882,6 +885,8 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
         cudaStreamCreateWithFlags(&ctx->s_out, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->ev_packed, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->ev_out_done, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->ev_na_in, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->ev_na_out, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess)
         return bail(RP_ERR_CUDA, "stream/event creation");
     if (cudaDeviceSynchronize() != cudaSuccess) return bail(RP_ERR_CUDA, "initial upload");
@@ -1175,9 +1180,21 @@ int rp_step_noalloc(rp_ctx* ctx, const rp_device_state* st, const double ex[3], 
         const int used[3] = {G.map[t_b - 1], G.map[t_c - 1], G.map[t_f - 1]};
         for (int q = 0; q < 3; q++) CK(cudaStreamWaitEvent(s, G.slot_ready[used[q]], 0));
     }
+    // order the step after the caller's queued work on its stream (NULL:
+    // the legacy default stream), and the caller's later work after the step
+    cudaStream_t cs = static_cast<cudaStream_t>(st->stream);
+    const bool other = cs != s;
+    if (other) {
+        CK(cudaEventRecord(ctx->ev_na_in, cs));
+        CK(cudaStreamWaitEvent(s, ctx->ev_na_in, 0));
+    }
     int nl = 0;
     if (st->n > 0)
         CK(rp::launch_step_noalloc(A, ctx->prm.field_dtype, ctx->npmax, ctx->device, s, ctx->num_sms, &nl));
+    if (other) {
+        CK(cudaEventRecord(ctx->ev_na_out, s));
+        CK(cudaStreamWaitEvent(cs, ctx->ev_na_out, 0));
+    }
     ctx->launches += nl;
     ctx->step_index++;
     return RP_OK;

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "rp_internal.h"
 #include "rp_step.cuh"
@@ -36,11 +37,18 @@ namespace {
 // symbol is only a host-side stand-in, so the address comes from
 // cudaGetSymbolAddress with the device current (once per device, on the
 // first call there -- which must therefore come before any stream capture).
+// The table is filled under a lock, so host threads driving contexts on
+// the same device may make their first calls at the same time.  The
+// address belongs to the device's primary context: after a cudaDeviceReset
+// the module is loaded again elsewhere and the cached address is stale, so
+// the entry point is not for processes that reset a device between calls.
 constexpr int kMaxDevices = 64;
 double* g_scratch[kMaxDevices] = {};
+std::mutex g_scratch_lock;
 
 cudaError_t scratch_for_device(int device, double** out) {
     if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> guard(g_scratch_lock);
     if (!g_scratch[device]) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, rp_noalloc_turbv);

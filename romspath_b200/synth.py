@@ -307,13 +307,15 @@ class Release:
 
 
 def uniform_release(spec: GridSpec, grid, frame1, n: int, seed: int = 0,
-                    dob: float = 0.0) -> Release:
+                    dob: float = 0.0, s_range=(-0.98, -0.02)) -> Release:
     """n particles uniform in (X, Y, s) over the wet interior of one grid.
 
     Positions are fractional rho indices in [2, xi_rho-1) x [2, eta_rho-1),
     the range the reference's bounds() accepts (boundary_module.f90:71);
     points whose four surrounding rho points are not all wet are redrawn.
-    z = zeta + (zeta + h) s with h, zeta bilinear at the point.
+    z = zeta + (zeta + h) s with h, zeta bilinear at the point and s
+    uniform over s_range: by default the column less its bottom and top
+    2 %, (-1, 0) for the whole column (a well-mixed start).
     """
     rng = np.random.default_rng(seed)
     nx, ny = spec.xi_rho, spec.eta_rho
@@ -335,7 +337,7 @@ def uniform_release(spec: GridSpec, grid, frame1, n: int, seed: int = 0,
         X[filled:filled + len(sel)] = xs[sel]
         Y[filled:filled + len(sel)] = ys[sel]
         filled += len(sel)
-    s = rng.uniform(-0.98, -0.02, n)
+    s = rng.uniform(s_range[0], s_range[1], n)
     I = np.floor(X).astype(np.int64)
     J = np.floor(Y).astype(np.int64)
     fx = X - I

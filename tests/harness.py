@@ -62,7 +62,9 @@ class Case:
 
 
 def make_case(name: str, npart: int, seed: int = 0, spec_over: Optional[dict] = None,
-              param_over: Optional[dict] = None) -> Case:
+              param_over: Optional[dict] = None, s_range=(-0.98, -0.02)) -> Case:
+    """The named workload with `npart` particles; a single grid's release is
+    uniform in s over `s_range` ((-1, 0): the whole water column)."""
     specs = synth.config_spec(name)
     if spec_over:
         specs = [dataclasses.replace(sp, **spec_over) for sp in specs]
@@ -75,7 +77,7 @@ def make_case(name: str, npart: int, seed: int = 0, spec_over: Optional[dict] = 
         c.scl, c.off = synth.nest_maps(specs)
         c.release = synth.nested_release(specs, grids, c.frame(1, len(specs)), npart, seed=seed)
     else:
-        c.release = synth.uniform_release(specs[0], grids[0], c.frame(1), npart, seed=seed)
+        c.release = synth.uniform_release(specs[0], grids[0], c.frame(1), npart, seed=seed, s_range=s_range)
     return c
 
 

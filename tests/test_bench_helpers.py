@@ -80,6 +80,12 @@ def test_measured_peaks_file_forms(tmp_path):
     assert bench.measured_peaks(str(p)) == (6549.5, "measured (MEASURED_PEAKS.json hbm_gbs)")
     p.write_text(json.dumps({"gpu0": {"hbm_gbs": 6400.0}}))
     assert bench.measured_peaks(str(p))[0] == 6400.0
+    p.write_text(json.dumps({"gpus": [{"index": 0}, {"hbm_gbs": 6300.0}]}))
+    assert bench.measured_peaks(str(p))[0] == 6300.0          # objects inside lists
+    p.write_text(json.dumps({"hbm_gbs": True, "detail": {"hbm_gbs": 6200.0}}))
+    assert bench.measured_peaks(str(p))[0] == 6200.0          # a boolean is not a bandwidth
+    p.write_text(json.dumps({"hbm_gbs": True}))
+    assert bench.measured_peaks(str(p)) == (6650.0, "fallback (6.65 TB/s)")
     p.write_text("not json")
     assert bench.measured_peaks(str(p)) == (6650.0, "fallback (6.65 TB/s)")
     assert bench.measured_peaks(str(tmp_path / "absent.json"))[1].startswith("fallback")

@@ -96,35 +96,30 @@ def _column_hist(st):
     return counts
 
 
-def test_mixed_well_mixed_condition():
-    """Visser (1997): a uniform distribution stays uniform under VTurb alone,
-    chi-square on 20 bins below 43.8 (19 dof, p = 0.001), at the sample
-    size where the reference algorithm itself passes it (3000 particles)."""
-    case = harness.make_case("tiny", 3000, seed=9, spec_over={"land": "none"},
-                             param_over={"scheme": 0, "hturb_on": 0})
-    mix, T = harness.run_gpu(case, 48, noise="philox", seed=21, field_dtype="mixed")
-    counts = _column_hist(mix)
+def _chi2(counts):
     exp = counts.sum() / 20
-    chi2 = float(((counts - exp) ** 2 / exp).sum())
-    print("mixed WMC chi2 (3000):", chi2)
-    assert chi2 < 43.8
-    T.close()
+    return float(((counts - exp) ** 2 / exp).sum())
 
 
-def test_mixed_column_profile_matches_fp64():
-    """With 20000 particles the reference algorithm's own random walk is
-    measurably non-uniform near the reflecting bottom and surface (the CPU
-    oracle gives chi-square ~90 on 20 bins, the end bins ~18 % short), so
-    the mixed form is held to the FP64 form's profile instead: same release,
-    same Philox noise, every bin within 3 sqrt(count) and total L1 below 2 %
-    of the particles."""
+def test_well_mixed_condition_exact_and_mixed():
+    """Visser (1997): a distribution uniform over the whole water column
+    stays uniform under VTurb alone: 20,000 particles, 48 steps, chi-square
+    on 20 bins below 43.8 (19 dof, p = 0.001).  The exact form's profile
+    equals the oracle's bin for bin (the runs are bit-identical); the mixed
+    form passes the test and its profile stays within 3 sqrt(count) of the
+    exact form's in every bin (total L1 below 2 % of the particles)."""
     case = harness.make_case("tiny", 20000, seed=9, spec_over={"land": "none"},
-                             param_over={"scheme": 0, "hturb_on": 0})
+                             param_over={"scheme": 0, "hturb_on": 0}, s_range=(-1.0, 0.0))
     ref, T0 = harness.run_gpu(case, 48, noise="philox", seed=21)
     mix, T1 = harness.run_gpu(case, 48, noise="philox", seed=21, field_dtype="mixed")
-    hr, hm = _column_hist(ref), _column_hist(mix)
-    print("fp64 profile:", hr.tolist())
-    print("mixed profile:", hm.tolist())
+    o, _ = harness.run_oracle(case, 48, noise="philox", seed=21)
+    hr, hm, ho = _column_hist(ref), _column_hist(mix), _column_hist(o)
+    print("oracle profile:", ho.tolist(), "chi2", _chi2(ho))
+    print("exact profile:", hr.tolist(), "chi2", _chi2(hr))
+    print("mixed profile:", hm.tolist(), "chi2", _chi2(hm))
+    assert np.array_equal(hr, ho)
+    assert _chi2(hr) < 43.8
+    assert _chi2(hm) < 43.8
     assert np.all(np.abs(hm - hr) <= 3 * np.sqrt(np.maximum(hr, 1)))
     assert np.abs(hm - hr).sum() < 0.02 * hr.sum()
     T0.close()

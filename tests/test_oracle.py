@@ -341,12 +341,15 @@ def test_vertical_reflection_formula():
 
 
 def test_well_mixed_condition_cpu():
-    """Visser (1997): a uniform particle distribution stays uniform under the
-    random displacement model with non-uniform K (VTurb only)."""
+    """Visser (1997): a particle distribution uniform over the whole water
+    column stays uniform under the random displacement model with
+    non-uniform K (VTurb only), 20,000 particles after 48 steps.  (A
+    release that leaves the bottom and top 2 % of the column empty fails
+    this after 48 steps, chi-square ~90, because those bins have not
+    filled yet; it passes after 2 days -- oracle/wmc_study.py.)"""
     from harness import make_case, run_oracle
-    case = make_case("tiny", 3000, seed=9, spec_over={"land": "none"},
-                     param_over={"scheme": 0, "hturb_on": 0})
-    # uniform in s-coordinate at a fixed flat-ish point: use the release as is
+    case = make_case("tiny", 20000, seed=9, spec_over={"land": "none"},
+                     param_over={"scheme": 0, "hturb_on": 0}, s_range=(-1.0, 0.0))
     o, m = run_oracle(case, 48, noise="philox", seed=21)
     rel = (o["z"] + o["bath"]) / (o["bath"] + o["zeta"])   # fraction of water column
     counts, _ = np.histogram(rel, bins=20, range=(0.0, 1.0))
