@@ -119,7 +119,7 @@ typedef struct rp_params {
  * the duration of rp_create(). */
 typedef struct rp_grid {
     int32_t xi_rho, eta_rho;             /* rho-point dimensions              */
-    int32_t n_rho;                       /* s_rho (N); s_w = N+1              */
+    int32_t n_rho;                       /* s_rho (N), 2..510; s_w = N+1      */
     int32_t vtransform;                  /* 1, 2 or 3                         */
     double hc;
     const double *h, *pm, *pn;           /* (xi_rho, eta_rho)                 */

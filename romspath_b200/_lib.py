@@ -12,6 +12,7 @@ from . import build as _build
 MAXNGRID = 5
 NOALLOC_MAX_PARTICLES = 1048576
 RP_OK = 0
+ERR_ARG, ERR_CUDA, ERR_STATE, ERR_NOMEM, ERR_UNSUPPORTED, ERR_NOEXT = -1, -2, -3, -4, -5, -6
 ERRORS = {-1: "RP_ERR_ARG", -2: "RP_ERR_CUDA", -3: "RP_ERR_STATE", -4: "RP_ERR_NOMEM",
           -5: "RP_ERR_UNSUPPORTED", -6: "RP_ERR_NOEXT"}
 FIELD_F64, FIELD_F32, FIELD_MIXED, FIELD_MIXED_I16 = 0, 1, 2, 3

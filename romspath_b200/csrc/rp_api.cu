@@ -741,7 +741,10 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
     for (int k = 0; k < ngrid; k++) {
         const rp_grid& R = grids[k];
         GridBuf& G = ctx->g[k];
-        if (R.xi_rho < 4 || R.eta_rho < 4 || R.n_rho < 1 || R.n_rho > 510) return bail(RP_ERR_ARG, "bad grid dims");
+        // N >= 2: with one s-level the reference's linint search (interpolation_module.f90:37-47)
+        // never ends for a resampling point below the first level
+        if (R.xi_rho < 4 || R.eta_rho < 4 || R.n_rho < 2 || R.n_rho > 510)
+            return bail(RP_ERR_ARG, "bad grid dims (xi_rho, eta_rho >= 4; 2 <= N <= 510)");
         if (R.vtransform < 1 || R.vtransform > 3) return bail(RP_ERR_ARG, "bad Vtransform");
         if (!R.h || !R.pm || !R.pn || !R.mask_rho || !R.mask_u || !R.mask_v || !R.s_rho || !R.cs_r || !R.s_w || !R.cs_w)
             return bail(RP_ERR_ARG, "null grid array");

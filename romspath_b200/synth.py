@@ -505,6 +505,17 @@ def config_spec(name: str) -> List[GridSpec]:
                          x0=14000.0, y0=9000.0, eddy=0.1, gyre_lx=lx, gyre_ly=ly)
         P.gyre_lx, P.gyre_ly = lx, ly
         return [child, P]
+    if name == "nest3_tiny":
+        # a parent with two sibling children, 5x (child B) and 3x (child A),
+        # in config 4's [child B, child A, parent] order
+        P = GridSpec(40, 32, 6, land="corner", field_dtype="f64")
+        lx, ly = (P.xi_rho - 1) * P.dx, (P.eta_rho - 1) * P.dy
+        A = GridSpec(31, 25, 6, land="none", field_dtype="f64", dx=1000.0 / 3, dy=1000.0 / 3,
+                     x0=4000.0, y0=5000.0, eddy=0.1, gyre_lx=lx, gyre_ly=ly)
+        B = GridSpec(31, 26, 6, land="none", field_dtype="f64", dx=200.0, dy=200.0,
+                     x0=22000.0, y0=12000.0, eddy=0.1, gyre_lx=lx, gyre_ly=ly)
+        P.gyre_lx, P.gyre_ly = lx, ly
+        return [B, A, P]
     if name == "cfg4":
         # parent 400x300x30; child A 240x180x30 (3x); child B 300x250x30 (5x)
         P = GridSpec(400, 300, 30, land="islands", land_frac=0.08, land_seed=4, field_dtype="f32",
@@ -534,7 +545,7 @@ def config_params(name: str) -> dict:
                 sub=4.0, deltat=30.0, aksback=1e-8, constant_hturb=[0.0] * 5)
     if name == "cfg2":
         base.update(hturb_on=1, constant_hturb=[1.0] * 5)
-    if name in ("tiny", "nest_tiny"):
+    if name in ("tiny", "nest_tiny", "nest3_tiny"):
         base.update(hturb_on=1, constant_hturb=[1.0] * 5)
     if name == "cfg4":
         base.update(hturb_on=1, constant_hturb=[1.0] * 5)

@@ -137,11 +137,13 @@ def run_gpu(case: Case, nsteps: int, noise: str = "philox", seed: int = 7,
 
 
 def run_oracle(case: Case, nsteps: int, noise: str = "philox", seed: int = 7,
-               hook: Optional[np.ndarray] = None, nthreads: int = 8, spline_stats: Optional[list] = None):
+               hook: Optional[np.ndarray] = None, nthreads: int = 8, spline_stats: Optional[list] = None,
+               spline_max_iter: int = 100):
     """The oracle's run of the same steps; ``spline_stats`` (a list) gets
     each step's (smoothing-spline fits, secant iterations)."""
     from oracle import oracle as O
-    m = O.OracleModel(case.specs, case.grids, case.params, scl=case.scl, off=case.off)
+    m = O.OracleModel(case.specs, case.grids, case.params, scl=case.scl, off=case.off,
+                      spline_max_iter=spline_max_iter)
     for (k, slot) in schedule.initial_loads():
         for ng in range(1, case.ngrid + 1):
             m.set_frame(ng, slot, case.stored(k, ng))

@@ -38,7 +38,8 @@ def _run(case, nsteps, field_dtype=None, graph=False, blocks_per_sm=0, resort=0,
     return st
 
 
-@pytest.mark.parametrize("name,npart,nsteps", [("tiny", 300, 40), ("nest_tiny", 400, 30)])
+@pytest.mark.parametrize("name,npart,nsteps", [("tiny", 300, 40), ("nest_tiny", 400, 30),
+                                               ("nest3_tiny", 600, 36)])
 def test_graph_steps_match_oracle(name, npart, nsteps):
     case = harness.make_case(name, npart, seed=5)
     g = _run(case, nsteps, graph=True, blocks_per_sm=2, resort=6)

@@ -148,17 +148,18 @@ def test_mixed_set_get_roundtrip_and_noalloc_refused():
     T.close()
 
 
-def test_mixed_nested_grids_handoff():
-    """Nested grids (a 3x child inside its parent): the mixed form hands
-    particles between grids like the FP64 form (same grid ids for at least
-    99 % of particles after 36 steps, RMS position difference below 2e-3
-    cells of the grid that holds them)."""
-    case = harness.make_case("nest_tiny", 400, seed=4)
+@pytest.mark.parametrize("name,ngrid", [("nest_tiny", 2), ("nest3_tiny", 3)])
+def test_mixed_nested_grids_handoff(name, ngrid):
+    """Nested grids (a 3x child inside its parent; a 5x and a 3x sibling
+    inside theirs): the mixed form hands particles between grids like the
+    FP64 form (same grid ids for at least 99 % of particles after 36 steps,
+    RMS position difference below 2e-3 cells of the grid that holds them)."""
+    case = harness.make_case(name, 400, seed=4)
     ref, T0 = harness.run_gpu(case, 36, noise="philox", seed=3)
     mix, T1 = harness.run_gpu(case, 36, noise="philox", seed=3, field_dtype="mixed-i16")
     same = ref["gid"] == mix["gid"]
     assert same.mean() >= 0.99
-    assert len(np.unique(ref["gid"])) == 2                # both grids hold particles
+    assert len(np.unique(ref["gid"])) == ngrid            # every grid holds particles
     ok = same & _moved(ref) & _moved(mix)
     d = np.hypot(mix["x"][ok] - ref["x"][ok], mix["y"][ok] - ref["y"][ok])
     print("nested mixed-i16 vs fp64: rms", float(np.sqrt(np.mean(d * d))), "gid agreement", same.mean())

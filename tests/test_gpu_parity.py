@@ -39,6 +39,10 @@ CASES = [
     ("nest-philox", "nest_tiny", 400, 72, "philox", None, None),
     ("nest-hook", "nest_tiny", 300, 36, "hook", None, None),
     ("nest-oob", "nest_tiny", 300, 60, "philox", None, {"open_ocean_boundary": 1}),
+    # two sibling children (5x and 3x) of one parent, config 4's grid order
+    ("nest3-det", "nest3_tiny", 600, 96, "off", None, {"vturb_on": 0, "hturb_on": 0}),
+    ("nest3-philox", "nest3_tiny", 600, 72, "philox", None, None),
+    ("nest3-hook", "nest3_tiny", 400, 36, "hook", None, None),
 ]
 
 
@@ -89,6 +93,20 @@ def test_nested_handoff_happens():
     T.close()
     assert (g0["gid"] != g["gid"]).sum() > 20
     assert set(np.unique(g["gid"])) == {1.0, 2.0}
+
+
+def test_sibling_nest_handoff_all_directions():
+    """The three-grid sibling case moves particles from each child to the
+    parent and from the parent into each child."""
+    import collections
+    case = harness.make_case("nest3_tiny", 600, seed=3)
+    g0, T0 = harness.run_gpu(case, 0)
+    T0.close()
+    g, T = harness.run_gpu(case, 72)
+    T.close()
+    moves = collections.Counter(zip(g0["gid"].astype(int), g["gid"].astype(int)))
+    for a, b in ((1, 3), (2, 3), (3, 1), (3, 2)):
+        assert moves[(a, b)] > 0, moves
 
 
 def test_split_contexts_match_one_context():

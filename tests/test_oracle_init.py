@@ -133,3 +133,32 @@ def test_host_nest_maps_match_oracle_search(case):
         np.testing.assert_array_equal(oo[1][2], [7.0 - 0.25, 6.0 - 0.25])
         # grid 1 -> grid 3: refine(2)^2 = 4
         np.testing.assert_array_equal(so[0][2], [0.25, 0.25])
+
+
+def test_synth_pair_maps_equal_reference_chain_maps():
+    """On a chain of nested grids (refinement 4 per level, finest first)
+    the affine maps the synthetic workloads use for every grid pair
+    (synth.nest_maps, which config 4's siblings also use) equal the
+    reference's own: grefine(a,b) = refine(|a-b|)^|a-b| and the offsets from
+    the first coincident lon/lat point (grid_module.f90:441-481), found both
+    by the oracle's search and by rp_nest_maps."""
+    from romspath_b200.tracker import nest_maps
+    specs = [synth.GridSpec(33, 29, 4, dx=64.0, dy=64.0, x0=6144.0, y0=4864.0),
+             synth.GridSpec(31, 25, 4, dx=256.0, dy=256.0, x0=5120.0, y0=4096.0),
+             synth.GridSpec(30, 24, 4, dx=1024.0, dy=1024.0)]
+    grids = [synth.make_grid(s) for s in specs]
+    for sp, g in zip(specs, grids):
+        lo, la = np.meshgrid(sp.x0 + np.arange(sp.xi_rho) * sp.dx, sp.y0 + np.arange(sp.eta_rho) * sp.dy,
+                             indexing="ij")
+        g["lon_rho"], g["lat_rho"] = np.asfortranarray(lo), np.asfortranarray(la)
+    refine = [4.0, 4.0]
+    s_syn, o_syn = synth.nest_maps(specs)
+    s_lib, o_lib = nest_maps(grids, refine)
+    m = O.OracleModel(specs, grids, synth.config_params("tiny"))
+    s_orc, o_orc = m.nest_maps(refine)
+    np.testing.assert_array_equal(s_lib, s_orc)
+    np.testing.assert_array_equal(o_lib, o_orc)
+    np.testing.assert_array_equal(np.asarray(s_lib), s_syn)
+    np.testing.assert_array_equal(np.asarray(o_lib), o_syn)
+    # fine -> parent skips a level: 1/refine(2)^2
+    np.testing.assert_array_equal(s_syn[0][2], [1.0 / 16.0, 1.0 / 16.0])
