@@ -2,9 +2,10 @@
 
 * The smoothing spline's secant search (pppack.f90:5275-5292) has no
   iteration cap in the reference; here it stops at rp_params.
-  spline_max_iter and sets RP_FLAG_SPLINE.  With the cap at 1 and jagged
-  AKs columns, the flag must be set on exactly the particles where the
-  oracle (same cap) sets it, with every other column bit-identical.
+  spline_max_iter and sets RP_FLAG_SPLINE.  With the cap at 4 and jagged
+  AKs columns (the oracle flags 111 of 300 particles in 36 steps), the flag
+  must be set on exactly the particles where the oracle (same cap) sets
+  it, with every other column bit-identical.
 * A frame with NaN diffusivities in one region and NaN velocities in
   another: the step returns RP_OK, every loop ends (bisections narrow, the
   secant search is capped, the column search is guarded), every status is
@@ -55,10 +56,10 @@ def _err(T):
 def test_spline_cap_flags_match_oracle(variant):
     case = harness.make_case("tiny", 300, seed=13)
     _jagged(case)
-    T = _tracker(case, spline_max_iter=1, variant=variant)
+    T = _tracker(case, spline_max_iter=4, variant=variant)
     g, _ = harness.run_gpu(case, 36, tracker=T)
     T.close()
-    o, _ = harness.run_oracle(case, 36, spline_max_iter=1)
+    o, _ = harness.run_oracle(case, 36, spline_max_iter=4)
     bad = {k: v for k, v in harness.compare(g, o).items() if v}
     assert not bad, bad
     hit = (g["flags"] & _lib.FLAG_SPLINE) != 0
