@@ -386,6 +386,12 @@ module rp_gpu_mod
       integer(c_int32_t), value :: resort, blocks_per_sm
     end function rp_set_launch
 
+    integer(c_int) function rp_set_kernel_form(ctx, form) bind(C, name="rp_set_kernel_form")
+      import :: c_int, c_int32_t, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: form
+    end function rp_set_kernel_form
+
     integer(c_int) function rp_last_step_stats(ctx, ms, kernels) bind(C, name="rp_last_step_stats")
       import :: c_int, c_int32_t, c_ptr, c_float
       type(c_ptr), value :: ctx

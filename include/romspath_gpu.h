@@ -99,7 +99,10 @@ typedef struct rp_params {
     uint64_t seed;                       /* Philox key of the turbulence noise */
     int32_t device;                      /* CUDA device ordinal               */
     int32_t reserved[7];                 /* [0]: kernel form, 0 fused (default),
-                                            1 split; [1]: re-sort the particle
+                                            1 split, 2 shared-memory split
+                                            and 3 fused without load-ahead
+                                            (mixed forms; rp_set_kernel_form);
+                                            [1]: re-sort the particle
                                             state by grid and cell every that
                                             many internal steps (0: never;
                                             results are unchanged, gathers
@@ -458,6 +461,18 @@ int rp_adj_replay(rp_ctx *ctx, const double *x0, const double *y0, const double 
  * steps; results do not depend on them (an autotuner times real steps of
  * the run under each setting).  No counterpart in the reference. */
 int rp_set_launch(rp_ctx *ctx, int32_t resort, int32_t blocks_per_sm);
+
+/* Change the kernel form of rp_params.reserved[0] between steps: 0 fused
+ * (one kernel per step, the fit's workspace in local memory), 1 split (a
+ * VTurb kernel writing each particle's displacement, then the advection
+ * kernel), and for the mixed forms 2, the split form with the VTurb
+ * kernel's spline workspace in shared memory, and 3, the fused kernel
+ * whose back substitution does not load u ahead (the exact forms run 2
+ * and 3 fused).  Results do not change beyond rounding (the exact forms:
+ * not at all); which form is fastest depends on the grid and the particle
+ * count, so an autotuner times them on the run.  No counterpart in the
+ * reference. */
+int rp_set_kernel_form(rp_ctx *ctx, int32_t form);
 
 /* Timing of the last rp_step launch sequence on the compute stream, in ms
  * (CUDA events), and the number of kernels it launched. */

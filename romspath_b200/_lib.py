@@ -28,6 +28,7 @@ EXPORTS = [
     "rp_get_diagnostics", "rp_reset_diagnostics", "rp_set_grid_lonlat", "rp_output_record", "rp_upload_frame_desc",
     "rp_set_behavior", "rp_get_behavior", "rp_set_grid_angle", "rp_locate_lonlat", "rp_nest_maps",
     "rp_output_record_async", "rp_output_wait", "rp_count_spline_passes", "rp_spline_pass_counts",
+    "rp_set_kernel_form",
 ]
 
 PD = C.POINTER(C.c_double)
@@ -153,6 +154,7 @@ def _declare(L):
                                   C.c_int32]
     L.rp_step_n.argtypes = [P, C.c_int32, PD, PD, PI32, PI32, PI32, PI32]
     L.rp_set_launch.argtypes = [P, C.c_int32, C.c_int32]
+    L.rp_set_kernel_form.argtypes = [P, C.c_int32]
     L.rp_adj_frames.argtypes = [P, C.c_int32]
     L.rp_adj_set_frame.argtypes = [P, C.c_int32, C.c_int32] + [PD] * 7
     L.rp_forward.argtypes = [P, C.c_int32, C.POINTER(RpAdjStep), C.c_double, C.c_int32]

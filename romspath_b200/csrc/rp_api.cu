@@ -716,6 +716,7 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
         return RP_ERR_ARG;
     if (p.reserved[3] & ~(RP_DIAG_SALTTEMP | RP_DIAG_SALTTEMP_MEAN | RP_DIAG_BOTTOM)) return RP_ERR_ARG;
     if (p.reserved[4] != 0 && p.reserved[4] != 1) return RP_ERR_ARG;
+    if (p.reserved[0] < 0 || p.reserved[0] > 3) return RP_ERR_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= p.device || p.device < 0) return RP_ERR_NOEXT;
     rp_ctx* ctx = new rp_ctx();
@@ -1059,7 +1060,7 @@ int step_launch(rp_ctx* ctx, const double ex[3], const double ix[3], int32_t ets
     }
     ctx->since_sort++;
     if (ctx->n > 0 && ctx->mixed)
-        CK(rp::launch_step_mixed(A, ctx->npmax, ctx->i16, (float*)ctx->turbv, ctx->prm.reserved[0] == 1, s,
+        CK(rp::launch_step_mixed(A, ctx->npmax, ctx->i16, (float*)ctx->turbv, ctx->prm.reserved[0], s,
                                  ctx->num_sms, nl));
     else if (ctx->n > 0)
         CK(rp::launch_step(A, ctx->prm.field_dtype, ctx->npmax, ctx->turbv, ctx->prm.reserved[0] == 1 ? 0 : 1, s,
@@ -1650,6 +1651,13 @@ int rp_set_launch(rp_ctx* ctx, int32_t resort, int32_t blocks_per_sm) {
     ctx->prm.reserved[1] = resort;
     ctx->prm.reserved[2] = blocks_per_sm;
     if (ctx->since_sort > resort) ctx->since_sort = resort;
+    return RP_OK;
+}
+
+int rp_set_kernel_form(rp_ctx* ctx, int32_t form) {
+    if (!ctx) return RP_ERR_ARG;
+    if (form < 0 || form > 3) return fail(ctx, RP_ERR_ARG, "rp_set_kernel_form: form must be 0..3");
+    ctx->prm.reserved[0] = form;
     return RP_OK;
 }
 

@@ -15,13 +15,13 @@ namespace rp {
 // Fused form: one thread per particle for the whole step.
 // FEAT: built with the options beyond the passive step (diagnostics,
 // WETDRY, behave); the passive variant is chosen when they are all off.
-template <typename E, int NPMAX, bool FEAT>
+template <typename E, int NPMAX, bool FEAT, bool PREF = true>
 __global__ void __launch_bounds__(kStepBlock, kMixedMinBlocks) k_step_mixed(const __grid_constant__ RpStepArgs A) {
     double buf[kMixedArrays * (NPMAX + 1)];
-    const MSpline<NPMAX> w{buf};
+    const MSpline<NPMAX, PREF> w{buf};
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < A.p.n; n += stride)
-        m_update_one<E, NPMAX, FEAT>(A, n, w, nullptr);
+        m_update_one<E, FEAT>(A, n, w, nullptr);
 }
 
 // Split form: VTurb alone at a resident-thread count whose spline
@@ -34,7 +34,28 @@ __global__ void __launch_bounds__(kStepBlock, kMixedVtMinBlocks) k_vturb_mixed(c
     const MSpline<NPMAX> w{buf};
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < A.p.n; n += stride)
-        m_vturb_one<E, NPMAX>(A, n, w, turbv);
+        m_vturb_one<E>(A, n, w, turbv);
+}
+
+// Split form with the fit's workspace in shared memory: VTurb alone, one
+// thread per particle, 64-thread blocks each holding its threads' u, factor
+// prefix and column (1.1 KB per thread at NPMAX 128: 3 blocks per SM).  The
+// fit's passes then read and write shared memory instead of streaming a
+// local-memory workspace through L2 and HBM.
+constexpr int kSmemBlock = 64;
+constexpr int kSmemKs = 32;              // factor rows 2..33 held in shared memory
+template <int NPMAX>
+using SmemView = MSmemSpline<NPMAX, kSmemKs, NPMAX / 4, kSmemBlock>;
+
+template <typename E, int NPMAX>
+__global__ void __launch_bounds__(kSmemBlock) k_vturb_smem(const __grid_constant__ RpStepArgs A,
+                                                           float* __restrict__ turbv) {
+    extern __shared__ float smf[];
+    float ovf[2 * (NPMAX + 1)];
+    const SmemView<NPMAX> w{smf + threadIdx.x, ovf};
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < A.p.n; n += stride)
+        m_vturb_one<E>(A, n, w, turbv);
 }
 
 template <typename E, bool FEAT>
@@ -43,7 +64,7 @@ __global__ void __launch_bounds__(kStepBlock, kMixedMinBlocks) k_advect_mixed(co
     const MSpline<1> none{nullptr};
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < A.p.n; n += stride)
-        m_update_one<E, 1, FEAT>(A, n, none, turbv);
+        m_update_one<E, FEAT>(A, n, none, turbv);
 }
 
 template <class K>
@@ -65,7 +86,44 @@ static cudaError_t launch_mixed_t(const RpStepArgs& A, float* turbv, int split, 
                                   int* nlaunch) {
     int64_t blocks = 0;
     cudaError_t e;
-    if (!split || !A.vturb_on) {
+    if (split == 2 && A.vturb_on) {
+        // the shared-memory column holds sw <= NPMAX/4 levels
+        int swmax = 0;
+        for (int k = 0; k < A.ngrid; k++) swmax = max(swmax, A.g[k].N + 1);
+        if (swmax > NPMAX / 4) split = 1;
+    }
+    if (split == 2 && A.vturb_on) {
+        const size_t smem = (size_t)SmemView<NPMAX>::kWords * kSmemBlock * sizeof(float);
+        static bool attr_set = false;
+        if (!attr_set) {
+            e = cudaFuncSetAttribute(k_vturb_smem<E, NPMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            attr_set = true;
+        }
+        int occ = 0;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_vturb_smem<E, NPMAX>, kSmemBlock, smem)) !=
+            cudaSuccess)
+            return e;
+        if (occ < 1) occ = 1;
+        blocks = (A.p.n + kSmemBlock - 1) / kSmemBlock;
+        if (blocks > (int64_t)num_sms * occ) blocks = (int64_t)num_sms * occ;
+        k_vturb_smem<E, NPMAX><<<(unsigned)(blocks < 1 ? 1 : blocks), kSmemBlock, smem, s>>>(A, turbv);
+        *nlaunch += 1;
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if ((e = resident_grid(k_advect_mixed<E, FEAT>, A.p.n, num_sms, A.grid_cap, &blocks)) != cudaSuccess) return e;
+        k_advect_mixed<E, FEAT><<<(unsigned)blocks, kStepBlock, 0, s>>>(A, turbv);
+        *nlaunch += 1;
+        return cudaGetLastError();
+    }
+    if (split == 3 && !FEAT) {                     // fused, u not loaded ahead
+        if ((e = resident_grid(k_step_mixed<E, NPMAX, false, false>, A.p.n, num_sms, A.grid_cap, &blocks)) !=
+            cudaSuccess)
+            return e;
+        k_step_mixed<E, NPMAX, false, false><<<(unsigned)blocks, kStepBlock, 0, s>>>(A);
+        *nlaunch += 1;
+        return cudaGetLastError();
+    }
+    if (split == 3 || !split || !A.vturb_on) {
         if ((e = resident_grid(k_step_mixed<E, NPMAX, FEAT>, A.p.n, num_sms, A.grid_cap, &blocks)) != cudaSuccess)
             return e;
         k_step_mixed<E, NPMAX, FEAT><<<(unsigned)blocks, kStepBlock, 0, s>>>(A);

@@ -291,6 +291,18 @@ __device__ __forceinline__ float m_level(const uint2* f, const float4* qs, const
     return acc;
 }
 
+// the same sum from a level's four corner words and scales already loaded
+template <typename E>
+__device__ __forceinline__ float m_level_of(const uint2 v[4], const float4& sc, const float cff[4],
+                                            const bool use[4], const MTime& t) {
+    const float wb = t.wb * m_pick4(sc, t.sb), wc = t.wc * m_pick4(sc, t.sc), wf = t.wf * m_pick4(sc, t.sf);
+    float acc = 0.f;
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+        if (use[q]) acc += cff[q] * (wb * m_slot<E>(v[q], t.sb) + wc * m_slot<E>(v[q], t.sc) + wf * m_slot<E>(v[q], t.sf));
+    return acc;
+}
+
 // zcff1*zprof(Ibot) + zcff2*zprof(Itop), time-interpolated
 template <typename E>
 __device__ __forceinline__ float m_col(const void* fv, const float* qs, const int64_t o[4], const float cff[4],
@@ -464,8 +476,18 @@ using MU = float;
 constexpr int kMixedBytesPerPoint = 2 * (int)sizeof(MRatio) + (int)sizeof(MU) + 4 * 4;
 constexpr int kMixedArrays = (kMixedBytesPerPoint + 7) / 8;
 
-template <int NPMAX>
+struct MFit;
+
+// The per-thread workspace in local memory (the fused step): every array
+// of the fit, the resampled data y stored by the first pass.  PREF: the
+// back substitution loads u four rows ahead (fewer stalls, more registers
+// live; which is faster depends on the workload).
+template <int NPMAX, bool PREF = true>
 struct MSpline {
+    static constexpr bool kStoreY = true;
+    static constexpr int kColBatch = 1;
+    static constexpr bool kLightCheck = false;
+    static constexpr bool kPrefetch = PREF;
     double* base;
     __device__ __forceinline__ MU& u(int i) const { return reinterpret_cast<MU*>(base)[i]; }  // u(i)/v(i,1), then u(i)
     __device__ __forceinline__ MRatio* rb() const {
@@ -480,6 +502,7 @@ struct MSpline {
     __device__ __forceinline__ float& cz(int k) const { return fb()[(NPMAX + 1) + k]; }      // column z(k)
     __device__ __forceinline__ float& cm(int k) const { return fb()[2 * (NPMAX + 1) + k]; }  // slope on [z(k), z(k+1)]
     __device__ __forceinline__ float& cb(int k) const { return fb()[3 * (NPMAX + 1) + k]; }  // intercept
+    __device__ __forceinline__ double yat(const MFit&, int i) const { return (double)y(i); }
 };
 
 struct MFit {
@@ -488,19 +511,53 @@ struct MFit {
     double serr, dy2;
 };
 
+// The workspace in shared memory (the split step's VTurb kernel): u, the
+// factor ratios of the rows before the factor turns stationary (rows
+// 2..KSM+1; later rows, met only when it does not, in the thread's local
+// array `ovf`), and the column's breaks, slopes and intercepts (sw <= CMAX).
+// Element k of a thread sits at word k * B of its own column (threads of a
+// block in consecutive banks).  The resampled data are not stored: ppvalu's
+// two values per piece come from the column (the same m x + b the fit's
+// sweep forms).
+template <int NPMAX, int KSM, int CMAX, int B>
+struct MSmemSpline {
+    static_assert(sizeof(MU) == 4 && sizeof(MRatio) == 4, "shared-memory workspace holds FP32 arrays");
+    static constexpr bool kStoreY = false;
+    static constexpr int kColBatch = 8;
+    static constexpr bool kLightCheck = true;
+    static constexpr bool kPrefetch = true;
+    static constexpr int kWords = NPMAX + 2 * KSM + 3 * CMAX;
+    float* sm;                     // this thread's first word
+    float* ovf;                    // 2 (NPMAX + 1) floats, local
+    __device__ __forceinline__ float& u(int i) const { return sm[(i - 1) * B]; }
+    __device__ __forceinline__ float& s1(int i) const {
+        return (i <= KSM + 1) ? sm[(NPMAX + i - 2) * B] : ovf[i];
+    }
+    __device__ __forceinline__ float& s2(int i) const {
+        return (i <= KSM + 1) ? sm[(NPMAX + KSM + i - 2) * B] : ovf[NPMAX + 1 + i];
+    }
+    __device__ __forceinline__ float& y(int) const { return ovf[0]; }        // never stored (kStoreY)
+    __device__ __forceinline__ float& cz(int k) const { return sm[(NPMAX + 2 * KSM + k - 1) * B]; }
+    __device__ __forceinline__ float& cm(int k) const { return sm[(NPMAX + 2 * KSM + CMAX + k - 1) * B]; }
+    __device__ __forceinline__ float& cb(int k) const { return sm[(NPMAX + 2 * KSM + 2 * CMAX + k - 1) * B]; }
+    // resampled value y(i) at z1 + (i-1) h: the column piece j with
+    // cz(j) <= x (j in 1..sw-1; 1 below cz(2)), found by bisection
+    __device__ __forceinline__ double yat(const MFit& f, int i) const;
+};
+
 // linint of the column at ascending points: the current piece j (slope,
 // intercept and upper end) is held in registers and advanced as needed
-template <int NPMAX>
+template <class W>
 struct MWalk {
     int j;
     double zn, m, b;               // cz(j+1), cm(j), cb(j)
-    __device__ __forceinline__ void init(const MSpline<NPMAX>& w) {
+    __device__ __forceinline__ void init(const W& w) {
         j = 1;
         zn = w.cz(2);
         m = w.cm(1);
         b = w.cb(1);
     }
-    __device__ __forceinline__ double at(const MSpline<NPMAX>& w, int sw, double x) {
+    __device__ __forceinline__ double at(const W& w, int sw, double x) {
         while (j < sw - 1 && zn <= x) {
             j++;
             zn = w.cz(j + 1);
@@ -511,13 +568,25 @@ struct MWalk {
     }
 };
 
+template <int NPMAX, int KSM, int CMAX, int B>
+__device__ __forceinline__ double MSmemSpline<NPMAX, KSM, CMAX, B>::yat(const MFit& f, int i) const {
+    const double x = (i == 1) ? f.z1 : f.z1 + (double)(i - 1) * f.h;
+    int lo = 1, hi = f.sw - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if ((double)cz(mid) <= x) lo = mid; else hi = mid - 1;
+    }
+    return (double)cm(lo) * x + (double)cb(lo);
+}
+
 // One chol1d pass at p: factorise, solve for u, form qu = Q u; returns
 // sum_i qu(i)^2 dy^2 and, on request, utru = sum v4 (u(i-1)(u(i-1)+u(i)) + u(i)^2).
 // With store_y the resampled values y(i) are also kept (for ppvalu); u is
 // written back only with store_u (a pass whose u may be the fit's).
-template <int NPMAX>
-__device__ double m_chol1d(const MSpline<NPMAX>& w, const MFit& f, double p, double* utru_out, bool store_y,
+template <class W>
+__device__ double m_chol1d(const W& w, const MFit& f, double p, double* utru_out, bool store_y,
                            bool store_u) {
+    store_y = store_y && W::kStoreY;
     const int np = f.np;
     const double r = f.serr * f.rh;
     const double r2 = r * r;
@@ -526,7 +595,7 @@ __device__ double m_chol1d(const MSpline<NPMAX>& w, const MFit& f, double p, dou
     const double E = six1mp * (-4.0 * r2) + p * f.h;
     const double F = six1mp * r2;
     // Q'y on the fly: qty(i) = (y(i+1) - 2 y(i) + y(i-1)) / h
-    MWalk<NPMAX> wk;
+    MWalk<W> wk;
     wk.init(w);
     double ym = wk.at(w, f.sw, f.z1);
     double y0 = wk.at(w, f.sw, f.z1 + f.h);
@@ -607,16 +676,21 @@ __device__ double m_chol1d(const MSpline<NPMAX>& w, const MFit& f, double p, dou
         up2 = up1;
         up1 = ui;
     }
-    // u(i) is loaded four rows ahead of its use (index 1 stands in past
-    // the start; that value is never used)
+    // with W::kPrefetch, u(i) is loaded four rows ahead of its use (index 1
+    // stands in past the start; that value is never used)
     MU q0 = w.u(np - 2), q1 = w.u(max(np - 3, 1)), q2 = w.u(max(np - 4, 1)), q3 = w.u(max(np - 5, 1));
 #pragma unroll 2
     for (int i = np - 2; i >= 2; i--) {
-        const double uq = (double)q0;
-        q0 = q1;
-        q1 = q2;
-        q2 = q3;
-        q3 = w.u(max(i - 4, 1));
+        double uq;
+        if constexpr (W::kPrefetch) {
+            uq = (double)q0;
+            q0 = q1;
+            q1 = q2;
+            q2 = q3;
+            q3 = w.u(max(i - 4, 1));
+        } else {
+            uq = (double)w.u(i);
+        }
         const bool held = (i >= ks && i <= np - 3);
         const double s1v = held ? (double)(MRatio)hr1 : (double)w.s1(i);
         const double s2v = held ? (double)(MRatio)hr2 : (double)w.s2(i);
@@ -642,10 +716,92 @@ __device__ double m_chol1d(const MSpline<NPMAX>& w, const MFit& f, double p, dou
 }
 
 // SF(q) = 36 sum qu^2 dy^2 / (1+q)^2 of one chol1d pass at p = q/(1+q)
-template <int NPMAX>
-__device__ __forceinline__ double m_sf(const MSpline<NPMAX>& w, const MFit& f, double q, bool store_y,
+template <class W>
+__device__ __forceinline__ double m_sf(const W& w, const MFit& f, double q, bool store_y,
                                        bool store_u) {
     return 36.0 * m_chol1d(w, f, q / (1.0 + q), nullptr, store_y, store_u) / ((1.0 + q) * (1.0 + q));
+}
+
+// The same sum S(p) = sum qu^2 dy^2 = u'Tu (T = Q'D^2Q) from one forward
+// sweep, with nothing stored and no back substitution.  With
+// M(p) = 6(1-p) T + p R the matrix of chol1d and b = Q'y, let
+// phi(p) = b'M^-1 b = sum_i w_i^2 / d_i over the forward-substituted values
+// w = L^-1 b and the pivots d of M = L diag(d) L'.  Since u'Mu = phi and
+// dphi/dp = -u'M'u = 6 u'Tu - u'Ru, phi + p phi' = 6 u'Tu, i.e.
+//   S(p) = (phi(p) + p phi'(p)) / 6,
+// and phi' is carried through the sweep as derivatives in p of the factor
+// (D, E, F are linear in p) and of w.  The factor turns stationary as in
+// m_chol1d (its ratios and their derivatives repeat in FP32); the last row
+// is factorised from the held state.
+template <class W>
+__device__ double m_light_S(const W& w, const MFit& f, double p) {
+    const int np = f.np;
+    const double r = f.serr * f.rh;
+    const double r2 = r * r;
+    const double six1mp = 6.0 * (1.0 - p);
+    const double D = six1mp * (6.0 * r2) + 4.0 * p * f.h;
+    const double E = six1mp * (-4.0 * r2) + p * f.h;
+    const double F = six1mp * r2;
+    const double Dd = -36.0 * r2 + 4.0 * f.h;          // dD/dp, dE/dp, dF/dp
+    const double Ed = 24.0 * r2 + f.h;
+    const double Fd = -6.0 * r2;
+    MWalk<W> wk;
+    wk.init(w);
+    double ym = wk.at(w, f.sw, f.z1);
+    double y0 = wk.at(w, f.sw, f.z1 + f.h);
+    double yp = wk.at(w, f.sw, f.z1 + 2.0 * f.h);
+    double a1 = D, a2 = E, b1 = D, a1d = Dd, a2d = Ed, b1d = Dd;
+    double wc = (yp - 2.0 * y0 + ym) * f.rh, wcd = 0.0, wp = 0.0, wpd = 0.0;   // w(i), w(i-1) and d/dp
+    double r2p = 0.0, r2pd = 0.0;                                               // ratio2(i-1)
+    double phi = 0.0, phid = 0.0;
+    bool held = false;
+    double hinv = 0.0, hinvd = 0.0, hr1 = 0.0, hr1d = 0.0, hr2 = 0.0, hr2d = 0.0;
+    float pr1 = 0.f, pr2 = 0.f, pr1d = 0.f, pr2d = 0.f;
+#pragma unroll 2
+    for (int i = 2; i <= np - 2; i++) {
+        double inv, invd, ratio1, ratio1d, ratio2, ratio2d;
+        if (!held || i == np - 2) {
+            const double Fi = (i <= np - 3) ? F : 0.0, Fid = (i <= np - 3) ? Fd : 0.0;
+            inv = 1.0 / a1;
+            invd = -a1d * inv * inv;
+            ratio1 = a2 * inv;
+            ratio1d = a2d * inv + a2 * invd;
+            ratio2 = Fi * inv;
+            ratio2d = Fid * inv + Fi * invd;
+            const float q1 = (float)ratio1, q2 = (float)ratio2, q1d = (float)ratio1d, q2d = (float)ratio2d;
+            if (i > 2 && i < np - 2 && q1 == pr1 && q2 == pr2 && q1d == pr1d && q2d == pr2d) {
+                held = true;
+                hinv = inv; hinvd = invd; hr1 = ratio1; hr1d = ratio1d; hr2 = ratio2; hr2d = ratio2d;
+            } else {
+                const double b1n = b1 - ratio1 * a2, b1nd = b1d - ratio1d * a2 - ratio1 * a2d;
+                const double c2 = E - ratio1 * Fi, c2d = Ed - ratio1d * Fi - ratio1 * Fid;
+                const double c1 = D - ratio2 * Fi, c1d = Dd - ratio2d * Fi - ratio2 * Fid;
+                a1 = b1n; a1d = b1nd;
+                a2 = c2; a2d = c2d;
+                b1 = c1; b1d = c1d;
+            }
+            pr1 = q1; pr2 = q2; pr1d = q1d; pr2d = q2d;
+        } else {
+            inv = hinv; invd = hinvd; ratio1 = hr1; ratio1d = hr1d; ratio2 = hr2; ratio2d = hr2d;
+        }
+        phi = phi + wc * wc * inv;
+        phid = phid + (2.0 * wc * wcd) * inv + wc * wc * invd;
+        ym = y0;
+        y0 = yp;
+        yp = wk.at(w, f.sw, f.z1 + (double)(i + 1) * f.h);
+        const double qn = (yp - 2.0 * y0 + ym) * f.rh;           // qty(i+1)
+        const double wn = qn - ratio1 * wc - r2p * wp;
+        const double wnd = -(ratio1d * wc + ratio1 * wcd + r2pd * wp + r2p * wpd);
+        wp = wc; wpd = wcd;
+        wc = wn; wcd = wnd;
+        r2p = ratio2; r2pd = ratio2d;
+    }
+    {                                                              // row np-1
+        const double inv = 1.0 / a1, invd = -a1d * inv * inv;
+        phi = phi + wc * wc * inv;
+        phid = phid + (2.0 * wc * wcd) * inv + wc * wc * invd;
+    }
+    return (phi + p * phid) * (1.0 / 6.0);
 }
 
 // smooth() (pppack.f90:5108-5317): the secant search for q = p/(1-p) on
@@ -655,12 +811,13 @@ __device__ __forceinline__ double m_sf(const MSpline<NPMAX>& w, const MFit& f, d
 // not; then secant steps.  Falls back to the reference's cold start (p = 0,
 // utru) when that does not converge.  q and g are returned in qstate and
 // gstate (q = 0 for p = 0; g <= 0 when unknown); passes = chol1d passes made.
-template <int NPMAX>
-__device__ double m_smooth(const MSpline<NPMAX>& w, const MFit& f, double s, int max_iter, double& qstate,
+template <class W>
+__device__ double m_smooth(const W& w, const MFit& f, double s, int max_iter, double& qstate,
                            double& gstate, uint32_t& fl, int& passes) {
-    // the first pass of every path also stores y(i); passes that are
-    // rarely the last one (the warm-start check, p = 0) do not store u and
-    // are repeated with it when they are
+    // the first full pass of every path also stores y(i); the warm-start
+    // check is a light pass (m_light_S: no workspace traffic), the p = 0
+    // pass does not store u; both are repeated as a full pass when their
+    // p is the fit's
     passes = 1;
     if (s <= 0.0) {
         m_chol1d(w, f, 1.0, nullptr, true, true);
@@ -669,10 +826,20 @@ __device__ double m_smooth(const MSpline<NPMAX>& w, const MFit& f, double s, int
     const double ooss = 1.0 / sqrt(s);
     double q = qstate;
     const bool warm = q > 0.0;
+    bool ys = false;                                 // y(i) stored by a pass already
     if (warm) {
-        double sfq = m_sf(w, f, q, true, false);
+        // the check at the previous q: a light pass where the view asks
+        // for it (one forward sweep, nothing stored; it needs registers the
+        // fused step does not have), else a pass that stores y but not u
+        double sfq;
+        if (W::kLightCheck) {
+            sfq = 36.0 * m_light_S(w, f, q / (1.0 + q)) / ((1.0 + q) * (1.0 + q));
+        } else {
+            sfq = m_sf(w, f, q, true, false);
+            ys = true;
+        }
         if (fabs(sfq - s) <= 0.01 * s) {
-            m_chol1d(w, f, q / (1.0 + q), nullptr, false, true);
+            m_chol1d(w, f, q / (1.0 + q), nullptr, !ys, true);
             passes = 2;
             return q / (1.0 + q);
         }
@@ -680,7 +847,8 @@ __device__ double m_smooth(const MSpline<NPMAX>& w, const MFit& f, double s, int
         const double qn = (gstate > 0.0) ? q + (ooss - prevsf) / gstate : 0.0;
         q = (qn > 0.0) ? qn : q * sqrt(sfq / s);
         for (int it = 0; it < 6 && q > 0.0; it++) {
-            sfq = m_sf(w, f, q, false, true);
+            sfq = m_sf(w, f, q, !ys, true);
+            ys = true;
             passes++;
             const double oosf = 1.0 / sqrt(sfq);
             const double g = (oosf - prevsf) / (q - prevq);
@@ -697,7 +865,7 @@ __device__ double m_smooth(const MSpline<NPMAX>& w, const MFit& f, double s, int
     }
     // cold start: the reference's sequence
     double utru = 0.0;
-    double sfq = 36.0 * m_chol1d(w, f, 0.0, &utru, !warm, false);
+    double sfq = 36.0 * m_chol1d(w, f, 0.0, &utru, !ys, false);
     passes += warm ? 1 : 0;
     if (!(s < sfq)) {
         m_chol1d(w, f, 0.0, nullptr, false, true);
@@ -741,8 +909,8 @@ struct MPiece {
     double xi, c1, c2, c3, c4;
 };
 
-template <int NPMAX>
-__device__ __forceinline__ void m_piece(const MSpline<NPMAX>& w, const MFit& f, double p, int i, MPiece& pc) {
+template <class W>
+__device__ __forceinline__ void m_piece(const W& w, const MFit& f, double p, int i, MPiece& pc) {
     const int np = f.np;
     const double um = (i >= 2) ? (double)w.u(i - 1) : 0.0;
     const double u0 = (double)w.u(i), u1 = (double)w.u(i + 1);
@@ -751,8 +919,8 @@ __device__ __forceinline__ void m_piece(const MSpline<NPMAX>& w, const MFit& f, 
     const double raw1 = (u1 - u0) * f.rh;                            // raw(i+1)
     const double raw2 = (i + 2 <= np) ? (u2 - u1) * f.rh : 0.0;      // raw(i+2)
     const double K1 = 6.0 * (1.0 - p) * f.dy2;
-    const double a1i = (double)w.y(i) - K1 * (raw1 - raw0);
-    const double a1n = (double)w.y(i + 1) - K1 * (raw2 - raw1);
+    const double a1i = w.yat(f, i) - K1 * (raw1 - raw0);
+    const double a1n = w.yat(f, i + 1) - K1 * (raw2 - raw1);
     const double a3i = u0 * 6.0 * p;
     const double a3n = u1 * 6.0 * p;
     const double a4i = (a3n - a3i) * f.rh;
@@ -766,8 +934,8 @@ __device__ __forceinline__ void m_piece(const MSpline<NPMAX>& w, const MFit& f, 
 
 // ppvalu (pppack.f90:4246-4362) of the fit at x; the piece is kept in
 // registers between calls (consecutive sub-step positions mostly share it).
-template <int NPMAX>
-__device__ __forceinline__ double m_ppvalu(const MSpline<NPMAX>& w, const MFit& f, double p, double x, int jderiv,
+template <class W>
+__device__ __forceinline__ double m_ppvalu(const W& w, const MFit& f, double p, double x, int jderiv,
                                            MPiece& pc) {
     const int np = f.np;
     // interv on uniform breaks: piece 1 below the first break, np-1 at or
@@ -783,9 +951,9 @@ __device__ __forceinline__ double m_ppvalu(const MSpline<NPMAX>& w, const MFit& 
 
 // VTurb (ver_turb_module.f90:31-329): column in FP32 from FP16 AKs, fit and
 // random-displacement sub-steps in FP64
-template <typename E, int NPMAX>
+template <typename E, class W>
 __device__ float m_vturb(const RpStepArgs& A, const RpGridDev& g, const MStage& S, float Zpar,
-                         uint32_t pid, double& qstate, double& gstate, uint32_t& fl, const MSpline<NPMAX>& w) {
+                         uint32_t pid, double& qstate, double& gstate, uint32_t& fl, const W& w) {
     const int sw = g.N + 1;
     MFit f;
     f.np = (int)((double)sw * A.sub);
@@ -802,20 +970,38 @@ __device__ float m_vturb(const RpStepArgs& A, const RpGridDev& g, const MStage& 
     const MTime tk = m_time(A, g, 0);
     const bool all[4] = {true, true, true, true};
     double zprev = 0.0, kprev = 0.0;
-    for (int k = 1; k <= sw; k++) {
-        // z_w(k) of the interpolated zeta (getWlevel is linear in zeta)
-        const double zk = (k == sw) ? zeta
-                                    : (double)m_zlev(g.vtransform, hc, h, den_r, (float)__ldg(g.sw + k - 1),
-                                                     (float)__ldg(g.csw + k - 1), S.zeta);
-        const double kk = (double)m_level<E>(aks, qs, S.rc.o, cwt, all, sw, k, tk);   // getInterpAKs
-        w.cz(k) = (float)zk;
-        if (k >= 2) {
-            const double m = (kk - kprev) / (zk - zprev);
-            w.cm(k - 1) = (float)m;
-            w.cb(k - 1) = (float)(kprev - m * zprev);
+    // levels in batches of kColBatch: the batch's 4 kColBatch corner loads
+    // are issued before any is used, so their latencies overlap (a
+    // workspace view for a kernel with registers to spare asks for more)
+    constexpr int kColBatch = W::kColBatch;
+    for (int k0 = 1; k0 <= sw; k0 += kColBatch) {
+        uint2 v[kColBatch][4];
+        float4 sc[kColBatch];
+#pragma unroll
+        for (int b = 0; b < kColBatch; b++) {
+            const int k = min(k0 + b, sw);
+            sc[b] = __ldg(qs + k - 1);
+#pragma unroll
+            for (int q = 0; q < 4; q++) v[b][q] = __ldg(aks + S.rc.o[q] * sw + k - 1);
         }
-        zprev = zk;
-        kprev = kk;
+#pragma unroll
+        for (int b = 0; b < kColBatch; b++) {
+            const int k = k0 + b;
+            if (k > sw) break;
+            // z_w(k) of the interpolated zeta (getWlevel is linear in zeta)
+            const double zk = (k == sw) ? zeta
+                                        : (double)m_zlev(g.vtransform, hc, h, den_r, (float)__ldg(g.sw + k - 1),
+                                                         (float)__ldg(g.csw + k - 1), S.zeta);
+            const double kk = (double)m_level_of<E>(v[b], sc[b], cwt, all, tk);   // getInterpAKs
+            w.cz(k) = (float)zk;
+            if (k >= 2) {
+                const double m = (kk - kprev) / (zk - zprev);
+                w.cm(k - 1) = (float)m;
+                w.cb(k - 1) = (float)(kprev - m * zprev);
+            }
+            zprev = zk;
+            kprev = kk;
+        }
     }
     f.z1 = w.cz(1);
     f.h = (zeta - f.z1) / (double)(f.np - 1);
@@ -1025,8 +1211,8 @@ __device__ __noinline__ double m_behave(const RpStepArgs& A, int64_t n, const Rp
 // VTurb of one particle on its own (the first kernel of the split form),
 // with the stage-1 z clamp of find_currents applied first when RK4 runs
 // (advection_module.f90:171-183), as RKAdvect hands Zpar to VTurb.
-template <typename E, int NPMAX>
-__device__ void m_vturb_one(const RpStepArgs& A, int64_t n, const MSpline<NPMAX>& w, float* turbv) {
+template <typename E, class W>
+__device__ void m_vturb_one(const RpStepArgs& A, int64_t n, const W& w, float* turbv) {
     const RpParticlesDev& Pt = A.p;
     if (!rp_active(A, n)) return;
     uint32_t fl = 0;
@@ -1053,8 +1239,8 @@ __device__ void m_vturb_one(const RpStepArgs& A, int64_t n, const MSpline<NPMAX>
 // FEAT: the kernel variant with the options beyond the passive step (the
 // diagnostics, WETDRY, behave); the passive variant carries none of their
 // code.
-template <typename E, int NPMAX, bool FEAT>
-__device__ void m_update_one(const RpStepArgs& A, int64_t n, const MSpline<NPMAX>& w, const float* turbv_in) {
+template <typename E, bool FEAT, class W>
+__device__ void m_update_one(const RpStepArgs& A, int64_t n, const W& w, const float* turbv_in) {
     const RpParticlesDev& Pt = A.p;
     if (!rp_active(A, n)) return;
     Pt.age[n] = Pt.age[n] + (double)(float)A.idt;

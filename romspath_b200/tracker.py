@@ -69,9 +69,11 @@ class Tracker:
         P.seed = int(seed)
         P.device = int(device)
         # kernel form: "fused" (one kernel, spline workspace in local
-        # memory) or "split" (VTurb kernel with the spline workspace in
-        # shared memory writing a scratch array, then the advection kernel)
-        P.reserved[0] = {"fused": 0, "split": 1}[variant]
+        # memory), "split" (a VTurb kernel writing each particle's
+        # displacement to a scratch array, then the advection kernel) or,
+        # in the mixed form, "smem" (the split form with the VTurb kernel's
+        # spline workspace in shared memory)
+        P.reserved[0] = self.FORMS[variant]
         # re-sort the particle state by grid and cell every `resort` internal
         # steps (0: never); results are unchanged
         P.reserved[1] = int(resort)
@@ -330,6 +332,13 @@ class Tracker:
                            i32([s.tf for s in steps]))
         rc = self.L.rp_step_n(self.h, k, _pd(ex), _pd(ix), *[a.ctypes.data_as(_lib.PI32) for a in (ets, tb, tc, tf)])
         self._check(rc, "rp_step_n")
+
+    FORMS = {"fused": 0, "split": 1, "smem": 2, "fused-noprefetch": 3}
+
+    def set_kernel_form(self, form: str):
+        """Kernel form between steps (rp_set_kernel_form): "fused", "split",
+        and in the mixed forms "smem" and "fused-noprefetch"."""
+        self._check(self.L.rp_set_kernel_form(self.h, self.FORMS[form]), "rp_set_kernel_form")
 
     def set_launch(self, resort: int, blocks_per_sm: int):
         """Re-sort interval (0: never) and resident blocks per SM (0: the

@@ -37,3 +37,33 @@ def test_times():
 def test_days_uses_single_precision_product():
     # seconds = int(days*86400.0) in REAL arithmetic
     assert len(list(schedule.external_steps(10.0, 3600, 300))) == 240
+
+
+def test_autotune_two_stages_with_a_fake_tracker():
+    """The tuner picks the fastest kernel form first, then the fastest
+    re-sort interval and occupancy for it, and leaves them in place."""
+    from romspath_b200 import autotune
+
+    class Fake:
+        field_dtype = "mixed"
+
+        def __init__(self):
+            self.form, self.launch, self.calls = "fused", (12, 0), []
+
+        def set_kernel_form(self, form):
+            self.form = form
+
+        def set_launch(self, resort, bps):
+            self.launch = (resort, bps)
+
+    T = Fake()
+    cost = {"fused": 3.0, "fused-noprefetch": 3.2, "smem": 2.5}
+
+    def interval():
+        resort, bps = T.launch
+        return cost[T.form] + (0.0 if resort == 24 else 0.1) + (0.05 if bps else 0.0)
+
+    out = autotune.tune(T, interval, reps=1)
+    assert T.form == "smem" and T.launch == (24, 0)
+    assert out["best"] == {"form": "smem", "resort": 24, "blocks_per_sm": 0, "ms_per_interval": 2.5}
+    assert [r["form"] for r in out["forms"]] == autotune.MIXED_FORMS
