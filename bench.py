@@ -84,6 +84,10 @@ def parse():
                     help="instead of timing: run the exact and the mixed form in lockstep on the same "
                          "frames and noise and report the mixed form's position / profile error")
     ap.add_argument("--days", type=float, default=10.0, help="error study length")
+    ap.add_argument("--error-days", type=float, default=1.0,
+                    help="length of the headline line's lockstep error check of the mixed forms (0: none)")
+    ap.add_argument("--error-particles", type=int, default=65536,
+                    help="particles of the headline line's lockstep error check")
     ap.add_argument("--batched", action="store_true",
                     help="instead of the single-grid workload: batched nested grids (400x300x30 parent, 3x and 5x "
                          "children; 3M / 800k / 200k particles + 16 release ensembles), one launch per internal "
@@ -329,6 +333,46 @@ def error_stats(ref, mix, spec):
             "rms_depth_frac_of_column": float(np.sqrt(np.mean((dz / depth) ** 2))) if dz.size else None,
             "vertical_profile_L1": float(np.abs(hv[0] - hv[1]).sum() / n),
             "horizontal_profile_L1": float(np.abs(hh[0] - hh[1]).sum() / n)}
+
+
+def lockstep_error(wl, kinds, days, npart, deterministic=False):
+    """The mixed forms `kinds` and the exact form stepped in lockstep on one
+    GPU for `days` (same grid, hourly frames, release and Philox noise),
+    error_stats of each against the exact form at the end."""
+    from romspath_b200 import Tracker
+    spec = synth.config_spec(wl)[0]
+    grid = synth.make_grid(spec)
+    params = dict(synth.config_params(wl))
+    if deterministic:
+        params.update(vturb_on=0, hturb_on=0)
+    cache = {}
+
+    def frame(k):
+        if k not in cache:
+            cache[k] = synth.make_frame(spec, grid, (k - 1) * float(params["dt"]))
+            for old in [j for j in cache if j < k - 3]:
+                del cache[old]
+        return cache[k]
+
+    rel = synth.uniform_release(spec, grid, frame(1), npart, seed=0)
+    forms = {"exact": spec.field_dtype, **{k: k for k in kinds}}
+    T = {f: Tracker([spec], [grid], params, numpar=npart, field_dtype=d, stokes=spec.stokes, seed=7, resort=12)
+         for f, d in forms.items()}
+    for (k, slot) in schedule.initial_loads():
+        for t in T.values():
+            t.upload_frame(1, slot, frame(k))
+    for t in T.values():
+        t.locate(rel, t_b=1)
+    for ext in schedule.external_steps(days, int(params["dt"]), int(params["idt"])):
+        for (k, slot) in ext.loads:
+            for t in T.values():
+                t.upload_frame(1, slot, frame(k))
+        for t in T.values():
+            t.step_n(ext.internal)
+    st = {f: t.get_particles() for f, t in T.items()}
+    for t in T.values():
+        t.close()
+    return {k: error_stats(st["exact"], st[k], spec) for k in kinds}
 
 
 def error_study(args):
@@ -869,7 +913,8 @@ def main():
     rel = synth.uniform_release(spec, grid, frames[0], npart, seed=rank)
     exts = list(schedule.external_steps(30.0, int(params["dt"]), int(params["idt"])))
     head = args.mixed_kind if args.form == "mixed" else spec.field_dtype
-    forms = [head] + [f for f in (spec.field_dtype, "f64") if f != head]
+    others = ("mixed-i16" if head == "mixed" else "mixed",) if head.startswith("mixed") else ()
+    forms = [head] + [f for f in others + (spec.field_dtype, "f64") if f != head]
 
     def barrier():
         if dist is not None:
@@ -1075,6 +1120,18 @@ def main():
     if "fp64_tflops" in spline:
         spline["fp64_frac"] = spline["fp64_tflops"] / FP64_PEAK_NOMINAL_TFLOPS
 
+    # ---------------- error of the mixed forms at this speed (lockstep)
+    err = None
+    if rank == 0 and head.startswith("mixed") and args.error_days > 0:
+        t0 = time.time()
+        kinds = [head] + [k for k in ("mixed", "mixed-i16") if k != head]
+        err = {"vs": f"the exact form (FP64 arithmetic on {spec.field_dtype}-stored fields, bit-identical to the "
+                     f"CPU restatement of the reference), stepped in lockstep on the same grid, hourly frames, "
+                     f"release and Philox noise; positions in grid cells over particles moved in both forms",
+               "days": args.error_days, "particles": args.error_particles,
+               **lockstep_error(wl, kinds, args.error_days, args.error_particles)}
+        err["wall_s"] = time.time() - t0
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -1106,7 +1163,8 @@ def main():
                           "avg_launch_ms": r["avg_launch_ms"], "desc": FORM_DESC[f],
                           "speedup_vs_plain_fp64": (r["value"] / plain["value"]) if plain else None}
                       for f, r in results.items()},
-            "roofline": roofline, "spline": spline, "cpu_baseline": cpu, "e2e": e2e, "clocks": hr["clocks"],
+            "roofline": roofline, "spline": spline, "error": err, "cpu_baseline": cpu, "e2e": e2e,
+            "clocks": hr["clocks"],
             "gpu_launches": int(hr["launches"]),
         }
         print(json.dumps(line), flush=True)
