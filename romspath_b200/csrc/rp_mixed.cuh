@@ -949,6 +949,27 @@ __device__ __forceinline__ double m_ppvalu(const W& w, const MFit& f, double p, 
     return (pc.c4 * 0.5 * hx + pc.c3) * hx + pc.c2;
 }
 
+// Normal deviates d and d+1 (d even) of a particle-step: the noise hook's
+// values when set, else the two Box-Muller deviates (cosine branch,
+// pdf_module.f90:26-40) of one Philox4x32-10 call at counter (pid, step,
+// d/2) -- the exact form's uniforms -- with the transform in FP32 (logf,
+// cospif: the deviates agree with the exact form's to about 1e-6).
+__device__ __forceinline__ void m_normal2(const RpStepArgs& A, uint32_t pid, uint32_t d, double& n0, double& n1) {
+    if (A.hook) {
+        const double* h = A.hook + (int64_t)(pid - A.pid_base) * A.ndraw + d;
+        n0 = h[0];
+        n1 = (d + 1 < (uint32_t)(2 + A.loop)) ? h[1] : 0.0;   // past the last sub-step: not read
+        return;
+    }
+    uint32_t c[4] = {pid, (uint32_t)A.step_index, (uint32_t)(A.step_index >> 32), d >> 1};
+    rp_philox(c, (uint32_t)A.seed, (uint32_t)(A.seed >> 32));
+    const float k = 2.3283064365386963e-10f;     // 2^-32
+    const float r0 = sqrtf(-2.f * logf(((float)c[0] + 0.5f) * k));
+    const float r1 = sqrtf(-2.f * logf(((float)c[2] + 0.5f) * k));
+    n0 = (double)(r0 * cospif(2.f * (((float)c[1] + 0.5f) * k)));
+    n1 = (double)(r1 * cospif(2.f * (((float)c[3] + 0.5f) * k)));
+}
+
 // VTurb (ver_turb_module.f90:31-329): column in FP32 from FP16 AKs, fit and
 // random-displacement sub-steps in FP64
 template <typename E, class W>
@@ -1013,7 +1034,11 @@ __device__ float m_vturb(const RpStepArgs& A, const RpGridDev& g, const MStage& 
     double ParZc = (double)Zpar;
     MPiece pc;
     pc.i = 0;
+    double dev_next = 0.0;
     for (int i = 1; i <= A.loop; i++) {
+        double DEV;                                    // draw 1+i; pairs (2,3), (4,5), ...
+        if (i & 1) m_normal2(A, pid, (uint32_t)(1 + i), DEV, dev_next);
+        else DEV = dev_next;
         double Kprimec = 0.0;
         if (!(ParZc <= tdepth || ParZc >= zeta)) Kprimec = m_ppvalu(w, f, p, ParZc, 1, pc);
         const double KprimeZc = Kprimec * deltat;
@@ -1025,7 +1050,6 @@ __device__ float m_vturb(const RpStepArgs& A, const RpGridDev& g, const MStage& 
             KH3rdc = m_ppvalu(w, f, p, Z3rdc, 0, pc);
             if (KH3rdc < A.aksback) KH3rdc = A.aksback;
         }
-        const double DEV = rp_normal(A, pid, (uint32_t)(1 + i));
         ParZc = ParZc + (KprimeZc + DEV * sqrt(2.0 * KH3rdc * deltat));
         if (ParZc <= tdepth) ParZc = tdepth + fabs(ParZc - tdepth);
         if (ParZc >= zeta) ParZc = zeta - fabs(ParZc - zeta);
@@ -1301,8 +1325,10 @@ __device__ void m_update_one(const RpStepArgs& A, int64_t n, const W& w, const f
     float TurbHx = 0.f, TurbHy = 0.f;
     if (A.hturb_on) {                                  // HTurb, hor_turb_module.f90:30-51
         const float sc = sqrtf(2.f * (float)A.khturb[gid - 1] * didt);
-        TurbHx = (float)rp_normal(A, pid, 0u) * sc;
-        TurbHy = (float)rp_normal(A, pid, 1u) * sc;
+        double nx, ny;
+        m_normal2(A, pid, 0u, nx, ny);
+        TurbHx = (float)nx * sc;
+        TurbHy = (float)ny * sc;
     }
     TurbHx *= pm;
     TurbHy *= pn;
