@@ -599,7 +599,8 @@ __device__ double m_chol1d(const W& w, const MFit& f, double p, double* utru_out
     wk.init(w);
     double ym = wk.at(w, f.sw, f.z1);
     double y0 = wk.at(w, f.sw, f.z1 + f.h);
-    double yp = wk.at(w, f.sw, f.z1 + 2.0 * f.h);
+    double xn = f.z1 + 2.0 * f.h;
+    double yp = wk.at(w, f.sw, xn);
     if (store_y) {
         w.y(1) = (float)ym;
         w.y(2) = (float)y0;
@@ -648,7 +649,8 @@ __device__ double m_chol1d(const W& w, const MFit& f, double p, double* utru_out
         w.u(i) = (MU)(ucur * inv);
         ym = y0;
         y0 = yp;
-        yp = wk.at(w, f.sw, f.z1 + (double)(i + 1) * f.h);
+        xn = xn + f.h;                               // z1 + (i+1) h, accumulated
+        yp = wk.at(w, f.sw, xn);
         if (store_y) w.y(i + 2) = (float)yp;
         const double qn = (yp - 2.0 * y0 + ym) * f.rh;     // qty(i+1)
         const double unext = qn - ratio1 * ucur - r2prev * uprev;
@@ -660,22 +662,24 @@ __device__ double m_chol1d(const W& w, const MFit& f, double p, double* utru_out
     // raw(k) = (u(k) - u(k-1))/h for 2 <= k <= np, raw(1) = raw(np+1) = 0,
     // qu(k) = raw(k+1) - raw(k)
     const double dy2 = f.dy2;
+    const bool want_utru = utru_out != nullptr;
     double up1 = 0.0;                                // u(np)
     double up2 = 0.0;                                // u(np+1), unused
     double rawp = 0.0;                               // raw(np+1)
-    double sum = 0.0, utru = 0.0;
+    double sum = 0.0, utru = 0.0;                    // sum of qu^2 (times dy2 at the end)
     if (store_u) w.u(np) = 0.0;
     {
         const double ui = ucur / a1;                 // u(np-1)
         if (store_u) w.u(np - 1) = (MU)ui;
         const double raw = (up1 - ui) * f.rh;        // raw(np)
         const double fin = rawp - raw;               // qu(np)
-        sum = sum + fin * fin * dy2;
-        utru = utru + f.h * (ui * (ui + up1) + up1 * up1);
+        sum = sum + fin * fin;
+        if (want_utru) utru = utru + f.h * (ui * (ui + up1) + up1 * up1);
         rawp = raw;
         up2 = up1;
         up1 = ui;
     }
+    const double h1 = (double)(MRatio)hr1, h2 = (double)(MRatio)hr2;   // the held rows' stored ratios
     // with W::kPrefetch, u(i) is loaded four rows ahead of its use (index 1
     // stands in past the start; that value is never used)
     MU q0 = w.u(np - 2), q1 = w.u(max(np - 3, 1)), q2 = w.u(max(np - 4, 1)), q3 = w.u(max(np - 5, 1));
@@ -692,14 +696,17 @@ __device__ double m_chol1d(const W& w, const MFit& f, double p, double* utru_out
             uq = (double)w.u(i);
         }
         const bool held = (i >= ks && i <= np - 3);
-        const double s1v = held ? (double)(MRatio)hr1 : (double)w.s1(i);
-        const double s2v = held ? (double)(MRatio)hr2 : (double)w.s2(i);
+        double s1v = h1, s2v = h2;
+        if (!held) {
+            s1v = (double)w.s1(i);
+            s2v = (double)w.s2(i);
+        }
         const double ui = uq - up1 * s1v - up2 * s2v;
         if (store_u) w.u(i) = (MU)ui;
         const double raw = (up1 - ui) * f.rh;        // raw(i+1)
         const double fin = rawp - raw;               // qu(i+1)
-        sum = sum + fin * fin * dy2;
-        utru = utru + f.h * (ui * (ui + up1) + up1 * up1);
+        sum = sum + fin * fin;
+        if (want_utru) utru = utru + f.h * (ui * (ui + up1) + up1 * up1);
         rawp = raw;
         up2 = up1;
         up1 = ui;
@@ -707,12 +714,12 @@ __device__ double m_chol1d(const W& w, const MFit& f, double p, double* utru_out
     {
         const double raw = up1 * f.rh;               // raw(2), u(1) = 0
         const double fin2 = rawp - raw;              // qu(2)
-        sum = sum + fin2 * fin2 * dy2 + raw * raw * dy2;   // qu(1) = raw(2)
-        utru = utru + f.h * (up1 * up1);
+        sum = sum + fin2 * fin2 + raw * raw;         // qu(1) = raw(2)
+        if (want_utru) utru = utru + f.h * (up1 * up1);
     }
     if (store_u) w.u(1) = 0.0;
-    if (utru_out) *utru_out = utru;
-    return sum;
+    if (want_utru) *utru_out = utru;
+    return sum * dy2;
 }
 
 // SF(q) = 36 sum qu^2 dy^2 / (1+q)^2 of one chol1d pass at p = q/(1+q)
@@ -749,7 +756,8 @@ __device__ double m_light_S(const W& w, const MFit& f, double p) {
     wk.init(w);
     double ym = wk.at(w, f.sw, f.z1);
     double y0 = wk.at(w, f.sw, f.z1 + f.h);
-    double yp = wk.at(w, f.sw, f.z1 + 2.0 * f.h);
+    double xn = f.z1 + 2.0 * f.h;
+    double yp = wk.at(w, f.sw, xn);
     double a1 = D, a2 = E, b1 = D, a1d = Dd, a2d = Ed, b1d = Dd;
     double wc = (yp - 2.0 * y0 + ym) * f.rh, wcd = 0.0, wp = 0.0, wpd = 0.0;   // w(i), w(i-1) and d/dp
     double r2p = 0.0, r2pd = 0.0;                                               // ratio2(i-1)
@@ -788,7 +796,8 @@ __device__ double m_light_S(const W& w, const MFit& f, double p) {
         phid = phid + (2.0 * wc * wcd) * inv + wc * wc * invd;
         ym = y0;
         y0 = yp;
-        yp = wk.at(w, f.sw, f.z1 + (double)(i + 1) * f.h);
+        xn = xn + f.h;                               // z1 + (i+1) h, accumulated
+        yp = wk.at(w, f.sw, xn);
         const double qn = (yp - 2.0 * y0 + ym) * f.rh;           // qty(i+1)
         const double wn = qn - ratio1 * wc - r2p * wp;
         const double wnd = -(ratio1d * wc + ratio1 * wcd + r2pd * wp + r2p * wpd);
