@@ -84,6 +84,9 @@ def parse():
                     help="instead of timing: run the exact and the mixed form in lockstep on the same "
                          "frames and noise and report the mixed form's position / profile error")
     ap.add_argument("--days", type=float, default=10.0, help="error study length")
+    ap.add_argument("--kernel-form", default="fused", choices=["fused", "split", "smem", "fused-noprefetch"],
+                    help="kernel form of the timed forms (rp_set_kernel_form; smem and fused-noprefetch: mixed "
+                         "forms only, the exact forms run those fused)")
     ap.add_argument("--error-days", type=float, default=1.0,
                     help="length of the headline line's lockstep error check of the mixed forms (0: none)")
     ap.add_argument("--error-particles", type=int, default=65536,
@@ -931,6 +934,7 @@ def main():
         T = Tracker([spec], [grid], params, numpar=npart, field_dtype=form, stokes=spec.stokes, seed=7,
                     device=local, resort=args.resort)
         T.set_id_base(rank * npart)     # global particle ids: rank r holds [r*npart, (r+1)*npart)
+        T.set_kernel_form(args.kernel_form)
         for k, slot in enumerate((1, 2, 3)):
             T.upload_frame(1, slot, frames[k])
         T.locate(rel, t_b=1)
@@ -1151,7 +1155,7 @@ def main():
             "data": "synthetic (analytic ROMS-shaped fields, seeded release)",
             "config": {"workload": WORKLOAD_DESCS.get(wl, wl), "particles_per_gpu": npart,
                        "step": "one hydro frame interval = 12 internal steps (idt=300 s)",
-                       "form": FORM_DESC[head],
+                       "form": FORM_DESC[head], "kernel_form": args.kernel_form,
                        "l2": ("inputs larger than L2 (frame ring 390 MB FP32 / 195 MB FP16, particle state "
                               "~80 MB, spline workspace in local memory ~0.5-1 GB)") if wl == "cfg2" else
                              ("frames L2-resident (8.4 MB per FP64 frame), particle state and spline workspace "
