@@ -67,6 +67,21 @@ __global__ void __launch_bounds__(kStepBlock, kMixedMinBlocks) k_advect_mixed(co
         m_update_one<E, FEAT>(A, n, none, turbv);
 }
 
+// The diagnostics of the particles the step just advanced (their tdepth in
+// A.diag_td; NaN for the others), as the end of update_particles computes
+// them (ROMSPath.f90:935-986).  A pass of its own keeps the diagnostics'
+// code and registers out of the step kernel.
+__global__ void __launch_bounds__(kStepBlock) k_diag_mixed(const __grid_constant__ RpStepArgs A) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < A.p.n; n += stride) {
+        const float td = A.diag_td[n];
+        if (!(td == td)) continue;
+        uint32_t fl = 0;
+        m_diag_one(A, n, td, fl);
+        if (fl) A.p.flags[n] |= fl;
+    }
+}
+
 template <class K>
 static cudaError_t resident_grid(K kernel, int64_t n, int num_sms, int cap_per_sm, int64_t* blocks) {
     int occ = 0;
@@ -157,10 +172,26 @@ static cudaError_t launch_mixed_e(const RpStepArgs& A, int npmax, float* turbv, 
                 : launch_mixed_f<E, false>(A, npmax, turbv, split, s, num_sms, nlaunch);
 }
 
-cudaError_t launch_step_mixed(const RpStepArgs& A, int npmax, int i16, float* turbv, int split, cudaStream_t s,
+cudaError_t launch_step_mixed(const RpStepArgs& A0, int npmax, int i16, float* turbv, int split, cudaStream_t s,
                               int num_sms, int* nlaunch) {
-    return i16 ? launch_mixed_e<int16_t>(A, npmax, turbv, split, s, num_sms, nlaunch)
-               : launch_mixed_e<__half>(A, npmax, turbv, split, s, num_sms, nlaunch);
+    RpStepArgs A = A0;
+    float* td = nullptr;
+    cudaError_t e;
+    if (A.diag) {
+        // the step's tdepth per particle goes to the second half of the
+        // scratch (the first half holds the split forms' VTurb displacement)
+        td = turbv + A.p.n;
+        A.diag_td = td;
+        if ((e = cudaMemsetAsync(td, 0xff, sizeof(float) * (size_t)A.p.n, s)) != cudaSuccess) return e;   // NaN
+    }
+    e = i16 ? launch_mixed_e<int16_t>(A, npmax, turbv, split, s, num_sms, nlaunch)
+            : launch_mixed_e<__half>(A, npmax, turbv, split, s, num_sms, nlaunch);
+    if (e != cudaSuccess || !A.diag) return e;
+    int64_t blocks = 0;
+    if ((e = resident_grid(k_diag_mixed, A.p.n, num_sms, 0, &blocks)) != cudaSuccess) return e;
+    k_diag_mixed<<<(unsigned)blocks, kStepBlock, 0, s>>>(A);
+    *nlaunch += 1;
+    return cudaGetLastError();
 }
 
 // ------------------------------------------------------ frame upload

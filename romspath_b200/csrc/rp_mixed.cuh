@@ -1410,6 +1410,6 @@ __device__ void m_update_one(const RpStepArgs& A, int64_t n, const W& w, const f
         Pt.isin[n] = 1;
         Pt.status[n] = -9.0;
     }
-    if (FEAT && A.diag) m_diag_one(A, n, tdepth, fl);
+    if (FEAT && A.diag) A.diag_td[n] = tdepth;        // the diagnostics run in their own pass
     if (fl) Pt.flags[n] |= fl;
 }
