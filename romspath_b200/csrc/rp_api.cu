@@ -59,7 +59,8 @@ struct rp_ctx {
     int32_t* gid = nullptr;
     int8_t* isin = nullptr;
     uint32_t *pid = nullptr, *flags = nullptr;
-    double* turbv = nullptr;                   // scratch: VTurb displacement per particle
+    double* turbv = nullptr;                   // scratch, 12 B per particle: the re-sort's gathers; the mixed
+                                               // form's VTurb displacement, tdepth and ZBehav (3 floats)
     // diagnostics (RP_DIAG_* bits of reserved[3]); null when off
     int diag = 0;
     double *d_salt = nullptr, *d_temp = nullptr, *d_mean_salt = nullptr, *d_mean_temp = nullptr;
@@ -857,7 +858,7 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
         dalloc(&ctx->wd, cap * 8) || dalloc(&ctx->zeta, cap * 8) || dalloc(&ctx->bath, cap * 8) ||
         dalloc(&ctx->gid, cap * 4) || dalloc(&ctx->isin, cap) || dalloc(&ctx->pid, cap * 4) ||
         dalloc(&ctx->flags, cap * 4) || dalloc(&ctx->tmp_gid, cap * 8) || dalloc(&ctx->tmp_isin, cap * 4) ||
-        dalloc(&ctx->turbv, cap * 8))
+        dalloc(&ctx->turbv, cap * 12))
         return bail(RP_ERR_NOMEM, "particle state allocation");
     if (ctx->wetdry) {
         size_t mmax = 0;

@@ -184,6 +184,7 @@ struct RpStepArgs {
     unsigned long long* spl;       // [0] smoothing-spline fits, [1] chol1d passes; nullptr: not counted
     float* diag_td;                // mixed form with diagnostics: the step's tdepth per particle (NaN:
                                    // not stepped), read by the diagnostics pass; nullptr: none
+    float* beh_z;                  // mixed form with behave: ZBehav per particle from the behave pass
     int ndraw;
     uint32_t pid_base;             // hook row of particle id p is p - pid_base
     RpGridDev g[RP_MAXNGRID_D];

@@ -82,6 +82,32 @@ __global__ void __launch_bounds__(kStepBlock) k_diag_mixed(const __grid_constant
     }
 }
 
+// behave (behavior_module.f90:186-393) of the particles the step is about to
+// advance, at their start position after find_currents' stage-1 z clamp
+// (the Zpar update_particles hands it, ROMSPath.f90:800-804): ZBehav to
+// A.beh_z, behave's outputs to the particle columns.  A pass of its own
+// keeps behave's code and registers out of the step kernel.
+__global__ void __launch_bounds__(kStepBlock) k_behave_mixed(const __grid_constant__ RpStepArgs A) {
+    const RpParticlesDev& Pt = A.p;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < Pt.n; n += stride) {
+        if (!rp_active(A, n)) continue;
+        uint32_t fl = 0;
+        const RpGridDev& g = A.g[Pt.gid[n] - 1];
+        const float Xpar = Pt.x32[n], Ypar = Pt.y32[n];
+        float Zpar = Pt.z32[n] - Pt.cz[n];
+        if (A.scheme == 1) {
+            MStage S1;
+            m_rho_cell(g, Xpar, Ypar, S1.rc, fl);
+            m_stage_2d(m_time(A, g, 0), g, S1);
+            if (Zpar < S1.tdepth) Zpar = S1.tdepth + 0.001f;
+            if (Zpar > S1.zeta) Zpar = S1.zeta - 0.001f;
+        }
+        A.beh_z[n] = (float)m_behave(A, n, g, Xpar, Ypar, Zpar, Pt.pid[n], fl);
+        if (fl) Pt.flags[n] |= fl;
+    }
+}
+
 template <class K>
 static cudaError_t resident_grid(K kernel, int64_t n, int num_sms, int cap_per_sm, int64_t* blocks) {
     int occ = 0;
@@ -177,6 +203,15 @@ cudaError_t launch_step_mixed(const RpStepArgs& A0, int npmax, int i16, float* t
     RpStepArgs A = A0;
     float* td = nullptr;
     cudaError_t e;
+    int64_t blocks = 0;
+    if (A.beh.behavior || A.beh.va || A.beh.wa) {
+        // ZBehav in the third part of the scratch (3 floats per particle)
+        A.beh_z = turbv + 2 * A.p.n;
+        if ((e = resident_grid(k_behave_mixed, A.p.n, num_sms, 0, &blocks)) != cudaSuccess) return e;
+        k_behave_mixed<<<(unsigned)blocks, kStepBlock, 0, s>>>(A);
+        *nlaunch += 1;
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
     if (A.diag) {
         // the step's tdepth per particle goes to the second half of the
         // scratch (the first half holds the split forms' VTurb displacement)
@@ -187,7 +222,6 @@ cudaError_t launch_step_mixed(const RpStepArgs& A0, int npmax, int i16, float* t
     e = i16 ? launch_mixed_e<int16_t>(A, npmax, turbv, split, s, num_sms, nlaunch)
             : launch_mixed_e<__half>(A, npmax, turbv, split, s, num_sms, nlaunch);
     if (e != cudaSuccess || !A.diag) return e;
-    int64_t blocks = 0;
     if ((e = resident_grid(k_diag_mixed, A.p.n, num_sms, 0, &blocks)) != cudaSuccess) return e;
     k_diag_mixed<<<(unsigned)blocks, kStepBlock, 0, s>>>(A);
     *nlaunch += 1;

@@ -1352,7 +1352,7 @@ __device__ void m_update_one(const RpStepArgs& A, int64_t n, const W& w, const f
     }
     float ZBehav = 0.f;                                // behave(), ROMSPath.f90:800-804
     if (FEAT && (A.beh.behavior || A.beh.va || A.beh.wa))
-        ZBehav = (float)m_behave(A, n, g, Xpar, Ypar, Zpar, pid, fl);
+        ZBehav = A.beh_z[n];                           // from the behave pass before the step
     // new position (Kahan), nest hand-off
     float nx = x, ncx = cx, ny = y, ncy = cy;
     m_kahan_add(nx, ncx, AdvectX + TurbHx);
