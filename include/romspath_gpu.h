@@ -99,8 +99,9 @@ typedef struct rp_params {
     uint64_t seed;                       /* Philox key of the turbulence noise */
     int32_t device;                      /* CUDA device ordinal               */
     int32_t reserved[7];                 /* [0]: kernel form, 0 fused (default),
-                                            1 split, 2 shared-memory split
-                                            and 3 fused without load-ahead
+                                            1 split, 2 shared-memory split,
+                                            3 fused without load-ahead, 4/5
+                                            fused in 64/256-thread blocks
                                             (mixed forms; rp_set_kernel_form);
                                             [1]: re-sort the particle
                                             state by grid and cell every that
@@ -466,9 +467,10 @@ int rp_set_launch(rp_ctx *ctx, int32_t resort, int32_t blocks_per_sm);
  * (one kernel per step, the fit's workspace in local memory), 1 split (a
  * VTurb kernel writing each particle's displacement, then the advection
  * kernel), and for the mixed forms 2, the split form with the VTurb
- * kernel's spline workspace in shared memory, and 3, the fused kernel
- * whose back substitution does not load u ahead (the exact forms run 2
- * and 3 fused).  Results do not change beyond rounding (the exact forms:
+ * kernel's spline workspace in shared memory, 3, the fused kernel whose
+ * back substitution does not load u ahead, and 4 and 5, the fused kernel
+ * in blocks of 64 and 256 threads instead of 128 (the exact forms run 2-5
+ * fused).  Results do not change beyond rounding (the exact forms:
  * not at all); which form is fastest depends on the grid and the particle
  * count, so an autotuner times them on the run.  No counterpart in the
  * reference. */

@@ -7,7 +7,8 @@ the fused kernel without the back substitution's load-ahead), the re-sort
 interval and the resident blocks per SM (hence particles per thread).  So
 the tuner times real frame intervals of the run under each candidate and
 keeps the fastest: no step is wasted.  It tunes in two stages: the kernel
-form at the default re-sort interval and occupancy, then the re-sort
+form (which includes the block size of the fused step: 64, 128 or 256
+threads) at the default re-sort interval and occupancy, then the re-sort
 interval and blocks per SM for the chosen form.  The best form depends on
 the grid and the particle count (on the 512x384x30 grid with 1,048,576
 particles the fused kernel wins; on the 130x98x20 grid with 4,194,304 the
@@ -17,7 +18,7 @@ from __future__ import annotations
 
 from typing import Callable, Dict, Iterable, List, Optional, Tuple
 
-MIXED_FORMS = ["fused", "fused-noprefetch", "smem"]
+MIXED_FORMS = ["fused", "fused-noprefetch", "smem", "fused-b64", "fused-b256"]
 EXACT_FORMS = ["fused", "split"]
 
 DEFAULT_CANDIDATES: List[Tuple[int, int]] = [

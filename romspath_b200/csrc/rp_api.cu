@@ -717,7 +717,7 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
         return RP_ERR_ARG;
     if (p.reserved[3] & ~(RP_DIAG_SALTTEMP | RP_DIAG_SALTTEMP_MEAN | RP_DIAG_BOTTOM)) return RP_ERR_ARG;
     if (p.reserved[4] != 0 && p.reserved[4] != 1) return RP_ERR_ARG;
-    if (p.reserved[0] < 0 || p.reserved[0] > 3) return RP_ERR_ARG;
+    if (p.reserved[0] < 0 || p.reserved[0] > 5) return RP_ERR_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= p.device || p.device < 0) return RP_ERR_NOEXT;
     rp_ctx* ctx = new rp_ctx();
@@ -1657,7 +1657,7 @@ int rp_set_launch(rp_ctx* ctx, int32_t resort, int32_t blocks_per_sm) {
 
 int rp_set_kernel_form(rp_ctx* ctx, int32_t form) {
     if (!ctx) return RP_ERR_ARG;
-    if (form < 0 || form > 3) return fail(ctx, RP_ERR_ARG, "rp_set_kernel_form: form must be 0..3");
+    if (form < 0 || form > 5) return fail(ctx, RP_ERR_ARG, "rp_set_kernel_form: form must be 0..5");
     ctx->prm.reserved[0] = form;
     return RP_OK;
 }

@@ -15,8 +15,11 @@ namespace rp {
 // Fused form: one thread per particle for the whole step.
 // FEAT: built with the options beyond the passive step (diagnostics,
 // WETDRY, behave); the passive variant is chosen when they are all off.
-template <typename E, int NPMAX, bool FEAT, bool PREF = true>
-__global__ void __launch_bounds__(kStepBlock, kMixedMinBlocks) k_step_mixed(const __grid_constant__ RpStepArgs A) {
+// BLK: threads per block (the register cap stays that of 128 x 8 resident
+// threads; the block is the scheduling unit of the grid-stride loop).
+template <typename E, int NPMAX, bool FEAT, bool PREF = true, int BLK = kStepBlock>
+__global__ void __launch_bounds__(BLK, kMixedMinBlocks * kStepBlock / BLK)
+    k_step_mixed(const __grid_constant__ RpStepArgs A) {
     double buf[kMixedArrays * (NPMAX + 1)];
     const MSpline<NPMAX, PREF> w{buf};
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -109,14 +112,15 @@ __global__ void __launch_bounds__(kStepBlock) k_behave_mixed(const __grid_consta
 }
 
 template <class K>
-static cudaError_t resident_grid(K kernel, int64_t n, int num_sms, int cap_per_sm, int64_t* blocks) {
+static cudaError_t resident_grid(K kernel, int64_t n, int num_sms, int cap_per_sm, int64_t* blocks,
+                                 int blk = kStepBlock) {
     int occ = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kStepBlock, 0);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, blk, 0);
     if (e != cudaSuccess) return e;
     if (occ < 1) occ = 1;
     if (cap_per_sm > 0 && occ > cap_per_sm) occ = cap_per_sm;
     int64_t b = (int64_t)num_sms * occ;
-    const int64_t need = (n + kStepBlock - 1) / kStepBlock;
+    const int64_t need = (n + blk - 1) / blk;
     if (need < b) b = need;
     *blocks = b < 1 ? 1 : b;
     return cudaSuccess;
@@ -156,6 +160,21 @@ static cudaError_t launch_mixed_t(const RpStepArgs& A, float* turbv, int split, 
         *nlaunch += 1;
         return cudaGetLastError();
     }
+    if ((split == 4 || split == 5) && !FEAT) {     // fused, 64- or 256-thread blocks
+        if (split == 4) {
+            if ((e = resident_grid(k_step_mixed<E, NPMAX, false, true, 64>, A.p.n, num_sms,
+                                   A.grid_cap ? 2 * A.grid_cap : 0, &blocks, 64)) != cudaSuccess)
+                return e;
+            k_step_mixed<E, NPMAX, false, true, 64><<<(unsigned)blocks, 64, 0, s>>>(A);
+        } else {
+            if ((e = resident_grid(k_step_mixed<E, NPMAX, false, true, 256>, A.p.n, num_sms,
+                                   A.grid_cap ? (A.grid_cap + 1) / 2 : 0, &blocks, 256)) != cudaSuccess)
+                return e;
+            k_step_mixed<E, NPMAX, false, true, 256><<<(unsigned)blocks, 256, 0, s>>>(A);
+        }
+        *nlaunch += 1;
+        return cudaGetLastError();
+    }
     if (split == 3 && !FEAT) {                     // fused, u not loaded ahead
         if ((e = resident_grid(k_step_mixed<E, NPMAX, false, false>, A.p.n, num_sms, A.grid_cap, &blocks)) !=
             cudaSuccess)
@@ -164,7 +183,7 @@ static cudaError_t launch_mixed_t(const RpStepArgs& A, float* turbv, int split, 
         *nlaunch += 1;
         return cudaGetLastError();
     }
-    if (split == 3 || !split || !A.vturb_on) {
+    if (split >= 3 || !split || !A.vturb_on) {
         if ((e = resident_grid(k_step_mixed<E, NPMAX, FEAT>, A.p.n, num_sms, A.grid_cap, &blocks)) != cudaSuccess)
             return e;
         k_step_mixed<E, NPMAX, FEAT><<<(unsigned)blocks, kStepBlock, 0, s>>>(A);

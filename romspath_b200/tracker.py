@@ -333,11 +333,12 @@ class Tracker:
         rc = self.L.rp_step_n(self.h, k, _pd(ex), _pd(ix), *[a.ctypes.data_as(_lib.PI32) for a in (ets, tb, tc, tf)])
         self._check(rc, "rp_step_n")
 
-    FORMS = {"fused": 0, "split": 1, "smem": 2, "fused-noprefetch": 3}
+    FORMS = {"fused": 0, "split": 1, "smem": 2, "fused-noprefetch": 3, "fused-b64": 4, "fused-b256": 5}
 
     def set_kernel_form(self, form: str):
         """Kernel form between steps (rp_set_kernel_form): "fused", "split",
-        and in the mixed forms "smem" and "fused-noprefetch"."""
+        and in the mixed forms "smem", "fused-noprefetch", "fused-b64" and
+        "fused-b256" (64- and 256-thread blocks)."""
         self._check(self.L.rp_set_kernel_form(self.h, self.FORMS[form]), "rp_set_kernel_form")
 
     def set_launch(self, resort: int, blocks_per_sm: int):

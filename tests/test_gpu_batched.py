@@ -88,7 +88,8 @@ def test_kernel_forms_switched_exact_form(name):
     """The exact form under every kernel form, switched between steps: bit
     for bit the oracle's result."""
     case = harness.make_case(name, 400, seed=5)
-    g = _run_forms(case, 36, case.spec.field_dtype, ["fused", "split", "smem", "fused-noprefetch"])
+    g = _run_forms(case, 36, case.spec.field_dtype, ["fused", "split", "smem", "fused-noprefetch", "fused-b64",
+                                                      "fused-b256"])
     o, _ = harness.run_oracle(case, 36, noise="philox", seed=7)
     bad = {k: v for k, v in harness.compare(g, o).items() if v}
     assert not bad, bad
@@ -107,6 +108,9 @@ def test_kernel_forms_mixed(name, kind):
     b = _run_forms(case, 36, kind, ["fused-noprefetch"])
     bad = {k: v for k, v in harness.compare(a, b).items() if v}
     assert not bad, bad
+    c = _run_forms(case, 36, kind, ["fused-b64", "fused-b256", "fused"])
+    bad = {k: v for k, v in harness.compare(a, c).items() if v}
+    assert not bad, bad                            # the block size changes nothing
     for forms in (["smem"], ["split"], ["fused", "smem", "split"]):
         c = _run_forms(case, 36, kind, forms)
         d = np.hypot(a["x"] - c["x"], a["y"] - c["y"])

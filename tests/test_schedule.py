@@ -57,7 +57,7 @@ def test_autotune_two_stages_with_a_fake_tracker():
             self.launch = (resort, bps)
 
     T = Fake()
-    cost = {"fused": 3.0, "fused-noprefetch": 3.2, "smem": 2.5}
+    cost = {"fused": 3.0, "fused-noprefetch": 3.2, "smem": 2.5, "fused-b64": 3.1, "fused-b256": 2.9}
 
     def interval():
         resort, bps = T.launch
