@@ -77,6 +77,7 @@ struct rp_ctx {
     float *x32 = nullptr, *y32 = nullptr, *z32 = nullptr, *cx = nullptr, *cy = nullptr, *cz = nullptr;
     double* qwarm = nullptr;
     double* gwarm = nullptr;
+    float* qwarm2 = nullptr;
     float* ftmp = nullptr;
     uint32_t* qmax = nullptr;
     double* tmp_gid = nullptr;                 // host-facing conversions
@@ -216,7 +217,7 @@ RpParticlesDev particles_dev(const rp_ctx* c) {
     P.wd = c->wd; P.zeta = c->zeta; P.bath = c->bath;
     P.gid = c->gid; P.isin = c->isin; P.pid = c->pid; P.flags = c->flags;
     P.x32 = c->x32; P.y32 = c->y32; P.z32 = c->z32; P.cx = c->cx; P.cy = c->cy; P.cz = c->cz;
-    P.qwarm = c->qwarm; P.gwarm = c->gwarm;
+    P.qwarm = c->qwarm; P.gwarm = c->gwarm; P.qwarm2 = c->qwarm2;
     P.salt = c->d_salt; P.temp = c->d_temp; P.mean_salt = c->d_mean_salt; P.mean_temp = c->d_mean_temp;
     P.hob = c->d_hob; P.bustr = c->d_bustr; P.bvstr = c->d_bvstr;
     P.acc = c->b_acc; P.vort = c->b_vort; P.behavew = c->b_behavew; P.ssf = c->b_ssf;
@@ -319,7 +320,7 @@ void free_ctx(rp_ctx* c) {
     }
     void* ptrs[] = {c->x, c->y, c->z, c->age, c->dob, c->status, c->wd, c->zeta, c->bath,
                     c->gid, c->isin, c->pid, c->flags, c->tmp_gid, c->tmp_isin, c->hook, c->turbv,
-                    c->dstage[0], c->dstage[1], c->x32, c->y32, c->z32, c->cx, c->cy, c->cz, c->qwarm, c->gwarm,
+                    c->dstage[0], c->dstage[1], c->x32, c->y32, c->z32, c->cx, c->cy, c->cz, c->qwarm, c->gwarm, c->qwarm2,
                     c->ftmp, c->qmax, c->sb.keys, c->sb.hist, c->sb.sums, c->sb.perm, c->sb.gbase,
                     c->adj.ck, c->adj.prec, c->adj.seg, c->adj.work, c->adj.lx, c->adj.ly, c->adj.lz,
                     c->adj.kbar, c->adj.tan, c->d_salt, c->d_temp, c->d_mean_salt, c->d_mean_temp,
@@ -850,7 +851,8 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
         }
         if (dalloc(&ctx->x32, cap * 4) || dalloc(&ctx->y32, cap * 4) || dalloc(&ctx->z32, cap * 4) ||
             dalloc(&ctx->cx, cap * 4) || dalloc(&ctx->cy, cap * 4) || dalloc(&ctx->cz, cap * 4) ||
-            dalloc(&ctx->qwarm, cap * 8) || dalloc(&ctx->gwarm, cap * 8) || dalloc(&ctx->ftmp, fmax * 4) || dalloc(&ctx->qmax, lmax * 4))
+            dalloc(&ctx->qwarm, cap * 8) || dalloc(&ctx->gwarm, cap * 8) || dalloc(&ctx->qwarm2, cap * 4) ||
+            dalloc(&ctx->ftmp, fmax * 4) || dalloc(&ctx->qmax, lmax * 4))
             return bail(RP_ERR_NOMEM, "mixed-form allocation");
     }
     if (dalloc(&ctx->x, cap * 8) || dalloc(&ctx->y, cap * 8) || dalloc(&ctx->z, cap * 8) ||

@@ -111,6 +111,7 @@ struct RpParticlesDev {
     float* cz;
     double* qwarm;
     double* gwarm;
+    float* qwarm2;                 // the smoothing parameter of the step before qwarm's
     // diagnostics (ROMSPath.f90:130-131): P_Salt, P_Temp, mean_salt,
     // mean_temp (running sums), P_HOB, P_bustr, P_bvstr
     double* salt;

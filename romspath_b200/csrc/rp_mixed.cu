@@ -375,6 +375,7 @@ __global__ void k_mixed_from_f64(RpParticlesDev P) {
     P.z32[n] = pz; P.cz[n] = (float)((double)pz - z);
     P.qwarm[n] = -1.0;
     P.gwarm[n] = 0.0;
+    P.qwarm2[n] = -1.f;
 }
 
 __global__ void k_mixed_to_f64(RpParticlesDev P) {

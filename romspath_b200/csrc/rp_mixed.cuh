@@ -815,41 +815,58 @@ __device__ double m_light_S(const W& w, const MFit& f, double p) {
 
 // smooth() (pppack.f90:5108-5317): the secant search for q = p/(1-p) on
 // 1/sqrt(SF) until |SF - s| <= 0.01 s.  Warm start: the particle's q of its
-// previous step (one pass when it still meets the criterion) and the slope
-// g of 1/sqrt(SF) in q found there, which gives a Newton step when it does
-// not; then secant steps.  Falls back to the reference's cold start (p = 0,
-// utru) when that does not converge.  q and g are returned in qstate and
-// gstate (q = 0 for p = 0; g <= 0 when unknown); passes = chol1d passes made.
+// previous step extrapolated with the one before (q2state), one pass when
+// that meets the criterion, and the slope g of 1/sqrt(SF) in q found at an
+// earlier step, which gives a Newton step when it does not; then secant
+// steps.  Falls back to the reference's cold start (p = 0, utru) when that
+// does not converge.  q and g are returned in qstate and gstate (q = 0 for
+// p = 0; g <= 0 when unknown), the incoming q in q2state; passes = chol1d
+// passes made.
 template <class W>
 __device__ double m_smooth(const W& w, const MFit& f, double s, int max_iter, double& qstate,
-                           double& gstate, uint32_t& fl, int& passes) {
-    // the first full pass of every path also stores y(i); the warm-start
-    // check is a light pass (m_light_S: no workspace traffic), the p = 0
-    // pass does not store u; both are repeated as a full pass when their
-    // p is the fit's
+                           double& gstate, float& q2state, uint32_t& fl, int& passes) {
+    // the first full pass of every path also stores y(i); the p = 0 pass
+    // does not store u and is repeated as a full pass when p = 0 is the fit
     passes = 1;
     if (s <= 0.0) {
         m_chol1d(w, f, 1.0, nullptr, true, true);
         return 1.0;
     }
     const double ooss = 1.0 / sqrt(s);
-    double q = qstate;
+    const double q_in = qstate;
+    double q = q_in;
     const bool warm = q > 0.0;
     bool ys = false;                                 // y(i) stored by a pass already
+    const double q2 = (double)q2state;               // the q of the step before the previous one
+    q2state = (float)q_in;                           // the previous q, for the next step
     if (warm) {
-        // the check at the previous q: a light pass where the view asks
-        // for it (one forward sweep, nothing stored; it needs registers the
-        // fused step does not have), else a pass that stores y but not u
+        // first guess: this step's q extrapolated from the previous two
+        // steps' (geometric, the ratio held to [1/2, 2]); the column changes
+        // smoothly from step to step, so this guess usually meets the
+        // criterion at once, where the previous q alone rarely does
+        if (q2 > 0.0) q = q * fmin(fmax(q / q2, 0.5), 2.0);
+        // the check: a full pass that stores u (the guess is usually the
+        // fit), or where the view asks for it a light pass (one forward
+        // sweep, nothing stored) followed by a full pass when it converged
         double sfq;
+        bool us = false;
         if (W::kLightCheck) {
             sfq = 36.0 * m_light_S(w, f, q / (1.0 + q)) / ((1.0 + q) * (1.0 + q));
         } else {
-            sfq = m_sf(w, f, q, true, false);
+            sfq = m_sf(w, f, q, true, true);
             ys = true;
+            us = true;
         }
         if (fabs(sfq - s) <= 0.01 * s) {
-            m_chol1d(w, f, q / (1.0 + q), nullptr, !ys, true);
-            passes = 2;
+            if (!us) {
+                m_chol1d(w, f, q / (1.0 + q), nullptr, !ys, true);
+                passes = 2;
+            }
+            // the history keeps the root estimate rather than the accepted
+            // q (any q inside the 1 % band is accepted; the extrapolation
+            // of such q's would carry the band's spread)
+            const double qr = (gstate > 0.0) ? q - (1.0 / sqrt(sfq) - ooss) / gstate : q;
+            qstate = (qr > 0.0) ? qr : q;
             return q / (1.0 + q);
         }
         double prevq = q, prevsf = 1.0 / sqrt(sfq);
@@ -862,7 +879,8 @@ __device__ double m_smooth(const W& w, const MFit& f, double s, int max_iter, do
             const double oosf = 1.0 / sqrt(sfq);
             const double g = (oosf - prevsf) / (q - prevq);
             if (fabs(sfq - s) <= 0.01 * s) {
-                qstate = q;
+                const double qr = q - (oosf - ooss) / g;
+                qstate = (g > 0.0 && qr > 0.0) ? qr : q;
                 gstate = g;
                 return q / (1.0 + q);
             }
@@ -895,7 +913,9 @@ __device__ double m_smooth(const W& w, const MFit& f, double s, int max_iter, do
         const double g = (oosf - prevsf) / (q - prevq);
         if (fabs(sfq - s) <= 0.01 * s) {
             gstate = g;
-            break;
+            const double qr = q - (oosf - ooss) / g;
+            qstate = (g > 0.0 && qr > 0.0) ? qr : q;
+            return q / (1.0 + q);
         }
         if (it >= max_iter) {
             fl |= RP_FL_SPLINE;
@@ -983,7 +1003,7 @@ __device__ __forceinline__ void m_normal2(const RpStepArgs& A, uint32_t pid, uin
 // random-displacement sub-steps in FP64
 template <typename E, class W>
 __device__ float m_vturb(const RpStepArgs& A, const RpGridDev& g, const MStage& S, float Zpar,
-                         uint32_t pid, double& qstate, double& gstate, uint32_t& fl, const W& w) {
+                         uint32_t pid, double& qstate, double& gstate, float& q2state, uint32_t& fl, const W& w) {
     const int sw = g.N + 1;
     MFit f;
     f.np = (int)((double)sw * A.sub);
@@ -1037,7 +1057,7 @@ __device__ float m_vturb(const RpStepArgs& A, const RpGridDev& g, const MStage& 
     f.h = (zeta - f.z1) / (double)(f.np - 1);
     f.rh = 1.0 / f.h;
     int passes;
-    const double p = m_smooth(w, f, A.smth, A.spline_max_iter, qstate, gstate, fl, passes);
+    const double p = m_smooth(w, f, A.smth, A.spline_max_iter, qstate, gstate, q2state, fl, passes);
     if (A.spl) rp_count_fit(A.spl, passes);
     const double deltat = A.deltat;
     double ParZc = (double)Zpar;
@@ -1261,9 +1281,11 @@ __device__ void m_vturb_one(const RpStepArgs& A, int64_t n, const W& w, float* t
         if (Zpar > S1.zeta) Zpar = S1.zeta - 0.001f;
     }
     double q = Pt.qwarm[n], gs = Pt.gwarm[n];
-    turbv[n] = m_vturb<E>(A, g, S1, Zpar, Pt.pid[n], q, gs, fl, w);
+    float q2 = Pt.qwarm2[n];
+    turbv[n] = m_vturb<E>(A, g, S1, Zpar, Pt.pid[n], q, gs, q2, fl, w);
     Pt.qwarm[n] = q;
     Pt.gwarm[n] = gs;
+    Pt.qwarm2[n] = q2;
     if (fl) Pt.flags[n] |= fl;
 }
 
@@ -1346,9 +1368,11 @@ __device__ void m_update_one(const RpStepArgs& A, int64_t n, const W& w, const f
         TurbV = turbv_in[n];
     } else if (A.vturb_on) {
         double q = Pt.qwarm[n], gs = Pt.gwarm[n];
-        TurbV = m_vturb<E>(A, g, S1, Zpar, pid, q, gs, fl, w);
+        float q2 = Pt.qwarm2[n];
+        TurbV = m_vturb<E>(A, g, S1, Zpar, pid, q, gs, q2, fl, w);
         Pt.qwarm[n] = q;
         Pt.gwarm[n] = gs;
+        Pt.qwarm2[n] = q2;
     }
     float ZBehav = 0.f;                                // behave(), ROMSPath.f90:800-804
     if (FEAT && (A.beh.behavior || A.beh.va || A.beh.wa))

@@ -146,7 +146,8 @@ cudaError_t launch_sort(const RpStepArgs& A, int mixed, const SortBufs& b, void*
         if (c) *nlaunch += 1;
     }
     float* f4[] = {mixed ? P.x32 : nullptr, mixed ? P.y32 : nullptr, mixed ? P.z32 : nullptr,
-                   mixed ? P.cx : nullptr,  mixed ? P.cy : nullptr,  mixed ? P.cz : nullptr};
+                   mixed ? P.cx : nullptr,  mixed ? P.cy : nullptr,  mixed ? P.cz : nullptr,
+                   mixed ? P.qwarm2 : nullptr};
     for (float* c : f4) {
         if ((e = permute_col(c, scratch8, b.perm, n, s)) != cudaSuccess) return e;
         if (c) *nlaunch += 1;
