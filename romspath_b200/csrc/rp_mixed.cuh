@@ -813,6 +813,12 @@ __device__ double m_light_S(const W& w, const MFit& f, double p) {
     return (phi + p * phid) * (1.0 / 6.0);
 }
 
+// True on the first internal step of an external step (ix(2) = ex(2)): the
+// three frame times move on, so the time-interpolated fields jump here and
+// the change of q over this step is no guide to the next one; the q history
+// is then dropped (the next step starts from this step's q alone).
+__device__ __forceinline__ bool m_stencil_moved(const RpStepArgs& A) { return A.ix[1] == A.ex[1]; }
+
 // smooth() (pppack.f90:5108-5317): the secant search for q = p/(1-p) on
 // 1/sqrt(SF) until |SF - s| <= 0.01 s.  Warm start: the particle's q of its
 // previous step extrapolated with the one before (q2state), one pass when
@@ -1285,7 +1291,7 @@ __device__ void m_vturb_one(const RpStepArgs& A, int64_t n, const W& w, float* t
     turbv[n] = m_vturb<E>(A, g, S1, Zpar, Pt.pid[n], q, gs, q2, fl, w);
     Pt.qwarm[n] = q;
     Pt.gwarm[n] = gs;
-    Pt.qwarm2[n] = q2;
+    Pt.qwarm2[n] = m_stencil_moved(A) ? -1.f : q2;
     if (fl) Pt.flags[n] |= fl;
 }
 
@@ -1372,7 +1378,7 @@ __device__ void m_update_one(const RpStepArgs& A, int64_t n, const W& w, const f
         TurbV = m_vturb<E>(A, g, S1, Zpar, pid, q, gs, q2, fl, w);
         Pt.qwarm[n] = q;
         Pt.gwarm[n] = gs;
-        Pt.qwarm2[n] = q2;
+        Pt.qwarm2[n] = m_stencil_moved(A) ? -1.f : q2;
     }
     float ZBehav = 0.f;                                // behave(), ROMSPath.f90:800-804
     if (FEAT && (A.beh.behavior || A.beh.va || A.beh.wa))
