@@ -860,7 +860,8 @@ def adjoint_run(args):
 
 FORM_DESC = {
     "mixed": "mixed precision: FP16 u/v/w/AKs with per-level power-of-two scales, FP32 zeta, FP32 positions with "
-             "Kahan compensation, FP32 interpolation/RK4, FP64 age, smoothing-spline fit and sub-steps",
+             "Kahan compensation, FP32 interpolation/RK4, FP64 age, secant search and sub-steps, smoothing-spline "
+             "factor rows in FP64 and substitution sweeps in FP32",
     "mixed-i16": "mixed precision with int16 fixed-point u/v/w/AKs (scale = level max / 32767)",
     "f32": "exact: FP64 arithmetic on FP32-stored fields (bit-identical to the CPU oracle)",
     "f64": "plain FP64: FP64-stored fields, FP64 arithmetic (bit-identical to the CPU oracle)",

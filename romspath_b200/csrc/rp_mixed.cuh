@@ -5,10 +5,11 @@
 //   * u, v, w, AKs stored in FP16 with a scale per (ring slot, level),
 //     zeta in FP32; interpolation, RK4 and reflections in FP32,
 //   * age in FP64,
-//   * the PPPACK smoothing-spline fit and the random-displacement sub-steps
-//     in FP64, with the secant search for the smoothing parameter started
-//     from the particle's value of the previous step (one chol1d pass when
-//     it still meets smooth()'s 1 % criterion).
+//   * the PPPACK smoothing-spline fit with its factor's leading rows, the
+//     secant search and the random-displacement sub-steps in FP64 and the
+//     substitution sweeps in FP32, the search for the smoothing parameter
+//     started from the particle's values of the previous steps (one chol1d
+//     pass when the guess meets smooth()'s 1 % criterion).
 // The 16-bit storage is FP16 (RP_FIELD_MIXED) or int16 fixed point
 // (RP_FIELD_MIXED_I16, |v| / scale <= 32767 with scale = level max / 32767).
 // The four ring slots of one (point, level) are one 8-byte load (16 bytes
@@ -458,8 +459,9 @@ __device__ __forceinline__ void m_find_currents(const RpStepArgs& A, const RpGri
 // Workspace: the chol1d arrays (ratio1, ratio2 and u), then four FP32
 // arrays for the data (the column and the resampled values carry FP32
 // information only).  RP_MIXED_WS sets the chol1d arrays' storage: 0 all
-// FP64, 1 the factor ratios FP32 and u FP64, 2 all FP32 (the arithmetic
-// stays FP64 in registers).  kMixedArrays (NPMAX+1) doubles in all.
+// FP64, 1 the factor ratios FP32 and u FP64, 2 all FP32 (the default; the
+// sweeps of m_chol1d compute in FP32 either way).  kMixedArrays (NPMAX+1)
+// doubles in all.
 #ifndef RP_MIXED_WS
 #define RP_MIXED_WS 2
 #endif
@@ -485,7 +487,7 @@ struct MFit;
 template <int NPMAX, bool PREF = true>
 struct MSpline {
     static constexpr bool kStoreY = true;
-    static constexpr int kColBatch = 1;
+    static constexpr int kColBatch = 2;
     static constexpr bool kLightCheck = false;
     static constexpr bool kPrefetch = PREF;
     double* base;
@@ -579,10 +581,36 @@ __device__ __forceinline__ double MSmemSpline<NPMAX, KSM, CMAX, B>::yat(const MF
     return (double)cm(lo) * x + (double)cb(lo);
 }
 
+// linint of the column at ascending points in FP32 (the column's breaks,
+// slopes and intercepts are stored in FP32)
+template <class W>
+struct MWalkF {
+    int j;
+    float zn, m, b;                // cz(j+1), cm(j), cb(j)
+    __device__ __forceinline__ void init(const W& w) {
+        j = 1;
+        zn = w.cz(2);
+        m = w.cm(1);
+        b = w.cb(1);
+    }
+    __device__ __forceinline__ float at(const W& w, int sw, float x) {
+        while (j < sw - 1 && zn <= x) {
+            j++;
+            zn = w.cz(j + 1);
+            m = w.cm(j);
+            b = w.cb(j);
+        }
+        return fmaf(m, x, b);
+    }
+};
+
 // One chol1d pass at p: factorise, solve for u, form qu = Q u; returns
 // sum_i qu(i)^2 dy^2 and, on request, utru = sum v4 (u(i-1)(u(i-1)+u(i)) + u(i)^2).
-// With store_y the resampled values y(i) are also kept (for ppvalu); u is
-// written back only with store_u (a pass whose u may be the fit's).
+// The factor's rows before it turns stationary are formed in FP64 and
+// stored in FP32; the substitutions, qu and its sum run in FP32 (the data,
+// the factor ratios and u are FP32 values).  With store_y the resampled
+// values y(i) are also kept (for ppvalu); u is written back only with
+// store_u (a pass whose u may be the fit's).
 template <class W>
 __device__ double m_chol1d(const W& w, const MFit& f, double p, double* utru_out, bool store_y,
                            bool store_u) {
@@ -594,66 +622,67 @@ __device__ double m_chol1d(const W& w, const MFit& f, double p, double* utru_out
     const double D = six1mp * (6.0 * r2) + 4.0 * p * f.h;
     const double E = six1mp * (-4.0 * r2) + p * f.h;
     const double F = six1mp * r2;
-    // Q'y on the fly: qty(i) = (y(i+1) - 2 y(i) + y(i-1)) / h
-    MWalk<W> wk;
+    const float hf = (float)f.h, rhf = (float)f.rh, z1f = (float)f.z1;
+    // Q'y on the fly: qty(i) = (y(i+1) - 2 y(i) + y(i-1)) / h, y at z1 + (i-1) h
+    MWalkF<W> wk;
     wk.init(w);
-    double ym = wk.at(w, f.sw, f.z1);
-    double y0 = wk.at(w, f.sw, f.z1 + f.h);
-    double xn = f.z1 + 2.0 * f.h;
-    double yp = wk.at(w, f.sw, xn);
+    float ym = wk.at(w, f.sw, z1f);
+    float y0 = wk.at(w, f.sw, z1f + hf);
+    float yp = wk.at(w, f.sw, fmaf(2.f, hf, z1f));
     if (store_y) {
-        w.y(1) = (float)ym;
-        w.y(2) = (float)y0;
-        w.y(3) = (float)yp;
+        w.y(1) = ym;
+        w.y(2) = y0;
+        w.y(3) = yp;
     }
     double a1 = D, a2 = E, b1 = D;
-    double uprev = 0.0, ucur = (yp - 2.0 * y0 + ym) * f.rh, r2prev = 0.0;
+    float uprev = 0.f, ucur = (yp - 2.f * y0 + ym) * rhf, r2prev = 0.f;
     // The bands are constant (uniform breaks), so the factor converges to
     // a fixed point: once a row's ratios round to the previous row's in
-    // the storage precision, rows ks..np-3 reuse them (no division, no
-    // store); the last row (F = 0 there) is factorised from the held state.
+    // FP32, rows ks..np-3 reuse them (no division, no store); the last row
+    // (F = 0 there) is factorised from the held state.
     int ks = np - 1;                                 // first reused row (np-1: none)
-    double hinv = 0.0, hr1 = 0.0, hr2 = 0.0;
-    MRatio pr1 = (MRatio)0, pr2 = (MRatio)0;
+    float hinv = 0.f, hr1 = 0.f, hr2 = 0.f;
+    float pr1 = 0.f, pr2 = 0.f;
 #pragma unroll 2
     for (int i = 2; i <= np - 2; i++) {
-        double inv, ratio1, ratio2;
+        float inv, ratio1, ratio2;
         if (i < ks || i == np - 2) {
             const double Fi = (i <= np - 3) ? F : 0.0;
-            inv = 1.0 / a1;                          // one division per row
-            ratio1 = a2 * inv;
-            const double b1n = b1 - ratio1 * a2;
-            const double c2 = E - ratio1 * Fi;
-            ratio2 = Fi * inv;
-            const double c1 = D - ratio2 * Fi;
-            const MRatio q1 = (MRatio)ratio1, q2 = (MRatio)ratio2;
-            if (i > 2 && i < np - 2 && q1 == pr1 && q2 == pr2) {
+            const double invd = 1.0 / a1;            // one division per row
+            const double ratio1d = a2 * invd;
+            const double b1n = b1 - ratio1d * a2;
+            const double c2 = E - ratio1d * Fi;
+            const double ratio2d = Fi * invd;
+            const double c1 = D - ratio2d * Fi;
+            inv = (float)invd;
+            ratio1 = (float)ratio1d;
+            ratio2 = (float)ratio2d;
+            if (i > 2 && i < np - 2 && ratio1 == pr1 && ratio2 == pr2) {
                 ks = i;
                 hinv = inv;
                 hr1 = ratio1;
                 hr2 = ratio2;
             } else {
-                w.s1(i) = q1;
-                w.s2(i) = q2;
+                w.s1(i) = ratio1;
+                w.s2(i) = ratio2;
                 a1 = b1n;
                 a2 = c2;
                 b1 = c1;
             }
-            pr1 = q1;
-            pr2 = q2;
+            pr1 = ratio1;
+            pr2 = ratio2;
         } else {
             inv = hinv;
             ratio1 = hr1;
             ratio2 = hr2;
         }
-        w.u(i) = (MU)(ucur * inv);
+        w.u(i) = ucur * inv;
         ym = y0;
         y0 = yp;
-        xn = xn + f.h;                               // z1 + (i+1) h, accumulated
-        yp = wk.at(w, f.sw, xn);
-        if (store_y) w.y(i + 2) = (float)yp;
-        const double qn = (yp - 2.0 * y0 + ym) * f.rh;     // qty(i+1)
-        const double unext = qn - ratio1 * ucur - r2prev * uprev;
+        yp = wk.at(w, f.sw, fmaf((float)(i + 1), hf, z1f));   // y(i+2) at z1 + (i+1) h
+        if (store_y) w.y(i + 2) = yp;
+        const float qn = (yp - 2.f * y0 + ym) * rhf;          // qty(i+1)
+        const float unext = qn - ratio1 * ucur - r2prev * uprev;
         uprev = ucur;
         ucur = unext;
         r2prev = ratio2;
@@ -661,65 +690,64 @@ __device__ double m_chol1d(const W& w, const MFit& f, double p, double* utru_out
     // back substitution, descending, with qu and its sum of squares:
     // raw(k) = (u(k) - u(k-1))/h for 2 <= k <= np, raw(1) = raw(np+1) = 0,
     // qu(k) = raw(k+1) - raw(k)
-    const double dy2 = f.dy2;
     const bool want_utru = utru_out != nullptr;
-    double up1 = 0.0;                                // u(np)
-    double up2 = 0.0;                                // u(np+1), unused
-    double rawp = 0.0;                               // raw(np+1)
-    double sum = 0.0, utru = 0.0;                    // sum of qu^2 (times dy2 at the end)
-    if (store_u) w.u(np) = 0.0;
+    float up1 = 0.f;                                 // u(np)
+    float up2 = 0.f;                                 // u(np+1), unused
+    float rawp = 0.f;                                // raw(np+1)
+    float sum = 0.f, utru = 0.f;                     // sum of qu^2 (times dy2 at the end)
+    if (store_u) w.u(np) = 0.f;
     {
-        const double ui = ucur / a1;                 // u(np-1)
-        if (store_u) w.u(np - 1) = (MU)ui;
-        const double raw = (up1 - ui) * f.rh;        // raw(np)
-        const double fin = rawp - raw;               // qu(np)
-        sum = sum + fin * fin;
-        if (want_utru) utru = utru + f.h * (ui * (ui + up1) + up1 * up1);
+        const float ui = (float)((double)ucur / a1); // u(np-1)
+        if (store_u) w.u(np - 1) = ui;
+        const float raw = (up1 - ui) * rhf;          // raw(np)
+        const float fin = rawp - raw;                // qu(np)
+        sum = fmaf(fin, fin, sum);
+        if (want_utru) utru = utru + hf * (ui * (ui + up1) + up1 * up1);
         rawp = raw;
         up2 = up1;
         up1 = ui;
     }
-    const double h1 = (double)(MRatio)hr1, h2 = (double)(MRatio)hr2;   // the held rows' stored ratios
+    const float h1 = hr1, h2 = hr2;                  // the held rows' ratios
     // with W::kPrefetch, u(i) is loaded four rows ahead of its use (index 1
     // stands in past the start; that value is never used)
-    MU q0 = w.u(np - 2), q1 = w.u(max(np - 3, 1)), q2 = w.u(max(np - 4, 1)), q3 = w.u(max(np - 5, 1));
+    float q0 = w.u(np - 2), q1 = w.u(max(np - 3, 1)), q2 = w.u(max(np - 4, 1)), q3 = w.u(max(np - 5, 1));
 #pragma unroll 2
     for (int i = np - 2; i >= 2; i--) {
-        double uq;
+        float uq;
         if constexpr (W::kPrefetch) {
-            uq = (double)q0;
+            uq = q0;
             q0 = q1;
             q1 = q2;
             q2 = q3;
             q3 = w.u(max(i - 4, 1));
         } else {
-            uq = (double)w.u(i);
+            uq = w.u(i);
         }
         const bool held = (i >= ks && i <= np - 3);
-        double s1v = h1, s2v = h2;
+        float s1v = h1, s2v = h2;
         if (!held) {
-            s1v = (double)w.s1(i);
-            s2v = (double)w.s2(i);
+            s1v = w.s1(i);
+            s2v = w.s2(i);
         }
-        const double ui = uq - up1 * s1v - up2 * s2v;
-        if (store_u) w.u(i) = (MU)ui;
-        const double raw = (up1 - ui) * f.rh;        // raw(i+1)
-        const double fin = rawp - raw;               // qu(i+1)
-        sum = sum + fin * fin;
-        if (want_utru) utru = utru + f.h * (ui * (ui + up1) + up1 * up1);
+        const float ui = uq - up1 * s1v - up2 * s2v;
+        if (store_u) w.u(i) = ui;
+        const float raw = (up1 - ui) * rhf;          // raw(i+1)
+        const float fin = rawp - raw;                // qu(i+1)
+        sum = fmaf(fin, fin, sum);
+        if (want_utru) utru = utru + hf * (ui * (ui + up1) + up1 * up1);
         rawp = raw;
         up2 = up1;
         up1 = ui;
     }
     {
-        const double raw = up1 * f.rh;               // raw(2), u(1) = 0
-        const double fin2 = rawp - raw;              // qu(2)
+        const float raw = up1 * rhf;                 // raw(2), u(1) = 0
+        const float fin2 = rawp - raw;               // qu(2)
         sum = sum + fin2 * fin2 + raw * raw;         // qu(1) = raw(2)
-        if (want_utru) utru = utru + f.h * (up1 * up1);
+        if (want_utru) utru = utru + hf * (up1 * up1);
     }
-    if (store_u) w.u(1) = 0.0;
-    if (want_utru) *utru_out = utru;
-    return sum * dy2;
+    if (store_u) w.u(1) = 0.f;
+    if (want_utru) *utru_out = (double)utru;
+    return (double)sum * f.dy2;
 }
 
 // SF(q) = 36 sum qu^2 dy^2 / (1+q)^2 of one chol1d pass at p = q/(1+q)
