@@ -1053,7 +1053,7 @@ __device__ float m_vturb(const RpStepArgs& A, const RpGridDev& g, const MStage& 
     const float4* qs = reinterpret_cast<const float4*>(g.qs_aks);
     const MTime tk = m_time(A, g, 0);
     const bool all[4] = {true, true, true, true};
-    double zprev = 0.0, kprev = 0.0;
+    float zprev = 0.f, kprev = 0.f;
     // levels in batches of kColBatch: the batch's 4 kColBatch corner loads
     // are issued before any is used, so their latencies overlap (a
     // workspace view for a kernel with registers to spare asks for more)
@@ -1073,15 +1073,15 @@ __device__ float m_vturb(const RpStepArgs& A, const RpGridDev& g, const MStage& 
             const int k = k0 + b;
             if (k > sw) break;
             // z_w(k) of the interpolated zeta (getWlevel is linear in zeta)
-            const double zk = (k == sw) ? zeta
-                                        : (double)m_zlev(g.vtransform, hc, h, den_r, (float)__ldg(g.sw + k - 1),
-                                                         (float)__ldg(g.csw + k - 1), S.zeta);
-            const double kk = (double)m_level_of<E>(v[b], sc[b], cwt, all, tk);   // getInterpAKs
-            w.cz(k) = (float)zk;
+            const float zk = (k == sw) ? S.zeta
+                                       : m_zlev(g.vtransform, hc, h, den_r, (float)__ldg(g.sw + k - 1),
+                                                (float)__ldg(g.csw + k - 1), S.zeta);
+            const float kk = m_level_of<E>(v[b], sc[b], cwt, all, tk);   // getInterpAKs
+            w.cz(k) = zk;
             if (k >= 2) {
-                const double m = (kk - kprev) / (zk - zprev);
-                w.cm(k - 1) = (float)m;
-                w.cb(k - 1) = (float)(kprev - m * zprev);
+                const float m = (kk - kprev) / (zk - zprev);
+                w.cm(k - 1) = m;
+                w.cb(k - 1) = kprev - m * zprev;
             }
             zprev = zk;
             kprev = kk;
