@@ -57,9 +57,10 @@ extern "C" {
 /* The mixed-precision form: u, v, w, AKs stored in FP16 with a power-of-two
  * scale per (slot, level), zeta in FP32; positions in FP32 with Kahan-
  * compensated accumulation; interpolation and RK4 in FP32; age, the
- * smoothing-spline fit and the random-displacement sub-steps in FP64, with
- * the spline's smoothing parameter warm-started from the particle's
- * previous step.  Not bit-exact; its error against RP_FIELD_F64 on the
+ * smoothing spline's factor rows and secant search and the random-
+ * displacement sub-steps in FP64, the spline's substitution sweeps in
+ * FP32, with its smoothing parameter extrapolated from the particle's
+ * previous two steps.  Not bit-exact; its error against RP_FIELD_F64 on the
  * same noise is measured by the tests. */
 #define RP_FIELD_MIXED 2
 /* The same form with u, v, w, AKs in int16 fixed point, scale = level
