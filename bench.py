@@ -87,6 +87,9 @@ def parse():
     ap.add_argument("--kernel-form", default="fused", choices=["fused", "split", "smem", "fused-noprefetch"],
                     help="kernel form of the timed forms (rp_set_kernel_form; smem and fused-noprefetch: mixed "
                          "forms only, the exact forms run those fused)")
+    ap.add_argument("--param", action="append", default=[], metavar="KEY=VALUE",
+                    help="override one of the workload's run parameters in the timed forms (e.g. vturb_on=0, "
+                         "sub=2, deltat=300) to time parts of the step; the line's config lists the overrides")
     ap.add_argument("--error-days", type=float, default=1.0,
                     help="length of the headline line's lockstep error check of the mixed forms (0: none)")
     ap.add_argument("--error-particles", type=int, default=65536,
@@ -139,6 +142,24 @@ def measured_peaks(path=None):
             elif isinstance(x, list):
                 stack.extend(reversed(x))
     return 6650.0, "fallback (6.65 TB/s)"
+
+
+def parse_params(items, params):
+    """--param KEY=VALUE overrides of the workload's run parameters; KEY must
+    be one of them and VALUE is read as a number (int where it is one)."""
+    out = {}
+    for it in items:
+        if "=" not in it:
+            raise SystemExit(f"--param wants KEY=VALUE, got {it!r}")
+        k, v = it.split("=", 1)
+        if k not in params:
+            raise SystemExit(f"--param: unknown parameter {k!r} (one of {sorted(params)})")
+        try:
+            val = int(v)
+        except ValueError:
+            val = float(v)
+        out[k] = val
+    return out
 
 
 def profile_traffic(workload, kernel, key="dram_bytes_per_launch"):
@@ -910,7 +931,9 @@ def main():
     wl = args.workload
     spec = synth.config_spec(wl)[0]
     grid = synth.make_grid(spec)
-    params = synth.config_params(wl)
+    params = dict(synth.config_params(wl))
+    overrides = parse_params(args.param, params)
+    params.update(overrides)
     npart = args.particles or synth.CONFIG_PARTICLES[wl]
     nframes = 4
     frames = [synth.make_frame(spec, grid, k * 3600.0) for k in range(nframes)]
@@ -1157,6 +1180,7 @@ def main():
             "config": {"workload": WORKLOAD_DESCS.get(wl, wl), "particles_per_gpu": npart,
                        "step": "one hydro frame interval = 12 internal steps (idt=300 s)",
                        "form": FORM_DESC[head], "kernel_form": args.kernel_form,
+                       **({"param_overrides": overrides} if overrides else {}),
                        "l2": ("inputs larger than L2 (frame ring 390 MB FP32 / 195 MB FP16, particle state "
                               "~80 MB, spline workspace in local memory ~0.5-1 GB)") if wl == "cfg2" else
                              ("frames L2-resident (8.4 MB per FP64 frame), particle state and spline workspace "

@@ -89,3 +89,14 @@ def test_measured_peaks_file_forms(tmp_path):
     p.write_text("not json")
     assert bench.measured_peaks(str(p)) == (6650.0, "fallback (6.65 TB/s)")
     assert bench.measured_peaks(str(tmp_path / "absent.json"))[1].startswith("fallback")
+
+
+def test_param_overrides():
+    params = {"vturb_on": 1, "sub": 4.0, "deltat": 30.0}
+    assert bench.parse_params([], params) == {}
+    assert bench.parse_params(["vturb_on=0", "sub=2.5", "deltat=300"], params) == \
+        {"vturb_on": 0, "sub": 2.5, "deltat": 300}
+    with pytest.raises(SystemExit):
+        bench.parse_params(["no_such=1"], params)
+    with pytest.raises(SystemExit):
+        bench.parse_params(["vturb_on"], params)
