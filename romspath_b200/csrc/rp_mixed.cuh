@@ -100,6 +100,7 @@ __device__ __forceinline__ float m_bil(const double* a, const MRho& c) {
 struct MTime {
     float wb, wc, wf;
     int sb, sc, sf;
+    float4 w4;                     // the same weights by physical slot (0 for the spare slot)
 };
 
 __device__ __forceinline__ float m_pick4(const float4& v, int s) {
@@ -114,7 +115,7 @@ __device__ __forceinline__ float m_zeta(const RpGridDev& g, const MRho& c, const
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         const float4 v = __ldg(z + c.o[q]);
-        acc += c.ci[q] * (t.wb * m_pick4(v, t.sb) + t.wc * m_pick4(v, t.sc) + t.wf * m_pick4(v, t.sf));
+        acc += c.ci[q] * fmaf(t.w4.w, v.w, fmaf(t.w4.z, v.z, fmaf(t.w4.y, v.y, t.w4.x * v.x)));
     }
     return acc;
 }
@@ -275,18 +276,39 @@ __device__ __forceinline__ float m_slot(const uint2& v, int s) {
     return m_dec<E>((s & 1) ? (word >> 16) : (word & 0xffffu));
 }
 
+// the four 16-bit slots of one (point, level) dotted with per-slot weights
+// (slot s is half s & 1 of word s >> 1)
+template <typename E>
+__device__ __forceinline__ float m_dot4(const uint2& v, const float4& w);
+template <>
+__device__ __forceinline__ float m_dot4<__half>(const uint2& v, const float4& w) {
+    const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&v.x));
+    const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&v.y));
+    return fmaf(w.w, b.y, fmaf(w.z, b.x, fmaf(w.y, a.y, w.x * a.x)));
+}
+template <>
+__device__ __forceinline__ float m_dot4<int16_t>(const uint2& v, const float4& w) {
+    const float a0 = (float)(int16_t)(v.x & 0xffffu), a1 = (float)((int32_t)v.x >> 16);
+    const float b0 = (float)(int16_t)(v.y & 0xffffu), b1 = (float)((int32_t)v.y >> 16);
+    return fmaf(w.w, b1, fmaf(w.z, b0, fmaf(w.y, a1, w.x * a0)));
+}
+
+// the level scales folded into the slot weights
+__device__ __forceinline__ float4 m_scaled_w4(const MTime& t, const float4& sc) {
+    return make_float4(t.w4.x * sc.x, t.w4.y * sc.y, t.w4.z * sc.z, t.w4.w * sc.w);
+}
+
 // sum over corners of cff * (time-interpolated, scaled value) at level lev
 template <typename E>
 __device__ __forceinline__ float m_level(const uint2* f, const float4* qs, const int64_t o[4], const float cff[4],
                                          const bool use[4], int nlev, int lev, const MTime& t) {
-    const float4 sc = __ldg(qs + lev - 1);             // level scales [k][slot4]
-    const float wb = t.wb * m_pick4(sc, t.sb), wc = t.wc * m_pick4(sc, t.sc), wf = t.wf * m_pick4(sc, t.sf);
+    const float4 ws = m_scaled_w4(t, __ldg(qs + lev - 1));   // level scales [k][slot4]
     float acc = 0.f;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         if (use[q]) {
             const uint2 v = __ldg(f + o[q] * nlev + lev - 1);
-            acc += cff[q] * (wb * m_slot<E>(v, t.sb) + wc * m_slot<E>(v, t.sc) + wf * m_slot<E>(v, t.sf));
+            acc += cff[q] * m_dot4<E>(v, ws);
         }
     }
     return acc;
@@ -296,11 +318,11 @@ __device__ __forceinline__ float m_level(const uint2* f, const float4* qs, const
 template <typename E>
 __device__ __forceinline__ float m_level_of(const uint2 v[4], const float4& sc, const float cff[4],
                                             const bool use[4], const MTime& t) {
-    const float wb = t.wb * m_pick4(sc, t.sb), wc = t.wc * m_pick4(sc, t.sc), wf = t.wf * m_pick4(sc, t.sf);
+    const float4 ws = m_scaled_w4(t, sc);
     float acc = 0.f;
 #pragma unroll
     for (int q = 0; q < 4; q++)
-        if (use[q]) acc += cff[q] * (wb * m_slot<E>(v[q], t.sb) + wc * m_slot<E>(v[q], t.sc) + wf * m_slot<E>(v[q], t.sf));
+        if (use[q]) acc += cff[q] * m_dot4<E>(v[q], ws);
     return acc;
 }
 
@@ -403,6 +425,13 @@ __device__ __forceinline__ MTime m_time(const RpStepArgs& A, const RpGridDev& g,
     t.sb = g.sb;
     t.sc = g.sc;
     t.sf = g.sf;
+    // by physical slot: the b, c and f weights of the slots they sit in
+    // (added where two of them share a slot)
+    float w[4];
+#pragma unroll
+    for (int s = 0; s < 4; s++)
+        w[s] = (t.sb == s ? t.wb : 0.f) + (t.sc == s ? t.wc : 0.f) + (t.sf == s ? t.wf : 0.f);
+    t.w4 = make_float4(w[0], w[1], w[2], w[3]);
     return t;
 }
 
@@ -1140,7 +1169,7 @@ __device__ __forceinline__ float m_f32_level(const float4* f, const int64_t o[4]
     for (int q = 0; q < 4; q++) {
         if (use[q]) {
             const float4 v = __ldg(f + o[q] * nlev + lev - 1);
-            acc += cff[q] * (t.wb * m_pick4(v, t.sb) + t.wc * m_pick4(v, t.sc) + t.wf * m_pick4(v, t.sf));
+            acc += cff[q] * fmaf(t.w4.w, v.w, fmaf(t.w4.z, v.z, fmaf(t.w4.y, v.y, t.w4.x * v.x)));
         }
     }
     return acc;
