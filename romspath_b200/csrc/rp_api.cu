@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -753,6 +754,9 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
             return bail(RP_ERR_ARG, "null grid array");
         if (ngrid > 1 && (!R.scl || !R.off)) return bail(RP_ERR_ARG, "nested grids need scl/off");
         G.nx = R.xi_rho; G.ny = R.eta_rho; G.N = R.n_rho; G.vtransform = R.vtransform; G.hc = R.hc;
+        // the mixed form indexes a grid's fields in 32 bits (corner * levels + level)
+        if (ctx->mixed && (int64_t)G.nx * G.ny * std::max(G.N + 1, RP_SLOTS) > (int64_t)INT32_MAX)
+            return bail(RP_ERR_UNSUPPORTED, "mixed form: xi_rho * eta_rho * max(N + 1, 4) must be below 2^31");
         const int sw = G.N + 1;
         const int np = (int)((double)sw * p.sub);
         if (np < 4 || np > kMaxNp || np < sw) return bail(RP_ERR_UNSUPPORTED, "spline point count int(s_w*sub) must be in [max(4,s_w), 144]");

@@ -27,8 +27,12 @@
 
 // ------------------------------------------------------------ cells (FP32)
 
+// Corner offsets (j * xi + i) in 32 bits: every field index of this form,
+// offset * levels + level, stays below 2^31 (rp_create checks the grids).
+using MOff = int32_t;
+
 struct MRho {
-    int64_t o[4];
+    MOff o[4];
     float X, Y;
     float cb[4];
     float ci[4];
@@ -74,10 +78,10 @@ __device__ __forceinline__ void m_rho_cell(const RpGridDev& g, float ip, float j
     c.Y = jp - (float)J;
     const int i0 = rp_clamp(I, 1, g.nx, fl), i1 = rp_clamp(I + 1, 1, g.nx, fl);
     const int j0 = rp_clamp(J, 1, g.ny, fl), j1 = rp_clamp(J + 1, 1, g.ny, fl);
-    c.o[0] = (int64_t)(j0 - 1) * g.nx + (i0 - 1);
-    c.o[1] = (int64_t)(j0 - 1) * g.nx + (i1 - 1);
-    c.o[2] = (int64_t)(j1 - 1) * g.nx + (i1 - 1);
-    c.o[3] = (int64_t)(j1 - 1) * g.nx + (i0 - 1);
+    c.o[0] = (j0 - 1) * g.nx + (i0 - 1);
+    c.o[1] = (j0 - 1) * g.nx + (i1 - 1);
+    c.o[2] = (j1 - 1) * g.nx + (i1 - 1);
+    c.o[3] = (j1 - 1) * g.nx + (i0 - 1);
     const float X = c.X, Y = c.Y;
     c.cb[0] = (1.f - X) * (1.f - Y);
     c.cb[1] = X * (1.f - Y);
@@ -121,7 +125,7 @@ __device__ __forceinline__ float m_zeta(const RpGridDev& g, const MRho& c, const
 }
 
 struct MUV {
-    int64_t o[4];
+    MOff o[4];
     float cff[4];
     bool use[4];
 };
@@ -147,7 +151,7 @@ __device__ __forceinline__ void m_uv_cell(const RpGridDev& g, float ip, float jp
         ci[0] = a; ci[1] = b; ci[2] = b; ci[3] = a;
         cj[0] = j0; cj[1] = j0; cj[2] = j1; cj[3] = j1;
 #pragma unroll
-        for (int k = 0; k < 4; k++) c.o[k] = (int64_t)(cj[k] - 1) * xi_u + (ci[k] - 1);
+        for (int k = 0; k < 4; k++) c.o[k] = (cj[k] - 1) * xi_u + (ci[k] - 1);
         const uint8_t* mm = mk ? mk : g.mu;
 #pragma unroll
         for (int k = 0; k < 4; k++) m[k] = (float)__ldg(mm + c.o[k] * ms + mo);
@@ -167,7 +171,7 @@ __device__ __forceinline__ void m_uv_cell(const RpGridDev& g, float ip, float jp
         if (Jn >= eta_v) { cj[0] = cj[1] = cj[2] = cj[3] = eta_v; }
         else { cj[0] = Jn; cj[1] = Jn; cj[2] = Jn + 1; cj[3] = Jn + 1; }
 #pragma unroll
-        for (int k = 0; k < 4; k++) c.o[k] = (int64_t)(cj[k] - 1) * xi_v + (ci[k] - 1);
+        for (int k = 0; k < 4; k++) c.o[k] = (cj[k] - 1) * xi_v + (ci[k] - 1);
         const uint8_t* mm = mk ? mk : g.mv;
 #pragma unroll
         for (int k = 0; k < 4; k++) m[k] = (float)__ldg(mm + c.o[k] * ms + mo);
@@ -300,7 +304,7 @@ __device__ __forceinline__ float4 m_scaled_w4(const MTime& t, const float4& sc) 
 
 // sum over corners of cff * (time-interpolated, scaled value) at level lev
 template <typename E>
-__device__ __forceinline__ float m_level(const uint2* f, const float4* qs, const int64_t o[4], const float cff[4],
+__device__ __forceinline__ float m_level(const uint2* f, const float4* qs, const MOff o[4], const float cff[4],
                                          const bool use[4], int nlev, int lev, const MTime& t) {
     const float4 ws = m_scaled_w4(t, __ldg(qs + lev - 1));   // level scales [k][slot4]
     float acc = 0.f;
@@ -328,7 +332,7 @@ __device__ __forceinline__ float m_level_of(const uint2 v[4], const float4& sc, 
 
 // zcff1*zprof(Ibot) + zcff2*zprof(Itop), time-interpolated
 template <typename E>
-__device__ __forceinline__ float m_col(const void* fv, const float* qs, const int64_t o[4], const float cff[4],
+__device__ __forceinline__ float m_col(const void* fv, const float* qs, const MOff o[4], const float cff[4],
                                        const bool use[4], int nlev, const MPick& L, const MTime& t) {
     const uint2* f = reinterpret_cast<const uint2*>(fv);
     const float4* q4 = reinterpret_cast<const float4*>(qs);
@@ -346,7 +350,7 @@ __device__ __forceinline__ float m_col(const void* fv, const float* qs, const in
 
 // one slot's value at level lev of a 16-bit field
 template <typename E>
-__device__ __forceinline__ float m_level_slot(const uint2* f, const float4* qs, const int64_t o[4],
+__device__ __forceinline__ float m_level_slot(const uint2* f, const float4* qs, const MOff o[4],
                                               const float cff[4], const bool use[4], int nlev, int lev, int s) {
     const float sc = m_pick4(__ldg(qs + lev - 1), s);
     float acc = 0.f;
@@ -357,7 +361,7 @@ __device__ __forceinline__ float m_level_slot(const uint2* f, const float4* qs, 
 }
 
 template <typename E>
-__device__ __forceinline__ float m_col_slot(const void* fv, const float* qs, const int64_t o[4], const float cff[4],
+__device__ __forceinline__ float m_col_slot(const void* fv, const float* qs, const MOff o[4], const float cff[4],
                                             const bool use[4], int nlev, const MPick& L, int s) {
     const uint2* f = reinterpret_cast<const uint2*>(fv);
     const float4* q4 = reinterpret_cast<const float4*>(qs);
@@ -1162,7 +1166,7 @@ __device__ __forceinline__ void m_kahan_add(float& p, float& c, float d) {
 // A field stored as FP32 for the four ring slots of each (point, level)
 // (the diagnostics' fields in this form): value at level lev of the corner
 // set, time-interpolated with the slot weights.
-__device__ __forceinline__ float m_f32_level(const float4* f, const int64_t o[4], const float cff[4],
+__device__ __forceinline__ float m_f32_level(const float4* f, const MOff o[4], const float cff[4],
                                              const bool use[4], int nlev, int lev, const MTime& t) {
     float acc = 0.f;
 #pragma unroll
