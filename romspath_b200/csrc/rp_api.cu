@@ -23,6 +23,7 @@ struct GridBuf {
     double hc = 0.0;
     double *h = nullptr, *pm = nullptr, *pn = nullptr;
     double *sr = nullptr, *csr = nullptr, *sw = nullptr, *csw = nullptr;
+    float2 *scs_r = nullptr, *scs_w = nullptr;   // the same in FP32 pairs (s, Cs)
     uint8_t *mrho = nullptr, *mu = nullptr, *mv = nullptr;
     void *zeta = nullptr, *u = nullptr, *v = nullptr, *w = nullptr, *aks = nullptr;
     void *salt = nullptr, *temp = nullptr, *bustr = nullptr, *bvstr = nullptr;  // diagnostics only
@@ -233,6 +234,7 @@ void fill_grids(const rp_ctx* c, RpStepArgs& A, int tb, int tc, int tf) {
         d.h = G.h; d.pm = G.pm; d.pn = G.pn;
         d.mrho = G.mrho; d.mu = G.mu; d.mv = G.mv;
         d.sr = G.sr; d.csr = G.csr; d.sw = G.sw; d.csw = G.csw;
+        d.scs_r = G.scs_r; d.scs_w = G.scs_w;
         d.zeta = G.zeta; d.u = G.u; d.v = G.v; d.w = G.w; d.aks = G.aks;
         d.salt = G.salt; d.temp = G.temp; d.bustr = G.bustr; d.bvstr = G.bvstr;
         d.lon = G.lon; d.lat = G.lat;
@@ -309,7 +311,7 @@ void free_ctx(rp_ctx* c) {
     if (!c) return;
     for (int k = 0; k < RP_MAXNGRID; k++) {
         GridBuf& G = c->g[k];
-        void* ptrs[] = {G.h, G.pm, G.pn, G.sr, G.csr, G.sw, G.csw, G.mrho, G.mu, G.mv,
+        void* ptrs[] = {G.h, G.pm, G.pn, G.sr, G.csr, G.sw, G.csw, G.scs_r, G.scs_w, G.mrho, G.mu, G.mv,
                         G.zeta, G.u, G.v, G.w, G.aks, G.qs_u, G.qs_v, G.qs_w, G.qs_aks,
                         G.salt, G.temp, G.bustr, G.bvstr, G.lon, G.lat, G.wd_rho, G.wd_u, G.wd_v,
                         G.turbaccel, G.turbvort, G.waveaccelu, G.waveaccelv, G.angle};
@@ -773,6 +775,7 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
         };
         if (dalloc(&G.h, n2 * 8) || dalloc(&G.pm, n2 * 8) || dalloc(&G.pn, n2 * 8) ||
             dalloc(&G.sr, G.N * 8) || dalloc(&G.csr, G.N * 8) || dalloc(&G.sw, sw * 8) || dalloc(&G.csw, sw * 8) ||
+            dalloc(&G.scs_r, G.N * sizeof(float2)) || dalloc(&G.scs_w, sw * sizeof(float2)) ||
             dalloc(&G.mrho, n2) || dalloc(&G.mu, nu) || dalloc(&G.mv, nv))
             return bail(RP_ERR_NOMEM, "grid allocation");
         cudaMemcpy(G.h, R.h, n2 * 8, cudaMemcpyHostToDevice);
@@ -782,6 +785,13 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
         cudaMemcpy(G.csr, R.cs_r, G.N * 8, cudaMemcpyHostToDevice);
         cudaMemcpy(G.sw, R.s_w, sw * 8, cudaMemcpyHostToDevice);
         cudaMemcpy(G.csw, R.cs_w, sw * 8, cudaMemcpyHostToDevice);
+        {
+            std::vector<float2> pr(G.N), pw(sw);
+            for (int k = 0; k < G.N; k++) pr[k] = make_float2((float)R.s_rho[k], (float)R.cs_r[k]);
+            for (int k = 0; k < sw; k++) pw[k] = make_float2((float)R.s_w[k], (float)R.cs_w[k]);
+            cudaMemcpy(G.scs_r, pr.data(), G.N * sizeof(float2), cudaMemcpyHostToDevice);
+            cudaMemcpy(G.scs_w, pw.data(), sw * sizeof(float2), cudaMemcpyHostToDevice);
+        }
         if (!mask8(R.mask_rho, n2)) return bail(RP_ERR_ARG, "mask_rho values must be 0 or 1");
         cudaMemcpy(G.mrho, m8.data(), n2, cudaMemcpyHostToDevice);
         if (!mask8(R.mask_u, nu)) return bail(RP_ERR_ARG, "mask_u values must be 0 or 1");

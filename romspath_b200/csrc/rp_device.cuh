@@ -52,6 +52,8 @@ struct RpGridDev {
     const double* csr;             // Cs_r[N]
     const double* sw;              // s_w[N+1]
     const double* csw;             // Cs_w[N+1]
+    const float2* scs_r;           // (s_rho, Cs_r)[N] in FP32 (the mixed form)
+    const float2* scs_w;           // (s_w, Cs_w)[N+1] in FP32
     const void* zeta;
     const void* u;
     const void* v;

@@ -224,10 +224,12 @@ __device__ __forceinline__ void m_walk2(const RpGridDev& g, float zeta, float de
     const float h = -depth;
     const float den_r = 1.f / (hc + h);
     auto zw = [&](int k) -> float {
-        return m_zlev(vt, hc, h, den_r, (float)__ldg(g.sw + k - 1), (float)__ldg(g.csw + k - 1), zeta);
+        const float2 a = __ldg(g.scs_w + k - 1);
+        return m_zlev(vt, hc, h, den_r, a.x, a.y, zeta);
     };
     auto zr = [&](int k) -> float {
-        return m_zlev(vt, hc, h, den_r, (float)__ldg(g.sr + k - 1), (float)__ldg(g.csr + k - 1), zeta);
+        const float2 a = __ldg(g.scs_r + k - 1);
+        return m_zlev(vt, hc, h, den_r, a.x, a.y, zeta);
     };
     int lo = 0, hi = N + 2;             // zw(lo) <= zpar < zw(hi) (virtual ends)
     while (hi - lo > 1) {
@@ -1106,9 +1108,8 @@ __device__ float m_vturb(const RpStepArgs& A, const RpGridDev& g, const MStage& 
             const int k = k0 + b;
             if (k > sw) break;
             // z_w(k) of the interpolated zeta (getWlevel is linear in zeta)
-            const float zk = (k == sw) ? S.zeta
-                                       : m_zlev(g.vtransform, hc, h, den_r, (float)__ldg(g.sw + k - 1),
-                                                (float)__ldg(g.csw + k - 1), S.zeta);
+            const float2 scs = __ldg(g.scs_w + k - 1);
+            const float zk = (k == sw) ? S.zeta : m_zlev(g.vtransform, hc, h, den_r, scs.x, scs.y, S.zeta);
             const float kk = m_level_of<E>(v[b], sc[b], cwt, all, tk);   // getInterpAKs
             w.cz(k) = zk;
             if (k >= 2) {
