@@ -24,6 +24,7 @@ struct GridBuf {
     double *h = nullptr, *pm = nullptr, *pn = nullptr;
     double *sr = nullptr, *csr = nullptr, *sw = nullptr, *csw = nullptr;
     float2 *scs_r = nullptr, *scs_w = nullptr;   // the same in FP32 pairs (s, Cs)
+    float2* hm = nullptr;                        // (h, mask_rho) in FP32
     uint8_t *mrho = nullptr, *mu = nullptr, *mv = nullptr;
     void *zeta = nullptr, *u = nullptr, *v = nullptr, *w = nullptr, *aks = nullptr;
     void *salt = nullptr, *temp = nullptr, *bustr = nullptr, *bvstr = nullptr;  // diagnostics only
@@ -234,7 +235,7 @@ void fill_grids(const rp_ctx* c, RpStepArgs& A, int tb, int tc, int tf) {
         d.h = G.h; d.pm = G.pm; d.pn = G.pn;
         d.mrho = G.mrho; d.mu = G.mu; d.mv = G.mv;
         d.sr = G.sr; d.csr = G.csr; d.sw = G.sw; d.csw = G.csw;
-        d.scs_r = G.scs_r; d.scs_w = G.scs_w;
+        d.scs_r = G.scs_r; d.scs_w = G.scs_w; d.hm = G.hm;
         d.zeta = G.zeta; d.u = G.u; d.v = G.v; d.w = G.w; d.aks = G.aks;
         d.salt = G.salt; d.temp = G.temp; d.bustr = G.bustr; d.bvstr = G.bvstr;
         d.lon = G.lon; d.lat = G.lat;
@@ -311,7 +312,7 @@ void free_ctx(rp_ctx* c) {
     if (!c) return;
     for (int k = 0; k < RP_MAXNGRID; k++) {
         GridBuf& G = c->g[k];
-        void* ptrs[] = {G.h, G.pm, G.pn, G.sr, G.csr, G.sw, G.csw, G.scs_r, G.scs_w, G.mrho, G.mu, G.mv,
+        void* ptrs[] = {G.h, G.pm, G.pn, G.sr, G.csr, G.sw, G.csw, G.scs_r, G.scs_w, G.hm, G.mrho, G.mu, G.mv,
                         G.zeta, G.u, G.v, G.w, G.aks, G.qs_u, G.qs_v, G.qs_w, G.qs_aks,
                         G.salt, G.temp, G.bustr, G.bvstr, G.lon, G.lat, G.wd_rho, G.wd_u, G.wd_v,
                         G.turbaccel, G.turbvort, G.waveaccelu, G.waveaccelv, G.angle};
@@ -776,6 +777,7 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
         if (dalloc(&G.h, n2 * 8) || dalloc(&G.pm, n2 * 8) || dalloc(&G.pn, n2 * 8) ||
             dalloc(&G.sr, G.N * 8) || dalloc(&G.csr, G.N * 8) || dalloc(&G.sw, sw * 8) || dalloc(&G.csw, sw * 8) ||
             dalloc(&G.scs_r, G.N * sizeof(float2)) || dalloc(&G.scs_w, sw * sizeof(float2)) ||
+            dalloc(&G.hm, n2 * sizeof(float2)) ||
             dalloc(&G.mrho, n2) || dalloc(&G.mu, nu) || dalloc(&G.mv, nv))
             return bail(RP_ERR_NOMEM, "grid allocation");
         cudaMemcpy(G.h, R.h, n2 * 8, cudaMemcpyHostToDevice);
@@ -794,6 +796,11 @@ int rp_create(const rp_params* params, int32_t ngrid, const rp_grid* grids, rp_c
         }
         if (!mask8(R.mask_rho, n2)) return bail(RP_ERR_ARG, "mask_rho values must be 0 or 1");
         cudaMemcpy(G.mrho, m8.data(), n2, cudaMemcpyHostToDevice);
+        {
+            std::vector<float2> hm(n2);
+            for (size_t i = 0; i < n2; i++) hm[i] = make_float2((float)R.h[i], (float)m8[i]);
+            cudaMemcpy(G.hm, hm.data(), n2 * sizeof(float2), cudaMemcpyHostToDevice);
+        }
         if (!mask8(R.mask_u, nu)) return bail(RP_ERR_ARG, "mask_u values must be 0 or 1");
         cudaMemcpy(G.mu, m8.data(), nu, cudaMemcpyHostToDevice);
         if (!mask8(R.mask_v, nv)) return bail(RP_ERR_ARG, "mask_v values must be 0 or 1");

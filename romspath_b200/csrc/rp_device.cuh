@@ -54,6 +54,7 @@ struct RpGridDev {
     const double* csw;             // Cs_w[N+1]
     const float2* scs_r;           // (s_rho, Cs_r)[N] in FP32 (the mixed form)
     const float2* scs_w;           // (s_w, Cs_w)[N+1] in FP32
+    const float2* hm;              // (h, mask_rho) per rho point in FP32 (the mixed form)
     const void* zeta;
     const void* u;
     const void* v;

@@ -36,6 +36,7 @@ struct MRho {
     float X, Y;
     float cb[4];
     float ci[4];
+    float hb;                      // h, bilinear (getInterp2D's rule for h)
     bool wet4;
 };
 
@@ -46,15 +47,17 @@ __device__ __forceinline__ int m_floor(float x) {
     return (int)f;
 }
 
+// getcoeff's inverse-distance weights; 1/dist from one reciprocal square
+// root of dist^2 (dist = 0 exactly where dist^2 = 0)
 __device__ __forceinline__ void m_getcoeff(float X, float Y, const float m[4], float cff[4], uint32_t& fl) {
-    float dist[4], W[4];
-    dist[0] = sqrtf(X * X + Y * Y);
-    dist[1] = sqrtf((1.f - X) * (1.f - X) + Y * Y);
-    dist[2] = sqrtf((1.f - X) * (1.f - X) + (1.f - Y) * (1.f - Y));
-    dist[3] = sqrtf(X * X + (1.f - Y) * (1.f - Y));
+    float d2[4], W[4];
+    d2[0] = X * X + Y * Y;
+    d2[1] = (1.f - X) * (1.f - X) + Y * Y;
+    d2[2] = (1.f - X) * (1.f - X) + (1.f - Y) * (1.f - Y);
+    d2[3] = X * X + (1.f - Y) * (1.f - Y);
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-        if (dist[k] == 0.f) {
+        if (d2[k] == 0.f) {
             fl |= RP_FL_NODE;
             if (m[k] != 0.f) {
 #pragma unroll
@@ -63,7 +66,7 @@ __device__ __forceinline__ void m_getcoeff(float X, float Y, const float m[4], f
             }
             W[k] = 0.f;
         } else {
-            W[k] = m[k] / dist[k];
+            W[k] = m[k] * rsqrtf(d2[k]);
         }
     }
     const float WT = W[0] + W[1] + W[2] + W[3];
@@ -87,9 +90,14 @@ __device__ __forceinline__ void m_rho_cell(const RpGridDev& g, float ip, float j
     c.cb[1] = X * (1.f - Y);
     c.cb[2] = X * Y;
     c.cb[3] = (1.f - X) * Y;
-    float m[4];
+    float m[4], hk[4];
 #pragma unroll
-    for (int k = 0; k < 4; k++) m[k] = (float)__ldg(g.mrho + c.o[k]);
+    for (int k = 0; k < 4; k++) {
+        const float2 a = __ldg(g.hm + c.o[k]);       // (h, mask_rho)
+        hk[k] = a.x;
+        m[k] = a.y;
+    }
+    c.hb = c.cb[0] * hk[0] + c.cb[1] * hk[1] + c.cb[2] * hk[2] + c.cb[3] * hk[3];
     c.wet4 = (m[0] + m[1] + m[2] + m[3]) >= 4.f;
     m_getcoeff(X, Y, m, c.ci, fl);
 }
@@ -419,7 +427,7 @@ struct MStage {
 
 // depth and time-interpolated zeta at the stage's cell S.rc
 __device__ __forceinline__ void m_stage_2d(const MTime& tz, const RpGridDev& g, MStage& S) {
-    S.tdepth = -m_bil(g.h, S.rc);
+    S.tdepth = -S.rc.hb;
     S.zeta = m_zeta(g, S.rc, tz);
 }
 
@@ -1304,7 +1312,7 @@ __device__ __noinline__ double m_behave(const RpStepArgs& A, int64_t n, const Rp
         MRho c;
         m_rho_cell(g, Xpar, Ypar, c, fl);
         const MTime t = m_time(A, g, 0);
-        const float depth = -m_bil(g.h, c);
+        const float depth = -c.hb;
         const float zeta = m_zeta(g, c, t);
         MPick Lr, Lw;
         m_walk2(g, zeta, depth, Zpar, Lr, Lw, fl);
@@ -1467,7 +1475,7 @@ __device__ void m_update_one(const RpStepArgs& A, int64_t n, const W& w, const f
     const RpGridDev& gn = A.g[gid - 1];
     MRho rn;
     m_rho_cell(gn, tx, ty, rn, fl);
-    const float tdepth = -m_bil(gn.h, rn);
+    const float tdepth = -rn.hb;
     const float P_zeta = m_zeta(gn, rn, m_time(A, gn, 0));
     Pt.wd[n] = (double)(-tdepth + P_zeta);
     Pt.zeta[n] = (double)P_zeta;
