@@ -489,6 +489,19 @@ int upload_frame(rp_ctx* ctx, int32_t ng, int32_t slot, const S* zeta, const S* 
     G.map[slot - 1] = phys;
     if (old >= 0) {
         // readers of the old physical slot are all queued on the compute stream
+        if (mx) {
+            // the mixed form reads all four slots of a (point, level) and
+            // weighs the spare one 0: clear it (values and scales), after
+            // its last reader and before the next upload into it
+            const int64_t n2 = (int64_t)nx * ny, nu = (int64_t)(nx - 1) * ny, nv = (int64_t)nx * (ny - 1);
+            const struct { void* p; int e; int64_t n; } rings[] = {
+                {G.zeta, 4, n2}, {G.u, 2, nu * N}, {G.v, 2, nv * N}, {G.w, 2, n2 * (N + 1)}, {G.aks, 2, n2 * (N + 1)},
+                {G.qs_u, 4, N + 1}, {G.qs_v, 4, N + 1}, {G.qs_w, 4, N + 1}, {G.qs_aks, 4, N + 1},
+                {G.salt, 4, n2 * N}, {G.temp, 4, n2 * N}, {G.bustr, 4, nu}, {G.bvstr, 4, nv},
+                {G.turbaccel, 4, n2 * (N + 1)}, {G.turbvort, 4, n2 * (N + 1)},
+                {G.waveaccelu, 4, n2 * (N + 1)}, {G.waveaccelv, 4, n2 * (N + 1)}};
+            for (const auto& r : rings) CK(rp::launch_clear_slot(r.p, r.e, r.n, old, ctx->num_sms, ctx->s_comp));
+        }
         CK(cudaEventRecord(G.slot_free[old], ctx->s_comp));
         G.free_recorded[old] = true;
         G.slot_loaded[old] = false;

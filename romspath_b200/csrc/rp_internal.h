@@ -48,6 +48,10 @@ cudaError_t launch_stage_f32(int src_f32, const void* src, const void* add, floa
 cudaError_t launch_quantize(const float* f, uint32_t* maxbits, float* qs, void* dst, int ni, int nj, int nk, int slot,
                             int i16, int num_sms, cudaStream_t s);
 cudaError_t launch_mixed_convert(const RpParticlesDev& P, int to_f64, cudaStream_t s);
+// Mixed form: clear one physical slot of a ring of `count` (point, level)
+// entries of `elem` bytes per slot (2: 16-bit fields, 4: FP32), so that a
+// slot read with weight 0 holds +0.
+cudaError_t launch_clear_slot(void* ring, int elem, int64_t count, int slot, int num_sms, cudaStream_t s);
 
 // Re-sorting of the particle state by (grid, tile of cells, cell) (rp_sort.cu)
 struct SortBufs {

@@ -365,6 +365,22 @@ cudaError_t launch_quantize(const float* f, uint32_t* maxbits, float* qs, void* 
 
 // FP64 columns -> compensated FP32 positions (value = p - c) and no
 // smoothing-parameter warm start
+template <typename T>
+__global__ void __launch_bounds__(256) k_clear_slot(T* ring, int64_t count, int slot) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < count; t += stride)
+        ring[t * RP_SLOTS + slot] = T(0);
+}
+
+cudaError_t launch_clear_slot(void* ring, int elem, int64_t count, int slot, int num_sms, cudaStream_t s) {
+    if (!ring || count <= 0) return cudaSuccess;
+    int64_t blocks = (count + 255) / 256;
+    if (blocks > (int64_t)num_sms * 8) blocks = (int64_t)num_sms * 8;
+    if (elem == 2) k_clear_slot<uint16_t><<<(unsigned)blocks, 256, 0, s>>>((uint16_t*)ring, count, slot);
+    else k_clear_slot<uint32_t><<<(unsigned)blocks, 256, 0, s>>>((uint32_t*)ring, count, slot);
+    return cudaGetLastError();
+}
+
 __global__ void k_mixed_from_f64(RpParticlesDev P) {
     const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= P.n) return;

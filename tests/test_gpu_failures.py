@@ -167,3 +167,39 @@ def test_one_level_grid_refused():
     sp = synth.GridSpec(24, 20, 1)
     with pytest.raises(RomsPathError):
         Tracker([sp], [synth.make_grid(sp)], synth.config_params("tiny"), numpar=10)
+
+
+@pytest.mark.parametrize("kind", ["mixed", "mixed-i16"])
+def test_spare_slot_contents_do_not_reach_the_mixed_step(kind):
+    """The ring's fourth physical slot (the one an upload fills next) is read
+    with every (point, level) word but weighs zero: a NaN frame parked there
+    must leave the step's results bit for bit as with a finite one."""
+    case = harness.make_case("tiny", 300, seed=21)
+    nanf = {k: np.full_like(np.asarray(v, dtype=np.float64), np.nan) if np.ndim(v) else v
+            for k, v in case.frame(1).items()}
+    outs = []
+    for parked in (case.frame(1), nanf):
+        T = _tracker(case, field_dtype=kind, resort=0)
+        for (k, slot) in schedule.initial_loads():
+            T.upload_frame(1, slot, case.frame(k))
+        # an upload writes the spare slot and frees the one it replaces:
+        # `parked` then frame 1 again into slot 1 leaves `parked` in the spare
+        T.upload_frame(1, 1, parked)
+        T.upload_frame(1, 1, case.frame(1))
+        T.locate(case.release, t_b=1)
+        n = 0
+        for ext in schedule.external_steps(1.0, int(case.params["dt"]), int(case.params["idt"])):
+            if ext.loads:
+                break                                  # no upload may overwrite the spare slot
+            for it in ext.internal:
+                T.step(it.ex, it.ix, it.ets, it.tb, it.tc, it.tf)
+                n += 1
+        st = T.get_particles()
+        T.close()
+        outs.append(st)
+    assert n >= 12
+    for key in ("x", "y", "z", "status", "age"):
+        a, b = np.asarray(outs[0][key]), np.asarray(outs[1][key])
+        assert np.array_equal(a.view(np.uint64) if a.dtype == np.float64 else a,
+                              b.view(np.uint64) if b.dtype == np.float64 else b), key
+    assert np.isfinite(np.asarray(outs[1]["z"])).all()
