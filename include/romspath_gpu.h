@@ -60,7 +60,8 @@ extern "C" {
  * smoothing spline's factor rows and secant search and the random-
  * displacement sub-steps in FP64, the spline's substitution sweeps in
  * FP32, with its smoothing parameter extrapolated from the particle's
- * previous two steps.  Not bit-exact; its error against RP_FIELD_F64 on the
+ * previous two steps.  Non-finite field values are stored as finite ones
+ * (FP16: NaN as 0, +-Inf as +-65504; int16: clamped).  Not bit-exact; its error against RP_FIELD_F64 on the
  * same noise is measured by the tests. */
 #define RP_FIELD_MIXED 2
 /* The same form with u, v, w, AKs in int16 fixed point, scale = level

@@ -293,6 +293,25 @@ RpPolint polint_consts(const double xa[3], double x) {
     return P;
 }
 
+// The mixed form's per-step slot data of every grid: A.lw summed by the
+// physical slot each of t_b, t_c, t_f sits in, and masks of the live FP32
+// slots (the spare one is read with every float4 and must meet a weight of
+// 0 and no bits of its own: an upload may be filling it)
+void slot_weights(RpStepArgs& A, int ngrid) {
+    for (int k = 0; k < ngrid; k++) {
+        RpGridDev& d = A.g[k];
+        const int sl[3] = {d.sb, d.sc, d.sf};
+        for (int which = 0; which < 2; which++) {
+            float w[4] = {0.f, 0.f, 0.f, 0.f};
+            for (int q = 0; q < 3; q++) w[sl[q]] += A.lw[which][q];
+            d.w4[which] = make_float4(w[0], w[1], w[2], w[3]);
+        }
+        uint32_t live[4];
+        for (int s = 0; s < 4; s++) live[s] = (sl[0] == s || sl[1] == s || sl[2] == s) ? 0xffffffffu : 0u;
+        d.m32 = make_uint4(live[0], live[1], live[2], live[3]);
+    }
+}
+
 // polintd's interpolant at x as Lagrange weights of its three values (the
 // mixed form folds them into the gathers): [0] for (b, c, f), [1] for the
 // u/v/w values, which at ets == 1 are (b, b, c) (advection_module.f90:277-287)
@@ -1087,6 +1106,7 @@ int step_launch(rp_ctx* ctx, const double ex[3], const double ix[3], int32_t ets
     for (int q = 0; q < 3; q++) { A.ex[q] = ex[q]; A.ix[q] = ix[q]; }
     A.pi = polint_consts(ex, ix[1]);
     lagrange_weights(ex, ix[1], ets, A.lw);
+    slot_weights(A, ctx->ngrid);
     A.ets = ets;
     A.step_index = ctx->step_index;
     A.hook = ctx->hook ? ctx->hook + ctx->hook_pos * ctx->n * ctx->ndraw : nullptr;
@@ -1213,6 +1233,7 @@ int rp_step_noalloc(rp_ctx* ctx, const rp_device_state* st, const double ex[3], 
     for (int q = 0; q < 3; q++) { A.ex[q] = ex[q]; A.ix[q] = ix[q]; }
     A.pi = polint_consts(ex, ix[1]);
     lagrange_weights(ex, ix[1], ets, A.lw);
+    slot_weights(A, ctx->ngrid);
     A.ets = ets;
     A.step_index = ctx->step_index;
     A.hook = nullptr;

@@ -81,6 +81,11 @@ struct RpGridDev {
     double scl[RP_MAXNGRID_D][2];  // GRIDS(ng)%scl(i,1:2)
     double off[RP_MAXNGRID_D][2];
     int sb, sc, sf;                // physical ring slots of t_b, t_c, t_f
+    // mixed form, per step (host-computed): the Lagrange weights by physical
+    // slot ([0] zeta/AKs/depths, [1] u/v/w), and bit masks of the three
+    // live slots of an FP32 float4
+    float4 w4[2];
+    uint4 m32;
     // mixed form: per-(level, slot) scales of the 16-bit fields, [k][slot4]
     const float* qs_u;
     const float* qs_v;

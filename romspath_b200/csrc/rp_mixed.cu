@@ -304,7 +304,12 @@ __device__ __forceinline__ float m_level_scale(uint32_t bits, bool i16) {
     return ldexpf(1.0f, e - 14);
 }
 
-__device__ __forceinline__ void m_store16(__half* d, float v) { *d = __float2half_rn(v); }
+// FP16 stores finite values only, as the int16 form's clamp does: NaN as 0,
+// +-Inf as +-65504 (the mixed form reads the spare ring slot with weight 0,
+// and an upload may be filling it while steps run)
+__device__ __forceinline__ void m_store16(__half* d, float v) {
+    *d = __float2half_rn(v != v ? 0.f : fminf(fmaxf(v, -65504.f), 65504.f));
+}
 __device__ __forceinline__ void m_store16(int16_t* d, float v) {
     const float r = fminf(fmaxf(rintf(v), -32767.0f), 32767.0f);
     *d = (int16_t)r;

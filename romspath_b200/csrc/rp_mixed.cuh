@@ -113,7 +113,17 @@ struct MTime {
     float wb, wc, wf;
     int sb, sc, sf;
     float4 w4;                     // the same weights by physical slot (0 for the spare slot)
+    uint4 m32;                     // bit masks of the three live slots of an FP32 float4
 };
+
+// The four FP32 slots of a value, the spare slot's bits cleared: the spare
+// slot (the one an upload may be filling) can hold anything, NaN included,
+// and its weight of 0 must not meet it.  (The 16-bit fields need no mask:
+// their quantisation stores finite values only and finite scales.)
+__device__ __forceinline__ float4 m_live4(const float4& v, const uint4& m) {
+    return make_float4(__uint_as_float(__float_as_uint(v.x) & m.x), __uint_as_float(__float_as_uint(v.y) & m.y),
+                       __uint_as_float(__float_as_uint(v.z) & m.z), __uint_as_float(__float_as_uint(v.w) & m.w));
+}
 
 __device__ __forceinline__ float m_pick4(const float4& v, int s) {
     return s == 0 ? v.x : (s == 1 ? v.y : (s == 2 ? v.z : v.w));
@@ -126,7 +136,7 @@ __device__ __forceinline__ float m_zeta(const RpGridDev& g, const MRho& c, const
     float acc = 0.f;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-        const float4 v = __ldg(z + c.o[q]);
+        const float4 v = m_live4(__ldg(z + c.o[q]), t.m32);
         acc += c.ci[q] * fmaf(t.w4.w, v.w, fmaf(t.w4.z, v.z, fmaf(t.w4.y, v.y, t.w4.x * v.x)));
     }
     return acc;
@@ -439,13 +449,9 @@ __device__ __forceinline__ MTime m_time(const RpStepArgs& A, const RpGridDev& g,
     t.sb = g.sb;
     t.sc = g.sc;
     t.sf = g.sf;
-    // by physical slot: the b, c and f weights of the slots they sit in
-    // (added where two of them share a slot)
-    float w[4];
-#pragma unroll
-    for (int s = 0; s < 4; s++)
-        w[s] = (t.sb == s ? t.wb : 0.f) + (t.sc == s ? t.wc : 0.f) + (t.sf == s ? t.wf : 0.f);
-    t.w4 = make_float4(w[0], w[1], w[2], w[3]);
+    // by physical slot, and the live slots' masks (host-computed per step)
+    t.w4 = g.w4[which];
+    t.m32 = g.m32;
     return t;
 }
 
@@ -1181,7 +1187,7 @@ __device__ __forceinline__ float m_f32_level(const float4* f, const MOff o[4], c
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         if (use[q]) {
-            const float4 v = __ldg(f + o[q] * nlev + lev - 1);
+            const float4 v = m_live4(__ldg(f + o[q] * nlev + lev - 1), t.m32);
             acc += cff[q] * fmaf(t.w4.w, v.w, fmaf(t.w4.z, v.z, fmaf(t.w4.y, v.y, t.w4.x * v.x)));
         }
     }
