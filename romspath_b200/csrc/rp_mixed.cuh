@@ -14,8 +14,11 @@
 // (RP_FIELD_MIXED_I16, |v| / scale <= 32767 with scale = level max / 32767).
 // The four ring slots of one (point, level) are one 8-byte load (16 bytes
 // for zeta), and polintd's time interpolation at ix(2) is applied as its
-// Lagrange weights on the b/c/f slots (host-computed, RpStepArgs::lw),
-// combined with the level scales before the corner sum.  polintd is linear
+// Lagrange weights on the b/c/f slots (RpStepArgs::lw), summed on the host
+// by the physical slot each sits in (RpGridDev::w4, the spare slot's
+// weight 0) and combined with the level scales before the corner sum; the
+// spare slot never holds a non-finite value there (finite quantisation,
+// masked FP32 slots, cleared when an upload frees it).  polintd is linear
 // in its values, so the s-level depths are formed once from the
 // interpolated zeta.  Results differ from the exact form by rounding; the
 // error is measured against the FP64 form on identical noise.
@@ -1082,8 +1085,9 @@ __device__ __forceinline__ void m_normal2(const RpStepArgs& A, uint32_t pid, uin
     n1 = (double)(r1 * cospif(2.f * (((float)c[3] + 0.5f) * k)));
 }
 
-// VTurb (ver_turb_module.f90:31-329): column in FP32 from FP16 AKs, fit and
-// random-displacement sub-steps in FP64
+// VTurb (ver_turb_module.f90:31-329): column in FP32 from the 16-bit AKs,
+// the fit as m_smooth / m_chol1d form it, random-displacement sub-steps in
+// FP64
 template <typename E, class W>
 __device__ float m_vturb(const RpStepArgs& A, const RpGridDev& g, const MStage& S, float Zpar,
                          uint32_t pid, double& qstate, double& gstate, float& q2state, uint32_t& fl, const W& w) {
